@@ -1,0 +1,541 @@
+// grb_runtime.cu: device init, stream pool, stream-ordered memory, CSR
+// upload/download, scans and zombie pruning for the B200 SpGEMM library.
+
+#include <mutex>
+#include <vector>
+#include <atomic>
+#include <cstring>
+#include <cstdio>
+#include "grb_runtime.h"
+
+namespace grb {
+
+static Runtime g_rt;
+static std::mutex g_mu;
+static std::vector<cudaStream_t> g_streams;
+static std::atomic<int64_t> g_fail_countdown{0};
+
+Runtime &runtime() { return g_rt; }
+
+int cuda_to_info(cudaError_t e)
+{
+    if (e == cudaSuccess) return SUCCESS;
+    if (e == cudaErrorMemoryAllocation) return OUT_OF_MEMORY;
+    return PANIC;
+}
+
+int init_device()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_rt.ready) return SUCCESS;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) { cudaGetLastError(); return PANIC; }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return PANIC;
+    g_rt.device = dev;
+    g_rt.num_sms = prop.multiProcessorCount;
+    g_rt.smem_optin = prop.sharedMemPerBlockOptin;
+    // keep freed pool memory cached instead of returning it to the driver
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thresh = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thresh);
+    }
+    g_rt.ready = true;
+    return SUCCESS;
+}
+
+cudaStream_t stream_acquire()
+{
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (!g_streams.empty()) {
+            cudaStream_t s = g_streams.back();
+            g_streams.pop_back();
+            return s;
+        }
+    }
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+        return nullptr;
+    return s;
+}
+
+void stream_release(cudaStream_t s)
+{
+    if (!s) return;
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_streams.push_back(s);
+}
+
+void set_alloc_fail_countdown(int64_t n) { g_fail_countdown.store(n); }
+
+static thread_local cudaStream_t t_stream = nullptr;
+void set_thread_stream(cudaStream_t s) { t_stream = s; }
+cudaStream_t thread_stream() { return t_stream; }
+
+// ---------------------------------------------------------------------------
+// kernel timing
+// ---------------------------------------------------------------------------
+
+struct ProfPending { const char *name; cudaEvent_t a, b; };
+struct ProfTotal { const char *name; double ms; int64_t count; };
+static std::atomic<bool> g_prof{false};
+static std::mutex g_prof_mu;
+static std::vector<ProfPending> g_pending;
+static std::vector<ProfTotal> g_totals;
+
+void prof_enable(bool on) { g_prof.store(on); }
+bool prof_on() { return g_prof.load(); }
+
+int prof_begin(const char *name, cudaStream_t s)
+{
+    if (!g_prof.load()) return -1;
+    ProfPending p{name, nullptr, nullptr};
+    cudaEventCreate(&p.a);
+    cudaEventCreate(&p.b);
+    cudaEventRecord(p.a, s);
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_pending.push_back(p);
+    return (int)g_pending.size() - 1;
+}
+
+void prof_end(int slot, cudaStream_t s)
+{
+    if (slot < 0) return;
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (slot < (int)g_pending.size()) cudaEventRecord(g_pending[slot].b, s);
+}
+
+void prof_flush()
+{
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    for (auto &p : g_pending) {
+        float ms = 0.0f;
+        cudaEventSynchronize(p.b);
+        if (cudaEventElapsedTime(&ms, p.a, p.b) != cudaSuccess) { cudaGetLastError(); ms = 0; }
+        bool found = false;
+        for (auto &t : g_totals)
+            if (strcmp(t.name, p.name) == 0) { t.ms += ms; t.count++; found = true; break; }
+        if (!found) g_totals.push_back({p.name, (double)ms, 1});
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    g_pending.clear();
+}
+
+void prof_reset()
+{
+    prof_flush();
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_totals.clear();
+}
+
+bool prof_read(const char *name, double *ms, int64_t *count)
+{
+    prof_flush();
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    for (auto &t : g_totals)
+        if (strcmp(t.name, name) == 0) { *ms = t.ms; *count = t.count; return true; }
+    *ms = 0; *count = 0;
+    return false;
+}
+
+void *dalloc(size_t bytes, cudaStream_t s)
+{
+    int64_t c = g_fail_countdown.load();
+    if (c > 0) {
+        int64_t left = g_fail_countdown.fetch_sub(1) - 1;
+        if (left == 0) return nullptr;          // injected failure
+    }
+    if (bytes == 0) bytes = 16;
+    void *p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, bytes, s);
+    if (e != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    return p;
+}
+
+void dfree(void *p, cudaStream_t s)
+{
+    if (p) cudaFreeAsync(p, s);
+}
+
+void dev_free(DevCSR &A, cudaStream_t s)
+{
+    dfree(A.p, s); dfree(A.j, s); dfree(A.x, s);
+    A.p = nullptr; A.j = nullptr; A.x = nullptr;
+    A.nnz = 0; A.nzombies = 0;
+}
+
+// ---------------------------------------------------------------------------
+// narrowing / widening copies
+// ---------------------------------------------------------------------------
+
+__global__ void k_narrow(const int64_t *__restrict__ in, int32_t *__restrict__ out,
+                         int64_t n)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; t < n; t += stride) out[t] = (int32_t)in[t];
+}
+
+__global__ void k_widen(const int32_t *__restrict__ in, int64_t *__restrict__ out,
+                        int64_t n)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; t < n; t += stride) out[t] = (int64_t)in[t];
+}
+
+static inline int grid_for(int64_t n, int threads)
+{
+    int64_t b = (n + threads - 1) / threads;
+    int64_t cap = (int64_t)runtime().num_sms * 16;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+int dev_upload(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
+               const int64_t *i, const void *x, int type, bool iso,
+               cudaStream_t s)
+{
+    int64_t nnz = p[nrows];
+    if (nrows >= INT32_MAX || ncols >= INT32_MAX || nnz >= INT32_MAX)
+        return NO_VALUE;
+    A.nrows = nrows; A.ncols = ncols; A.nnz = nnz; A.type = type; A.iso = iso;
+    A.nzombies = 0;
+    size_t ts = type_size(type);
+    // stage int64 arrays through one device buffer, then narrow on the device
+    int64_t stage_n = (nrows + 1 > nnz) ? nrows + 1 : nnz;
+    int64_t *stage = (int64_t *)dalloc((size_t)stage_n * 8, s);
+    A.p = (int32_t *)dalloc((size_t)(nrows + 1) * 4, s);
+    A.j = (int32_t *)dalloc((size_t)(nnz ? nnz : 1) * 4, s);
+    A.x = nullptr;
+    if (x) A.x = dalloc(iso ? ts : (size_t)(nnz ? nnz : 1) * ts, s);
+    if (!stage || !A.p || !A.j || (x && !A.x)) {
+        dfree(stage, s); dev_free(A, s); return OUT_OF_MEMORY;
+    }
+    cudaMemcpyAsync(stage, p, (size_t)(nrows + 1) * 8, cudaMemcpyHostToDevice, s);
+    k_narrow<<<grid_for(nrows + 1, 256), 256, 0, s>>>(stage, A.p, nrows + 1);
+    if (nnz > 0) {
+        cudaMemcpyAsync(stage, i, (size_t)nnz * 8, cudaMemcpyHostToDevice, s);
+        k_narrow<<<grid_for(nnz, 256), 256, 0, s>>>(stage, A.j, nnz);
+    }
+    if (x) cudaMemcpyAsync(A.x, x, iso ? ts : (size_t)nnz * ts,
+                           cudaMemcpyHostToDevice, s);
+    dfree(stage, s);
+    return cuda_to_info(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------------------
+// exclusive scans (three passes: block totals, scan of totals, block scans)
+// ---------------------------------------------------------------------------
+
+static constexpr int SCAN_THREADS = 512;
+static constexpr int SCAN_ITEMS = 8;
+static constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+template <typename T>
+__global__ void k_scan_totals(const T *__restrict__ in, int64_t n,
+                              int64_t *__restrict__ totals)
+{
+    __shared__ int64_t warp_sums[SCAN_THREADS / 32];
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+    int64_t sum = 0;
+    for (int it = 0; it < SCAN_ITEMS; it++) {
+        int64_t idx = base + (int64_t)it * SCAN_THREADS + threadIdx.x;
+        if (idx < n) sum += (int64_t)in[idx];
+    }
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int64_t v = threadIdx.x < SCAN_THREADS / 32 ? warp_sums[threadIdx.x] : 0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) totals[blockIdx.x] = v;
+    }
+}
+
+// scan one tile per block; offsets[b] is the exclusive prefix of the tile
+template <typename T>
+__global__ void k_scan_tiles(const T *__restrict__ in, int64_t *__restrict__ out,
+                             int64_t n, const int64_t *__restrict__ offsets)
+{
+    __shared__ int64_t warp_sums[SCAN_THREADS / 32];
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    int64_t v[SCAN_ITEMS];
+    int64_t local = 0;
+    #pragma unroll
+    for (int it = 0; it < SCAN_ITEMS; it++) {
+        int64_t idx = base + it;
+        v[it] = idx < n ? (int64_t)in[idx] : 0;
+        local += v[it];
+    }
+    // warp inclusive scan of per-thread totals
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int64_t inc = local;
+    for (int o = 1; o < 32; o <<= 1) {
+        int64_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) warp_sums[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        int64_t w = lane < SCAN_THREADS / 32 ? warp_sums[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < SCAN_THREADS / 32) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    int64_t prefix = offsets[blockIdx.x] + (warp > 0 ? warp_sums[warp - 1] : 0) +
+                     (inc - local);
+    #pragma unroll
+    for (int it = 0; it < SCAN_ITEMS; it++) {
+        int64_t idx = base + it;
+        if (idx < n) out[idx] = prefix;
+        prefix += v[it];
+    }
+}
+
+template <typename T>
+static int scan_impl(const T *in, int64_t *out, int64_t n, cudaStream_t s)
+{
+    if (n <= 0) return SUCCESS;
+    int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    int64_t *totals = (int64_t *)dalloc((size_t)(nb + 1) * 8, s);
+    if (!totals) return OUT_OF_MEMORY;
+    k_scan_totals<T><<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, totals);
+    int info = SUCCESS;
+    if (nb > 1) info = scan_impl<int64_t>(totals, totals, nb, s);
+    else cudaMemsetAsync(totals, 0, 8, s);
+    if (info == SUCCESS)
+        k_scan_tiles<T><<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, totals);
+    dfree(totals, s);
+    if (info != SUCCESS) return info;
+    return cuda_to_info(cudaGetLastError());
+}
+
+int scan_exclusive_i64(const int64_t *in, int64_t *out, int64_t n, cudaStream_t s)
+{
+    return scan_impl<int64_t>(in, out, n, s);
+}
+
+int scan_exclusive_i32_to_i64(const int32_t *in, int64_t *out, int64_t n,
+                              cudaStream_t s)
+{
+    return scan_impl<int32_t>(in, out, n, s);
+}
+
+// ---------------------------------------------------------------------------
+// zombie pruning and download
+// ---------------------------------------------------------------------------
+
+// live entries per row (one warp per row)
+__global__ void k_count_live(const int32_t *__restrict__ Ap,
+                             const int32_t *__restrict__ Aj, int64_t nrows,
+                             int64_t *__restrict__ cnt)
+{
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    int lane = threadIdx.x & 31;
+    for (int64_t r = warp; r < nrows; r += nwarps) {
+        int32_t lo = Ap[r], hi = Ap[r + 1];
+        int32_t c = 0;
+        for (int32_t p = lo + lane; p < hi; p += 32) c += (Aj[p] >= 0);
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+        if (lane == 0) cnt[r] = c;
+    }
+}
+
+// copy live entries of each row to their new positions (order preserved)
+__global__ void k_compact_live(const int32_t *__restrict__ Ap,
+                               const int32_t *__restrict__ Aj,
+                               const char *__restrict__ Ax, size_t ts, bool iso,
+                               int64_t nrows, const int64_t *__restrict__ newp,
+                               int32_t *__restrict__ Bj, char *__restrict__ Bx)
+{
+    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    int lane = threadIdx.x & 31;
+    for (int64_t r = warp; r < nrows; r += nwarps) {
+        int32_t lo = Ap[r], hi = Ap[r + 1];
+        int64_t w = newp[r];
+        for (int32_t base = lo; base < hi; base += 32) {
+            int32_t p = base + lane;
+            bool live = (p < hi) && (Aj[p] >= 0);
+            unsigned m = __ballot_sync(0xffffffffu, live);
+            if (live) {
+                int64_t q = w + __popc(m & ((1u << lane) - 1));
+                Bj[q] = Aj[p];
+                if (Ax && !iso) {
+                    for (size_t b = 0; b < ts; b++) Bx[q * ts + b] = Ax[(int64_t)p * ts + b];
+                }
+            }
+            w += __popc(m);
+        }
+    }
+}
+
+__global__ void k_i64_to_i32(const int64_t *__restrict__ in, int32_t *__restrict__ out,
+                             int64_t n)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; t < n; t += stride) out[t] = (int32_t)in[t];
+}
+
+int dev_prune_zombies(DevCSR &A, cudaStream_t s)
+{
+    if (A.nzombies == 0) return SUCCESS;
+    size_t ts = type_size(A.type);
+    int64_t *cnt = (int64_t *)dalloc((size_t)(A.nrows + 1) * 8, s);
+    if (!cnt) return OUT_OF_MEMORY;
+    int threads = 256;
+    int grid = grid_for(A.nrows * 32, threads);
+    k_count_live<<<grid, threads, 0, s>>>(A.p, A.j, A.nrows, cnt);
+    cudaMemsetAsync(cnt + A.nrows, 0, 8, s);
+    int info = scan_exclusive_i64(cnt, cnt, A.nrows + 1, s);
+    if (info != SUCCESS) { dfree(cnt, s); return info; }
+    int64_t live = A.nnz - A.nzombies;
+    int32_t *Bj = (int32_t *)dalloc((size_t)(live ? live : 1) * 4, s);
+    char *Bx = nullptr;
+    if (A.x && !A.iso) Bx = (char *)dalloc((size_t)(live ? live : 1) * ts, s);
+    int32_t *Bp = (int32_t *)dalloc((size_t)(A.nrows + 1) * 4, s);
+    if (!Bj || !Bp || (A.x && !A.iso && !Bx)) {
+        dfree(cnt, s); dfree(Bj, s); dfree(Bx, s); dfree(Bp, s);
+        return OUT_OF_MEMORY;
+    }
+    k_compact_live<<<grid, threads, 0, s>>>(A.p, A.j, (const char *)A.x, ts,
+                                            A.iso, A.nrows, cnt, Bj, Bx);
+    k_i64_to_i32<<<grid_for(A.nrows + 1, 256), 256, 0, s>>>(cnt, Bp, A.nrows + 1);
+    dfree(cnt, s);
+    dfree(A.p, s); dfree(A.j, s);
+    if (A.x && !A.iso) { dfree(A.x, s); A.x = Bx; }
+    A.p = Bp; A.j = Bj; A.nnz = live; A.nzombies = 0;
+    return cuda_to_info(cudaGetLastError());
+}
+
+// entries of a valued mask whose value is false become zombies
+__global__ void k_mask_false_to_zombie(const int32_t *__restrict__ Mj,
+                                       const void *__restrict__ Mx, int mtype,
+                                       int64_t n, int32_t *__restrict__ Oj,
+                                       unsigned long long *__restrict__ nz)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned long long c = 0;
+    for (; t < n; t += stride) {
+        bool v;
+        switch (mtype) {
+            case T_BOOL: v = ((const uint8_t *)Mx)[t] != 0; break;
+            case T_INT32: case T_UINT32: v = ((const uint32_t *)Mx)[t] != 0; break;
+            case T_FP32: v = ((const float *)Mx)[t] != 0.0f; break;
+            case T_FP64: v = ((const double *)Mx)[t] != 0.0; break;
+            default: v = ((const uint64_t *)Mx)[t] != 0; break;
+        }
+        int32_t j = Mj[t];
+        if (j >= 0 && !v) { Oj[t] = flip(j); c++; }
+        else Oj[t] = j;
+    }
+    if (c) atomicAdd(nz, c);
+}
+
+int dev_mask_to_struct(DevCSR &out, const DevCSR &M, cudaStream_t s)
+{
+    out = DevCSR();
+    out.nrows = M.nrows; out.ncols = M.ncols; out.nnz = M.nnz; out.type = T_BOOL;
+    out.p = (int32_t *)dalloc((size_t)(M.nrows + 1) * 4, s);
+    out.j = (int32_t *)dalloc((size_t)(M.nnz ? M.nnz : 1) * 4, s);
+    unsigned long long *nz = (unsigned long long *)dalloc(8, s);
+    if (!out.p || !out.j || !nz) { dev_free(out, s); dfree(nz, s); return OUT_OF_MEMORY; }
+    cudaMemcpyAsync(out.p, M.p, (size_t)(M.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemsetAsync(nz, 0, 8, s);
+    if (M.iso) {
+        // iso mask: all true or all false
+        uint64_t v = 0;
+        cudaMemcpyAsync(&v, M.x, type_size(M.type), cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        bool t;
+        if (M.type == T_FP32) { float f; memcpy(&f, &v, 4); t = f != 0.0f; }
+        else if (M.type == T_FP64) { double d; memcpy(&d, &v, 8); t = d != 0.0; }
+        else t = v != 0;
+        if (t) {
+            cudaMemcpyAsync(out.j, M.j, (size_t)M.nnz * 4, cudaMemcpyDeviceToDevice, s);
+            out.nzombies = M.nzombies;
+        } else {
+            dfree(out.j, s);
+            out.j = (int32_t *)dalloc(4, s);
+            cudaMemsetAsync(out.p, 0, (size_t)(M.nrows + 1) * 4, s);
+            out.nnz = 0;
+            out.nzombies = 0;
+        }
+        dfree(nz, s);
+        return cuda_to_info(cudaStreamSynchronize(s));
+    }
+    if (M.nnz > 0)
+        k_mask_false_to_zombie<<<grid_for(M.nnz, 256), 256, 0, s>>>(M.j, M.x, M.type, M.nnz, out.j, nz);
+    unsigned long long h = 0;
+    cudaMemcpyAsync(&h, nz, 8, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    dfree(nz, s);
+    if (e != cudaSuccess) { dev_free(out, s); return cuda_to_info(e); }
+    out.nzombies = (int64_t)h + M.nzombies;
+    return dev_prune_zombies(out, s);
+}
+
+int dev_download(const DevCSR &A0, int64_t **p, int64_t **i, void **x,
+                 bool keep_zombies, alloc_fn alloc, cudaStream_t s)
+{
+    DevCSR A = A0;              // shallow copy
+    bool owned = false;
+    if (!keep_zombies && A.nzombies > 0) {
+        // prune into a private copy so the caller's matrix is untouched
+        DevCSR B = A0;
+        size_t ts = type_size(A0.type);
+        B.p = (int32_t *)dalloc((size_t)(A0.nrows + 1) * 4, s);
+        B.j = (int32_t *)dalloc((size_t)(A0.nnz ? A0.nnz : 1) * 4, s);
+        B.x = nullptr;
+        if (A0.x) B.x = dalloc(A0.iso ? ts : (size_t)(A0.nnz ? A0.nnz : 1) * ts, s);
+        if (!B.p || !B.j || (A0.x && !B.x)) { dev_free(B, s); return OUT_OF_MEMORY; }
+        cudaMemcpyAsync(B.p, A0.p, (size_t)(A0.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(B.j, A0.j, (size_t)A0.nnz * 4, cudaMemcpyDeviceToDevice, s);
+        if (A0.x) cudaMemcpyAsync(B.x, A0.x, A0.iso ? ts : (size_t)A0.nnz * ts,
+                                  cudaMemcpyDeviceToDevice, s);
+        int info = dev_prune_zombies(B, s);
+        if (info != SUCCESS) { dev_free(B, s); return info; }
+        A = B; owned = true;
+    }
+    size_t ts = type_size(A.type);
+    int64_t nnz = A.nnz;
+    *p = (int64_t *)alloc((size_t)(A.nrows + 1) * 8);
+    *i = (int64_t *)alloc((size_t)(nnz ? nnz : 1) * 8);
+    *x = nullptr;
+    if (A.x) *x = alloc(A.iso ? ts : (size_t)(nnz ? nnz : 1) * ts);
+    int64_t *stage = (int64_t *)dalloc((size_t)((A.nrows + 1 > nnz ? A.nrows + 1 : nnz)) * 8, s);
+    if (!*p || !*i || (A.x && !*x) || !stage) {
+        dfree(stage, s);
+        if (owned) dev_free(A, s);
+        return OUT_OF_MEMORY;
+    }
+    k_widen<<<grid_for(A.nrows + 1, 256), 256, 0, s>>>(A.p, stage, A.nrows + 1);
+    cudaMemcpyAsync(*p, stage, (size_t)(A.nrows + 1) * 8, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    if (nnz > 0) {
+        k_widen<<<grid_for(nnz, 256), 256, 0, s>>>(A.j, stage, nnz);
+        cudaMemcpyAsync(*i, stage, (size_t)nnz * 8, cudaMemcpyDeviceToHost, s);
+    }
+    if (A.x) cudaMemcpyAsync(*x, A.x, A.iso ? ts : (size_t)nnz * ts,
+                             cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    dfree(stage, s);
+    if (owned) dev_free(A, s);
+    return cuda_to_info(e);
+}
+
+}  // namespace grb

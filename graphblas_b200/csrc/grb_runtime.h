@@ -1,0 +1,135 @@
+// grb_runtime.h: host-side runtime of the B200 SpGEMM library (C++).
+//
+// One process drives one device.  Device memory comes from the stream-ordered
+// pool (cudaMallocAsync) with a release threshold that keeps freed blocks
+// cached, so repeated calls do not return memory to the driver.  Every public
+// call runs on a stream taken from a small pool and synchronises before it
+// returns, as the reference's GPU gateway does (CUDA/GB_cuda_AxB_dot3.cpp:54,
+// one stream per call, synchronised at the end).
+
+#pragma once
+#include <cstdint>
+#include <cstddef>
+#include <cuda_runtime.h>
+#include "grb_common.cuh"
+
+namespace grb {
+
+struct Runtime {
+    int device = 0;
+    int num_sms = 148;
+    size_t smem_optin = 0;        // max dynamic shared memory per block
+    bool ready = false;
+};
+
+Runtime &runtime();
+
+// initialise the device (idempotent); returns an Info code
+int init_device();
+
+// stream pool: acquire/release a non-blocking stream
+cudaStream_t stream_acquire();
+void stream_release(cudaStream_t s);
+
+// a caller-chosen stream for this host thread (nullptr: use the pool)
+void set_thread_stream(cudaStream_t s);
+cudaStream_t thread_stream();
+
+// kernel timing with CUDA events on the launching stream (off by default):
+// prof_begin/prof_end bracket a launch; prof_flush, called after the stream
+// is synchronised, adds the elapsed time to the kernel's running total
+void prof_enable(bool on);
+bool prof_on();
+int prof_begin(const char *name, cudaStream_t s);
+void prof_end(int slot, cudaStream_t s);
+void prof_flush();
+void prof_reset();
+bool prof_read(const char *name, double *ms, int64_t *count);
+
+// stream-ordered allocation; returns nullptr on failure (and records it)
+void *dalloc(size_t bytes, cudaStream_t s);
+void dfree(void *p, cudaStream_t s);
+
+// host-side allocation fault injection (the reference's malloc_debug
+// counter, Source/global/GB_Global.c:83-93): when armed with n > 0, the n-th
+// following device allocation fails.  0 disarms.
+void set_alloc_fail_countdown(int64_t n);
+
+// map a CUDA error to the reference's convention (CUDA/include/
+// GB_cuda_error.hpp:22-35): out of memory -> OUT_OF_MEMORY, else PANIC
+int cuda_to_info(cudaError_t e);
+
+// scratch buffers that live for one call on one stream
+struct Scratch {
+    cudaStream_t s;
+    void *ptrs[64];
+    int n = 0;
+    bool failed = false;
+    explicit Scratch(cudaStream_t st) : s(st) {}
+    template <typename T> T *get(size_t count) {
+        if (n >= 64) { failed = true; return nullptr; }
+        void *p = dalloc(count * sizeof(T) + 16, s);
+        if (!p) { failed = true; return nullptr; }
+        ptrs[n++] = p;
+        return reinterpret_cast<T *>(p);
+    }
+    ~Scratch() { for (int i = 0; i < n; i++) dfree(ptrs[i], s); }
+};
+
+// ---- device matrix management ----
+void dev_free(DevCSR &A, cudaStream_t s);
+
+// upload a host CSR (int64 p/i as in GB_matrix.h) into a DevCSR (int32)
+int dev_upload(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
+               const int64_t *i, const void *x, int type, bool iso,
+               cudaStream_t s);
+
+// download a DevCSR to host int64 arrays allocated with `alloc`; zombies are
+// kept as flipped indices when keep_zombies, else they are removed
+typedef void *(*alloc_fn)(size_t);
+int dev_download(const DevCSR &A, int64_t **p, int64_t **i, void **x,
+                 bool keep_zombies, alloc_fn alloc, cudaStream_t s);
+
+// structural copy of a valued mask: entries whose value is false dropped
+int dev_mask_to_struct(DevCSR &out, const DevCSR &M, cudaStream_t s);
+
+// remove zombies in place (GB_wait's zombie pruning), producing a clean CSR
+int dev_prune_zombies(DevCSR &A, cudaStream_t s);
+
+// ---- scans ----
+// exclusive scan of n int64 values in place; out[n] receives the total when
+// `with_total`.  `in` and `out` may alias.
+int scan_exclusive_i64(const int64_t *in, int64_t *out, int64_t n,
+                       cudaStream_t s);
+int scan_exclusive_i32_to_i64(const int32_t *in, int64_t *out, int64_t n,
+                              cudaStream_t s);
+
+// ---- operations (device matrices) ----
+
+struct SemiringCode { int add, mult, type; };
+
+// C<M> = A*B' by dot products over M's pattern (Source/mxm/GB_AxB_dot3.c:37).
+// C gets M's pattern with zombies for empty dot products.
+int dot3(DevCSR &C, const DevCSR &M, bool mask_struct, const DevCSR &A,
+         const DevCSR &B, SemiringCode sr, cudaStream_t s);
+
+// C<M> = A*B row by row (Source/mxm/GB_AxB_saxpy3.c:119); M may be null.
+// Output rows are sorted, no zombies.
+int saxpy3(DevCSR &C, const DevCSR *M, bool mask_comp, bool mask_struct,
+           const DevCSR &A, const DevCSR &B, SemiringCode sr, cudaStream_t s);
+
+// s = reduce(A) with a monoid over live entries (zombies skipped)
+// (Source/reduce/GB_reduce_to_scalar.c:41); result written to host *out
+int reduce_scalar(void *out, const DevCSR &A, int monoid, cudaStream_t s);
+
+// C<M,replace> = accum(C,T)  (Source/mask/GB_accum_mask.c:126)
+int accum_mask(DevCSR &C, const DevCSR &T, const DevCSR *M, bool mask_comp,
+               bool mask_struct, bool replace, int accum, cudaStream_t s);
+
+// B = A' (Source/transpose/GB_transpose_cast.c:18)
+int transpose(DevCSR &B, const DevCSR &A, cudaStream_t s);
+
+// supported semiring?  (declines with NO_VALUE otherwise)
+bool semiring_supported(SemiringCode sr);
+
+}  // namespace grb

@@ -1,0 +1,178 @@
+/* grb_b200.h: C-ABI of the B200 semiring sparse-matrix-multiply library.
+ *
+ * Two groups of entry points, all extern "C" with plain pointers and sizes:
+ *
+ *  1. The drop-in boundary for SuiteSparse:GraphBLAS v9.3.1.  These take
+ *     matrices exactly as the library's internal kernels see them (vectors of
+ *     length vlen, int64 offsets/indices, GB_Type_code, GB_Opcode) and return
+ *     results allocated with the library's own allocator, so a maintainer can
+ *     call them from the library's method selectors in place of the CPU
+ *     kernels (see INTEGRATION.md for the shim).
+ *
+ *  2. Device-resident matrices (grb_b200_dmatrix), used by the by-row host API
+ *     in GraphBLAS_b200.h, by the batched kernel and by the request server:
+ *     matrices stay in HBM between calls.
+ *
+ * Every call synchronises its own stream before returning.  Return values are
+ * the reference's GrB_Info codes (Include/GraphBLAS.h:358-381):
+ *   0 GrB_SUCCESS, 1 GrB_NO_VALUE (declined: the caller keeps its own path),
+ *   -102 GrB_OUT_OF_MEMORY, -101 GrB_PANIC, -3 GrB_INVALID_VALUE,
+ *   -6 GrB_DIMENSION_MISMATCH.
+ */
+#ifndef GRB_B200_H
+#define GRB_B200_H
+
+#include <stdint.h>
+#include <stdbool.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A sparse matrix as a set of vdim vectors of length vlen: the fields of
+ * struct GB_Matrix_opaque the multiply kernels read
+ * (Source/builtin/include/GB_matrix.h:213-235, 390, 455-515).  For a by-row
+ * matrix the vectors are rows (vdim = nrows, vlen = ncols). */
+typedef struct
+{
+    int64_t vlen;       /* length of each vector */
+    int64_t vdim;       /* number of vectors */
+    int64_t *p;         /* vdim+1 offsets */
+    int64_t *i;         /* indices; a zombie holds -(i)-2 (GB_zombie.h:37) */
+    void *x;            /* values: nnz entries, or 1 if iso; NULL = iso true */
+    int type;           /* GB_Type_code (Source/builtin/include/GB_opaque.h:28) */
+    bool iso;           /* all values equal x[0] */
+    bool jumbled;       /* indices within a vector may be unsorted */
+    int64_t nzombies;   /* number of zombies */
+} grb_b200_matrix;
+
+/* A built-in semiring: opcodes of the additive monoid and the multiplier
+ * (GB_Opcode, Source/builtin/include/GB_opaque.h:209-247) and the type code
+ * of the monoid (= the type of C). */
+typedef struct
+{
+    int add_opcode;
+    int mult_opcode;
+    int type;
+} grb_b200_semiring;
+
+typedef void *(*grb_b200_malloc_fn)(size_t);
+typedef void (*grb_b200_free_fn)(void *);
+
+/* Initialise the device (idempotent).  Replaces GB_cuda_init
+ * (CUDA/GB_cuda_init.c:18). */
+int grb_b200_init(void);
+
+/* Release cached device memory and streams.  No counterpart call in the
+ * reference (its rmm pool is torn down by rmm_wrap_finalize,
+ * rmm_wrap/rmm_wrap.h). */
+int grb_b200_finalize(void);
+
+/* Allocator used for every host array returned by the drop-in calls: the
+ * library's GB_malloc function (Source/global/GB_Global.c:83-93,
+ * GB_Global_malloc_function).  Default: malloc / free. */
+void grb_b200_set_allocator(grb_b200_malloc_fn m, grb_b200_free_fn f);
+
+/* True if the GPU takes this dot3 problem (sparse inputs, built-in semiring
+ * in the compiled list, n and nnz below 2^31).  Replaces
+ * GB_cuda_AxB_dot3_branch (CUDA/GB_cuda_AxB_dot3_branch.cpp:15). */
+bool grb_b200_AxB_dot3_branch(const grb_b200_matrix *M,
+                              const grb_b200_matrix *A,
+                              const grb_b200_matrix *B,
+                              const grb_b200_semiring *semiring, bool flipxy);
+
+/* C<M> = A'*B by dot products (vector i of A with vector j of B, for every
+ * entry i of vector j of M).  C gets M's pattern; empty dot products are
+ * zombies, counted in C->nzombies; C->jumbled = M->jumbled.  Replaces
+ * GB_AxB_dot3 (Source/mxm/GB_AxB_dot3.c:37-49) and GB_cuda_AxB_dot3
+ * (CUDA/GB_cuda_AxB_dot3.cpp:35).  C->p, C->i, C->x are allocated with the
+ * allocator above and owned by the caller. */
+int grb_b200_AxB_dot3(grb_b200_matrix *C, const grb_b200_matrix *M,
+                      bool Mask_struct, const grb_b200_matrix *A,
+                      const grb_b200_matrix *B,
+                      const grb_b200_semiring *semiring, bool flipxy);
+
+/* C<M> = A*B by the saxpy method (C(:,j) = sum over k of A(:,k)*B(k,j), the
+ * vectors of C being the vectors of B); M may be NULL, complemented or
+ * structural.  The result is sorted, has no zombies, and *mask_applied is set
+ * when M was used.  do_sort is accepted for signature parity; rows always come
+ * back sorted.  Replaces GB_AxB_saxpy3 (Source/mxm/GB_AxB_saxpy3.h:19-36). */
+int grb_b200_AxB_saxpy3(grb_b200_matrix *C, const grb_b200_matrix *M,
+                        bool Mask_comp, bool Mask_struct,
+                        const grb_b200_matrix *A, const grb_b200_matrix *B,
+                        const grb_b200_semiring *semiring, bool flipxy,
+                        bool *mask_applied, int do_sort);
+
+/* s = reduce(A) with a built-in monoid (opcode, type of A), zombies skipped.
+ * `out` receives one value of A's type.  Replaces GB_cuda_reduce_to_scalar
+ * (CUDA/GB_cuda_reduce_to_scalar.cpp) / GB_reduce_to_scalar
+ * (Source/reduce/GB_reduce_to_scalar.c:41). */
+int grb_b200_reduce_to_scalar(void *out, const grb_b200_matrix *A,
+                              int monoid_opcode);
+
+/* Arm host-side allocation fault injection: the n-th following device
+ * allocation fails (0 disarms), as the reference's malloc_debug counter does
+ * for its own allocations (Source/global/GB_Global.c:83-93). */
+void grb_b200_debug_fail_alloc(int64_t n);
+
+/* Run this host thread's subsequent calls on the caller's CUDA stream
+ * (a cudaStream_t; NULL returns to the library's stream pool).  Calls still
+ * synchronise that stream before returning.  No counterpart in the
+ * reference, whose GPU calls create a private stream each
+ * (CUDA/GB_cuda_AxB_dot3.cpp:54). */
+void grb_b200_set_stream(void *stream);
+
+/* Kernel timing with CUDA events recorded on the launching stream around
+ * each launch of the hot kernels ("dot3", "saxpy3_numeric", ...).  Off by
+ * default; the reference's equivalent is its GpuTimer
+ * (CUDA/include/GB_cuda_timer.hpp) around the dot3 launches. */
+void grb_b200_profile_enable(bool on);
+void grb_b200_profile_reset(void);
+int grb_b200_profile(const char *kernel, double *total_ms, int64_t *launches);
+
+/* ------------------------------------------------------------------------ */
+/* Device-resident matrices (by-row CSR held in HBM)                        */
+/* ------------------------------------------------------------------------ */
+
+typedef struct grb_b200_dmatrix_s *grb_b200_dmatrix;
+
+/* Upload host CSR (int64 offsets/indices, reference layout).  x == NULL makes
+ * an iso-true pattern matrix. */
+int grb_b200_dmatrix_upload(grb_b200_dmatrix *D, int64_t nrows, int64_t ncols,
+                            const int64_t *p, const int64_t *i, const void *x,
+                            int type, bool iso);
+
+/* Download to host arrays allocated with the allocator above (zombies pruned
+ * when prune is true, else returned as -(j)-2). */
+int grb_b200_dmatrix_download(grb_b200_dmatrix D, int64_t **p, int64_t **i,
+                              void **x, bool prune);
+
+int grb_b200_dmatrix_free(grb_b200_dmatrix *D);
+
+/* nrows, ncols, stored entries (zombies included), zombies, type, iso */
+int grb_b200_dmatrix_info(grb_b200_dmatrix D, int64_t *nrows, int64_t *ncols,
+                          int64_t *nnz, int64_t *nzombies, int *type,
+                          bool *iso);
+
+/* C<M> = A*B' over M's pattern (row i of A . row j of B); zombies kept */
+int grb_b200_dmxm_dot3(grb_b200_dmatrix *C, grb_b200_dmatrix M,
+                       bool mask_struct, grb_b200_dmatrix A,
+                       grb_b200_dmatrix B, const grb_b200_semiring *s);
+
+/* C<M> = A*B row by row; M may be NULL */
+int grb_b200_dmxm_saxpy3(grb_b200_dmatrix *C, grb_b200_dmatrix M,
+                         bool mask_comp, bool mask_struct, grb_b200_dmatrix A,
+                         grb_b200_dmatrix B, const grb_b200_semiring *s);
+
+/* out = reduce(D) over live entries */
+int grb_b200_dreduce(void *out, grb_b200_dmatrix D, int monoid_opcode);
+
+/* Remove zombies (the zombie pruning of GB_wait, Source/wait/GB_wait.c:62) */
+int grb_b200_dwait(grb_b200_dmatrix D);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

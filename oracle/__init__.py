@@ -1,0 +1,259 @@
+"""The oracle: test infrastructure for the semiring SpGEMM path.
+
+Two checkers live here, both CPU-only:
+
+* ``Oracle`` wraps ``liboracle.so``, a plain-C restatement of the
+  reference's algorithm (``oracle/oracle.c``; every function there cites the
+  SuiteSparse:GraphBLAS file:line it follows).
+* ``Reference`` wraps ``_ref/libref_runner.so``, which drives the reference
+  library itself (built from its own sources by ``oracle/ref.mk``) through its
+  public C API.  It pins the restatement and serves as the CPU baseline.
+
+Only the tests, the smoke check and the CPU-baseline leg of ``bench.py`` use
+this package, and only as the checker: the product (``graphblas_b200``) never
+imports it.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_P = np.ctypeslib.ndpointer
+
+TYPE_CODES = {"bool": 1, "int32": 6, "uint32": 7, "int64": 8, "uint64": 9,
+              "fp32": 10, "fp64": 11}
+NP_TYPES = {1: np.bool_, 6: np.int32, 7: np.uint32, 8: np.int64, 9: np.uint64,
+            10: np.float32, 11: np.float64}
+OPS = {"FIRST": 72, "SECOND": 73, "ANY": 74, "PAIR": 75, "MIN": 76, "MAX": 77,
+       "PLUS": 78, "MINUS": 79, "RMINUS": 80, "TIMES": 81, "DIV": 82, "LOR": 91,
+       "LAND": 92, "LXOR": 93, "EQ": 102, "FIRSTI": 115, "FIRSTJ": 117,
+       "SECONDI": 119, "SECONDJ": 121}
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _i64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int64)
+
+
+class Oracle:
+    """ctypes front end of the C restatement (liboracle.so)."""
+
+    def __init__(self, path=None):
+        path = path or os.path.join(HERE, "liboracle.so")
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        vp = ctypes.c_void_p
+        L.oracle_saxpy.restype = vp
+        L.oracle_saxpy.argtypes = [ctypes.c_int64, ctypes.c_int64,
+                                   vp, vp, vp, ctypes.c_int, vp, vp, vp,
+                                   ctypes.c_int, vp, vp, vp, ctypes.c_int,
+                                   ctypes.c_bool, ctypes.c_bool, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int]
+        L.oracle_dot3.restype = vp
+        L.oracle_dot3.argtypes = [ctypes.c_int64, ctypes.c_int64,
+                                  vp, vp, vp, ctypes.c_int, vp, vp, vp,
+                                  ctypes.c_int, vp, vp, vp, ctypes.c_int,
+                                  ctypes.c_bool, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_int]
+        L.oracle_accum_mask.restype = vp
+        L.oracle_accum_mask.argtypes = [ctypes.c_int64, ctypes.c_int64,
+                                        vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                        ctypes.c_int, ctypes.c_bool,
+                                        ctypes.c_bool, ctypes.c_bool,
+                                        ctypes.c_int, ctypes.c_int]
+        L.oracle_nnz.restype = ctypes.c_int64
+        L.oracle_nnz.argtypes = [vp]
+        L.oracle_export.argtypes = [vp, vp, vp, vp]
+        L.oracle_free.argtypes = [vp]
+        L.oracle_tricount.restype = ctypes.c_int64
+        L.oracle_tricount.argtypes = [ctypes.c_int64, vp, vp, vp, vp]
+        L.oracle_bfs.restype = ctypes.c_int
+        L.oracle_bfs.argtypes = [ctypes.c_int64, vp, vp, ctypes.c_int64, vp, vp]
+
+    def _take(self, h, m, ctype):
+        L = self.lib
+        nnz = L.oracle_nnz(h)
+        p = np.empty(m + 1, np.int64)
+        i = np.empty(max(nnz, 1), np.int64)
+        x = np.empty(max(nnz, 1), NP_TYPES[ctype])
+        L.oracle_export(h, _ptr(p), _ptr(i), _ptr(x))
+        L.oracle_free(h)
+        return p, i[:nnz], x[:nnz]
+
+    def saxpy(self, m, ncols, A, B, add, mult, ctype, M=None,
+              mask_struct=True, mask_comp=False):
+        """C<M> = A*B row by row.  A, B, M are (p, i, x, type) tuples."""
+        Ap, Ai, Ax, at = A
+        Bp, Bi, Bx, bt = B
+        Mp = Mi = Mx = None
+        mt = 1
+        if M is not None:
+            Mp, Mi, Mx, mt = M
+        keep = [_i64(Ap), _i64(Ai), _i64(Bp), _i64(Bi), _i64(Mp), _i64(Mi)]
+        h = self.lib.oracle_saxpy(m, ncols, _ptr(keep[0]), _ptr(keep[1]),
+                                  _ptr(Ax), at, _ptr(keep[2]), _ptr(keep[3]),
+                                  _ptr(Bx), bt, _ptr(keep[4]), _ptr(keep[5]),
+                                  _ptr(Mx), mt, mask_struct, mask_comp,
+                                  OPS[add], OPS[mult], ctype)
+        return self._take(h, m, ctype)
+
+    def dot3(self, m, ncols, A, B, M, add, mult, ctype, mask_struct=True):
+        """C<M> = A*B' (row i of A dot row j of B), zombies removed."""
+        Ap, Ai, Ax, at = A
+        Bp, Bi, Bx, bt = B
+        Mp, Mi, Mx, mt = M
+        keep = [_i64(Ap), _i64(Ai), _i64(Bp), _i64(Bi), _i64(Mp), _i64(Mi)]
+        h = self.lib.oracle_dot3(m, ncols, _ptr(keep[0]), _ptr(keep[1]),
+                                 _ptr(Ax), at, _ptr(keep[2]), _ptr(keep[3]),
+                                 _ptr(Bx), bt, _ptr(keep[4]), _ptr(keep[5]),
+                                 _ptr(Mx), mt, mask_struct, OPS[add],
+                                 OPS[mult], ctype)
+        return self._take(h, m, ctype)
+
+    def accum_mask(self, m, ncols, C, T, ctype, M=None, mask_struct=True,
+                   mask_comp=False, replace=False, accum=None):
+        Cp, Ci, Cx = C
+        Tp, Ti, Tx = T
+        Mp = Mi = Mx = None
+        mt = 1
+        if M is not None:
+            Mp, Mi, Mx, mt = M
+        keep = [_i64(Cp), _i64(Ci), _i64(Tp), _i64(Ti), _i64(Mp), _i64(Mi)]
+        h = self.lib.oracle_accum_mask(
+            m, ncols, _ptr(keep[0]), _ptr(keep[1]), _ptr(Cx), _ptr(keep[2]),
+            _ptr(keep[3]), _ptr(Tx), _ptr(keep[4]), _ptr(keep[5]), _ptr(Mx),
+            mt, mask_struct, mask_comp, replace, OPS[accum] if accum else 0,
+            ctype)
+        return self._take(h, m, ctype)
+
+    def tricount(self, n, Lp, Li, Up, Ui):
+        keep = [_i64(Lp), _i64(Li), _i64(Up), _i64(Ui)]
+        return int(self.lib.oracle_tricount(n, *[_ptr(k) for k in keep]))
+
+    def bfs(self, n, Sp, Si, src):
+        parent = np.empty(n, np.int64)
+        level = np.empty(n, np.int64)
+        keep = [_i64(Sp), _i64(Si)]
+        self.lib.oracle_bfs(n, _ptr(keep[0]), _ptr(keep[1]), src,
+                            _ptr(parent), _ptr(level))
+        return parent, level
+
+
+class Reference:
+    """ctypes front end of the reference library itself (oracle/_ref)."""
+
+    def __init__(self, nthreads=None, path=None):
+        path = path or os.path.join(HERE, "_ref", "libref_runner.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        vp = ctypes.c_void_p
+        L.ref_init.argtypes = [ctypes.c_int]
+        L.ref_set_nthreads.argtypes = [ctypes.c_int]
+        L.ref_mxm.restype = vp
+        L.ref_mxm.argtypes = ([ctypes.c_int64] * 3 + [vp, vp, vp, ctypes.c_int]
+                              + [ctypes.c_int64, vp, vp, vp, ctypes.c_int]
+                              + [vp, vp, vp, ctypes.c_int] + [vp, vp, vp]
+                              + [ctypes.c_bool] * 4 + [ctypes.c_int] * 5
+                              + [ctypes.POINTER(ctypes.c_int)])
+        L.ref_nnz.restype = ctypes.c_int64
+        L.ref_nnz.argtypes = [vp]
+        L.ref_seconds.restype = ctypes.c_double
+        L.ref_seconds.argtypes = [vp]
+        L.ref_export.argtypes = [vp, vp, vp, vp]
+        L.ref_free.argtypes = [vp]
+        L.ref_tricount.argtypes = [ctypes.c_int64, vp, vp, vp, vp, ctypes.c_int,
+                                   vp, vp]
+        L.ref_bfs.argtypes = [ctypes.c_int64, vp, vp, ctypes.c_int64, vp, vp, vp]
+        L.ref_batch_square.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp,
+                                       ctypes.c_int, ctypes.c_int, vp, vp]
+        self.nthreads = nthreads or os.cpu_count()
+        info = L.ref_init(self.nthreads)
+        if info != 0:
+            raise RuntimeError("GrB_init failed: %d" % info)
+
+    def set_nthreads(self, n):
+        self.nthreads = n
+        self.lib.ref_set_nthreads(n)
+
+    def mxm(self, m, n, ncols, A, B, add, mult, ctype, M=None,
+            mask_struct=True, mask_comp=False, replace=False,
+            transpose_b=False, accum=None, C=None, method=0):
+        """C<M> = accum(C, A*B or A*B') with the reference GrB_mxm; returns
+        the sorted CSR (p, i, x) after GrB_Matrix_wait."""
+        Ap, Ai, Ax, at = A
+        Bp, Bi, Bx, bt = B
+        Mp = Mi = Mx = None
+        mt = 1
+        if M is not None:
+            Mp, Mi, Mx, mt = M
+        Cp = Ci = Cx = None
+        if C is not None:
+            Cp, Ci, Cx = C
+        bn = len(Bp) - 1
+        keep = [_i64(a) for a in (Ap, Ai, Bp, Bi, Mp, Mi, Cp, Ci)]
+        info = ctypes.c_int(0)
+        h = self.lib.ref_mxm(m, n, ncols, _ptr(keep[0]), _ptr(keep[1]),
+                             _ptr(Ax), at, bn, _ptr(keep[2]), _ptr(keep[3]),
+                             _ptr(Bx), bt, _ptr(keep[4]), _ptr(keep[5]),
+                             _ptr(Mx), mt, _ptr(keep[6]), _ptr(keep[7]),
+                             _ptr(Cx), mask_struct, mask_comp, replace,
+                             transpose_b, OPS[accum] if accum else 0,
+                             OPS[add], OPS[mult], ctype, method,
+                             ctypes.byref(info))
+        if not h:
+            raise RuntimeError("reference GrB_mxm failed: %d" % info.value)
+        L = self.lib
+        nnz = L.ref_nnz(h)
+        p = np.empty(m + 1, np.int64)
+        i = np.empty(max(nnz, 1), np.int64)
+        x = np.empty(max(nnz, 1), NP_TYPES[ctype])
+        L.ref_export(h, _ptr(p), _ptr(i), _ptr(x))
+        L.ref_free(h)
+        return p, i[:nnz], x[:nnz]
+
+    def tricount(self, n, Lp, Li, Up, Ui, reps=1):
+        keep = [_i64(a) for a in (Lp, Li, Up, Ui)]
+        times = np.zeros(reps, np.float64)
+        ntri = np.zeros(1, np.int64)
+        info = self.lib.ref_tricount(n, *[_ptr(k) for k in keep], reps,
+                                     _ptr(times), _ptr(ntri))
+        if info != 0:
+            raise RuntimeError("reference tricount failed: %d" % info)
+        return int(ntri[0]), times
+
+    def bfs(self, n, Sp, Si, src):
+        keep = [_i64(Sp), _i64(Si)]
+        parent = np.empty(n, np.int64)
+        secs = np.zeros(1, np.float64)
+        nlev = np.zeros(1, np.int32)
+        info = self.lib.ref_bfs(n, _ptr(keep[0]), _ptr(keep[1]), src,
+                                _ptr(parent), _ptr(secs), _ptr(nlev))
+        if info != 0:
+            raise RuntimeError("reference bfs failed: %d" % info)
+        return parent, float(secs[0]), int(nlev[0])
+
+    def batch_square(self, nsz, poff, ioff, Ap, Ai, Ax, add="MIN", mult="PLUS"):
+        count = len(nsz)
+        keep = [_i64(nsz), _i64(poff), _i64(ioff), _i64(Ap), _i64(Ai)]
+        Ax = np.ascontiguousarray(Ax, dtype=np.float32)
+        nnz_out = np.zeros(count, np.int64)
+        secs = np.zeros(1, np.float64)
+        info = self.lib.ref_batch_square(count, *[_ptr(k) for k in keep],
+                                         _ptr(Ax), OPS[add], OPS[mult],
+                                         _ptr(nnz_out), _ptr(secs))
+        if info != 0:
+            raise RuntimeError("reference batch failed: %d" % info)
+        return nnz_out, float(secs[0])
+
+
+def reference_available():
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_runner.so"))

@@ -1,0 +1,41 @@
+# Builds the reference SuiteSparse:GraphBLAS v9.3.1 library from its own
+# sources (read-only tree given by REF) with plain gcc, no cmake.  Output goes
+# only to oracle/_ref/.  The configuration matches a stock release build with
+# the CPU JIT off (-DNJIT), OpenMP on and the factory kernels compiled in.
+# The cpu_features helper is disabled (-DGBNCPUFEAT); the library then picks
+# its AVX paths from compiler macros instead of a run-time probe.
+#
+#   make -f oracle/ref.mk REF=/root/reference -j8
+#
+# The library is test infrastructure: the parity tests and the CPU-baseline
+# leg of bench.py load it as the checker; no product code links it.
+
+REF    ?= /root/reference
+OUT    := oracle/_ref
+OBJ    := $(OUT)/obj
+CC     := /usr/bin/gcc
+INCS   := -I$(REF) -I$(REF)/Source -I$(REF)/Include -I$(REF)/Config \
+          -I$(REF)/xxHash -I$(REF)/lz4 -I$(REF)/zstd -I$(REF)/zstd/zstd_subset \
+          -I$(REF)/JITpackage -I$(REF)/Demo/Include \
+          $(foreach d,apply assign builder builtin callback concat convert ewise \
+            hyper jit_kernels math memory monoid mxm ok omp print reduce select \
+            split slice transpose type wait werk,-I$(REF)/Source/$(d))
+CFLAGS := -O3 -DNDEBUG -fPIC -fopenmp -std=c11 -Wno-pragmas -Wundef -w \
+          -fexcess-precision=fast -fcx-limited-range -fno-math-errno -fwrapv \
+          -DNJIT -DGBNCPUFEAT
+
+SRCS := $(wildcard $(REF)/PreJIT/*.c) $(wildcard $(REF)/Config/*.c) \
+        $(wildcard $(REF)/Source/*/*.c) $(REF)/JITpackage/GB_JITpackage.c \
+        $(wildcard $(REF)/FactoryKernels/*.c)
+OBJS := $(patsubst $(REF)/%.c,$(OBJ)/%.o,$(SRCS))
+
+all: $(OUT)/libgraphblas_ref.so
+
+$(OBJ)/%.o: $(REF)/%.c
+	@mkdir -p $(dir $@)
+	@$(CC) $(CFLAGS) $(INCS) -c $< -o $@
+
+$(OUT)/libgraphblas_ref.so: $(OBJS)
+	$(CC) -shared -fopenmp -o $@ $(OBJS) -lm -ldl -Wl,-soname,libgraphblas_ref.so
+
+.PHONY: all

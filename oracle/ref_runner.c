@@ -1,0 +1,406 @@
+// ref_runner.c: drives the reference SuiteSparse:GraphBLAS library (built
+// from its own sources into oracle/_ref/ by oracle/ref.mk) through its public
+// C API, on CSR arrays handed over from Python.  Test infrastructure only: it
+// pins the oracle restatement to the reference's real output and times the
+// reference's CPU path for the CPU baseline.  No product code links it.
+//
+// Matrices are moved in and out with GxB_Matrix_pack_CSR / unpack_CSR
+// (Include/GraphBLAS.h:9449, :9976), so both sides see identical bytes.
+// Operator / type codes are the reference's GB_Opcode / GB_Type_code numbers
+// (Source/builtin/include/GB_opaque.h:28-42, 209-247).
+
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <stdbool.h>
+#include <omp.h>
+#include "GraphBLAS.h"
+
+enum { T_BOOL = 1, T_INT32 = 6, T_UINT32 = 7, T_INT64 = 8, T_UINT64 = 9,
+       T_FP32 = 10, T_FP64 = 11 };
+enum { OP_FIRST = 72, OP_SECOND = 73, OP_ANY = 74, OP_PAIR = 75, OP_MIN = 76,
+       OP_MAX = 77, OP_PLUS = 78, OP_MINUS = 79, OP_RMINUS = 80, OP_TIMES = 81,
+       OP_DIV = 82, OP_LOR = 91, OP_LAND = 92, OP_LXOR = 93, OP_EQ = 102,
+       OP_FIRSTI = 115, OP_FIRSTJ = 117, OP_SECONDI = 119, OP_SECONDJ = 121 };
+
+static GrB_Type type_of(int t)
+{
+    switch (t)
+    {
+        case T_BOOL: return GrB_BOOL;
+        case T_INT32: return GrB_INT32;
+        case T_UINT32: return GrB_UINT32;
+        case T_INT64: return GrB_INT64;
+        case T_UINT64: return GrB_UINT64;
+        case T_FP32: return GrB_FP32;
+        case T_FP64: return GrB_FP64;
+    }
+    return NULL;
+}
+
+static size_t tsize(int t)
+{
+    switch (t)
+    {
+        case T_BOOL: return 1;
+        case T_INT32: case T_UINT32: case T_FP32: return 4;
+        default: return 8;
+    }
+}
+
+#define BY_TYPE(PFX, SFX, t)                                                \
+    switch (t) {                                                            \
+        case T_BOOL: return PFX##BOOL##SFX;                                 \
+        case T_INT32: return PFX##INT32##SFX;                               \
+        case T_UINT32: return PFX##UINT32##SFX;                             \
+        case T_INT64: return PFX##INT64##SFX;                               \
+        case T_UINT64: return PFX##UINT64##SFX;                             \
+        case T_FP32: return PFX##FP32##SFX;                                 \
+        case T_FP64: return PFX##FP64##SFX;                                 \
+    } return NULL;
+
+#define BY_TYPE_NB(PFX, SFX, t)                                             \
+    switch (t) {                                                            \
+        case T_INT32: return PFX##INT32##SFX;                               \
+        case T_UINT32: return PFX##UINT32##SFX;                             \
+        case T_INT64: return PFX##INT64##SFX;                               \
+        case T_UINT64: return PFX##UINT64##SFX;                             \
+        case T_FP32: return PFX##FP32##SFX;                                 \
+        case T_FP64: return PFX##FP64##SFX;                                 \
+    } return NULL;
+
+static GrB_Monoid monoid_of(int op, int t)
+{
+    if (t == T_BOOL)
+    {
+        // boolean PLUS/MAX are LOR and TIMES/MIN are LAND
+        switch (op)
+        {
+            case OP_PLUS: case OP_MAX: case OP_LOR: return GrB_LOR_MONOID_BOOL;
+            case OP_TIMES: case OP_MIN: case OP_LAND: return GrB_LAND_MONOID_BOOL;
+            case OP_ANY: return GxB_ANY_BOOL_MONOID;
+            case OP_LXOR: return GrB_LXOR_MONOID_BOOL;
+        }
+        return NULL;
+    }
+    switch (op)
+    {
+        case OP_PLUS:  { BY_TYPE_NB(GrB_PLUS_MONOID_, , t) }
+        case OP_TIMES: { BY_TYPE_NB(GrB_TIMES_MONOID_, , t) }
+        case OP_MIN:   { BY_TYPE_NB(GrB_MIN_MONOID_, , t) }
+        case OP_MAX:   { BY_TYPE_NB(GrB_MAX_MONOID_, , t) }
+        case OP_ANY:   { BY_TYPE_NB(GxB_ANY_, _MONOID, t) }
+        case OP_LOR:   return GrB_LOR_MONOID_BOOL;
+        case OP_LAND:  return GrB_LAND_MONOID_BOOL;
+        case OP_LXOR:  return GrB_LXOR_MONOID_BOOL;
+    }
+    return NULL;
+}
+
+static GrB_BinaryOp binop_of(int op, int t)
+{
+    switch (op)
+    {
+        case OP_FIRST:  { BY_TYPE(GrB_FIRST_, , t) }
+        case OP_SECOND: { BY_TYPE(GrB_SECOND_, , t) }
+        case OP_PAIR:   { BY_TYPE(GxB_PAIR_, , t) }
+        case OP_PLUS:   { BY_TYPE(GrB_PLUS_, , t) }
+        case OP_MINUS:  { BY_TYPE(GrB_MINUS_, , t) }
+        case OP_RMINUS: { BY_TYPE(GxB_RMINUS_, , t) }
+        case OP_TIMES:  { BY_TYPE(GrB_TIMES_, , t) }
+        case OP_DIV:    { BY_TYPE(GrB_DIV_, , t) }
+        case OP_MIN:    { BY_TYPE(GrB_MIN_, , t) }
+        case OP_MAX:    { BY_TYPE(GrB_MAX_, , t) }
+        case OP_LOR:    { BY_TYPE(GxB_LOR_, , t) }
+        case OP_LAND:   { BY_TYPE(GxB_LAND_, , t) }
+        case OP_FIRSTI:  return t == T_INT32 ? GxB_FIRSTI_INT32 : GxB_FIRSTI_INT64;
+        case OP_FIRSTJ:  return t == T_INT32 ? GxB_FIRSTJ_INT32 : GxB_FIRSTJ_INT64;
+        case OP_SECONDI: return t == T_INT32 ? GxB_SECONDI_INT32 : GxB_SECONDI_INT64;
+        case OP_SECONDJ: return t == T_INT32 ? GxB_SECONDJ_INT32 : GxB_SECONDJ_INT64;
+    }
+    return NULL;
+}
+
+int ref_init(int nthreads)
+{
+    static int done = 0;
+    if (!done)
+    {
+        GrB_Info info = GrB_init(GrB_NONBLOCKING);
+        if (info != GrB_SUCCESS) return (int)info;
+        done = 1;
+    }
+    return (int)GxB_Global_Option_set_INT32(GxB_NTHREADS, nthreads);
+}
+
+int ref_set_nthreads(int nthreads)
+{
+    return (int)GxB_Global_Option_set_INT32(GxB_NTHREADS, nthreads);
+}
+
+// Build a by-row GrB_Matrix from CSR copies of the caller's arrays.
+// x == NULL builds an iso-true pattern matrix of type t.
+static GrB_Info make_csr(GrB_Matrix *A, int t, int64_t nrows, int64_t ncols,
+                         const int64_t *p, const int64_t *i, const void *x)
+{
+    GrB_Info info = GrB_Matrix_new(A, type_of(t), nrows, ncols);
+    if (info != GrB_SUCCESS) return info;
+    GxB_Matrix_Option_set_INT32(*A, GxB_FORMAT, GxB_BY_ROW);
+    int64_t nnz = p[nrows];
+    size_t ts = tsize(t);
+    GrB_Index *Ap = malloc((nrows + 1) * sizeof(int64_t));
+    GrB_Index *Aj = malloc((nnz ? nnz : 1) * sizeof(int64_t));
+    memcpy(Ap, p, (nrows + 1) * sizeof(int64_t));
+    memcpy(Aj, i, nnz * sizeof(int64_t));
+    void *Ax;
+    bool iso = (x == NULL);
+    if (iso)
+    {
+        Ax = calloc(1, 8);
+        switch (t)
+        {
+            case T_BOOL: *(bool *)Ax = true; break;
+            case T_INT32: *(int32_t *)Ax = 1; break;
+            case T_UINT32: *(uint32_t *)Ax = 1; break;
+            case T_INT64: *(int64_t *)Ax = 1; break;
+            case T_UINT64: *(uint64_t *)Ax = 1; break;
+            case T_FP32: *(float *)Ax = 1; break;
+            case T_FP64: *(double *)Ax = 1; break;
+        }
+    }
+    else
+    {
+        Ax = malloc((nnz ? nnz : 1) * ts);
+        memcpy(Ax, x, nnz * ts);
+    }
+    return GxB_Matrix_pack_CSR(*A, &Ap, &Aj, &Ax, (nrows + 1) * sizeof(int64_t),
+                               (nnz ? nnz : 1) * sizeof(int64_t),
+                               iso ? 8 : (nnz ? nnz : 1) * ts, iso, false, NULL);
+}
+
+typedef struct
+{
+    int64_t nrows, nnz;
+    int type;
+    GrB_Index *p, *i;
+    void *x;
+    double seconds;
+} ref_csr;
+
+void ref_free(ref_csr *C)
+{
+    if (!C) return;
+    free(C->p); free(C->i); free(C->x); free(C);
+}
+
+int64_t ref_nnz(const ref_csr *C) { return C->nnz; }
+double ref_seconds(const ref_csr *C) { return C->seconds; }
+
+void ref_export(const ref_csr *C, int64_t *p, int64_t *i, void *x)
+{
+    memcpy(p, C->p, (C->nrows + 1) * sizeof(int64_t));
+    memcpy(i, C->i, C->nnz * sizeof(int64_t));
+    if (x) memcpy(x, C->x, C->nnz * tsize(C->type));
+}
+
+// C<M> = accum (C, A*B) (or A*B') with the reference's GrB_mxm.
+//   method: 0 auto, 1 dot (GxB_AxB_DOT), 2 Gustavson, 3 hash
+//   transpose_b: the GrB_INP1 = GrB_TRAN descriptor (C = A*B')
+//   Cin == NULL (Cp_in == NULL) starts from an empty C.
+// Returns NULL on error; *info_out gets the GrB_Info.
+ref_csr *ref_mxm(int64_t m, int64_t n, int64_t ncols,
+    const int64_t *Ap, const int64_t *Ai, const void *Ax, int atype,
+    int64_t bnrows, const int64_t *Bp, const int64_t *Bi, const void *Bx, int btype,
+    const int64_t *Mp, const int64_t *Mi, const void *Mx, int mtype,
+    const int64_t *Cp_in, const int64_t *Ci_in, const void *Cx_in,
+    bool mask_struct, bool mask_comp, bool replace, bool transpose_b,
+    int accum, int add, int mult, int ctype, int method, int *info_out)
+{
+    GrB_Matrix A = NULL, B = NULL, M = NULL, C = NULL;
+    GrB_Semiring S = NULL;
+    GrB_Descriptor D = NULL;
+    ref_csr *R = NULL;
+    GrB_Info info;
+    int64_t bncols = transpose_b ? n : ncols;
+    (void)bncols;
+    #define TRY(x) { info = (x); if (info != GrB_SUCCESS) goto done; }
+    TRY(make_csr(&A, atype, m, n, Ap, Ai, Ax));
+    TRY(make_csr(&B, btype, bnrows, transpose_b ? n : ncols, Bp, Bi, Bx));
+    if (Mp) TRY(make_csr(&M, mtype, m, ncols, Mp, Mi, Mx));
+    if (Cp_in) TRY(make_csr(&C, ctype, m, ncols, Cp_in, Ci_in, Cx_in))
+    else
+    {
+        TRY(GrB_Matrix_new(&C, type_of(ctype), m, ncols));
+        GxB_Matrix_Option_set_INT32(C, GxB_FORMAT, GxB_BY_ROW);
+    }
+    TRY(GrB_Semiring_new(&S, monoid_of(add, ctype), binop_of(mult, ctype)));
+    TRY(GrB_Descriptor_new(&D));
+    if (mask_struct && mask_comp)
+        TRY(GrB_Descriptor_set(D, GrB_MASK, GrB_COMP_STRUCTURE))
+    else if (mask_struct) TRY(GrB_Descriptor_set(D, GrB_MASK, GrB_STRUCTURE))
+    else if (mask_comp) TRY(GrB_Descriptor_set(D, GrB_MASK, GrB_COMP))
+    if (replace) TRY(GrB_Descriptor_set(D, GrB_OUTP, GrB_REPLACE));
+    if (transpose_b) TRY(GrB_Descriptor_set(D, GrB_INP1, GrB_TRAN));
+    if (method == 1) TRY(GrB_Descriptor_set(D, GxB_AxB_METHOD, GxB_AxB_DOT))
+    else if (method == 2) TRY(GrB_Descriptor_set(D, GxB_AxB_METHOD, GxB_AxB_GUSTAVSON))
+    else if (method == 3) TRY(GrB_Descriptor_set(D, GxB_AxB_METHOD, GxB_AxB_HASH))
+    double t0 = omp_get_wtime();
+    TRY(GrB_mxm(C, M, accum ? binop_of(accum, ctype) : NULL, S, A, B, D));
+    TRY(GrB_Matrix_wait(C, GrB_MATERIALIZE));
+    double t1 = omp_get_wtime();
+    R = calloc(1, sizeof(ref_csr));
+    R->nrows = m; R->type = ctype; R->seconds = t1 - t0;
+    GrB_Index psize, isize, xsize;
+    bool iso = false;
+    TRY(GxB_Matrix_unpack_CSR(C, &R->p, &R->i, &R->x, &psize, &isize, &xsize,
+                              &iso, NULL, NULL));
+    R->nnz = R->p[m];
+    if (iso && R->nnz > 0)
+    {
+        size_t ts = tsize(ctype);
+        void *x = malloc(R->nnz * ts);
+        for (int64_t k = 0; k < R->nnz; k++)
+            memcpy((char *)x + k * ts, R->x, ts);
+        free(R->x);
+        R->x = x;
+    }
+done:
+    GrB_Matrix_free(&A); GrB_Matrix_free(&B); GrB_Matrix_free(&M);
+    GrB_Matrix_free(&C); GrB_Semiring_free(&S); GrB_Descriptor_free(&D);
+    if (info_out) *info_out = (int)info;
+    if (info != GrB_SUCCESS) { ref_free(R); return NULL; }
+    return R;
+    #undef TRY
+}
+
+// Triangle count with the reference's dot3 path, as LAGraph does it:
+// C<L> = L*U' (plus_pair int64, structural mask), ntri = sum (C).
+// Runs `reps` timed repetitions; times[r] gets each one (mxm + reduce).
+int ref_tricount(int64_t n, const int64_t *Lp, const int64_t *Li,
+                 const int64_t *Up, const int64_t *Ui, int reps,
+                 double *times, int64_t *ntri)
+{
+    GrB_Matrix L = NULL, U = NULL, C = NULL;
+    GrB_Info info;
+    #define TRY(x) { info = (x); if (info != GrB_SUCCESS) goto done; }
+    TRY(make_csr(&L, T_BOOL, n, n, Lp, Li, NULL));
+    TRY(make_csr(&U, T_BOOL, n, n, Up, Ui, NULL));
+    for (int r = 0; r < reps; r++)
+    {
+        double t0 = omp_get_wtime();
+        TRY(GrB_Matrix_new(&C, GrB_INT64, n, n));
+        TRY(GrB_mxm(C, L, NULL, GxB_PLUS_PAIR_INT64, L, U, GrB_DESC_ST1));
+        int64_t s = 0;
+        TRY(GrB_Matrix_reduce_INT64(&s, NULL, GrB_PLUS_MONOID_INT64, C, NULL));
+        double t1 = omp_get_wtime();
+        GrB_Matrix_free(&C);
+        times[r] = t1 - t0;
+        *ntri = s;
+    }
+done:
+    GrB_Matrix_free(&L); GrB_Matrix_free(&U); GrB_Matrix_free(&C);
+    return (int)info;
+    #undef TRY
+}
+
+// Level-synchronous BFS parents as in LAGraph's push step:
+//   q<!struct(p), replace> = q any_secondi S ; p<struct(q)> = q
+// The frontier is kept sparse (GxB_SPARSITY_CONTROL).  parent[v] = -1 when
+// unreached.  Returns GrB_Info; *seconds gets the loop time.
+int ref_bfs(int64_t n, const int64_t *Sp, const int64_t *Si, int64_t src,
+            int64_t *parent, double *seconds, int *nlevels)
+{
+    GrB_Matrix S = NULL;
+    GrB_Vector q = NULL, p = NULL;
+    GrB_Info info;
+    #define TRY(x) { info = (x); if (info != GrB_SUCCESS) goto done; }
+    TRY(make_csr(&S, T_BOOL, n, n, Sp, Si, NULL));
+    double t0 = omp_get_wtime();
+    TRY(GrB_Vector_new(&q, GrB_INT64, n));
+    TRY(GrB_Vector_new(&p, GrB_INT64, n));
+    GxB_Vector_Option_set_INT32(q, GxB_SPARSITY_CONTROL, GxB_SPARSE);
+    GxB_Vector_Option_set_INT32(p, GxB_SPARSITY_CONTROL, GxB_SPARSE);
+    TRY(GrB_Vector_setElement_INT64(q, src, src));
+    TRY(GrB_Vector_setElement_INT64(p, src, src));
+    GrB_Index nq = 1;
+    int lev = 0;
+    while (nq > 0)
+    {
+        lev++;
+        TRY(GrB_vxm(q, p, NULL, GxB_ANY_SECONDI_INT64, q, S, GrB_DESC_RSC));
+        TRY(GrB_Vector_nvals(&nq, q));
+        if (nq == 0) break;
+        TRY(GrB_Vector_assign(p, q, NULL, q, GrB_ALL, n, GrB_DESC_S));
+    }
+    TRY(GrB_Vector_wait(p, GrB_MATERIALIZE));
+    *seconds = omp_get_wtime() - t0;
+    *nlevels = lev;
+    for (int64_t v = 0; v < n; v++) parent[v] = -1;
+    {
+        GrB_Index np = 0;
+        TRY(GrB_Vector_nvals(&np, p));
+        GrB_Index *Iv = malloc((np ? np : 1) * sizeof(GrB_Index));
+        int64_t *Xv = malloc((np ? np : 1) * sizeof(int64_t));
+        GrB_Index nn = np;
+        info = GrB_Vector_extractTuples_INT64(Iv, Xv, &nn, p);
+        if (info == GrB_SUCCESS)
+            for (GrB_Index t = 0; t < nn; t++) parent[Iv[t]] = Xv[t];
+        free(Iv); free(Xv);
+    }
+done:
+    GrB_Matrix_free(&S); GrB_Vector_free(&q); GrB_Vector_free(&p);
+    return (int)info;
+    #undef TRY
+}
+
+// A loop of `count` independent C_i = A_i*A_i (min_plus fp32 by default),
+// the reference's per-call path for a batch of small problems.  Instance i
+// uses rows [off[i], off[i+1]) of the concatenated row pointer arrays:
+// Ap + poff[i] (n_i + 1 entries) indexes Ai + ioff[i] / Ax + ioff[i].
+// nnz_out[i] gets nnz(C_i); returns GrB_Info, *seconds the loop time.
+int ref_batch_square(int count, const int64_t *nsz, const int64_t *poff,
+                     const int64_t *ioff, const int64_t *Ap, const int64_t *Ai,
+                     const float *Ax, int add, int mult, int64_t *nnz_out,
+                     double *seconds)
+{
+    GrB_Info info = GrB_SUCCESS;
+    GrB_Semiring S = NULL;
+    GrB_Matrix *As = calloc(count, sizeof(GrB_Matrix));
+    GrB_Matrix *Cs = calloc(count, sizeof(GrB_Matrix));
+    #define TRY(x) { info = (x); if (info != GrB_SUCCESS) goto done; }
+    TRY(GrB_Semiring_new(&S, monoid_of(add, T_FP32), binop_of(mult, T_FP32)));
+    for (int b = 0; b < count; b++)
+    {
+        int64_t n = nsz[b];
+        // rebase this instance's row pointers to start at zero
+        int64_t *p = malloc((n + 1) * sizeof(int64_t));
+        for (int64_t r = 0; r <= n; r++) p[r] = Ap[poff[b] + r] - Ap[poff[b]];
+        info = make_csr(&As[b], T_FP32, n, n, p, Ai + ioff[b], Ax + ioff[b]);
+        free(p);
+        if (info != GrB_SUCCESS) goto done;
+        TRY(GrB_Matrix_new(&Cs[b], GrB_FP32, n, n));
+    }
+    double t0 = omp_get_wtime();
+    for (int b = 0; b < count; b++)
+    {
+        TRY(GrB_mxm(Cs[b], NULL, NULL, S, As[b], As[b], NULL));
+        TRY(GrB_Matrix_wait(Cs[b], GrB_MATERIALIZE));
+    }
+    *seconds = omp_get_wtime() - t0;
+    for (int b = 0; b < count; b++)
+    {
+        GrB_Index nv = 0;
+        GrB_Matrix_nvals(&nv, Cs[b]);
+        nnz_out[b] = (int64_t)nv;
+    }
+done:
+    for (int b = 0; b < count; b++)
+    {
+        GrB_Matrix_free(&As[b]);
+        GrB_Matrix_free(&Cs[b]);
+    }
+    free(As); free(Cs);
+    GrB_Semiring_free(&S);
+    return (int)info;
+    #undef TRY
+}

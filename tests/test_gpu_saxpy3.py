@@ -1,0 +1,166 @@
+"""GPU parity of row-wise saxpy3, C<M> = A*B, against the oracle
+(oracle/oracle.c restating the coarse Gustavson/hash tasks of
+Source/mxm/template/GB_AxB_saxpy3_template.c), called through the C-ABI.
+Every bin is covered: shared-memory hash rows of each size class, heavy rows
+in the dense accumulator (sequential-k and atomic variants), masks and
+complemented masks.
+"""
+
+import numpy as np
+import pytest
+
+from graphblas_b200 import workloads as W
+from tests.helpers import assert_exact, assert_roundoff, random_csr
+
+pytestmark = pytest.mark.gpu
+
+
+def _saxpy_dev(gb, A, B, sr, M=None, mask_comp=False, mask_struct=True,
+               type_name=None):
+    dA = gb.DMatrix.upload(A, type_name=type_name)
+    dB = gb.DMatrix.upload(B, type_name=type_name)
+    dM = None
+    if M is not None:
+        dM = gb.DMatrix.upload(M, type_name=None if M.x is not None else "bool")
+    C = gb.saxpy3(dA, dB, sr, M=dM, mask_comp=mask_comp, mask_struct=mask_struct)
+    out = C.download(prune=True)
+    for d in (dA, dB, dM, C):
+        if d is not None:
+            d.free()
+    return out
+
+
+def test_er_plus_times_fp64_exact(gpu, oracle):
+    """The saxpy3 configuration (Erdos-Renyi, 8 per row, U[-1,1]) at 4096."""
+    gb = gpu
+    A = W.er_fixed(4096, 4096, 8, seed=1)
+    B = W.er_fixed(4096, 4096, 8, seed=2)
+    got = _saxpy_dev(gb, A, B, gb.semiring("PLUS", "TIMES", "fp64"))
+    want = oracle.saxpy(4096, 4096, (A.p, A.i, A.x, 11), (B.p, B.i, B.x, 11),
+                        "PLUS", "TIMES", 11)
+    assert_roundoff(got, want, 4096, "er fp64")
+    assert_exact(got, want, "er fp64 (k-ordered accumulation)")
+
+
+SEMIRINGS = [
+    ("PLUS", "TIMES", "fp64", np.float64),
+    ("PLUS", "TIMES", "fp32", np.float32),
+    ("PLUS", "TIMES", "int64", np.int64),
+    ("PLUS", "TIMES", "int32", np.int32),
+    ("MIN", "PLUS", "fp32", np.float32),
+    ("MIN", "PLUS", "fp64", np.float64),
+    ("MIN", "PLUS", "int32", np.int32),
+    ("MAX", "PLUS", "fp32", np.float32),
+    ("PLUS", "PAIR", "int64", np.int64),
+    ("ANY", "SECONDI", "int64", np.int64),
+    ("ANY", "FIRSTJ", "int64", np.int64),
+    ("ANY", "SECONDJ", "int64", np.int64),
+    ("MIN", "SECONDI", "int64", np.int64),
+    ("MAX", "SECONDI", "int64", np.int64),
+    ("LOR", "LAND", "bool", np.bool_),
+    ("PLUS", "SECOND", "fp64", np.float64),
+    ("ANY", "TIMES", "fp64", np.float64),
+]
+
+
+@pytest.mark.parametrize("add,mult,tname,np_t", SEMIRINGS)
+@pytest.mark.parametrize("density", [0.01, 0.05, 0.3])
+def test_saxpy_semirings_nomask(gpu, oracle, add, mult, tname, np_t, density):
+    gb = gpu
+    tc = gb.TYPES[tname]
+    m, k, n = 150, 180, 160
+    A = random_csr(m, k, density, 21, np_t, empty_rows=0.1)
+    B = random_csr(k, n, density, 22, np_t, empty_rows=0.1)
+    got = _saxpy_dev(gb, A, B, gb.semiring(add, mult, tname))
+    want = oracle.saxpy(m, n, (A.p, A.i, A.x, tc), (B.p, B.i, B.x, tc), add, mult, tc)
+    assert_exact(got, want, "%s_%s_%s" % (add, mult, tname))
+
+
+@pytest.mark.parametrize("add,mult,tname,np_t", SEMIRINGS[:10])
+@pytest.mark.parametrize("comp", [False, True])
+def test_saxpy_masked(gpu, oracle, add, mult, tname, np_t, comp):
+    gb = gpu
+    tc = gb.TYPES[tname]
+    m, k, n = 130, 140, 150
+    A = random_csr(m, k, 0.08, 31, np_t)
+    B = random_csr(k, n, 0.08, 32, np_t)
+    M = random_csr(m, n, 0.15, 33, np.bool_)
+    M.x = None
+    got = _saxpy_dev(gb, A, B, gb.semiring(add, mult, tname), M=M, mask_comp=comp)
+    want = oracle.saxpy(m, n, (A.p, A.i, A.x, tc), (B.p, B.i, B.x, tc), add, mult,
+                        tc, M=(M.p, M.i, None, 1), mask_comp=comp)
+    assert_exact(got, want, "masked comp=%s" % comp)
+
+
+def test_saxpy_valued_mask(gpu, oracle):
+    gb = gpu
+    A = random_csr(80, 90, 0.1, 41)
+    B = random_csr(90, 70, 0.1, 42)
+    M = random_csr(80, 70, 0.3, 43)
+    M.x = (np.arange(M.nnz) % 2).astype(np.float64)
+    got = _saxpy_dev(gb, A, B, gb.semiring("PLUS", "TIMES", "fp64"), M=M,
+                     mask_struct=False)
+    want = oracle.saxpy(80, 70, (A.p, A.i, A.x, 11), (B.p, B.i, B.x, 11), "PLUS",
+                        "TIMES", 11, M=(M.p, M.i, M.x, 11), mask_struct=False)
+    assert_exact(got, want, "valued mask")
+
+
+@pytest.mark.parametrize("add,mult,tname", [("PLUS", "PAIR", "int64"),
+                                            ("PLUS", "TIMES", "fp64"),
+                                            ("MIN", "PLUS", "fp32")])
+def test_saxpy_rmat_square_heavy_rows(gpu, oracle, add, mult, tname):
+    """R-MAT A*A: hub rows exceed every shared-memory bin (dense accumulator),
+    both the atomic (order-free) and the sequential-k (floating PLUS) kinds."""
+    gb = gpu
+    S = W.rmat(11, 16, seed=3)
+    rng = np.random.default_rng(1)
+    np_t = {"int64": np.int64, "fp64": np.float64, "fp32": np.float32}[tname]
+    tc = gb.TYPES[tname]
+    x = (0.1 + 9.9 * rng.random(S.nnz)).astype(np_t)
+    A = W.Csr(S.nrows, S.ncols, S.p, S.i, x)
+    got = _saxpy_dev(gb, A, A, gb.semiring(add, mult, tname))
+    want = oracle.saxpy(S.nrows, S.ncols, (A.p, A.i, A.x, tc), (A.p, A.i, A.x, tc),
+                        add, mult, tc)
+    assert_exact(got, want, "rmat A*A %s_%s" % (add, mult))
+
+
+def test_vxm_bfs_step_complemented(gpu, oracle):
+    """One BFS push step: q<!p> = q any_secondi S on R-MAT (a single heavy row)."""
+    gb = gpu
+    S = W.rmat(12, 16, seed=9)
+    n = S.nrows
+    rng = np.random.default_rng(2)
+    front = np.sort(rng.choice(n, 300, replace=False)).astype(np.int64)
+    visited = np.sort(np.unique(np.concatenate([front, rng.choice(n, 900, replace=False)])))
+    q = W.Csr(1, n, np.array([0, len(front)], np.int64), front, front.copy())
+    p = W.Csr(1, n, np.array([0, len(visited)], np.int64), visited.astype(np.int64))
+    Sx = W.Csr(n, n, S.p, S.i)
+    got = _saxpy_dev(gb, q, Sx, gb.semiring("ANY", "SECONDI", "int64"), M=p,
+                     mask_comp=True, type_name="int64")
+    want = oracle.saxpy(1, n, (q.p, q.i, q.x, 8), (S.p, S.i, None, 1), "ANY",
+                        "SECONDI", 8, M=(p.p, p.i, None, 1), mask_comp=True)
+    assert_exact(got, want, "bfs step")
+
+
+def test_saxpy_edge_cases(gpu, oracle):
+    gb = gpu
+    sr = gb.semiring("PLUS", "TIMES", "fp64")
+    # A with no entries
+    A0 = W.Csr(20, 30, np.zeros(21, np.int64), np.zeros(0, np.int64), np.zeros(0))
+    B = random_csr(30, 25, 0.3, 1)
+    got = _saxpy_dev(gb, A0, B, sr)
+    assert got[0][-1] == 0 and len(got[0]) == 21
+    # B with empty rows hit by A (zero-flop rows)
+    A = random_csr(20, 30, 0.3, 2)
+    B0 = W.Csr(30, 25, np.zeros(31, np.int64), np.zeros(0, np.int64), np.zeros(0))
+    got = _saxpy_dev(gb, A, B0, sr)
+    assert got[0][-1] == 0
+    # a mask with no entries: nothing allowed
+    M0 = W.Csr(20, 25, np.zeros(21, np.int64), np.zeros(0, np.int64))
+    got = _saxpy_dev(gb, A, B, sr, M=M0)
+    assert got[0][-1] == 0
+    # its complement allows everything
+    got = _saxpy_dev(gb, A, B, sr, M=M0, mask_comp=True)
+    want = oracle.saxpy(20, 25, (A.p, A.i, A.x, 11), (B.p, B.i, B.x, 11), "PLUS",
+                        "TIMES", 11)
+    assert_exact(got, want, "complement of empty mask")
