@@ -379,6 +379,88 @@ int grb_b200_dreduce(void *out, grb_b200_dmatrix D, int monoid_opcode)
     return reduce_scalar(out, D->A, monoid_opcode, g.s);
 }
 
+int grb_b200_dmatrix_empty(grb_b200_dmatrix *D, int64_t nrows, int64_t ncols,
+                           int type)
+{
+    if (!D) return NULL_POINTER;
+    int info = init_device();
+    if (info != SUCCESS) return info;
+    if (type_size(type) == 0) return INVALID_VALUE;
+    if (nrows >= INT32_MAX || ncols >= INT32_MAX) return NO_VALUE;
+    StreamGuard g;
+    grb_b200_dmatrix h = new grb_b200_dmatrix_s();
+    h->A.nrows = nrows; h->A.ncols = ncols; h->A.nnz = 0; h->A.type = type;
+    h->A.p = (int32_t *)dalloc((size_t)(nrows + 1) * 4, g.s);
+    h->A.j = (int32_t *)dalloc(4, g.s);
+    h->A.x = dalloc(type_size(type), g.s);
+    if (!h->A.p || !h->A.j || !h->A.x) { dev_free(h->A, g.s); delete h; return OUT_OF_MEMORY; }
+    cudaMemsetAsync(h->A.p, 0, (size_t)(nrows + 1) * 4, g.s);
+    cudaError_t e = cudaStreamSynchronize(g.s);
+    if (e != cudaSuccess) { dev_free(h->A, g.s); delete h; return cuda_to_info(e); }
+    *D = h;
+    return SUCCESS;
+}
+
+int grb_b200_dmatrix_dup(grb_b200_dmatrix *D, grb_b200_dmatrix A)
+{
+    if (!D || !A) return NULL_POINTER;
+    StreamGuard g;
+    cudaStream_t s = g.s;
+    const DevCSR &X = A->A;
+    grb_b200_dmatrix h = new grb_b200_dmatrix_s();
+    h->A = X;
+    size_t ts = type_size(X.type);
+    h->A.p = (int32_t *)dalloc((size_t)(X.nrows + 1) * 4, s);
+    h->A.j = (int32_t *)dalloc((size_t)(X.nnz ? X.nnz : 1) * 4, s);
+    h->A.x = X.x ? dalloc(X.iso ? ts : (size_t)(X.nnz ? X.nnz : 1) * ts, s) : nullptr;
+    if (!h->A.p || !h->A.j || (X.x && !h->A.x)) { dev_free(h->A, s); delete h; return OUT_OF_MEMORY; }
+    cudaMemcpyAsync(h->A.p, X.p, (size_t)(X.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(h->A.j, X.j, (size_t)X.nnz * 4, cudaMemcpyDeviceToDevice, s);
+    if (X.x) cudaMemcpyAsync(h->A.x, X.x, X.iso ? ts : (size_t)X.nnz * ts, cudaMemcpyDeviceToDevice, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { dev_free(h->A, s); delete h; return cuda_to_info(e); }
+    *D = h;
+    return SUCCESS;
+}
+
+int grb_b200_daccum_mask(grb_b200_dmatrix C, grb_b200_dmatrix T, grb_b200_dmatrix M,
+                         bool mask_comp, bool mask_struct, bool replace,
+                         int accum_opcode)
+{
+    if (!C || !T) return NULL_POINTER;
+    StreamGuard g;
+    int info = accum_mask(C->A, T->A, M ? &M->A : nullptr, mask_comp, mask_struct,
+                          replace, accum_opcode, g.s);
+    cudaError_t e = cudaStreamSynchronize(g.s);
+    return info != SUCCESS ? info : cuda_to_info(e);
+}
+
+int grb_b200_dtranspose(grb_b200_dmatrix *B, grb_b200_dmatrix A)
+{
+    if (!B || !A) return NULL_POINTER;
+    StreamGuard g;
+    grb_b200_dmatrix h = new grb_b200_dmatrix_s();
+    int info = transpose(h->A, A->A, g.s);
+    if (info != SUCCESS) { delete h; return info; }
+    *B = h;
+    return SUCCESS;
+}
+
+int grb_b200_dmxv(grb_b200_dmatrix *w, grb_b200_dmatrix mask, bool mask_comp,
+                  bool mask_struct, grb_b200_dmatrix A, grb_b200_dmatrix u,
+                  const grb_b200_semiring *sr)
+{
+    if (!w || !A || !u || !sr) return NULL_POINTER;
+    StreamGuard g;
+    grb_b200_dmatrix h = new grb_b200_dmatrix_s();
+    SemiringCode sc{sr->add_opcode, sr->mult_opcode, sr->type};
+    int info = mxv(h->A, mask ? &mask->A : nullptr, mask_comp, mask_struct, A->A,
+                   u->A, sc, g.s);
+    if (info != SUCCESS) { delete h; return info; }
+    *w = h;
+    return SUCCESS;
+}
+
 int grb_b200_dwait(grb_b200_dmatrix D)
 {
     if (!D) return NULL_POINTER;

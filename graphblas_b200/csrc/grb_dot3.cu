@@ -3,30 +3,33 @@
 // reference's GB_AxB_dot3 (Source/mxm/GB_AxB_dot3.c:37) and of its draft GPU
 // kernels (CUDA/template/GB_cuda_jit_AxB_dot3_phase{1,2,3_vsvs,3_mp}.cuh).
 //
-// Design (one launch, no host round trip):
-//   * A warp owns one mask row i at a time, taken from a global work counter
-//     (rows are uneven: R-MAT degrees span 1..65k).  A(i,:) is staged once in
-//     the warp's shared-memory slice and reused by every entry of M(i,:).
-//   * Each lane takes one entry (i,j) of the row and trims both lists to their
-//     overlap [max(first), min(last)] with binary searches (the reference's
-//     dot3 trims when one list is much longer, GB_AxB_dot_cij.c:538-617).
-//     Empty overlaps become zombies at once; short overlaps are merged by the
-//     lane itself (the reference's VSVS bucket, phase3_vsvs.cuh:133).
-//   * Long overlaps are queued and taken by the whole warp, one at a time:
-//     lanes walk 32 consecutive elements of one list (coalesced) and locate
-//     each in the other list by binary search, advancing the search window
-//     chunk by chunk (a merge-path partition of the two lists).  The list that
-//     is scanned is the shorter one in cost: B when it is at most 8x longer
-//     than A (A is in shared memory), otherwise A, searched in global B.
-//   * Matches come out of __ballot_sync in ascending k, so order-dependent
-//     monoids (floating PLUS/TIMES, ANY) fold them in exactly the reference's
-//     sequential order, first match assigned and later ones added
-//     (GB_AxB_dot_cij.c:516-652); order-free monoids keep per-lane partials
-//     and finish with a warp reduction.
-//   * ANY is terminal: the first match ends the dot product.
-//   * Empty results are zombies, Cj[p] = flip(j) (GB_zombie.h:37), counted in
-//     C.nzombies; C keeps M's row pointers, as the reference's dot3 does
-//     (GB_AxB_dot3.c:172-197).
+// Two launches, no host round trip between them:
+//
+//  1. classify (one warp per 32 consecutive mask entries, flat over M): each
+//     lane takes one entry (i,j), trims A(i,:) and B(j,:) to their overlap
+//     [max(first), min(last)] with binary searches (the reference trims when
+//     one list is much longer, GB_AxB_dot_cij.c:538-617), turns an empty
+//     overlap into a zombie at once and merges a short overlap itself (the
+//     reference's VSVS bucket, phase3_vsvs.cuh:133).  Long overlaps go to a
+//     global work queue (warp-aggregated append).
+//  2. intersect (persistent warps pull queue entries in batches): one warp
+//     per entry.  Balanced lists are merged with a register merge-path: each
+//     step loads 32 elements of each list (coalesced), every lane locates its
+//     B element in the A window by a 5-step shuffle binary search, and the
+//     window that ends first advances.  Lopsided lists (the long one about
+//     log2(n) times longer or more) are intersected by taking 32 elements of
+//     the short list at a time and binary-searching each in the long one, the
+//     search window advancing chunk by chunk.  The queue spreads R-MAT's
+//     heavy entries over every warp of the GPU.
+//
+// Matches come out of __ballot_sync in ascending k, so order-dependent
+// monoids (floating PLUS/TIMES, ANY) fold them in exactly the reference's
+// sequential order, first match assigned and later ones added
+// (GB_AxB_dot_cij.c:516-652); order-free monoids keep per-lane partials and
+// finish with a warp reduction.  ANY is terminal: the first match ends the
+// dot product.  Empty results are zombies, Cj[p] = flip(j) (GB_zombie.h:37),
+// counted in C.nzombies; C keeps M's row pointers, as the reference's dot3
+// does (GB_AxB_dot3.c:172-197).
 
 #include <cstdio>
 #include <cstring>
@@ -35,9 +38,8 @@
 
 namespace grb {
 
-static constexpr int D3_WARPS = 8;        // warps per block
-static constexpr int D3_CAP = 1024;       // A(i,:) entries staged per warp
-static constexpr int D3_SMALL = 48;       // per-lane merge threshold (nA+nB)
+static constexpr int D3_SMALL = 32;        // per-lane merge threshold (nA+nB)
+static constexpr int D3_BATCH = 8;         // queue entries taken per grab
 
 __device__ __forceinline__ bool mask_value_true(const void *Mx, int mtype,
                                                 int64_t p)
@@ -63,176 +65,248 @@ combine(Part<typename SR::z_t> a, Part<typename SR::z_t> b)
     return {SR::M::add(a.v, b.v), true};
 }
 
-template <class SR, int WARPS, int CAP>
-__global__ void __launch_bounds__(WARPS * 32)
-k_dot3(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
-       const void *__restrict__ Mx, int mtype, bool mask_struct,
-       const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
-       const void *__restrict__ Ax, bool a_iso,
-       const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
-       const void *__restrict__ Bx, bool b_iso,
-       int32_t *__restrict__ Cj, typename SR::z_t *__restrict__ Cx,
-       int64_t nrows, int *__restrict__ row_counter,
-       unsigned long long *__restrict__ nzombies)
+// queued entry: mask position, row, column, trimmed ranges (absolute)
+struct __align__(32) D3Work { int32_t pm, i, j, a0, a1, b0, b1, pad; };
+
+// ---------------------------------------------------------------------------
+// launch 1: classify
+// ---------------------------------------------------------------------------
+
+template <class SR>
+__global__ void __launch_bounds__(256)
+k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
+                const void *__restrict__ Mx, int mtype, bool mask_struct,
+                int64_t mnz, int64_t nrows,
+                const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+                const void *__restrict__ Ax, bool a_iso,
+                const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
+                const void *__restrict__ Bx, bool b_iso,
+                int32_t *__restrict__ Cj, typename SR::z_t *__restrict__ Cx,
+                D3Work *__restrict__ queue, int *__restrict__ qlen,
+                unsigned long long *__restrict__ nzombies)
 {
     using Z = typename SR::z_t;
-    __shared__ int32_t sA_all[WARPS][CAP];
     const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    int32_t *sA = sA_all[warp];
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long zcount = 0;
-
-    while (true) {
-        int r = 0;
-        if (lane == 0) r = atomicAdd(row_counter, 1);
-        r = __shfl_sync(0xffffffffu, r, 0);
-        if (r >= nrows) break;
-        const int64_t i = r;
-        const int32_t mp0 = Mp[i], mp1 = Mp[i + 1];
-        if (mp0 == mp1) continue;
-        const int32_t pa0 = Ap[i];
-        const int32_t na = Ap[i + 1] - pa0;
-        const int32_t *a_idx;
-        if (na <= CAP) {
-            for (int32_t t = lane; t < na; t += 32) sA[t] = Aj[pa0 + t];
-            __syncwarp();
-            a_idx = sA;
-        } else {
-            a_idx = Aj + pa0;
-        }
-
-        for (int32_t cb = mp0; cb < mp1; cb += 32) {
-            const int32_t pm = cb + lane;
-            const bool valid = pm < mp1;
-            int32_t j = 0, ia0 = 0, ia1 = 0, ib0 = 0, ib1 = 0;
-            bool coop = false, exists = false;
-            Z cij = Z();
-            if (valid) {
-                j = Mj[pm];
-                bool mval = mask_struct || Mx == nullptr || mask_value_true(Mx, mtype, pm);
-                if (mval && na > 0) {
-                    const int32_t pb0 = Bp[j], pb1 = Bp[j + 1];
-                    if (pb1 > pb0) {
-                        const int32_t blo = Bj[pb0], bhi = Bj[pb1 - 1];
-                        ia0 = lower_bound(a_idx, 0, na, blo);
-                        ia1 = upper_bound(a_idx, ia0, na, bhi);
-                        if (ia1 > ia0) {
-                            const int32_t alo = a_idx[ia0], ahi = a_idx[ia1 - 1];
-                            ib0 = lower_bound(Bj, pb0, pb1, alo);
-                            ib1 = upper_bound(Bj, ib0, pb1, ahi);
-                            if (ib1 > ib0) {
-                                if ((ia1 - ia0) + (ib1 - ib0) <= D3_SMALL) {
-                                    // per-lane two-pointer merge
-                                    int32_t a = ia0, b = ib0;
-                                    while (a < ia1 && b < ib1) {
-                                        const int32_t ka = a_idx[a], kb = Bj[b];
-                                        if (ka < kb) a++;
-                                        else if (kb < ka) b++;
-                                        else {
-                                            Z av = Z(), bv = Z();
-                                            if (SR::needs_a) av = ld_val<Z>(Ax, pa0 + a, a_iso);
-                                            if (SR::needs_b) bv = ld_val<Z>(Bx, b, b_iso);
-                                            Z t = SR::F::f(av, bv, i, ka, j);
-                                            if (!exists) { cij = t; exists = true; }
-                                            else cij = SR::M::add(cij, t);
-                                            if (SR::M::any) break;
-                                            a++; b++;
-                                        }
-                                    }
-                                } else {
-                                    coop = true;
+    for (int64_t base = warp * 32; base < mnz; base += nwarps * 32) {
+        const int64_t pm = base + lane;
+        const bool valid = pm < mnz;
+        // row of the chunk's first entry, then each lane walks forward
+        int32_t r0 = 0;
+        if (lane == 0) r0 = upper_bound(Mp, 0, (int32_t)nrows + 1, (int32_t)base) - 1;
+        r0 = __shfl_sync(0xffffffffu, r0, 0);
+        int32_t i = r0;
+        if (valid) while (Mp[i + 1] <= pm) i++;
+        int32_t j = 0, a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+        bool coop = false, exists = false;
+        Z cij = Z();
+        if (valid) {
+            j = Mj[pm];
+            const bool mval = mask_struct || Mx == nullptr || mask_value_true(Mx, mtype, pm);
+            const int32_t pa0 = Ap[i], pa1 = Ap[i + 1];
+            const int32_t pb0 = Bp[j], pb1 = Bp[j + 1];
+            if (mval && pa1 > pa0 && pb1 > pb0) {
+                const int32_t blo = Bj[pb0], bhi = Bj[pb1 - 1];
+                a0 = lower_bound(Aj, pa0, pa1, blo);
+                a1 = upper_bound(Aj, a0, pa1, bhi);
+                if (a1 > a0) {
+                    const int32_t alo = Aj[a0], ahi = Aj[a1 - 1];
+                    b0 = lower_bound(Bj, pb0, pb1, alo);
+                    b1 = upper_bound(Bj, b0, pb1, ahi);
+                    if (b1 > b0) {
+                        if ((a1 - a0) + (b1 - b0) <= D3_SMALL) {
+                            int32_t a = a0, b = b0;
+                            while (a < a1 && b < b1) {
+                                const int32_t ka = Aj[a], kb = Bj[b];
+                                if (ka < kb) a++;
+                                else if (kb < ka) b++;
+                                else {
+                                    Z av = Z(), bv = Z();
+                                    if (SR::needs_a) av = ld_val<Z>(Ax, a, a_iso);
+                                    if (SR::needs_b) bv = ld_val<Z>(Bx, b, b_iso);
+                                    const Z t = SR::F::f(av, bv, i, ka, j);
+                                    if (!exists) { cij = t; exists = true; }
+                                    else cij = SR::M::add(cij, t);
+                                    if (SR::M::any) break;
+                                    a++; b++;
                                 }
                             }
+                        } else {
+                            coop = true;
                         }
                     }
                 }
             }
-            if (valid && !coop) {
+            if (!coop) {
                 if (exists) { Cj[pm] = j; Cx[pm] = cij; }
                 else { Cj[pm] = flip(j); zcount++; }
             }
+        }
+        // warp-aggregated append of the long entries
+        const unsigned q = __ballot_sync(0xffffffffu, coop);
+        if (q) {
+            int qbase = 0;
+            if (lane == 0) qbase = atomicAdd(qlen, __popc(q));
+            qbase = __shfl_sync(0xffffffffu, qbase, 0);
+            if (coop) {
+                const int slot = qbase + __popc(q & ((1u << lane) - 1));
+                queue[slot] = D3Work{(int32_t)pm, i, j, a0, a1, b0, b1, 0};
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) zcount += __shfl_down_sync(0xffffffffu, zcount, o);
+    if (lane == 0 && zcount) atomicAdd(nzombies, zcount);
+}
 
-            // warp-cooperative intersections, one queued entry at a time
-            unsigned q = __ballot_sync(0xffffffffu, coop);
-            while (q) {
-                const int src = __ffs(q) - 1;
-                q &= q - 1;
-                const int32_t qpm = __shfl_sync(0xffffffffu, pm, src);
-                const int32_t qj = __shfl_sync(0xffffffffu, j, src);
-                const int32_t qa0 = __shfl_sync(0xffffffffu, ia0, src);
-                const int32_t qa1 = __shfl_sync(0xffffffffu, ia1, src);
-                const int32_t qb0 = __shfl_sync(0xffffffffu, ib0, src);
-                const int32_t qb1 = __shfl_sync(0xffffffffu, ib1, src);
-                const int32_t nA = qa1 - qa0, nB = qb1 - qb0;
-                Part<Z> part{Z(), false};      // order-free partial (per lane)
-                Z acc = Z();                   // in-order fold (uniform)
-                bool acc_has = false;
-                const bool scanB = (nB <= 8 * nA);
-                const int32_t s0 = scanB ? qb0 : qa0;     // scanned list range
-                const int32_t s1 = scanB ? qb1 : qa1;
-                int32_t lo = scanB ? qa0 : qb0;           // searched list window
-                const int32_t hi = scanB ? qa1 : qb1;
+// ---------------------------------------------------------------------------
+// launch 2: warp-cooperative intersections of the queued entries
+// ---------------------------------------------------------------------------
+
+// fold the matches flagged in `mm` (lane order = ascending k) into the result
+template <class SR>
+__device__ __forceinline__ void fold_matches(unsigned mm, bool match,
+                                             typename SR::z_t t,
+                                             Part<typename SR::z_t> &part,
+                                             typename SR::z_t &acc, bool &acc_has)
+{
+    using Z = typename SR::z_t;
+    if (SR::order_free && !SR::M::any) {
+        if (match) part = combine<SR>(part, Part<Z>{t, true});
+    } else {
+        while (mm) {
+            const int b = __ffs(mm) - 1;
+            mm &= mm - 1;
+            const Z tv = shfl<Z>(t, b);
+            if (!acc_has) { acc = tv; acc_has = true; }
+            else acc = SR::M::add(acc, tv);
+            if (SR::M::any) break;
+        }
+    }
+}
+
+template <class SR>
+__global__ void __launch_bounds__(256)
+k_dot3_intersect(const D3Work *__restrict__ queue, const int *__restrict__ qlen_p,
+                 int *__restrict__ qnext,
+                 const int32_t *__restrict__ Aj, const void *__restrict__ Ax, bool a_iso,
+                 const int32_t *__restrict__ Bj, const void *__restrict__ Bx, bool b_iso,
+                 int32_t *__restrict__ Cj, typename SR::z_t *__restrict__ Cx,
+                 unsigned long long *__restrict__ nzombies)
+{
+    using Z = typename SR::z_t;
+    const int lane = threadIdx.x & 31;
+    const int qlen = *qlen_p;
+    unsigned long long zcount = 0;
+    while (true) {
+        int w0 = 0;
+        if (lane == 0) w0 = atomicAdd(qnext, D3_BATCH);
+        w0 = __shfl_sync(0xffffffffu, w0, 0);
+        if (w0 >= qlen) break;
+        const int w1 = min(w0 + D3_BATCH, qlen);
+        for (int w = w0; w < w1; w++) {
+            const D3Work e = queue[w];
+            const int32_t nA = e.a1 - e.a0, nB = e.b1 - e.b0;
+            const int32_t nS = nA < nB ? nA : nB, nL = nA < nB ? nB : nA;
+            Part<Z> part{Z(), false};
+            Z acc = Z();
+            bool acc_has = false;
+            // lopsided: search the short list's elements in the long list
+            const int lg = 32 - __clz(nL);
+            const bool probe = (int64_t)nS * (lg + 2) < (int64_t)(nA + nB);
+            if (probe) {
+                const bool shortA = nA <= nB;
+                const int32_t *S = shortA ? Aj : Bj;
+                const int32_t *Lg = shortA ? Bj : Aj;
+                const int32_t s0 = shortA ? e.a0 : e.b0, s1 = shortA ? e.a1 : e.b1;
+                int32_t lo = shortA ? e.b0 : e.a0;
+                const int32_t hi = shortA ? e.b1 : e.a1;
                 for (int32_t c0 = s0; c0 < s1; c0 += 32) {
                     const int32_t sp = c0 + lane;
                     const bool has = sp < s1;
-                    int32_t key = INT32_MAX, pos;
-                    if (scanB) {
-                        if (has) key = Bj[sp];
-                        pos = lower_bound(a_idx, lo, hi, key);
-                    } else {
-                        if (has) key = a_idx[sp];
-                        pos = lower_bound(Bj, lo, hi, key);
-                    }
-                    bool match = false;
-                    if (has && pos < hi)
-                        match = scanB ? (a_idx[pos] == key) : (Bj[pos] == key);
+                    const int32_t key = has ? S[sp] : INT32_MAX;
+                    const int32_t pos = lower_bound(Lg, lo, hi, key);
+                    const bool match = has && pos < hi && Lg[pos] == key;
                     Z t = Z();
                     if (match) {
-                        const int32_t apos = scanB ? pos : sp;
-                        const int32_t bpos = scanB ? sp : pos;
+                        const int32_t apos = shortA ? sp : pos;
+                        const int32_t bpos = shortA ? pos : sp;
                         Z av = Z(), bv = Z();
-                        if (SR::needs_a) av = ld_val<Z>(Ax, pa0 + apos, a_iso);
+                        if (SR::needs_a) av = ld_val<Z>(Ax, apos, a_iso);
                         if (SR::needs_b) bv = ld_val<Z>(Bx, bpos, b_iso);
-                        t = SR::F::f(av, bv, i, key, qj);
+                        t = SR::F::f(av, bv, e.i, key, e.j);
                     }
-                    const unsigned mm = __ballot_sync(0xffffffffu, match);
-                    if (SR::order_free && !SR::M::any) {
-                        if (match) part = combine<SR>(part, Part<Z>{t, true});
-                    } else {
-                        // fold in ascending k, exactly as the sequential merge
-                        unsigned m2 = mm;
-                        while (m2) {
-                            const int b = __ffs(m2) - 1;
-                            m2 &= m2 - 1;
-                            const Z tv = shfl<Z>(t, b);
-                            if (!acc_has) { acc = tv; acc_has = true; }
-                            else acc = SR::M::add(acc, tv);
-                            if (SR::M::any) break;
-                        }
-                        if (SR::M::any && acc_has) break;
-                    }
+                    fold_matches<SR>(__ballot_sync(0xffffffffu, match), match, t,
+                                     part, acc, acc_has);
+                    if (SR::M::any && acc_has) break;
                     lo = __shfl_sync(0xffffffffu, pos, 31);
                     if (lo >= hi) break;
                 }
-                if (SR::order_free && !SR::M::any) {
-                    // warp reduction of the per-lane partials
-                    for (int o = 16; o > 0; o >>= 1) {
-                        Part<Z> other;
-                        other.v = shfl_down<Z>(part.v, o);
-                        other.has = shfl_down<bool>(part.has, o);
-                        part = combine<SR>(part, other);
+            } else {
+                // register merge-path over 32-element windows of both lists
+                int32_t a = e.a0, b = e.b0;
+                while (a < e.a1 && b < e.b1) {
+                    const int32_t ka = (a + lane < e.a1) ? Aj[a + lane] : INT32_MAX;
+                    const int32_t kb = (b + lane < e.b1) ? Bj[b + lane] : INT32_MAX;
+                    const int32_t alast = min(e.a1 - a, 32) - 1;
+                    const int32_t blast = min(e.b1 - b, 32) - 1;
+                    const int32_t amx = __shfl_sync(0xffffffffu, ka, alast);
+                    const int32_t bmx = __shfl_sync(0xffffffffu, kb, blast);
+                    // locate kb in the A window (5-step shuffle binary search:
+                    // lo ends at the first lane whose ka >= kb, or 31)
+                    int lo = 0;
+                    #pragma unroll
+                    for (int step = 16; step > 0; step >>= 1) {
+                        const int32_t v = __shfl_sync(0xffffffffu, ka, lo + step - 1);
+                        if (v < kb) lo += step;
                     }
-                    acc = part.v; acc_has = part.has;
-                }
-                if (lane == 0) {
-                    if (acc_has) { Cj[qpm] = qj; Cx[qpm] = acc; }
-                    else { Cj[qpm] = flip(qj); zcount++; }
+                    const int32_t vlo = __shfl_sync(0xffffffffu, ka, lo);
+                    // this window decides every B element up to its last A element
+                    const bool match = (lane <= blast) && kb <= amx && vlo == kb;
+                    Z t = Z();
+                    if (match) {
+                        Z av = Z(), bv = Z();
+                        if (SR::needs_a) av = ld_val<Z>(Ax, a + lo, a_iso);
+                        if (SR::needs_b) bv = ld_val<Z>(Bx, b + lane, b_iso);
+                        t = SR::F::f(av, bv, e.i, kb, e.j);
+                    }
+                    fold_matches<SR>(__ballot_sync(0xffffffffu, match), match, t,
+                                     part, acc, acc_has);
+                    if (SR::M::any && acc_has) break;
+                    if (amx < bmx) {
+                        // the A window is used up; B elements <= amx are decided
+                        const unsigned done = __ballot_sync(0xffffffffu, lane <= blast && kb <= amx);
+                        a += alast + 1;
+                        b += __popc(done);
+                    } else if (bmx < amx) {
+                        // every B element is decided; A elements <= bmx are spent
+                        const unsigned done = __ballot_sync(0xffffffffu, lane <= alast && ka <= bmx);
+                        b += blast + 1;
+                        a += __popc(done);
+                    } else {
+                        a += alast + 1;
+                        b += blast + 1;
+                    }
                 }
             }
+            if (SR::order_free && !SR::M::any) {
+                for (int o = 16; o > 0; o >>= 1) {
+                    Part<Z> other;
+                    other.v = shfl_down<Z>(part.v, o);
+                    other.has = shfl_down<bool>(part.has, o);
+                    part = combine<SR>(part, other);
+                }
+                acc = part.v;
+                acc_has = part.has;
+            }
+            if (lane == 0) {
+                if (acc_has) { Cj[e.pm] = e.j; Cx[e.pm] = acc; }
+                else { Cj[e.pm] = flip(e.j); zcount++; }
+            }
         }
-        __syncwarp();
     }
-    if (zcount) atomicAdd(nzombies, zcount);
+    if (lane == 0 && zcount) atomicAdd(nzombies, zcount);
 }
 
 template <class SR>
@@ -240,31 +314,39 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
                        const DevCSR &A, const DevCSR &B, cudaStream_t s)
 {
     using Z = typename SR::z_t;
-    int64_t mnz = M.nnz;
+    const int64_t mnz = M.nnz;
     C.nrows = M.nrows; C.ncols = M.ncols; C.nnz = mnz; C.type = 0; C.iso = false;
     C.p = (int32_t *)dalloc((size_t)(M.nrows + 1) * 4, s);
     C.j = (int32_t *)dalloc((size_t)(mnz ? mnz : 1) * 4, s);
     C.x = dalloc((size_t)(mnz ? mnz : 1) * sizeof(Z), s);
     int *counter = (int *)dalloc(64, s);
-    if (!C.p || !C.j || !C.x || !counter) {
-        dev_free(C, s); dfree(counter, s); return OUT_OF_MEMORY;
+    D3Work *queue = (D3Work *)dalloc((size_t)(mnz ? mnz : 1) * sizeof(D3Work), s);
+    if (!C.p || !C.j || !C.x || !counter || !queue) {
+        dev_free(C, s); dfree(counter, s); dfree(queue, s); return OUT_OF_MEMORY;
     }
     cudaMemcpyAsync(C.p, M.p, (size_t)(M.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
     cudaMemsetAsync(counter, 0, 64, s);
+    int *qlen = counter, *qnext = counter + 1;
     unsigned long long *zc = (unsigned long long *)((char *)counter + 32);
     if (mnz > 0 && M.nrows > 0) {
-        int blocks = runtime().num_sms * 6;
-        int ps = prof_begin("dot3", s);
-        k_dot3<SR, D3_WARPS, D3_CAP><<<blocks, D3_WARPS * 32, 0, s>>>(
-            M.p, M.j, mask_struct ? nullptr : M.x, M.type, mask_struct,
-            A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
-            C.j, (Z *)C.x, M.nrows, counter, zc);
+        const int nsm = runtime().num_sms;
+        int64_t warps_needed = (mnz + 31) / 32;
+        int64_t blocks = (warps_needed + 7) / 8;
+        if (blocks > (int64_t)nsm * 16) blocks = (int64_t)nsm * 16;
+        const int ps = prof_begin("dot3", s);
+        k_dot3_classify<SR><<<(unsigned)blocks, 256, 0, s>>>(
+            M.p, M.j, mask_struct ? nullptr : M.x, M.type, mask_struct, mnz, M.nrows,
+            A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso, C.j, (Z *)C.x,
+            queue, qlen, zc);
+        k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
+            queue, qlen, qnext, A.j, A.x, A.iso, B.j, B.x, B.iso, C.j, (Z *)C.x, zc);
         prof_end(ps, s);
     }
     unsigned long long hz = 0;
     cudaMemcpyAsync(&hz, zc, 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     dfree(counter, s);
+    dfree(queue, s);
     if (e != cudaSuccess) { dev_free(C, s); return cuda_to_info(e); }
     C.nzombies = (int64_t)hz;
     return SUCCESS;
@@ -300,6 +382,7 @@ int dot3(DevCSR &C, const DevCSR &M, bool mask_struct, const DevCSR &A,
 {
     if (A.ncols != B.ncols || M.nrows != A.nrows || M.ncols != B.nrows)
         return DIMENSION_MISMATCH;
+    if (M.nzombies > 0) return NO_VALUE;   // the mask must be free of zombies
     // an iso valued mask is all-true (structural) or all-false (every entry
     // of C is a zombie)
     bool all_false = false;

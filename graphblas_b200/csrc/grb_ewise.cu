@@ -1,0 +1,482 @@
+// grb_ewise.cu: the write-back and layout kernels around the multiply:
+//
+//   accum_mask   C<M,replace> = accum(C,T), the B200 replacement of
+//                GB_accum_mask (Source/mask/GB_accum_mask.c:126) for sparse
+//                C, T and M.  Flat over entries (no row is too long): every
+//                entry of T and of C decides, by binary searches in its row of
+//                C/T and M, whether it survives; two scans give each survivor
+//                its rank inside its row (the union of two sorted lists), and
+//                a scatter writes the sorted result.
+//   transpose    B = A' (Source/transpose/GB_transpose_cast.c:18): column
+//                counts, scan, atomic scatter, then each row of B is sorted
+//                by its (unique) indices with a bitonic network.
+//
+// Semantics (GraphBLAS C API, as the reference implements them):
+//   Z = accum(C,T) on the union of the patterns (or Z = T without accum);
+//   where the mask allows (i,j): C(i,j) = Z(i,j) if present, else deleted;
+//   elsewhere C(i,j) keeps its old value unless replace is set.  A valued
+//   mask is reduced to its true entries first; "no mask" allows everything,
+//   and its complement allows nothing.
+
+#include <cstring>
+#include <vector>
+#include "grb_runtime.h"
+
+namespace grb {
+
+template <typename Z>
+__device__ __forceinline__ Z apply_accum(int op, Z c, Z t)
+{
+    switch (op) {
+        case OP_PLUS: return rn_add<Z>(c, t);
+        case OP_TIMES: return rn_mul<Z>(c, t);
+        case OP_MIN: return op_min<Z>(c, t);
+        case OP_MAX: return op_max<Z>(c, t);
+        case OP_MINUS: return (Z)(c - t);
+        case OP_RMINUS: return (Z)(t - c);
+        case OP_FIRST: return c;
+        case OP_LOR: return (Z)((c != (Z)0) || (t != (Z)0));
+        case OP_LAND: return (Z)((c != (Z)0) && (t != (Z)0));
+        case OP_PAIR: return (Z)1;
+        default: return t;                // SECOND, ANY
+    }
+}
+template <> __device__ __forceinline__ bool apply_accum(int op, bool c, bool t)
+{
+    switch (op) {
+        case OP_PLUS: case OP_LOR: case OP_MAX: return c || t;
+        case OP_TIMES: case OP_LAND: case OP_MIN: return c && t;
+        case OP_MINUS: case OP_RMINUS: case OP_LXOR: return c != t;
+        case OP_FIRST: return c;
+        case OP_PAIR: return true;
+        default: return t;
+    }
+}
+
+__device__ __forceinline__ int32_t row_of(const int32_t *__restrict__ p,
+                                          int64_t nrows, int64_t e)
+{
+    return upper_bound(p, 0, (int32_t)nrows + 1, (int32_t)e) - 1;
+}
+
+__device__ __forceinline__ bool mask_allows(const int32_t *__restrict__ Mp,
+                                            const int32_t *__restrict__ Mj,
+                                            bool comp, int32_t i, int32_t j)
+{
+    if (Mp == nullptr) return !comp;
+    const int32_t lo = Mp[i], hi = Mp[i + 1];
+    const int32_t q = lower_bound(Mj, lo, hi, j);
+    const bool present = q < hi && Mj[q] == j;
+    return comp ? !present : present;
+}
+
+template <typename Z>
+__global__ void k_am_tside(int64_t m, const int32_t *__restrict__ Tp,
+                           const int32_t *__restrict__ Tj, const Z *__restrict__ Tx,
+                           bool t_iso, int64_t nT,
+                           const int32_t *__restrict__ Cp, const int32_t *__restrict__ Cj,
+                           const Z *__restrict__ Cx, bool c_iso,
+                           const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
+                           bool comp, int accum, int64_t *__restrict__ keepT,
+                           Z *__restrict__ valT)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nT;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t i = row_of(Tp, m, e), j = Tj[e];
+        const bool ok = mask_allows(Mp, Mj, comp, i, j);
+        Z t = Tx[t_iso ? 0 : e];
+        if (ok && accum) {
+            const int32_t q = lower_bound(Cj, Cp[i], Cp[i + 1], j);
+            if (q < Cp[i + 1] && Cj[q] == j) t = apply_accum<Z>(accum, Cx[c_iso ? 0 : q], t);
+        }
+        keepT[e] = ok ? 1 : 0;
+        valT[e] = t;
+    }
+}
+
+template <typename Z>
+__global__ void k_am_cside(int64_t m, const int32_t *__restrict__ Cp,
+                           const int32_t *__restrict__ Cj, int64_t nC,
+                           const int32_t *__restrict__ Tp, const int32_t *__restrict__ Tj,
+                           const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
+                           bool comp, bool replace, int accum,
+                           int64_t *__restrict__ keepC)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nC;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t i = row_of(Cp, m, e), j = Cj[e];
+        const bool ok = mask_allows(Mp, Mj, comp, i, j);
+        bool keep;
+        if (ok) {
+            const int32_t q = lower_bound(Tj, Tp[i], Tp[i + 1], j);
+            const bool in_t = q < Tp[i + 1] && Tj[q] == j;
+            keep = !in_t && accum != 0;       // Z(i,j) = C(i,j) when only C has it
+        } else {
+            keep = !replace;
+        }
+        keepC[e] = keep ? 1 : 0;
+    }
+}
+
+__global__ void k_am_rowptr(int64_t m, const int32_t *__restrict__ Cp,
+                            const int32_t *__restrict__ Tp,
+                            const int64_t *__restrict__ sC, const int64_t *__restrict__ sT,
+                            int32_t *__restrict__ Rp)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= m;
+         i += (int64_t)gridDim.x * blockDim.x)
+        Rp[i] = (int32_t)(sC[Cp[i]] + sT[Tp[i]]);
+}
+
+// scatter the survivors of one side; `other` is the opposite side's list
+template <typename Z>
+__global__ void k_am_write(int64_t m, const int32_t *__restrict__ Xp,
+                           const int32_t *__restrict__ Xj, const Z *__restrict__ Xv,
+                           bool x_iso, int64_t nX, const int64_t *__restrict__ sX,
+                           const int32_t *__restrict__ Yp, const int32_t *__restrict__ Yj,
+                           const int64_t *__restrict__ sY,
+                           const int32_t *__restrict__ Rp, int32_t *__restrict__ Rj,
+                           Z *__restrict__ Rx)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nX;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        if (sX[e + 1] == sX[e]) continue;           // not kept
+        const int32_t i = row_of(Xp, m, e), j = Xj[e];
+        const int32_t q = lower_bound(Yj, Yp[i], Yp[i + 1], j);
+        const int64_t rank = (sX[e] - sX[Xp[i]]) + (sY[q] - sY[Yp[i]]);
+        const int64_t pos = Rp[i] + rank;
+        Rj[pos] = j;
+        Rx[pos] = Xv[x_iso ? 0 : e];
+    }
+}
+
+static inline int grid_n(int64_t n, int threads = 256)
+{
+    int64_t b = (n + threads - 1) / threads;
+    int64_t cap = (int64_t)runtime().num_sms * 16;
+    if (b > cap) b = cap;
+    return b < 1 ? 1 : (int)b;
+}
+
+template <typename Z>
+static int accum_mask_t(DevCSR &C, const DevCSR &T, const DevCSR *M, bool comp,
+                        bool replace, int accum, cudaStream_t s)
+{
+    const int64_t m = T.nrows, nT = T.nnz, nC = C.nnz;
+    Scratch ws(s);
+    int64_t *keepT = ws.get<int64_t>(nT + 1);
+    int64_t *keepC = ws.get<int64_t>(nC + 1);
+    Z *valT = ws.get<Z>(nT + 1);
+    if (ws.failed) return OUT_OF_MEMORY;
+    const int32_t *Mp = M ? M->p : nullptr, *Mj = M ? M->j : nullptr;
+    if (nT > 0)
+        k_am_tside<Z><<<grid_n(nT), 256, 0, s>>>(m, T.p, T.j, (const Z *)T.x, T.iso, nT,
+            C.p, C.j, (const Z *)C.x, C.iso, Mp, Mj, comp, accum, keepT, valT);
+    if (nC > 0)
+        k_am_cside<Z><<<grid_n(nC), 256, 0, s>>>(m, C.p, C.j, nC, T.p, T.j, Mp, Mj,
+            comp, replace, accum, keepC);
+    cudaMemsetAsync(keepT + nT, 0, 8, s);
+    cudaMemsetAsync(keepC + nC, 0, 8, s);
+    int info = scan_exclusive_i64(keepT, keepT, nT + 1, s);
+    if (info == SUCCESS) info = scan_exclusive_i64(keepC, keepC, nC + 1, s);
+    if (info != SUCCESS) return info;
+    int64_t tot[2] = {0, 0};
+    cudaMemcpyAsync(&tot[0], keepT + nT, 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&tot[1], keepC + nC, 8, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_to_info(e);
+    const int64_t nR = tot[0] + tot[1];
+    if (nR >= INT32_MAX) return OUT_OF_MEMORY;
+    DevCSR R;
+    R.nrows = m; R.ncols = T.ncols; R.nnz = nR; R.type = T.type; R.iso = false;
+    R.p = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
+    R.j = (int32_t *)dalloc((size_t)(nR ? nR : 1) * 4, s);
+    R.x = dalloc((size_t)(nR ? nR : 1) * sizeof(Z), s);
+    if (!R.p || !R.j || !R.x) { dev_free(R, s); return OUT_OF_MEMORY; }
+    k_am_rowptr<<<grid_n(m + 1), 256, 0, s>>>(m, C.p, T.p, keepC, keepT, R.p);
+    if (nT > 0)
+        k_am_write<Z><<<grid_n(nT), 256, 0, s>>>(m, T.p, T.j, valT, false, nT, keepT,
+            C.p, C.j, keepC, R.p, R.j, (Z *)R.x);
+    if (nC > 0)
+        k_am_write<Z><<<grid_n(nC), 256, 0, s>>>(m, C.p, C.j, (const Z *)C.x, C.iso, nC,
+            keepC, T.p, T.j, keepT, R.p, R.j, (Z *)R.x);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { dev_free(R, s); return cuda_to_info(e); }
+    dev_free(C, s);
+    C = R;
+    return SUCCESS;
+}
+
+int accum_mask(DevCSR &C, const DevCSR &T0, const DevCSR *M0, bool mask_comp,
+               bool mask_struct, bool replace, int accum, cudaStream_t s)
+{
+    if (C.nrows != T0.nrows || C.ncols != T0.ncols) return DIMENSION_MISMATCH;
+    if (M0 && (M0->nrows != C.nrows || M0->ncols != C.ncols)) return DIMENSION_MISMATCH;
+    if (C.nnz > 0 && C.type != T0.type) return DOMAIN_MISMATCH;
+    // zombie-free operands with sorted rows
+    DevCSR T = T0, Ms;
+    bool ownT = false, ownM = false;
+    int info = SUCCESS;
+    if (T0.nzombies > 0) {
+        T = DevCSR();
+        T.nrows = T0.nrows; T.ncols = T0.ncols; T.nnz = T0.nnz; T.type = T0.type;
+        T.iso = T0.iso; T.nzombies = T0.nzombies;
+        size_t ts = type_size(T0.type);
+        T.p = (int32_t *)dalloc((size_t)(T0.nrows + 1) * 4, s);
+        T.j = (int32_t *)dalloc((size_t)(T0.nnz ? T0.nnz : 1) * 4, s);
+        T.x = dalloc(T0.iso ? ts : (size_t)(T0.nnz ? T0.nnz : 1) * ts, s);
+        if (!T.p || !T.j || !T.x) { dev_free(T, s); return OUT_OF_MEMORY; }
+        cudaMemcpyAsync(T.p, T0.p, (size_t)(T0.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(T.j, T0.j, (size_t)T0.nnz * 4, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(T.x, T0.x, T0.iso ? ts : (size_t)T0.nnz * ts, cudaMemcpyDeviceToDevice, s);
+        info = dev_prune_zombies(T, s);
+        ownT = true;
+    }
+    if (info == SUCCESS && C.nzombies > 0) info = dev_prune_zombies(C, s);
+    const DevCSR *M = M0;
+    if (info == SUCCESS && M0 && (!mask_struct && M0->x)) {
+        info = dev_mask_to_struct(Ms, *M0, s);
+        M = &Ms; ownM = true;
+    } else if (info == SUCCESS && M0 && M0->nzombies > 0) {
+        info = NO_VALUE;
+    }
+    if (info == SUCCESS) {
+        if (C.nnz == 0 && C.type != T.type) C.type = T.type;
+        switch (T.type) {
+            case T_BOOL:   info = accum_mask_t<bool>(C, T, M, mask_comp, replace, accum, s); break;
+            case T_INT32:  info = accum_mask_t<int32_t>(C, T, M, mask_comp, replace, accum, s); break;
+            case T_UINT32: info = accum_mask_t<uint32_t>(C, T, M, mask_comp, replace, accum, s); break;
+            case T_INT64:  info = accum_mask_t<int64_t>(C, T, M, mask_comp, replace, accum, s); break;
+            case T_UINT64: info = accum_mask_t<uint64_t>(C, T, M, mask_comp, replace, accum, s); break;
+            case T_FP32:   info = accum_mask_t<float>(C, T, M, mask_comp, replace, accum, s); break;
+            case T_FP64:   info = accum_mask_t<double>(C, T, M, mask_comp, replace, accum, s); break;
+            default: info = NO_VALUE;
+        }
+    }
+    if (ownT) dev_free(T, s);
+    if (ownM) dev_free(Ms, s);
+    return info;
+}
+
+// ---------------------------------------------------------------------------
+// transpose
+// ---------------------------------------------------------------------------
+
+__global__ void k_col_count(const int32_t *__restrict__ Aj, int64_t nnz,
+                            int32_t *__restrict__ cnt)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz;
+         e += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&cnt[Aj[e]], 1);
+}
+
+template <typename Z>
+__global__ void k_tr_scatter(int64_t m, const int32_t *__restrict__ Ap,
+                             const int32_t *__restrict__ Aj, const Z *__restrict__ Ax,
+                             bool iso, int64_t nnz, const int64_t *__restrict__ Bp,
+                             int32_t *__restrict__ fill, int32_t *__restrict__ Bj,
+                             Z *__restrict__ Bx)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t i = row_of(Ap, m, e), j = Aj[e];
+        const int64_t pos = Bp[j] + atomicAdd(&fill[j], 1);
+        Bj[pos] = i;
+        if (Bx) Bx[pos] = Ax[iso ? 0 : e];
+    }
+}
+
+// sort every row by index: one warp per row of up to SORT_W entries in shared
+// memory; longer rows are sorted by a whole block in global memory
+template <typename Z, int SORT_W>
+__global__ void __launch_bounds__(128)
+k_sort_rows_warp(int64_t m, const int64_t *__restrict__ Bp, int32_t *__restrict__ Bj,
+                 Z *__restrict__ Bx)
+{
+    __shared__ int32_t sk[4][SORT_W];
+    __shared__ Z sv[4][SORT_W];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m;
+         r += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int64_t lo = Bp[r];
+        const int n = (int)(Bp[r + 1] - lo);
+        if (n <= 1 || n > SORT_W) continue;
+        int n2 = 1;
+        while (n2 < n) n2 <<= 1;
+        for (int q = lane; q < n2; q += 32) {
+            if (q < n) { sk[w][q] = Bj[lo + q]; if (Bx) sv[w][q] = Bx[lo + q]; }
+            else sk[w][q] = INT32_MAX;
+        }
+        __syncwarp();
+        for (int size = 2; size <= n2; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int q = lane; q < n2; q += 32) {
+                    const int pq = q ^ stride;
+                    if (pq > q) {
+                        const bool up = (q & size) == 0;
+                        const int32_t a = sk[w][q], b = sk[w][pq];
+                        if ((a > b) == up) {
+                            sk[w][q] = b; sk[w][pq] = a;
+                            if (Bx) { Z t = sv[w][q]; sv[w][q] = sv[w][pq]; sv[w][pq] = t; }
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        for (int q = lane; q < n; q += 32) { Bj[lo + q] = sk[w][q]; if (Bx) Bx[lo + q] = sv[w][q]; }
+        __syncwarp();
+    }
+}
+
+// one block per long row: bitonic sort over a padded scratch copy
+template <typename Z>
+__global__ void __launch_bounds__(512)
+k_sort_rows_block(const int32_t *__restrict__ rows, int nrows_long,
+                  const int64_t *__restrict__ Bp, int32_t *__restrict__ Bj,
+                  Z *__restrict__ Bx, int32_t *__restrict__ sk_all, Z *__restrict__ sv_all,
+                  const int64_t *__restrict__ soff)
+{
+    for (int t = blockIdx.x; t < nrows_long; t += gridDim.x) {
+        const int32_t r = rows[t];
+        const int64_t lo = Bp[r];
+        const int64_t n = Bp[r + 1] - lo;
+        int64_t n2 = 1;
+        while (n2 < n) n2 <<= 1;
+        int32_t *sk = sk_all + soff[t];
+        Z *sv = sv_all + soff[t];
+        for (int64_t q = threadIdx.x; q < n2; q += blockDim.x) {
+            if (q < n) { sk[q] = Bj[lo + q]; if (Bx) sv[q] = Bx[lo + q]; }
+            else sk[q] = INT32_MAX;
+        }
+        __syncthreads();
+        for (int64_t size = 2; size <= n2; size <<= 1)
+            for (int64_t stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int64_t q = threadIdx.x; q < n2; q += blockDim.x) {
+                    const int64_t pq = q ^ stride;
+                    if (pq > q) {
+                        const bool up = (q & size) == 0;
+                        const int32_t a = sk[q], b = sk[pq];
+                        if ((a > b) == up) {
+                            sk[q] = b; sk[pq] = a;
+                            if (Bx) { Z tv = sv[q]; sv[q] = sv[pq]; sv[pq] = tv; }
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        for (int64_t q = threadIdx.x; q < n; q += blockDim.x) {
+            Bj[lo + q] = sk[q];
+            if (Bx) Bx[lo + q] = sv[q];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_i64_to_i32_e(const int64_t *__restrict__ in, int32_t *__restrict__ out,
+                               int64_t n)
+{
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x)
+        out[t] = (int32_t)in[t];
+}
+
+template <typename Z>
+static int transpose_t(DevCSR &B, const DevCSR &A, cudaStream_t s)
+{
+    const int64_t m = A.nrows, n = A.ncols, nnz = A.nnz;
+    constexpr int SORT_W = 512;
+    Scratch ws(s);
+    int32_t *cnt = ws.get<int32_t>(n + 1);
+    int64_t *Bp64 = ws.get<int64_t>(n + 1);
+    int32_t *fill = ws.get<int32_t>(n + 1);
+    if (ws.failed) return OUT_OF_MEMORY;
+    cudaMemsetAsync(cnt, 0, (size_t)(n + 1) * 4, s);
+    cudaMemsetAsync(fill, 0, (size_t)(n + 1) * 4, s);
+    if (nnz > 0) k_col_count<<<grid_n(nnz), 256, 0, s>>>(A.j, nnz, cnt);
+    int info = scan_exclusive_i32_to_i64(cnt, Bp64, n + 1, s);
+    if (info != SUCCESS) return info;
+    B = DevCSR();
+    B.nrows = n; B.ncols = m; B.nnz = nnz; B.type = A.type; B.iso = A.iso;
+    size_t ts = type_size(A.type);
+    B.p = (int32_t *)dalloc((size_t)(n + 1) * 4, s);
+    B.j = (int32_t *)dalloc((size_t)(nnz ? nnz : 1) * 4, s);
+    B.x = A.x ? dalloc(A.iso ? ts : (size_t)(nnz ? nnz : 1) * ts, s) : nullptr;
+    if (!B.p || !B.j || (A.x && !B.x)) { dev_free(B, s); return OUT_OF_MEMORY; }
+    k_i64_to_i32_e<<<grid_n(n + 1), 256, 0, s>>>(Bp64, B.p, n + 1);
+    Z *Bx = (A.x && !A.iso) ? (Z *)B.x : nullptr;
+    if (A.x && A.iso) cudaMemcpyAsync(B.x, A.x, ts, cudaMemcpyDeviceToDevice, s);
+    if (nnz > 0) {
+        k_tr_scatter<Z><<<grid_n(nnz), 256, 0, s>>>(m, A.p, A.j, (const Z *)A.x, A.iso,
+            nnz, Bp64, fill, B.j, Bx);
+        k_sort_rows_warp<Z, SORT_W><<<grid_n(n * 32, 128), 128, 0, s>>>(n, Bp64, B.j, Bx);
+        // long rows: gather their ids and sort each with a block
+        std::vector<int64_t> hp((size_t)n + 1);
+        cudaMemcpyAsync(hp.data(), Bp64, (size_t)(n + 1) * 8, cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) { dev_free(B, s); return cuda_to_info(e); }
+        std::vector<int32_t> longr;
+        std::vector<int64_t> off;
+        int64_t tot = 0;
+        for (int64_t r = 0; r < n; r++) {
+            int64_t len = hp[r + 1] - hp[r];
+            if (len > SORT_W) {
+                int64_t n2 = 1;
+                while (n2 < len) n2 <<= 1;
+                longr.push_back((int32_t)r);
+                off.push_back(tot);
+                tot += n2;
+            }
+        }
+        if (!longr.empty()) {
+            int32_t *drows = ws.get<int32_t>(longr.size());
+            int64_t *doff = ws.get<int64_t>(off.size());
+            int32_t *sk = ws.get<int32_t>(tot);
+            Z *sv = ws.get<Z>(tot);
+            if (ws.failed) { dev_free(B, s); return OUT_OF_MEMORY; }
+            cudaMemcpyAsync(drows, longr.data(), longr.size() * 4, cudaMemcpyHostToDevice, s);
+            cudaMemcpyAsync(doff, off.data(), off.size() * 8, cudaMemcpyHostToDevice, s);
+            int nb = (int)longr.size();
+            k_sort_rows_block<Z><<<nb < 1024 ? nb : 1024, 512, 0, s>>>(drows, nb, Bp64,
+                B.j, Bx, sk, sv, doff);
+        }
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { dev_free(B, s); return cuda_to_info(e); }
+    return SUCCESS;
+}
+
+int transpose(DevCSR &B, const DevCSR &A0, cudaStream_t s)
+{
+    DevCSR A = A0;
+    DevCSR P;
+    bool own = false;
+    if (A0.nzombies > 0) {
+        // transpose the live entries only
+        P = DevCSR();
+        P.nrows = A0.nrows; P.ncols = A0.ncols; P.nnz = A0.nnz; P.type = A0.type;
+        P.iso = A0.iso; P.nzombies = A0.nzombies;
+        size_t ts = type_size(A0.type);
+        P.p = (int32_t *)dalloc((size_t)(A0.nrows + 1) * 4, s);
+        P.j = (int32_t *)dalloc((size_t)(A0.nnz ? A0.nnz : 1) * 4, s);
+        P.x = A0.x ? dalloc(A0.iso ? ts : (size_t)(A0.nnz ? A0.nnz : 1) * ts, s) : nullptr;
+        if (!P.p || !P.j || (A0.x && !P.x)) { dev_free(P, s); return OUT_OF_MEMORY; }
+        cudaMemcpyAsync(P.p, A0.p, (size_t)(A0.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(P.j, A0.j, (size_t)A0.nnz * 4, cudaMemcpyDeviceToDevice, s);
+        if (A0.x) cudaMemcpyAsync(P.x, A0.x, A0.iso ? ts : (size_t)A0.nnz * ts,
+                                  cudaMemcpyDeviceToDevice, s);
+        int info = dev_prune_zombies(P, s);
+        if (info != SUCCESS) { dev_free(P, s); return info; }
+        A = P; own = true;
+    }
+    int info;
+    switch (type_size(A.type)) {
+        case 1: info = transpose_t<uint8_t>(B, A, s); break;
+        case 4: info = transpose_t<uint32_t>(B, A, s); break;
+        case 8: info = transpose_t<uint64_t>(B, A, s); break;
+        default: info = NO_VALUE;
+    }
+    if (own) dev_free(P, s);
+    return info;
+}
+
+}  // namespace grb

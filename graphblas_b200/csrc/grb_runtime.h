@@ -129,6 +129,10 @@ int accum_mask(DevCSR &C, const DevCSR &T, const DevCSR *M, bool mask_comp,
 // B = A' (Source/transpose/GB_transpose_cast.c:18)
 int transpose(DevCSR &B, const DevCSR &A, cudaStream_t s);
 
+// w<m> = A*u, u and w sparse 1-by-n rows (GrB_mxv, Source/mxm/GrB_mxv.c:18)
+int mxv(DevCSR &w, const DevCSR *mask, bool mask_comp, bool mask_struct,
+        const DevCSR &A, const DevCSR &u, SemiringCode sr, cudaStream_t s);
+
 // supported semiring?  (declines with NO_VALUE otherwise)
 bool semiring_supported(SemiringCode sr);
 

@@ -171,6 +171,29 @@ int grb_b200_dreduce(void *out, grb_b200_dmatrix D, int monoid_opcode);
 /* Remove zombies (the zombie pruning of GB_wait, Source/wait/GB_wait.c:62) */
 int grb_b200_dwait(grb_b200_dmatrix D);
 
+/* An empty nrows-by-ncols device matrix of a type (GrB_Matrix_new,
+ * Source/matrix/GrB_Matrix_new.c) */
+int grb_b200_dmatrix_empty(grb_b200_dmatrix *D, int64_t nrows, int64_t ncols,
+                           int type);
+
+/* A device copy (GrB_Matrix_dup, Source/matrix/GrB_Matrix_dup.c) */
+int grb_b200_dmatrix_dup(grb_b200_dmatrix *D, grb_b200_dmatrix A);
+
+/* C<M,replace> = accum(C,T) in place; accum_opcode 0 = none.  Replaces
+ * GB_accum_mask (Source/mask/GB_accum_mask.c:126). */
+int grb_b200_daccum_mask(grb_b200_dmatrix C, grb_b200_dmatrix T,
+                         grb_b200_dmatrix M, bool mask_comp, bool mask_struct,
+                         bool replace, int accum_opcode);
+
+/* B = A' (GB_transpose_cast, Source/transpose/GB_transpose_cast.c:18) */
+int grb_b200_dtranspose(grb_b200_dmatrix *B, grb_b200_dmatrix A);
+
+/* w<m> = A*u with u, m and w held as 1-by-n rows (GrB_mxv,
+ * Source/mxm/GrB_mxv.c:18) */
+int grb_b200_dmxv(grb_b200_dmatrix *w, grb_b200_dmatrix mask, bool mask_comp,
+                  bool mask_struct, grb_b200_dmatrix A, grb_b200_dmatrix u,
+                  const grb_b200_semiring *sr);
+
 #ifdef __cplusplus
 }
 #endif
