@@ -33,6 +33,8 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include "../../include/grb_b200.h"
 #include "grb_runtime.h"
 #include "grb_semirings.h"
 
@@ -418,4 +420,117 @@ bool semiring_supported(SemiringCode sr)
     return false;
 }
 
+
+// ---------------------------------------------------------------------------
+// dot3 with no allocation at all
+//
+// Some callers cannot allocate device memory: a host application whose
+// device memory is owned by another allocator (a framework's caching pool or
+// a preallocated arena it must not bypass), or a latency-bound loop that may
+// not call cudaMalloc/cudaFree because they can synchronise the device.  For
+// them grb_b200_dot3_noalloc runs the same two kernels as dot3 above, with
+// every input and output in caller-owned device memory and the work queue
+// and counters in the fixed array below.  The array lives in the library's
+// device image: every GPU that loads the library holds its 32 MiB until the
+// process exits.  All calls share it and it keeps the last call's contents;
+// the counters are cleared at the start of each call.  Calls that overlap on
+// the same GPU (from concurrent streams or host threads) race on the array
+// and must be serialised by the caller; each GPU has its own copy.
+// ---------------------------------------------------------------------------
+
+static constexpr size_t NOALLOC_BYTES = (size_t)32 << 20;
+static constexpr size_t NOALLOC_HEAD = 256;        // counters, then the queue
+static constexpr int64_t NOALLOC_MAX_ENTRIES =
+    (int64_t)((NOALLOC_BYTES - NOALLOC_HEAD) / sizeof(D3Work));
+
+static __device__ __align__(256) unsigned char g_dot3_scratch[NOALLOC_BYTES];
+
+// Device address of the array, looked up once per device with that device
+// current (host code may not use the symbol's host-side name as a pointer).
+static std::mutex g_scratch_mu;
+static void *g_scratch_addr[128];
+
+static int noalloc_scratch(void **addr)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 128) return PANIC;
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (g_scratch_addr[dev] == nullptr) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_dot3_scratch);
+        if (e != cudaSuccess || p == nullptr) { cudaGetLastError(); return PANIC; }
+        g_scratch_addr[dev] = p;
+    }
+    *addr = g_scratch_addr[dev];
+    return SUCCESS;
+}
+
+template <class SR>
+static int dot3_noalloc_launch(int64_t nrows, int64_t mnz, const int32_t *Mp,
+                               const int32_t *Mj, const int32_t *Ap, const int32_t *Aj,
+                               const void *Ax, bool a_iso, const int32_t *Bp,
+                               const int32_t *Bj, const void *Bx, bool b_iso,
+                               int32_t *Cj, void *Cx, int64_t *nzombies,
+                               cudaStream_t s)
+{
+    using Z = typename SR::z_t;
+    if ((SR::needs_a && Ax == nullptr) || (SR::needs_b && Bx == nullptr)) return NULL_POINTER;
+    void *scratch = nullptr;
+    int info = noalloc_scratch(&scratch);
+    if (info != SUCCESS) return info;
+    int *qlen = (int *)scratch, *qnext = qlen + 1;
+    unsigned long long *zc = (unsigned long long *)((char *)scratch + 32);
+    D3Work *queue = (D3Work *)((char *)scratch + NOALLOC_HEAD);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, NOALLOC_HEAD, s);
+    if (e != cudaSuccess) return cuda_to_info(e);
+    if (mnz > 0 && nrows > 0) {
+        const int nsm = runtime().num_sms;
+        int64_t blocks = ((mnz + 31) / 32 + 7) / 8;
+        if (blocks > (int64_t)nsm * 16) blocks = (int64_t)nsm * 16;
+        k_dot3_classify<SR><<<(unsigned)blocks, 256, 0, s>>>(
+            Mp, Mj, nullptr, T_BOOL, true, mnz, nrows, Ap, Aj, Ax, a_iso,
+            Bp, Bj, Bx, b_iso, Cj, (Z *)Cx, queue, qlen, zc);
+        k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
+            queue, qlen, qnext, Aj, Ax, a_iso, Bj, Bx, b_iso, Cj, (Z *)Cx, zc);
+    }
+    unsigned long long hz = 0;
+    e = cudaMemcpyAsync(&hz, zc, sizeof(hz), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_to_info(e);
+    if (nzombies) *nzombies = (int64_t)hz;
+    return SUCCESS;
+}
+
 }  // namespace grb
+
+extern "C" int grb_b200_dot3_noalloc(
+    int64_t nrows, int64_t ncols, int64_t mnz,
+    const int32_t *Mp, const int32_t *Mj,
+    const int32_t *Ap, const int32_t *Aj, const void *Ax, bool A_iso,
+    const int32_t *Bp, const int32_t *Bj, const void *Bx, bool B_iso,
+    const grb_b200_semiring *semiring, int32_t *Cj, void *Cx, int64_t *nzombies,
+    void *stream)
+{
+    using namespace grb;
+    if (!Mp || !Mj || !Ap || !Aj || !Bp || !Bj || !Cj || !Cx || !semiring)
+        return NULL_POINTER;
+    if (nrows < 0 || ncols < 0 || mnz < 0) return INVALID_VALUE;
+    if (mnz > NOALLOC_MAX_ENTRIES || nrows >= INT32_MAX || ncols >= INT32_MAX) {
+        fprintf(stderr, "grb_b200_dot3_noalloc: %lld mask entries exceed the fixed "
+                "scratch capacity of %lld entries\n", (long long)mnz,
+                (long long)NOALLOC_MAX_ENTRIES);
+        return INVALID_VALUE;
+    }
+    int info = init_device();
+    if (info != SUCCESS) return info;
+    cudaStream_t s = (cudaStream_t)stream;
+    SemiringCode sr{semiring->add_opcode, semiring->mult_opcode, semiring->type};
+#define GRB_NOALLOC_CASE(ADD, MULT, TC, CT)                                      \
+    if (sr.add == ADD && sr.mult == MULT && sr.type == TC)                       \
+        return dot3_noalloc_launch<Semiring<ADD, MULT, CT>>(nrows, mnz, Mp, Mj,  \
+            Ap, Aj, Ax, A_iso, Bp, Bj, Bx, B_iso, Cj, Cx, nzombies, s);
+    GRB_FOR_EACH_SEMIRING(GRB_NOALLOC_CASE)
+#undef GRB_NOALLOC_CASE
+    return NO_VALUE;
+}

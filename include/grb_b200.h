@@ -194,6 +194,46 @@ int grb_b200_dmxv(grb_b200_dmatrix *w, grb_b200_dmatrix mask, bool mask_comp,
                   bool mask_struct, grb_b200_dmatrix A, grb_b200_dmatrix u,
                   const grb_b200_semiring *sr);
 
+/* ------------------------------------------------------------------------ */
+/* Masked dot products without any allocation                               */
+/* ------------------------------------------------------------------------ */
+
+/* Largest mask (number of entries) grb_b200_dot3_noalloc accepts. */
+#define GRB_B200_DOT3_NOALLOC_MAX_ENTRIES 1048568
+
+/* C<M> = A*B' over M's pattern, like grb_b200_dmxm_dot3, for callers that
+ * cannot allocate device memory: a host application whose GPU memory belongs
+ * to another allocator (a framework's caching pool or a preallocated arena
+ * that must not be bypassed), or a latency-bound loop that must not call
+ * cudaMalloc / cudaFree because those can synchronise the whole device.
+ * This entry point has no counterpart in the reference.
+ *
+ * Every array is caller-owned device memory, by-row CSR with int32 offsets
+ * and indices: M is nrows-by-ncols (structural; Mp has nrows+1 entries, Mj
+ * has mnz), A is nrows-by-k and B is ncols-by-k (rows of both are the
+ * operands of each dot product).  Ax/Bx hold values of the semiring's type
+ * (one value when *_iso) and may be NULL when the multiplier does not read
+ * them.  Outputs: Cj[p] = j for a live entry or -(j)-2 for a zombie (empty
+ * dot product), Cx[p] its value, p over the mnz entries of M; C's row
+ * offsets are Mp.  *nzombies (host) gets the zombie count.
+ *
+ * The work queue and counters live in a fixed 32 MiB device array inside the
+ * library (held by every GPU that loads it until the process exits), so masks
+ * above GRB_B200_DOT3_NOALLOC_MAX_ENTRIES entries are rejected with
+ * GrB_INVALID_VALUE.  The first call on each device looks up that array's
+ * device address, so make it before any stream capture.  Calls share the
+ * array: calls that overlap on the same GPU (concurrent streams or threads)
+ * race and must be serialised by the caller.  Runs on `stream` (a
+ * cudaStream_t, NULL = legacy default stream) and synchronises it before
+ * returning. */
+int grb_b200_dot3_noalloc(int64_t nrows, int64_t ncols, int64_t mnz,
+                          const int32_t *Mp, const int32_t *Mj,
+                          const int32_t *Ap, const int32_t *Aj, const void *Ax,
+                          bool A_iso, const int32_t *Bp, const int32_t *Bj,
+                          const void *Bx, bool B_iso,
+                          const grb_b200_semiring *semiring, int32_t *Cj,
+                          void *Cx, int64_t *nzombies, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
