@@ -1,33 +1,43 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 semiring SpGEMM path.
+"""Benchmark of the B200 semiring SpGEMM path (SuiteSparse:GraphBLAS GrB_mxm).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--config tc|saxpy|bfs|batch|serve]
 
-Default workload (the headline): masked dot3 triangle counting,
-C<L> = L*U' with plus_pair int64 followed by a sum reduction, on a
-symmetrised R-MAT graph of scale 20, edge factor 16, (a,b,c,d) =
-(0.57,0.19,0.19,0.05), self-loops and duplicates removed (seeded synthetic
-input of the graph500 shape; no dataset).  One step = one GrB_mxm + reduce
-over the whole graph.  Metric: triangles/s.
+Workloads (seeded synthetic inputs of the graph500 / Erdos-Renyi shapes the
+reference is measured on; no dataset is read):
 
-* value: device time with L and U resident in HBM, CUDA events on the
-  launching stream, L2 flushed (256 MB write) between steps, max over ranks.
-* e2e: the same step through the public C-ABI from pinned host buffers
-  (upload L and U, multiply, reduce, read the count back), timed the same way.
-* roofline: the dot3 kernel's algorithmic bytes per launch
-  (4*(sum_i nnz(L(i,:))^2 + sum_j nnz(U(j,:))^2) merge reads + 16*nnz(L)
-  mask read and C write) over its event-timed duration, against the measured
-  HBM copy bandwidth.
+  tc     (default, the headline) masked dot3 triangle counting,
+         C<L> = L*U' with plus_pair int64 then a sum reduction, on a
+         symmetrised R-MAT graph of scale 20, edge factor 16,
+         (a,b,c,d) = (0.57,0.19,0.19,0.05), self-loops and duplicates removed.
+         One step = GrB_mxm + GrB_reduce over the whole graph; metric
+         triangles/s.
+  saxpy  C = A*B, plus_times fp64, A and B 16384x16384 Erdos-Renyi with 8
+         uniform columns per row, values U[-1,1]; metric GFLOP/s (2 flops per
+         product).
+  bfs    level-synchronous BFS parents (GrB_vxm any_secondi int64 with a
+         complemented structural mask and replace, then GrB_assign) on R-MAT
+         scale 22, edge factor 16; metric TEPS (undirected edges / s).
+  batch  4096 independent C_k = A_k*A_k, min_plus fp32, n_k log-uniform in
+         [64, 8192], Poisson(6) entries per row; metric GFLOP/s.
+
+* value: device time with the inputs resident in HBM, CUDA events on the
+  launching stream, L2 flushed (a 256 MB write) between steps, max over ranks.
+* e2e: the same step through the public API from pinned host buffers, the
+  host->device copies and the result read-back inside the timed region.
+* roofline: the dominant kernel's algorithmic bytes per launch over its
+  event-timed duration, against the measured HBM copy bandwidth.
 * cpu_baseline: the reference library (oracle/_ref, SuiteSparse:GraphBLAS
-  built from its own sources) on this host's cores, same graph.
+  built from its own sources) on this host's cores, same inputs.
 
---impl reference times that reference CPU path alone and prints its line.
+--impl reference times the reference's CPU path alone and prints its line.
 Multi-GPU (torchrun): every rank runs an independent replica (the path has no
-exchange step); value = all ranks' triangles / max step time.
+exchange step); value = all ranks' units / the max step time.
 """
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -81,18 +91,18 @@ class ClockSampler:
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.25)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        ok = [r for r in self.rows if len(r) >= 9]
+        sm = [float(r[1]) for r in ok if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in ok if r[2].replace(".", "").isdigit()]
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
-            if len(r) < 9:
-                continue
+        for r in ok:
             for k, nm in enumerate(names):
                 if r[5 + k].lower().startswith("active"):
                     reasons.add(nm)
@@ -101,16 +111,272 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def tc_inputs(scale, ef, seed):
-    S = W.rmat(scale, ef, seed=seed)
-    L, U = W.tril_triu(S)
-    dL = np.diff(L.p).astype(np.float64)
-    dU = np.diff(U.p).astype(np.float64)
-    alg_bytes = 4.0 * (np.sum(dL * dL) + np.sum(dU * dU)) + 16.0 * L.nnz
-    return S, L, U, alg_bytes
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+
+class TriCount:
+    metric, unit, dtype, kernel = "triangles/s", "triangles/s", "int64", "dot3"
+
+    def __init__(self, args):
+        self.scale = args.scale or 20
+        S = W.rmat(self.scale, 16, seed=args.seed)
+        self.S = S
+        self.L, self.U = W.tril_triu(S)
+        dL = np.diff(self.L.p).astype(np.float64)
+        dU = np.diff(self.U.p).astype(np.float64)
+        # merge reads of every (i,j) in L plus mask read and C write
+        self.alg_bytes = 4.0 * (np.sum(dL * dL) + np.sum(dU * dU)) + 16.0 * self.L.nnz
+        self.workload = "tricount_rmat%d_ef16_dot3_plus_pair" % self.scale
+
+    def config(self):
+        return {"n": int(self.S.nrows), "nnz_L": int(self.L.nnz),
+                "triangles": int(getattr(self, "ntri", -1))}
+
+    def dev_setup(self, gb):
+        self.gb = gb
+        self.dL = gb.DMatrix.upload(self.L, "bool")
+        self.dU = gb.DMatrix.upload(self.U, "bool")
+        self.sr = gb.semiring("PLUS", "PAIR", "int64")
+
+    def step_dev(self):
+        gb = self.gb
+        C = gb.dot3(self.dL, self.dL, self.dU, self.sr)
+        n = int(gb.reduce(C, "PLUS", np.int64))
+        C.free()
+        self.ntri = n
+        return n
+
+    def e2e_setup(self, torch):
+        self.pin = {k: torch.from_numpy(v).pin_memory() for k, v in
+                    (("Lp", self.L.p), ("Li", self.L.i), ("Up", self.U.p), ("Ui", self.U.i))}
+        return sum(int(t.numel() * t.element_size()) for t in self.pin.values()), 8
+
+    def step_e2e(self):
+        gb = self.gb
+        L_ = gb.lib()
+        hL, hU = ctypes.c_void_p(), ctypes.c_void_p()
+        gb.check(L_.grb_b200_dmatrix_upload(ctypes.byref(hL), self.L.nrows, self.L.ncols,
+                                            self.pin["Lp"].data_ptr(), self.pin["Li"].data_ptr(),
+                                            None, 1, True))
+        gb.check(L_.grb_b200_dmatrix_upload(ctypes.byref(hU), self.U.nrows, self.U.ncols,
+                                            self.pin["Up"].data_ptr(), self.pin["Ui"].data_ptr(),
+                                            None, 1, True))
+        dl, du = gb.DMatrix(hL.value), gb.DMatrix(hU.value)
+        C = gb.dot3(dl, dl, du, self.sr)
+        n = int(gb.reduce(C, "PLUS", np.int64))
+        for d in (C, dl, du):
+            d.free()
+        assert n == self.ntri
+        return n
+
+    def launches_per_step(self):
+        return 4            # classify, intersect, reduce partial, reduce final
+
+    def cpu_baseline(self, R, ncores):
+        ntri, times = R.tricount(self.S.nrows, self.L.p, self.L.i, self.U.p, self.U.i, reps=1)
+        assert ntri == self.ntri, "CPU and GPU triangle counts differ"
+        return ntri / float(times[0]), "whole graph, one GrB_mxm + GrB_reduce (%.2f s)" % times[0]
+
+    def reference_steps(self, R, steps, warmup):
+        for _ in range(warmup):
+            R.tricount(self.S.nrows, self.L.p, self.L.i, self.U.p, self.U.i, reps=1)
+        ntri, times = R.tricount(self.S.nrows, self.L.p, self.L.i, self.U.p, self.U.i,
+                                 reps=steps)
+        self.ntri = ntri
+        return ntri * steps, float(np.sum(times)), "whole graph per step (GrB_mxm + GrB_reduce)"
+
+    def free(self):
+        for d in ("dL", "dU"):
+            if hasattr(self, d):
+                getattr(self, d).free()
 
 
-def run_reference(args):
+class Saxpy:
+    metric, unit, dtype, kernel = "GFLOP/s", "GFLOP/s", "fp64", "saxpy3_numeric"
+
+    def __init__(self, args):
+        n = 16384
+        self.n = n
+        self.A = W.er_fixed(n, n, 8, seed=args.seed + 1)
+        self.B = W.er_fixed(n, n, 8, seed=args.seed + 2)
+        deg = np.diff(self.B.p)
+        self.products = int(np.sum(deg[self.A.i]))
+        self.flops = 2.0 * self.products
+        self.workload = "saxpy3_er16384_d8_plus_times_fp64"
+
+    def config(self):
+        return {"n": self.n, "nnz_A": int(self.A.nnz), "products": self.products,
+                "nnz_C": int(getattr(self, "nnz_c", -1))}
+
+    def dev_setup(self, gb):
+        from graphblas_b200.grb import API
+        self.gb = gb
+        self.api = API()
+        self.Ag = self.api.matrix_from_csr(self.A)
+        self.Bg = self.api.matrix_from_csr(self.B)
+        self.Cg = self.api.matrix_new(11, self.n, self.n)
+        self.api.mxm(self.Cg, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", self.Ag, self.Bg)
+        self.nnz_c = self.api.nvals(self.Cg)
+        # algorithmic bytes (4 B index, 8 B value): A once, B rows per product, C once
+        self.alg_bytes = (4.0 * (self.n + 1) + 12.0 * self.A.nnz + 12.0 * self.products +
+                          12.0 * self.nnz_c + 4.0 * (self.n + 1))
+
+    def step_dev(self):
+        self.api.mxm(self.Cg, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", self.Ag, self.Bg)
+        return self.flops / 1e9
+
+    def e2e_setup(self, torch):
+        self.hbytes = 2 * (8 * (self.n + 1) + 16 * self.A.nnz)
+        return self.hbytes, 8 * (self.n + 1) + 16 * self.nnz_c
+
+    def step_e2e(self):
+        api = self.api
+        A = api.matrix_from_csr(self.A)
+        B = api.matrix_from_csr(self.B)
+        C = api.matrix_new(11, self.n, self.n)
+        api.mxm(C, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", A, B)
+        p, i, x = api.matrix_to_csr(C, 11, self.n)
+        for X in (A, B, C):
+            api.free(X)
+        assert int(p[-1]) == self.nnz_c
+        return self.flops / 1e9
+
+    def launches_per_step(self):
+        return 9
+
+    def cpu_baseline(self, R, ncores):
+        t = 0.0
+        reps = 5
+        for _ in range(reps):
+            _, _, _ = R.mxm(self.n, self.n, self.n, (self.A.p, self.A.i, self.A.x, 11),
+                            (self.B.p, self.B.i, self.B.x, 11), "PLUS", "TIMES", 11)
+        # the runner times GrB_mxm + wait itself; re-run for the timing
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            R.mxm(self.n, self.n, self.n, (self.A.p, self.A.i, self.A.x, 11),
+                  (self.B.p, self.B.i, self.B.x, 11), "PLUS", "TIMES", 11)
+        t = (time.perf_counter() - t0) / reps
+        return self.flops / 1e9 / t, "whole product, %d reps incl. CSR pack/unpack (%.1f ms)" % (reps, 1e3 * t)
+
+    def reference_steps(self, R, steps, warmup):
+        for _ in range(warmup):
+            R.mxm(self.n, self.n, self.n, (self.A.p, self.A.i, self.A.x, 11),
+                  (self.B.p, self.B.i, self.B.x, 11), "PLUS", "TIMES", 11)
+        tot = 0.0
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            R.mxm(self.n, self.n, self.n, (self.A.p, self.A.i, self.A.x, 11),
+                  (self.B.p, self.B.i, self.B.x, 11), "PLUS", "TIMES", 11)
+            tot += time.perf_counter() - t0
+        return self.flops / 1e9 * steps, tot, "whole product per step (GrB_mxm + wait + CSR pack/unpack)"
+
+    def free(self):
+        if hasattr(self, "api"):
+            for X in (self.Ag, self.Bg, self.Cg):
+                self.api.free(X)
+
+
+class Bfs:
+    metric, unit, dtype, kernel = "TEPS", "edges/s", "int64", "saxpy3_numeric"
+
+    def __init__(self, args):
+        self.scale = args.scale or 22
+        self.S = W.rmat(self.scale, 16, seed=args.seed)
+        self.n = self.S.nrows
+        deg = np.diff(self.S.p)
+        self.src = int(np.argmax(deg > 0))          # first vertex with an edge
+        self.edges = self.S.nnz // 2
+        self.workload = "bfs_rmat%d_ef16_vxm_any_secondi" % self.scale
+
+    def config(self):
+        return {"n": int(self.n), "nnz_S": int(self.S.nnz), "source": self.src,
+                "levels": int(getattr(self, "levels", -1)),
+                "reached": int(getattr(self, "reached", -1))}
+
+    def dev_setup(self, gb):
+        from graphblas_b200.grb import API
+        self.gb = gb
+        self.api = API()
+        self.Sg = self.api.matrix_from_csr(self.S, 1)
+        # algorithmic bytes of the whole traversal: every reached vertex's row
+        # (8 B row pointer + 4 B per index) once, plus 8 B parent writes
+        self.alg_bytes = 8.0 * self.n + 4.0 * self.S.nnz + 8.0 * self.n
+
+    def bfs(self, Sg):
+        api = self.api
+        n, src = self.n, self.src
+        q = api.vector_from([src], [src], 8, n)
+        p = api.vector_from([src], [src], 8, n)
+        lev = 0
+        while True:
+            lev += 1
+            api.vxm(q, p, None, "GxB_ANY_SECONDI_INT64", q, Sg, "GrB_DESC_RSC")
+            if api.vnvals(q) == 0:
+                break
+            api.assign_all(p, q, None, q, n, "GrB_DESC_S")
+        self.levels = lev
+        return q, p
+
+    def step_dev(self):
+        q, p = self.bfs(self.Sg)
+        self.reached = self.api.vnvals(p)
+        self.api.vfree(q)
+        self.api.vfree(p)
+        return self.edges
+
+    def e2e_setup(self, torch):
+        return 8 * (self.n + 1) + 8 * self.S.nnz, 16 * self.n
+
+    def step_e2e(self):
+        api = self.api
+        Sg = api.matrix_from_csr(self.S, 1)
+        q, p = self.bfs(Sg)
+        idx, par = api.vector_to(p, 8)
+        for v in (q, p):
+            api.vfree(v)
+        api.free(Sg)
+        return self.edges
+
+    def launches_per_step(self):
+        return 12 * max(getattr(self, "levels", 1), 1)
+
+    def cpu_baseline(self, R, ncores):
+        parent, secs, nlev = R.bfs(self.n, self.S.p, self.S.i, self.src)
+        return self.edges / secs, "whole traversal, vxm + assign per level (%.2f s)" % secs
+
+    def reference_steps(self, R, steps, warmup):
+        for _ in range(warmup):
+            R.bfs(self.n, self.S.p, self.S.i, self.src)
+        tot = 0.0
+        for _ in range(steps):
+            _, secs, _ = R.bfs(self.n, self.S.p, self.S.i, self.src)
+            tot += secs
+        return self.edges * steps, tot, "whole traversal per step"
+
+    def free(self):
+        if hasattr(self, "api"):
+            self.api.free(self.Sg)
+
+
+CONFIGS = {"tc": TriCount, "saxpy": Saxpy, "bfs": Bfs}
+
+
+def make_batch(args):
+    from graphblas_b200 import batch as B
+    return B.BenchBatch(args)
+
+
+def make_serve(args):
+    from graphblas_b200 import serve as S
+    return S.BenchServe(args)
+
+
+# ---------------------------------------------------------------------------
+# harness
+# ---------------------------------------------------------------------------
+
+def run_reference(args, cfg):
     """The reference's own CPU path (oracle/_ref) on this host's cores."""
     from oracle import Reference, reference_available
     rank = int(os.environ.get("RANK", "0"))
@@ -122,24 +388,23 @@ def run_reference(args):
         return 0
     ncores = os.cpu_count()
     R = Reference(nthreads=ncores)
-    S, L, U, _ = tc_inputs(args.scale, 16, args.seed)
-    for _ in range(args.warmup):
-        R.tricount(S.nrows, L.p, L.i, U.p, U.i, reps=1)
-    ntri, times = R.tricount(S.nrows, L.p, L.i, U.p, U.i, reps=args.steps)
-    t = float(np.sum(times))
-    val = ntri * args.steps / t
-    line = {"metric": "triangles/s", "value": val, "unit": "triangles/s",
+    work = cfg(args)
+    try:
+        units, secs, sample = work.reference_steps(R, args.steps, args.warmup)
+    except NotImplementedError:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the reference has no request server for this workload"}))
+        return 0
+    val = units / secs
+    line = {"metric": work.metric, "value": val, "unit": work.unit,
             "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "int64", "data": "synthetic",
-            "config": {"workload": "tricount_rmat%d_ef16_dot3_plus_pair" % args.scale,
-                       "nnz_L": int(L.nnz), "triangles": int(ntri),
-                       "threads": ncores},
-            "cpu_baseline": {"value": val, "unit": "triangles/s", "cores": ncores,
-                             "kind": "reference",
-                             "sample": "whole graph per step (GrB_mxm + GrB_reduce)"},
-            "e2e": {"value": val, "unit": "triangles/s", "h2d_bytes_per_step": 0,
+            "dtype": work.dtype, "data": "synthetic",
+            "config": dict(workload=work.workload, threads=ncores, **work.config()),
+            "cpu_baseline": {"value": val, "unit": work.unit, "cores": ncores,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": val, "unit": work.unit, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -152,13 +417,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="tc")
-    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--scale", type=int, default=0)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    cfg = CONFIGS.get(args.config) or {"batch": make_batch, "serve": make_serve}.get(args.config)
+    if cfg is None:
+        raise SystemExit("unknown --config %s" % args.config)
     if args.impl == "reference":
-        return run_reference(args)
+        return run_reference(args, cfg)
 
     import torch
     import graphblas_b200 as gb
@@ -169,16 +437,14 @@ def main():
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
-        import torch.distributed as dist
         import datetime
+        import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     gb.init()
     L_ = gb.lib()
     stream = torch.cuda.Stream()
-    L_.grb_b200_set_stream(ctypes_ptr(stream.cuda_stream))
-
-    S, L, U, alg_bytes = tc_inputs(args.scale, 16, args.seed + 0)
-    sr = gb.semiring("PLUS", "PAIR", "int64")
+    L_.grb_b200_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    work = cfg(args)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def barrier():
@@ -186,181 +452,140 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    # ---- device-resident step ----
-    dL = gb.DMatrix.upload(L, "bool")
-    dU = gb.DMatrix.upload(U, "bool")
+    def timed(fn, k_steps, profile_kernel=None):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k_steps)]
+        units = 0.0
+        if profile_kernel:
+            L_.grb_b200_profile_reset()
+            L_.grb_b200_profile_enable(True)
+        with torch.cuda.stream(stream):
+            for k in range(k_steps):
+                flush.fill_(k & 0xff)
+                ev[k][0].record(stream)
+                units += fn()
+                ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        if profile_kernel:
+            L_.grb_b200_profile_enable(False)
+        return units, sum(a.elapsed_time(b) for a, b in ev)
 
-    def step_dev():
-        C = gb.dot3(dL, dL, dU, sr)
-        n = gb.reduce(C, "PLUS", np.int64)
-        C.free()
-        return int(n)
-
+    work.dev_setup(gb)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
-            ntri = step_dev()
+            work.step_dev()
     barrier()
     sampler = ClockSampler(local)
     sampler.start()
-    L_.grb_b200_profile_reset()
-    L_.grb_b200_profile_enable(True)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    with torch.cuda.stream(stream):
-        for k in range(args.steps):
-            flush.fill_(k & 0xff)
-            ev[k][0].record(stream)
-            ntri = step_dev()
-            ev[k][1].record(stream)
-    torch.cuda.synchronize()
-    L_.grb_b200_profile_enable(False)
+    units, dev_ms = timed(work.step_dev, args.steps, profile_kernel=work.kernel)
     clocks = sampler.stop()
-    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
-    kms, kcount = profile(L_, "dot3")
+    kms, kcount = profile(L_, work.kernel)
     barrier()
     t_max = allreduce_max(dist, dev_ms)
-    ntri_all = allreduce_sum(dist, float(ntri) * args.steps)
+    units_all = allreduce_sum(dist, units)
 
-    # ---- end-to-end step through the C-ABI from pinned host buffers ----
-    pin = {}
-    for name, arr in (("Lp", L.p), ("Li", L.i), ("Up", U.p), ("Ui", U.i)):
-        t = torch.from_numpy(arr).pin_memory()
-        pin[name] = t
-    h2d = sum(int(t.numel() * t.element_size()) for t in pin.values())
-
-    def step_e2e():
-        hL = ctypes_void()
-        hU = ctypes_void()
-        gb.check(L_.grb_b200_dmatrix_upload(byref(hL), L.nrows, L.ncols,
-                                            pin["Lp"].data_ptr(), pin["Li"].data_ptr(),
-                                            None, 1, True))
-        gb.check(L_.grb_b200_dmatrix_upload(byref(hU), U.nrows, U.ncols,
-                                            pin["Up"].data_ptr(), pin["Ui"].data_ptr(),
-                                            None, 1, True))
-        dl, du = gb.DMatrix(hL.value), gb.DMatrix(hU.value)
-        C = gb.dot3(dl, dl, du, sr)
-        n = gb.reduce(C, "PLUS", np.int64)
-        for d in (C, dl, du):
-            d.free()
-        return int(n)
-
+    h2d, d2h = work.e2e_setup(torch)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
-            step_e2e()
+            work.step_e2e()
     barrier()
-    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
-    with torch.cuda.stream(stream):
-        for k in range(args.steps):
-            flush.fill_(k & 0xff)
-            ev2[k][0].record(stream)
-            n2 = step_e2e()
-            ev2[k][1].record(stream)
-    torch.cuda.synchronize()
-    assert n2 == ntri
-    e2e_ms = allreduce_max(dist, sum(a.elapsed_time(b) for a, b in ev2))
+    units2, e2e_ms = timed(work.step_e2e, args.steps)
+    e2e_max = allreduce_max(dist, e2e_ms)
+    units2_all = allreduce_sum(dist, units2)
 
+    if hasattr(work, "finish"):
+        work.finish(t_max / args.steps)
     hbm_peak, peak_kind = peaks()
     kernel_ms = kms / max(kcount, 1)
-    achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
-    line = None
+    launches_per_step = max(kcount // max(args.steps, 1), 1)
+    if getattr(work, "kernel_ms_override", None):
+        # numeric phase replayed as a CUDA graph: timed in a separate eager run
+        kernel_ms, launches_per_step = work.kernel_ms_override, 1
+    alg_per_launch = work.alg_bytes / launches_per_step
+    achieved = alg_per_launch / (kernel_ms * 1e-3) / 1e9 if kernel_ms > 0 else None
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline:
-            cpu = cpu_baseline(S, L, U, ntri)
-        val = ntri_all / (t_max * 1e-3)
+            cpu = cpu_baseline(work)
         line = {
-            "metric": "triangles/s", "value": val, "unit": "triangles/s",
+            "metric": work.metric, "value": units_all / (t_max * 1e-3), "unit": work.unit,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+            "scaling": "weak", "vs_baseline": None, "dtype": work.dtype,
             "data": "synthetic",
-            "config": {"workload": "tricount_rmat%d_ef16_dot3_plus_pair" % args.scale,
-                       "n": int(S.nrows), "nnz_L": int(L.nnz), "triangles": int(ntri),
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "flushed (256 MB write) between steps",
-                       "edges_per_s": int(L.nnz) * args.steps * world / (t_max * 1e-3)},
-            "e2e": {"value": ntri_all / (e2e_ms * 1e-3), "unit": "triangles/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 8,
-                    "ms_per_step": e2e_ms / args.steps},
-            "gpu_launches": 4 * args.steps,
+            "config": dict(workload=work.workload,
+                           parallelism="replicas" if world > 1 else "single",
+                           l2="flushed (256 MB write) between steps", **work.config()),
+            "e2e": {"value": units2_all / (e2e_max * 1e-3), "unit": work.unit,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_max / args.steps},
+            "gpu_launches": work.launches_per_step() * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                         "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "unit": "GB/s",
+                         "frac": (achieved / hbm_peak) if achieved else None,
                          "peak_kind": peak_kind, "traffic": None,
-                         "kernel": "k_dot3", "kernel_ms": kernel_ms,
-                         "algorithmic_bytes": alg_bytes},
+                         "kernel": work.kernel, "kernel_ms_per_launch": kernel_ms,
+                         "algorithmic_bytes_per_launch": alg_per_launch},
             "clocks": clocks,
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line))
-    for d in (dL, dU):
-        d.free()
+    work.free()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     return 0
 
 
-def cpu_baseline(S, L, U, ntri_gpu):
-    """The reference library on this host's cores, one whole-graph run
-    (GrB_mxm + GrB_reduce), checked against the GPU count."""
+def cpu_baseline(work):
+    """The reference library on this host's cores, checked against the GPU."""
     try:
         from oracle import Reference, reference_available
         if not reference_available():
-            return {"value": None, "unit": "triangles/s", "cores": 0,
-                    "kind": "reference", "sample": "unavailable: oracle/_ref not built"}
+            return {"value": None, "unit": work.unit, "cores": 0, "kind": "reference",
+                    "sample": "unavailable: oracle/_ref not built"}
         ncores = os.cpu_count()
         R = Reference(nthreads=ncores)
-        ntri, times = R.tricount(S.nrows, L.p, L.i, U.p, U.i, reps=1)
-        assert ntri == ntri_gpu, "CPU and GPU triangle counts differ"
-        return {"value": ntri / float(times[0]), "unit": "triangles/s",
-                "cores": ncores, "kind": "reference",
-                "sample": "whole graph, one GrB_mxm + GrB_reduce (%.2f s)" % times[0]}
+        val, sample = work.cpu_baseline(R, ncores)
+        return {"value": val, "unit": work.unit, "cores": ncores, "kind": "reference",
+                "sample": sample}
     except Exception as e:   # the baseline is reported, never required
-        return {"value": None, "unit": "triangles/s", "cores": 0,
-                "kind": "reference", "sample": "failed: %s" % e}
+        return {"value": None, "unit": work.unit, "cores": 0, "kind": "reference",
+                "sample": "failed: %s" % e}
 
 
 def profile(L_, name):
-    import ctypes
     ms = ctypes.c_double()
     cnt = ctypes.c_int64()
     L_.grb_b200_profile(name.encode(), ctypes.byref(ms), ctypes.byref(cnt))
     return ms.value, cnt.value
 
 
-def allreduce_max(dist, v):
+def _reduce(dist, v, op):
     if dist is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cpu" if dist.get_backend() == "gloo" else "cuda"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def allreduce_max(dist, v):
+    """The slowest rank's time (replicas: the job ends when the last ends)."""
+    return _reduce(dist, v, None if dist is None else dist.ReduceOp.MAX)
 
 
 def allreduce_sum(dist, v):
-    if dist is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    """All ranks' units of work."""
+    return _reduce(dist, v, None if dist is None else dist.ReduceOp.SUM)
 
 
-def ctypes_ptr(v):
-    import ctypes
-    return ctypes.c_void_p(v)
-
-
-def ctypes_void():
-    import ctypes
-    return ctypes.c_void_p()
-
-
-def byref(x):
-    import ctypes
-    return ctypes.byref(x)
+def replica_value(dist, units, ms):
+    """Whole-job throughput of N independent replicas: the units every rank
+    processed over the slowest rank's time."""
+    return allreduce_sum(dist, units) / (allreduce_max(dist, ms) * 1e-3)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,588 @@
+// grb_batch.cu: thousands of independent SpGEMMs C_k = A_k * B_k in one pass.
+//
+// The reference has no batched multiply: a caller loops over GrB_mxm (one
+// GB_AxB_saxpy3 per instance, Source/mxm/GB_AxB_saxpy3.c:119).  Here the
+// instances are laid out as one block-diagonal matrix in HBM (instance k's
+// rows follow instance k-1's, its column indices shifted by the columns before
+// it), so a single row-wise saxpy3 over that matrix computes every C_k: each
+// row of the block-diagonal product touches only its own instance, which
+// keeps every C_k bit-identical to a separate product.  The row work list of
+// the whole batch is binned by flops once (symbolic phase), and the numeric
+// phase - the persistent, binned hash kernels over the (instance, row-bin)
+// list, the row-count scan and the pack - runs with no host synchronisation,
+// so it is captured once in a CUDA graph and replayed.
+//
+// The bin thresholds, hash-table sizes and threads per row are chosen by a
+// small autotuner: it times a fixed set of candidate configurations on the
+// batch itself (CUDA events, after a warm-up) and caches the winner in a JSON
+// file keyed by semiring, type and the batch's size class.
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <mutex>
+#include <dlfcn.h>
+#include "../../include/grb_b200.h"
+#include "grb_saxpy3.h"
+
+using namespace grb;
+
+struct grb_b200_batch_s {
+    int count = 0;
+    SemiringCode sr{0, 0, 0};
+    size_t zsize = 0;
+    std::vector<int64_t> am, an, bn;         // shapes: A_k am x an, B_k an x bn
+    std::vector<int64_t> roff, acoff, bcoff; // row / A-column / B-column offsets
+    std::vector<int64_t> annz_off, bnnz_off; // entry offsets of each instance
+    DevCSR A, B;                             // block-diagonal operands
+    bool b_is_a = false;
+    SaxpyPlan *plan = nullptr;
+    SaxpyConfig cfg;
+    bool tuned = false;
+    double tuned_ms = 0;
+    DevCSR C;                                // block-diagonal result (capacity)
+    int64_t *nnz_d = nullptr;
+    cudaStream_t s = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int64_t last_nnz = -1;
+};
+
+namespace {
+
+// instance k: rebuild its local CSR into the block-diagonal arrays
+__global__ void k_blockdiag(int count, const int64_t *__restrict__ nrows,
+                            const int64_t *__restrict__ poff,   // local ptr offset
+                            const int64_t *__restrict__ roff,   // global row offset
+                            const int64_t *__restrict__ eoff,   // entry offset
+                            const int64_t *__restrict__ coff,   // column offset
+                            const int64_t *__restrict__ Ploc,   // concatenated local ptrs
+                            const int64_t *__restrict__ Jloc,   // concatenated local idx
+                            int32_t *__restrict__ Pg, int32_t *__restrict__ Jg)
+{
+    for (int k = blockIdx.x; k < count; k += gridDim.x) {
+        const int64_t n = nrows[k], p0 = poff[k], r0 = roff[k], e0 = eoff[k];
+        const int64_t c0 = coff[k];
+        const int64_t base = Ploc[p0];
+        for (int64_t r = threadIdx.x; r < n; r += blockDim.x)
+            Pg[r0 + r] = (int32_t)(e0 + Ploc[p0 + r] - base);
+        const int64_t nnz = Ploc[p0 + n] - base;
+        for (int64_t e = threadIdx.x; e < nnz; e += blockDim.x)
+            Jg[e0 + e] = (int32_t)(Jloc[base + e] + c0);
+    }
+}
+
+// block-diagonal C back to per-instance local CSR (int64 offsets/indices)
+__global__ void k_split(int count, const int64_t *__restrict__ nrows,
+                        const int64_t *__restrict__ roff, const int64_t *__restrict__ coff,
+                        const int64_t *__restrict__ poff_out,
+                        const int32_t *__restrict__ Cp, const int32_t *__restrict__ Cj,
+                        int64_t *__restrict__ Pout, int64_t *__restrict__ Jout)
+{
+    for (int k = blockIdx.x; k < count; k += gridDim.x) {
+        const int64_t n = nrows[k], r0 = roff[k], c0 = coff[k], po = poff_out[k];
+        const int64_t base = Cp[r0];
+        for (int64_t r = threadIdx.x; r <= n; r += blockDim.x)
+            Pout[po + r] = Cp[r0 + r];
+        const int64_t nnz = Cp[r0 + n] - base;
+        for (int64_t e = threadIdx.x; e < nnz; e += blockDim.x)
+            Jout[base + e] = (int64_t)Cj[base + e] - c0;
+    }
+}
+
+template <typename T> T *upload_vec(const std::vector<T> &v, cudaStream_t s)
+{
+    T *d = (T *)dalloc(v.size() * sizeof(T) + 8, s);
+    if (d) cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+    return d;
+}
+
+// build one block-diagonal operand from concatenated local CSR arrays
+int build_blockdiag(DevCSR &D, int count, const std::vector<int64_t> &rows,
+                    const std::vector<int64_t> &cols, const int64_t *P, const int64_t *J,
+                    const void *X, size_t zsize, bool iso, int type,
+                    std::vector<int64_t> &roff, std::vector<int64_t> &coff,
+                    std::vector<int64_t> &eoff, cudaStream_t s)
+{
+    roff.assign(count + 1, 0);
+    coff.assign(count + 1, 0);
+    eoff.assign(count + 1, 0);
+    std::vector<int64_t> poff(count + 1, 0);
+    for (int k = 0; k < count; k++) {
+        poff[k + 1] = poff[k] + rows[k] + 1;
+        roff[k + 1] = roff[k] + rows[k];
+        coff[k + 1] = coff[k] + cols[k];
+        eoff[k + 1] = eoff[k] + (P[poff[k] + rows[k]] - P[poff[k]]);
+    }
+    const int64_t m = roff[count], n = coff[count], nnz = eoff[count];
+    if (m >= INT32_MAX || n >= INT32_MAX || nnz >= INT32_MAX) return NO_VALUE;
+    D = DevCSR();
+    D.nrows = m; D.ncols = n; D.nnz = nnz; D.type = type; D.iso = iso;
+    D.p = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
+    D.j = (int32_t *)dalloc((size_t)(nnz + 1) * 4, s);
+    D.x = dalloc(iso ? zsize : (size_t)(nnz + 1) * zsize, s);
+    int64_t *dP = (int64_t *)dalloc((size_t)poff[count] * 8 + 8, s);
+    int64_t *dJ = (int64_t *)dalloc((size_t)(nnz + 1) * 8, s);
+    int64_t *d_rows = upload_vec(rows, s), *d_poff = upload_vec(poff, s);
+    int64_t *d_roff = upload_vec(roff, s), *d_eoff = upload_vec(eoff, s);
+    int64_t *d_coff = upload_vec(coff, s);
+    int info = SUCCESS;
+    if (!D.p || !D.j || !D.x || !dP || !dJ || !d_rows || !d_poff || !d_roff ||
+        !d_eoff || !d_coff) {
+        info = OUT_OF_MEMORY;
+    } else {
+        cudaMemcpyAsync(dP, P, (size_t)poff[count] * 8, cudaMemcpyHostToDevice, s);
+        // entries of every instance are contiguous in the concatenated arrays
+        cudaMemcpyAsync(dJ, J + P[0], (size_t)nnz * 8, cudaMemcpyHostToDevice, s);
+        if (X) cudaMemcpyAsync(D.x, (const char *)X + (iso ? 0 : P[0] * zsize),
+                               iso ? zsize : (size_t)nnz * zsize, cudaMemcpyHostToDevice, s);
+        // the local pointers index J from P[0]; rebase so instance entries start at 0
+        k_blockdiag<<<count < 65535 ? count : 65535, 128, 0, s>>>(count, d_rows, d_poff,
+            d_roff, d_eoff, d_coff, dP, dJ, D.p, D.j);
+        const int32_t mm = (int32_t)nnz;
+        cudaMemcpyAsync(D.p + m, &mm, 4, cudaMemcpyHostToDevice, s);
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) info = cuda_to_info(e);
+    }
+    dfree(dP, s); dfree(dJ, s); dfree(d_rows, s); dfree(d_poff, s);
+    dfree(d_roff, s); dfree(d_eoff, s); dfree(d_coff, s);
+    if (info != SUCCESS) dev_free(D, s);
+    return info;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner
+// ---------------------------------------------------------------------------
+
+std::vector<SaxpyConfig> candidates()
+{
+    std::vector<SaxpyConfig> v;
+    SaxpyConfig c = saxpy_default_config();
+    v.push_back(c);                                            // 64/8, 256/32, ...
+    SaxpyConfig a;
+    a.nb = 4;
+    a.bin[0] = {32, 4, 64}; a.bin[1] = {128, 16, 256};
+    a.bin[2] = {512, 32, 1024}; a.bin[3] = {4096, 256, 8192};
+    v.push_back(a);
+    SaxpyConfig b = c;
+    b.bin[0] = {64, 16, 128};
+    v.push_back(b);
+    SaxpyConfig d = c;
+    d.bin[0] = {64, 4, 128};
+    d.bin[1] = {256, 16, 512};
+    v.push_back(d);
+    SaxpyConfig e;
+    e.nb = 5;
+    e.bin[0] = {16, 4, 32}; e.bin[1] = {64, 8, 128}; e.bin[2] = {256, 32, 512};
+    e.bin[3] = {1024, 32, 2048}; e.bin[4] = {4096, 256, 8192};
+    v.push_back(e);
+    SaxpyConfig f = c;
+    f.bin[0] = {128, 8, 256};
+    v.push_back(f);
+    for (int bps : {8, 32}) {
+        SaxpyConfig g = c;
+        g.blocks_per_sm = bps;
+        v.push_back(g);
+    }
+    return v;
+}
+
+std::string config_to_json(const SaxpyConfig &c)
+{
+    std::string s = "{\"blocks_per_sm\": " + std::to_string(c.blocks_per_sm) + ", \"bins\": [";
+    for (int q = 0; q < c.nb; q++) {
+        if (q) s += ", ";
+        s += "[" + std::to_string(c.bin[q].limit) + ", " + std::to_string(c.bin[q].tpr) +
+             ", " + std::to_string(c.bin[q].cap) + "]";
+    }
+    return s + "]}";
+}
+
+bool config_from_json(const char *p, SaxpyConfig &c)
+{
+    // {"blocks_per_sm": N, "bins": [[l, t, c], ...]}
+    const char *b = strstr(p, "\"blocks_per_sm\"");
+    if (!b) return false;
+    c.blocks_per_sm = atoi(strchr(b, ':') + 1);
+    const char *q = strstr(p, "\"bins\"");
+    if (!q) return false;
+    q = strchr(q, '[');
+    if (!q) return false;
+    q++;
+    c.nb = 0;
+    while (c.nb < 6) {
+        const char *o = strchr(q, '[');
+        const char *end = strchr(q, ']');
+        if (!o || (end && end < o)) break;
+        long long l = 0; int t = 0, cp = 0;
+        if (sscanf(o, "[%lld, %d, %d]", &l, &t, &cp) != 3) break;
+        c.bin[c.nb++] = {(int64_t)l, t, cp};
+        q = strchr(o, ']') + 1;
+    }
+    return c.nb > 0;
+}
+
+std::string cache_path()
+{
+    const char *env = getenv("GRB_B200_TUNE_CACHE");
+    if (env && *env) return env;
+    Dl_info info;
+    if (dladdr((void *)&cache_path, &info) && info.dli_fname) {
+        std::string f = info.dli_fname;
+        size_t slash = f.rfind('/');
+        if (slash != std::string::npos) return f.substr(0, slash) + "/tune_cache.json";
+    }
+    return "tune_cache.json";
+}
+
+std::string batch_key(const grb_b200_batch_s *B)
+{
+    // size class: log2 of the average flops per row and of the row count
+    int64_t rows = B->A.nrows;
+    double nnz_per_row = rows ? (double)B->A.nnz / rows : 0;
+    int fr = 0;
+    for (double f = nnz_per_row * nnz_per_row; f > 1 && fr < 40; f /= 2) fr++;
+    int rr = 0;
+    for (int64_t r = rows; r > 1 && rr < 40; r >>= 1) rr++;
+    return std::to_string(B->sr.add) + ":" + std::to_string(B->sr.mult) + ":" +
+           std::to_string(B->sr.type) + ":f" + std::to_string(fr) + ":r" + std::to_string(rr);
+}
+
+std::mutex g_cache_mu;
+
+bool cache_lookup(const std::string &key, SaxpyConfig &c, double *ms)
+{
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    FILE *f = fopen(cache_path().c_str(), "r");
+    if (!f) return false;
+    std::string text;
+    char buf[4096];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, n);
+    fclose(f);
+    std::string pat = "\"" + key + "\":";
+    size_t pos = text.find(pat);
+    if (pos == std::string::npos) return false;
+    const char *entry = text.c_str() + pos + pat.size();
+    const char *m = strstr(entry, "\"ms\"");
+    const char *eol = strchr(entry, '\n');
+    if (ms) *ms = (m && (!eol || m < eol)) ? atof(strchr(m, ':') + 1) : 0.0;
+    return config_from_json(entry, c);
+}
+
+void cache_store(const std::string &key, const SaxpyConfig &c, double ms)
+{
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    std::string path = cache_path();
+    // one entry per line: "key": {...}, "ms": x
+    std::vector<std::string> lines;
+    FILE *f = fopen(path.c_str(), "r");
+    if (f) {
+        char line[2048];
+        while (fgets(line, sizeof(line), f)) {
+            std::string l = line;
+            if (l.find("\"" + key + "\":") != std::string::npos) continue;
+            if (l.find("\":") != std::string::npos && l[0] == ' ') {
+                while (!l.empty() && (l.back() == '\n' || l.back() == ',')) l.pop_back();
+                lines.push_back(l);
+            }
+        }
+        fclose(f);
+    }
+    char tail[64];
+    snprintf(tail, sizeof(tail), ", \"ms\": %.4f}", ms);
+    std::string cfg = config_to_json(c);
+    cfg.pop_back();                                     // reopen the object
+    lines.push_back("  \"" + key + "\": " + cfg + tail);
+    f = fopen(path.c_str(), "w");
+    if (!f) return;
+    fprintf(f, "{\n");
+    for (size_t i = 0; i < lines.size(); i++)
+        fprintf(f, "%s%s\n", lines[i].c_str(), i + 1 < lines.size() ? "," : "");
+    fprintf(f, "}\n");
+    fclose(f);
+}
+
+// (re)build the plan and output buffers of a batch for a configuration
+int batch_prepare(grb_b200_batch_s *B, const SaxpyConfig &cfg)
+{
+    cudaStream_t s = B->s;
+    if (B->gexec) { cudaGraphExecDestroy(B->gexec); B->gexec = nullptr; }
+    if (B->graph) { cudaGraphDestroy(B->graph); B->graph = nullptr; }
+    if (B->plan) { saxpy_plan_free(B->plan, s); B->plan = nullptr; }
+    dev_free(B->C, s);
+    const DevCSR &Bop = B->b_is_a ? B->A : B->B;
+    int info = saxpy_plan_create(&B->plan, nullptr, false, B->A, Bop, B->sr, cfg, s);
+    if (info != SUCCESS) return info;
+    B->cfg = cfg;
+    const int64_t cap = saxpy_plan_capacity(B->plan), m = B->A.nrows;
+    B->C = DevCSR();
+    B->C.nrows = m; B->C.ncols = Bop.ncols; B->C.type = B->sr.type;
+    B->C.p = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
+    B->C.j = (int32_t *)dalloc((size_t)(cap + 1) * 4, s);
+    B->C.x = dalloc((size_t)(cap + 1) * B->zsize, s);
+    if (!B->C.p || !B->C.j || !B->C.x) return OUT_OF_MEMORY;
+    return cuda_to_info(cudaStreamSynchronize(s));
+}
+
+int batch_exec_eager(grb_b200_batch_s *B)
+{
+    const DevCSR &Bop = B->b_is_a ? B->A : B->B;
+    return saxpy_plan_exec(B->plan, nullptr, B->A, Bop, B->C.p, B->C.j, B->C.x,
+                           B->nnz_d, B->s);
+}
+
+int batch_capture(grb_b200_batch_s *B)
+{
+    cudaError_t e = cudaStreamBeginCapture(B->s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_to_info(e);
+    int info = batch_exec_eager(B);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(B->s, &g);
+    if (info != SUCCESS || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return info != SUCCESS ? info : cuda_to_info(e);
+    }
+    e = cudaGraphInstantiate(&B->gexec, g, 0);
+    if (e != cudaSuccess) { cudaGraphDestroy(g); cudaGetLastError(); return cuda_to_info(e); }
+    B->graph = g;
+    return SUCCESS;
+}
+
+double time_exec(grb_b200_batch_s *B, int reps)
+{
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    batch_exec_eager(B);                               // warm-up
+    cudaEventRecord(a, B->s);
+    for (int r = 0; r < reps; r++) batch_exec_eager(B);
+    cudaEventRecord(b, B->s);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms / reps;
+}
+
+}  // namespace
+
+extern "C" {
+
+int grb_b200_batch_create(grb_b200_batch *Bout, int count, const int64_t *a_nrows,
+                          const int64_t *a_ncols, const int64_t *Ap, const int64_t *Aj,
+                          const void *Ax, const int64_t *b_ncols, const int64_t *Bp,
+                          const int64_t *Bj, const void *Bx,
+                          const grb_b200_semiring *semiring)
+{
+    if (!Bout || !a_nrows || !a_ncols || !Ap || !Aj || !semiring) return NULL_POINTER;
+    if (count <= 0 || Ap[0] != 0 || (Bp && Bp[0] != 0)) return INVALID_VALUE;
+    int info = init_device();
+    if (info != SUCCESS) return info;
+    SemiringCode sr{semiring->add_opcode, semiring->mult_opcode, semiring->type};
+    if (!semiring_supported(sr)) return NO_VALUE;
+    const bool b_is_a = (Bp == nullptr);
+    grb_b200_batch_s *B = new grb_b200_batch_s();
+    B->count = count;
+    B->sr = sr;
+    B->zsize = type_size(sr.type);
+    B->b_is_a = b_is_a;
+    B->am.assign(a_nrows, a_nrows + count);
+    B->an.assign(a_ncols, a_ncols + count);
+    B->bn.assign(b_is_a ? a_ncols : b_ncols, (b_is_a ? a_ncols : b_ncols) + count);
+    if (b_is_a)
+        for (int k = 0; k < count; k++)
+            if (B->am[k] != B->an[k]) { delete B; return DIMENSION_MISMATCH; }
+    cudaStreamCreateWithFlags(&B->s, cudaStreamNonBlocking);
+    std::vector<int64_t> eo;
+    info = build_blockdiag(B->A, count, B->am, B->an, Ap, Aj, Ax, B->zsize, Ax == nullptr,
+                           sr.type, B->roff, B->acoff, B->annz_off, B->s);
+    if (info == SUCCESS && Ax == nullptr) {
+        // pattern input: iso one of the type
+        unsigned char one[8] = {0};
+        if (sr.type == T_FP32) { float f = 1; memcpy(one, &f, 4); }
+        else if (sr.type == T_FP64) { double d = 1; memcpy(one, &d, 8); }
+        else one[0] = 1;
+        cudaMemcpyAsync(B->A.x, one, B->zsize, cudaMemcpyHostToDevice, B->s);
+    }
+    if (info == SUCCESS && !b_is_a) {
+        std::vector<int64_t> broff;
+        info = build_blockdiag(B->B, count, B->an, B->bn, Bp, Bj, Bx, B->zsize,
+                               Bx == nullptr, sr.type, broff, B->bcoff, B->bnnz_off, B->s);
+    } else {
+        B->bcoff = B->acoff;
+    }
+    B->nnz_d = (int64_t *)dalloc(8, B->s);
+    if (info == SUCCESS && !B->nnz_d) info = OUT_OF_MEMORY;
+    if (info == SUCCESS) info = batch_prepare(B, saxpy_default_config());
+    if (info != SUCCESS) { grb_b200_batch_free(&B); return info; }
+    *Bout = B;
+    return SUCCESS;
+}
+
+int grb_b200_batch_tune(grb_b200_batch B, bool use_cache, double *best_ms)
+{
+    if (!B) return NULL_POINTER;
+    const std::string key = batch_key(B);
+    SaxpyConfig best;
+    double cached_ms = 0;
+    if (use_cache && cache_lookup(key, best, &cached_ms) && saxpy_config_valid(best, B->zsize)) {
+        // cached: take the configuration without timing it again
+        int info = batch_prepare(B, best);
+        if (info != SUCCESS) return info;
+        B->tuned = true;
+        B->tuned_ms = cached_ms;
+        if (best_ms) *best_ms = B->tuned_ms;
+        return SUCCESS;
+    }
+    double best_t = 1e30;
+    bool found = false;
+    for (const SaxpyConfig &c : candidates()) {
+        if (!saxpy_config_valid(c, B->zsize)) continue;
+        if (batch_prepare(B, c) != SUCCESS) continue;
+        const double t = time_exec(B, 3);
+        if (t < best_t) { best_t = t; best = c; found = true; }
+    }
+    if (!found) return PANIC;
+    int info = batch_prepare(B, best);
+    if (info != SUCCESS) return info;
+    B->tuned = true;
+    B->tuned_ms = best_t;
+    cache_store(key, best, best_t);
+    if (best_ms) *best_ms = best_t;
+    return SUCCESS;
+}
+
+int grb_b200_batch_run(grb_b200_batch B, bool use_graph)
+{
+    if (!B) return NULL_POINTER;
+    int info = SUCCESS;
+    // the caller's stream for this thread (grb_b200_set_stream), else the batch's
+    cudaStream_t st = thread_stream() ? thread_stream() : B->s;
+    if (st != B->s) {
+        // order the batch's own stream (setup work) before the caller's
+        cudaStreamSynchronize(B->s);
+    }
+    if (use_graph) {
+        if (!B->gexec) info = batch_capture(B);
+        if (info != SUCCESS) return info;
+        cudaError_t e = cudaGraphLaunch(B->gexec, st);
+        if (e != cudaSuccess) return cuda_to_info(e);
+    } else {
+        cudaStream_t keep = B->s;
+        B->s = st;
+        info = batch_exec_eager(B);
+        B->s = keep;
+        if (info != SUCCESS) return info;
+    }
+    int64_t nnz = 0;
+    cudaMemcpyAsync(&nnz, B->nnz_d, 8, cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_to_info(e);
+    B->last_nnz = nnz;
+    return SUCCESS;
+}
+
+int grb_b200_batch_enqueue(grb_b200_batch B, void *stream)
+{
+    // graph replay on the caller's stream, no host synchronisation
+    if (!B) return NULL_POINTER;
+    if (!B->gexec) {
+        int info = batch_capture(B);
+        if (info != SUCCESS) return info;
+    }
+    return cuda_to_info(cudaGraphLaunch(B->gexec, stream ? (cudaStream_t)stream : B->s));
+}
+
+int grb_b200_batch_info(grb_b200_batch B, int64_t *total_rows, int64_t *nnz_c,
+                        int64_t *capacity, int *nbins, double *tuned_ms,
+                        int *graph_kernels)
+{
+    if (!B) return NULL_POINTER;
+    if (graph_kernels) *graph_kernels = 0;
+    if (graph_kernels && B->graph) {
+        // kernel launches in the captured numeric phase
+        size_t n = 0;
+        cudaGraphGetNodes(B->graph, nullptr, &n);
+        std::vector<cudaGraphNode_t> nodes(n);
+        cudaGraphGetNodes(B->graph, nodes.data(), &n);
+        int k = 0;
+        for (size_t q = 0; q < n; q++) {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+        }
+        *graph_kernels = k;
+    }
+    if (total_rows) *total_rows = B->A.nrows;
+    if (nnz_c) *nnz_c = B->last_nnz;
+    if (capacity) *capacity = saxpy_plan_capacity(B->plan);
+    if (nbins) *nbins = B->cfg.nb;
+    if (tuned_ms) *tuned_ms = B->tuned ? B->tuned_ms : -1.0;
+    return SUCCESS;
+}
+
+int grb_b200_batch_result(grb_b200_batch B, int64_t **Cp, int64_t **Cj, void **Cx,
+                          int64_t *nnz_per_instance)
+{
+    if (!B || !Cp || !Cj || !Cx) return NULL_POINTER;
+    cudaStream_t s = B->s;
+    const int count = B->count;
+    const int64_t m = B->A.nrows;
+    int64_t nnz = 0;
+    cudaMemcpyAsync(&nnz, B->C.p + m, 4, cudaMemcpyDeviceToHost, s);   // int32
+    cudaStreamSynchronize(s);
+    nnz = (int64_t)(int32_t)nnz;
+    std::vector<int64_t> pout(count + 1, 0);
+    for (int k = 0; k < count; k++) pout[k + 1] = pout[k] + B->am[k] + 1;
+    int64_t *dn = upload_vec(B->am, s), *dr = upload_vec(B->roff, s);
+    int64_t *dc = upload_vec(B->bcoff, s), *dpo = upload_vec(pout, s);
+    int64_t *dP = (int64_t *)dalloc((size_t)pout[count] * 8 + 8, s);
+    int64_t *dJ = (int64_t *)dalloc((size_t)(nnz + 1) * 8, s);
+    *Cp = (int64_t *)malloc((size_t)pout[count] * 8 + 8);
+    *Cj = (int64_t *)malloc((size_t)(nnz + 1) * 8);
+    *Cx = malloc((size_t)(nnz + 1) * B->zsize);
+    int info = SUCCESS;
+    if (!dn || !dr || !dc || !dpo || !dP || !dJ || !*Cp || !*Cj || !*Cx) info = OUT_OF_MEMORY;
+    if (info == SUCCESS) {
+        k_split<<<count < 65535 ? count : 65535, 128, 0, s>>>(count, dn, dr, dc, dpo,
+            B->C.p, B->C.j, dP, dJ);
+        cudaMemcpyAsync(*Cp, dP, (size_t)pout[count] * 8, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(*Cj, dJ, (size_t)nnz * 8, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(*Cx, B->C.x, (size_t)nnz * B->zsize, cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) info = cuda_to_info(e);
+    }
+    dfree(dn, s); dfree(dr, s); dfree(dc, s); dfree(dpo, s); dfree(dP, s); dfree(dJ, s);
+    if (info == SUCCESS && nnz_per_instance)
+        for (int k = 0; k < count; k++)
+            nnz_per_instance[k] = (*Cp)[pout[k] + B->am[k]] - (*Cp)[pout[k]];
+    if (info != SUCCESS) {
+        free(*Cp); free(*Cj); free(*Cx);
+        *Cp = nullptr; *Cj = nullptr; *Cx = nullptr;
+    }
+    return info;
+}
+
+int grb_b200_batch_free(grb_b200_batch *Bp)
+{
+    if (!Bp || !*Bp) return SUCCESS;
+    grb_b200_batch_s *B = *Bp;
+    cudaStream_t s = B->s;
+    if (B->gexec) cudaGraphExecDestroy(B->gexec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    if (B->plan) saxpy_plan_free(B->plan, s);
+    dev_free(B->A, s);
+    dev_free(B->B, s);
+    dev_free(B->C, s);
+    dfree(B->nnz_d, s);
+    if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+    delete B;
+    *Bp = nullptr;
+    return SUCCESS;
+}
+
+}  // extern "C"

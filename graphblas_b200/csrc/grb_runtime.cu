@@ -326,6 +326,38 @@ int scan_exclusive_i64(const int64_t *in, int64_t *out, int64_t n, cudaStream_t 
     return scan_impl<int64_t>(in, out, n, s);
 }
 
+// the same scan with caller-provided workspace (no allocation, no host sync:
+// usable inside CUDA graph capture)
+size_t scan_ws_elems(int64_t n)
+{
+    size_t tot = 0;
+    while (n > 1) {
+        int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+        tot += (size_t)nb + 1;
+        if (nb <= 1) break;
+        n = nb;
+    }
+    return tot + 2;
+}
+
+template <typename T>
+static void scan_ws_impl(const T *in, int64_t *out, int64_t n, int64_t *ws, cudaStream_t s)
+{
+    if (n <= 0) return;
+    int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    int64_t *totals = ws;
+    k_scan_totals<T><<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, totals);
+    if (nb > 1) scan_ws_impl<int64_t>(totals, totals, nb, ws + nb + 1, s);
+    else cudaMemsetAsync(totals, 0, 8, s);
+    k_scan_tiles<T><<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, totals);
+}
+
+void scan_exclusive_i64_ws(const int64_t *in, int64_t *out, int64_t n, int64_t *ws,
+                           cudaStream_t s)
+{
+    scan_ws_impl<int64_t>(in, out, n, ws, s);
+}
+
 int scan_exclusive_i32_to_i64(const int32_t *in, int64_t *out, int64_t n,
                               cudaStream_t s)
 {

@@ -103,6 +103,10 @@ int scan_exclusive_i64(const int64_t *in, int64_t *out, int64_t n,
                        cudaStream_t s);
 int scan_exclusive_i32_to_i64(const int32_t *in, int64_t *out, int64_t n,
                               cudaStream_t s);
+// allocation-free variant: ws holds scan_ws_elems(n) int64 values
+size_t scan_ws_elems(int64_t n);
+void scan_exclusive_i64_ws(const int64_t *in, int64_t *out, int64_t n, int64_t *ws,
+                           cudaStream_t s);
 
 // ---- operations (device matrices) ----
 

@@ -33,10 +33,12 @@
 
 #include <cstdio>
 #include <cstring>
-#include "grb_runtime.h"
+#include "grb_saxpy3.h"
 #include "grb_semirings.h"
 
 namespace grb {
+
+static constexpr int MAX_SMEM_BINS = 6;
 
 // slot states
 static constexpr uint8_t S_EMPTY = 0, S_ALLOWED = 1, S_SET = 2, S_FORBID = 3;
@@ -76,15 +78,13 @@ __global__ void k_flops(const int32_t *__restrict__ Ap, const int32_t *__restric
     }
 }
 
-// bin of a row: 0 empty, 1..NB_SMEM smem hash bins, NB_SMEM+1 heavy
-static constexpr int NB_SMEM = 4;
-// max flops (+ mask entries) handled by each shared-memory bin
-__constant__ int64_t c_bin_limit[NB_SMEM] = {64, 256, 1024, 4096};
+// bin of a row: 0 empty, 1..nb shared-memory hash bins (by the config's
+// limits on flops + mask entries), nb+1 heavy (dense accumulator)
+struct BinLimits { int nb; int64_t limit[MAX_SMEM_BINS]; };
 
 __global__ void k_bin_rows(const int64_t *__restrict__ flops,
                            const int32_t *__restrict__ Mp, bool has_mask,
-                           int64_t nrows, int *__restrict__ bin_count,
-                           int32_t *__restrict__ bin_rows_scratch,
+                           int64_t nrows, BinLimits lim, int *__restrict__ bin_count,
                            int8_t *__restrict__ row_bin)
 {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -95,9 +95,9 @@ __global__ void k_bin_rows(const int64_t *__restrict__ flops,
         if (f == 0) b = 0;
         else {
             int64_t need = f + (has_mask ? (int64_t)(Mp[r + 1] - Mp[r]) : 0);
-            b = NB_SMEM + 1;
-            for (int q = 0; q < NB_SMEM; q++)
-                if (need <= c_bin_limit[q]) { b = q + 1; break; }
+            b = lim.nb + 1;
+            for (int q = 0; q < lim.nb; q++)
+                if (need <= lim.limit[q]) { b = q + 1; break; }
         }
         row_bin[r] = (int8_t)b;
         if (b > 0) atomicAdd(&bin_count[b], 1);
@@ -147,20 +147,17 @@ __device__ __forceinline__ uint32_t hslot(int32_t j, uint32_t mask)
 // phase 3a: shared-memory hash rows
 // ---------------------------------------------------------------------------
 
-template <class SR, int TPR, int CAP>
-struct HashLayout {
-    using Z = typename SR::z_t;
-    static constexpr int GROUPS = (TPR >= 256) ? 1 : (128 / TPR);   // per block
-    static constexpr int THREADS = GROUPS * TPR;
-    // per group: keys[CAP] int32, vals[CAP] Z, state[CAP] u8
-    static constexpr size_t GROUP_BYTES =
-        ((CAP * 4 + CAP * sizeof(Z) + CAP + 15) / 16) * 16;
-    static constexpr size_t BYTES = GROUP_BYTES * GROUPS;
-};
+// shared memory of one row group: keys[cap] int32, vals[cap] Z, state[cap] u8
+template <typename Z> __host__ __device__ inline size_t group_bytes(int cap)
+{
+    return ((size_t)cap * (4 + sizeof(Z) + 1) + 15) / 16 * 16;
+}
 
-template <class SR, int TPR, int CAP>
-__global__ void __launch_bounds__(HashLayout<SR, TPR, CAP>::THREADS)
-k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin,
+// A group of TPR threads (TPR = 4..32 inside a 128-thread block, or the whole
+// 256-thread block when BLOCK) owns one row and one hash table of cap slots.
+template <class SR, bool BLOCK>
+__global__ void __launch_bounds__(BLOCK ? 256 : 128)
+k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin, int tpr_log2, int cap,
              const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
              const void *__restrict__ Ax, bool a_iso,
              const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
@@ -172,21 +169,27 @@ k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin,
              int32_t *__restrict__ row_cnt)
 {
     using Z = typename SR::z_t;
-    using L = HashLayout<SR, TPR, CAP>;
     extern __shared__ __align__(16) unsigned char smem[];
-    const int g = threadIdx.x / TPR;
-    const int t = threadIdx.x % TPR;
-    unsigned char *base = smem + (size_t)g * L::GROUP_BYTES;
+    __shared__ int s_cnt[32];
+    const int TPR = BLOCK ? (int)blockDim.x : (1 << tpr_log2);
+    const int G = BLOCK ? 1 : ((int)blockDim.x >> tpr_log2);
+    const int g = BLOCK ? 0 : ((int)threadIdx.x >> tpr_log2);
+    const int t = BLOCK ? (int)threadIdx.x : ((int)threadIdx.x & (TPR - 1));
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned gmask = (TPR >= 32) ? 0xffffffffu
+                         : (((1u << TPR) - 1u) << ((lane >> tpr_log2) << tpr_log2));
+    auto gsync = [&]() { if (BLOCK) __syncthreads(); else __syncwarp(gmask); };
+    unsigned char *base = smem + (size_t)g * group_bytes<Z>(cap);
     int32_t *keys = (int32_t *)base;
-    Z *vals = (Z *)(base + CAP * 4);
-    uint8_t *state = (uint8_t *)(base + CAP * 4 + CAP * sizeof(Z));
-    const uint32_t hmask = CAP - 1;
+    Z *vals = (Z *)(base + (size_t)cap * 4);
+    uint8_t *state = (uint8_t *)(base + (size_t)cap * (4 + sizeof(Z)));
+    const uint32_t hmask = (uint32_t)cap - 1;
 
-    for (int64_t rb = (int64_t)blockIdx.x * L::GROUPS + g; rb < nrows_bin;
-         rb += (int64_t)gridDim.x * L::GROUPS) {
+    for (int64_t rb = (int64_t)blockIdx.x * G + g; rb < nrows_bin;
+         rb += (int64_t)gridDim.x * G) {
         const int32_t i = rows[rb];
-        for (int s = t; s < CAP; s += TPR) { keys[s] = -1; state[s] = S_EMPTY; }
-        group_sync<TPR>();
+        for (int s = t; s < cap; s += TPR) { keys[s] = -1; state[s] = S_EMPTY; }
+        gsync();
         // scatter the mask row
         if (has_mask) {
             const uint8_t st = mask_comp ? S_FORBID : S_ALLOWED;
@@ -199,7 +202,7 @@ k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin,
                     h = (h + 1) & hmask;
                 }
             }
-            group_sync<TPR>();
+            gsync();
         }
         // k loop in ascending order; threads split B(k,:)
         const int32_t pa0 = Ap[i], pa1 = Ap[i + 1];
@@ -240,22 +243,21 @@ k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin,
                     state[found] = S_SET;
                 }
             }
-            group_sync<TPR>();
+            gsync();
         }
-        // gather the set slots into the row's output slot, then sort them
-        // by column in the (now free) table memory with a bitonic network
+        // gather the set slots into the row's output slot, then sort them by
+        // column in the (now free) table memory with a bitonic network
         const int64_t off = slot_off[i];
-        __shared__ int s_cnt[L::GROUPS];
         if (t == 0) s_cnt[g] = 0;
-        group_sync<TPR>();
-        for (int s = t; s < CAP; s += TPR) {
+        gsync();
+        for (int s = t; s < cap; s += TPR) {
             if (state[s] == S_SET) {
                 int q = atomicAdd(&s_cnt[g], 1);
                 Tj[off + q] = keys[s];
                 Tx[off + q] = vals[s];
             }
         }
-        group_sync<TPR>();
+        gsync();
         const int cnt = s_cnt[g];
         int n2 = 1;
         while (n2 < cnt) n2 <<= 1;
@@ -263,7 +265,7 @@ k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin,
             if (q < cnt) { keys[q] = Tj[off + q]; vals[q] = Tx[off + q]; }
             else keys[q] = INT32_MAX;
         }
-        group_sync<TPR>();
+        gsync();
         for (int size = 2; size <= n2; size <<= 1) {
             for (int stride = size >> 1; stride > 0; stride >>= 1) {
                 for (int q = t; q < n2; q += TPR) {
@@ -277,12 +279,12 @@ k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin,
                         }
                     }
                 }
-                group_sync<TPR>();
+                gsync();
             }
         }
         for (int q = t; q < cnt; q += TPR) { Tj[off + q] = keys[q]; Tx[off + q] = vals[q]; }
         if (t == 0) row_cnt[i] = cnt;
-        group_sync<TPR>();
+        gsync();
     }
 }
 
@@ -619,11 +621,85 @@ k_dense_gather(const int32_t *__restrict__ rows, int nrows_bin, int64_t ncols,
     }
 }
 
+// grid-wide ordered compaction of dense heavy rows: blocks own 4096-column
+// chunks of a row (grid.y = row); one pass counts, a scan places the chunks,
+// a second pass writes (so a single long row uses the whole GPU)
+static constexpr int DG_THREADS = 256, DG_ITEMS = 16, DG_CHUNK = DG_THREADS * DG_ITEMS;
+
+__global__ void __launch_bounds__(DG_THREADS)
+k_dense_count(int nrows_bin, int64_t ncols, int cblocks, const int64_t *__restrict__ flag_all,
+              int64_t *__restrict__ cnt)
+{
+    __shared__ int s_w[DG_THREADS / 32];
+    for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
+        const int64_t *flag = flag_all + rb * ncols;
+        const int64_t c0 = (int64_t)blockIdx.x * DG_CHUNK;
+        int c = 0;
+        for (int it = 0; it < DG_ITEMS; it++) {
+            const int64_t j = c0 + (int64_t)it * DG_THREADS + threadIdx.x;
+            c += (j < ncols && flag[j] == 3);
+        }
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+        if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            for (int q = 0; q < DG_THREADS / 32; q++) t += s_w[q];
+            cnt[rb * cblocks + blockIdx.x] = t;
+        }
+        __syncthreads();
+    }
+}
+
+template <class SR>
+__global__ void __launch_bounds__(DG_THREADS)
+k_dense_write(const int32_t *__restrict__ rows, int nrows_bin, int64_t ncols, int cblocks,
+              const int64_t *__restrict__ flag_all,
+              const typename SR::z_t *__restrict__ val_all,
+              const int64_t *__restrict__ off /* scanned counts */,
+              const int64_t *__restrict__ slot_off, int32_t *__restrict__ Tj,
+              typename SR::z_t *__restrict__ Tx, int32_t *__restrict__ row_cnt)
+{
+    __shared__ int s_w[DG_THREADS / 32];
+    __shared__ int s_base;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
+        const int32_t i = rows[rb];
+        const int64_t *flag = flag_all + rb * ncols;
+        const typename SR::z_t *val = val_all + rb * ncols;
+        const int64_t row0 = off[rb * cblocks];
+        int64_t pos = slot_off[i] + (off[rb * cblocks + blockIdx.x] - row0);
+        const int64_t c0 = (int64_t)blockIdx.x * DG_CHUNK;
+        for (int it = 0; it < DG_ITEMS; it++) {
+            const int64_t j = c0 + (int64_t)it * DG_THREADS + threadIdx.x;
+            const bool on = j < ncols && flag[j] == 3;
+            const unsigned m = __ballot_sync(0xffffffffu, on);
+            if (lane == 0) s_w[w] = __popc(m);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int acc = 0;
+                for (int q = 0; q < DG_THREADS / 32; q++) { int c = s_w[q]; s_w[q] = acc; acc += c; }
+                s_base = acc;
+            }
+            __syncthreads();
+            if (on) {
+                const int64_t q = pos + s_w[w] + __popc(m & ((1u << lane) - 1));
+                Tj[q] = (int32_t)j;
+                Tx[q] = val[j];
+            }
+            pos += s_base;
+            __syncthreads();
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            row_cnt[i] = (int32_t)(off[(rb + 1) * cblocks] - row0);
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------------------
-// phase 4: sort each row's slot by column and pack the slots into CSR
+// phase 4: pack each row's (sorted) slot into CSR
 // ---------------------------------------------------------------------------
 
-// copy each row's (sorted) slot to its place in C (one warp per row)
 template <typename Z>
 __global__ void __launch_bounds__(256)
 k_pack(int64_t nrows, const int64_t *__restrict__ slot_off,
@@ -649,16 +725,101 @@ __global__ void k_cnt_to_i64(const int32_t *__restrict__ cnt, const int8_t *__re
     for (; t < n; t += stride) out[t] = row_bin[t] ? (int64_t)cnt[t] : 0;
 }
 
-__global__ void k_i64_to_i32_p(const int64_t *__restrict__ in, int32_t *__restrict__ out, int64_t n)
+__global__ void k_i64_to_i32_p(const int64_t *__restrict__ in, int32_t *__restrict__ out,
+                               int64_t n, int64_t *__restrict__ nnz64)
 {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; t < n; t += stride) out[t] = (int32_t)in[t];
+    if (nnz64 && t == 0) *nnz64 = in[n - 1];
+}
+
+__global__ void k_copy_i64(const int64_t *__restrict__ in, int64_t *__restrict__ out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) *out = *in;
 }
 
 // ---------------------------------------------------------------------------
-// driver
+// configuration, plan, execution
 // ---------------------------------------------------------------------------
+
+SaxpyConfig saxpy_default_config()
+{
+    SaxpyConfig c;
+    c.nb = 4;
+    c.bin[0] = {64, 8, 128};
+    c.bin[1] = {256, 32, 512};
+    c.bin[2] = {1024, 32, 2048};
+    c.bin[3] = {4096, 256, 8192};
+    c.blocks_per_sm = 16;
+    return c;
+}
+
+// raise a kernel's dynamic shared-memory limit to what the device allows
+// beside the kernel's static shared memory
+static void allow_dynamic_smem(const void *fn)
+{
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) { cudaGetLastError(); return; }
+    const int dyn = (int)runtime().smem_optin - (int)fa.sharedSizeBytes;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess)
+        cudaGetLastError();
+}
+
+static size_t bin_smem(const BinSpec &b, size_t zsize)
+{
+    const size_t gb = ((size_t)b.cap * (4 + zsize + 1) + 15) / 16 * 16;
+    return b.tpr >= 256 ? gb : gb * (128 / b.tpr);
+}
+
+bool saxpy_config_valid(const SaxpyConfig &cfg, size_t zsize)
+{
+    if (cfg.nb < 0 || cfg.nb > MAX_SMEM_BINS) return false;
+    int64_t prev = 0;
+    for (int q = 0; q < cfg.nb; q++) {
+        const BinSpec &b = cfg.bin[q];
+        if (b.limit <= prev || (int64_t)b.cap < 2 * b.limit) return false;
+        if ((b.cap & (b.cap - 1)) != 0) return false;
+        if (!(b.tpr == 4 || b.tpr == 8 || b.tpr == 16 || b.tpr == 32 || b.tpr == 256)) return false;
+        if (bin_smem(b, zsize) + 256 > runtime().smem_optin) return false;
+        prev = b.limit;
+    }
+    return cfg.blocks_per_sm >= 1 && cfg.blocks_per_sm <= 64;
+}
+
+struct SaxpyPlan {
+    SemiringCode sr;
+    SaxpyConfig cfg;
+    size_t zsize = 8;
+    bool order_free = false;
+    int64_t m = 0, ncols = 0;
+    bool has_mask = false, mask_comp = false;
+    int64_t total_cap = 0;
+    int h_bins[MAX_SMEM_BINS + 2] = {0};
+    int h_start[MAX_SMEM_BINS + 2] = {0};
+    // device buffers
+    int64_t *flops = nullptr, *slot_off = nullptr, *Cp64 = nullptr, *scan_ws = nullptr;
+    int8_t *row_bin = nullptr;
+    int32_t *bin_rows = nullptr, *row_cnt = nullptr, *Tj = nullptr;
+    void *Tx = nullptr;
+    int *bins = nullptr;
+    int64_t heavy_chunk = 0;
+    int64_t *flag = nullptr;
+    void *val = nullptr;
+    int64_t *dg_cnt = nullptr, *dg_ws = nullptr;   // dense-row compaction
+};
+
+void saxpy_plan_free(SaxpyPlan *P, cudaStream_t s)
+{
+    if (!P) return;
+    dfree(P->flops, s); dfree(P->slot_off, s); dfree(P->Cp64, s); dfree(P->scan_ws, s);
+    dfree(P->row_bin, s); dfree(P->bin_rows, s); dfree(P->row_cnt, s); dfree(P->Tj, s);
+    dfree(P->Tx, s); dfree(P->bins, s); dfree(P->flag, s); dfree(P->val, s);
+    dfree(P->dg_cnt, s); dfree(P->dg_ws, s);
+    delete P;
+}
+
+int64_t saxpy_plan_capacity(const SaxpyPlan *P) { return P->total_cap; }
 
 static inline int nblocks(int64_t n, int threads, int per_sm = 8)
 {
@@ -668,149 +829,224 @@ static inline int nblocks(int64_t n, int threads, int per_sm = 8)
     return b < 1 ? 1 : (int)b;
 }
 
-template <class SR, int TPR, int CAP>
-static void launch_hash_bin(const int32_t *rows, int cnt, const DevCSR &A,
-                            const DevCSR &B, const DevCSR *M, bool mask_comp,
-                            const int64_t *slot_off, int32_t *Tj,
-                            typename SR::z_t *Tx, int32_t *row_cnt, cudaStream_t s)
-{
-    using L = HashLayout<SR, TPR, CAP>;
-    if (cnt == 0) return;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_saxpy_hash<SR, TPR, CAP>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
-        attr_set = true;
-    }
-    int64_t groups_needed = cnt;
-    int blocks = (int)((groups_needed + L::GROUPS - 1) / L::GROUPS);
-    int cap = runtime().num_sms * 16;
-    if (blocks > cap) blocks = cap;
-    k_saxpy_hash<SR, TPR, CAP><<<blocks, L::THREADS, L::BYTES, s>>>(
-        rows, cnt, A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
-        M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, mask_comp,
-        slot_off, Tj, Tx, row_cnt);
-}
-
 template <class SR>
-static int saxpy3_t(DevCSR &C, const DevCSR *M, bool mask_comp,
-                    const DevCSR &A, const DevCSR &B, cudaStream_t s)
+static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A,
+                  const DevCSR &B, cudaStream_t s)
 {
     using Z = typename SR::z_t;
     const int64_t m = A.nrows, ncols = B.ncols;
-    Scratch ws(s);
-    int64_t *flops = ws.get<int64_t>(m + 1);
-    int64_t *capv = ws.get<int64_t>(m + 1);
-    int8_t *row_bin = ws.get<int8_t>(m + 1);
-    int *bins = ws.get<int>(64);
-    int32_t *bin_rows = ws.get<int32_t>(m + 1);
-    int32_t *row_cnt = ws.get<int32_t>(m + 1);
-    if (ws.failed) return OUT_OF_MEMORY;
+    P->zsize = sizeof(Z);
+    P->order_free = SR::order_free;
+    P->m = m; P->ncols = ncols;
+    P->has_mask = M != nullptr; P->mask_comp = mask_comp;
+    P->flops = (int64_t *)dalloc((size_t)(m + 1) * 8, s);
+    P->slot_off = (int64_t *)dalloc((size_t)(m + 1) * 8, s);
+    P->Cp64 = (int64_t *)dalloc((size_t)(m + 2) * 8, s);
+    P->scan_ws = (int64_t *)dalloc(scan_ws_elems(m + 1) * 8, s);
+    P->row_bin = (int8_t *)dalloc((size_t)(m + 1), s);
+    P->bin_rows = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
+    P->row_cnt = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
+    P->bins = (int *)dalloc(64 * sizeof(int), s);
+    if (!P->flops || !P->slot_off || !P->Cp64 || !P->scan_ws || !P->row_bin ||
+        !P->bin_rows || !P->row_cnt || !P->bins)
+        return OUT_OF_MEMORY;
     const bool mask_bounds = (M != nullptr) && !mask_comp;
     if (m > 0)
         k_flops<<<nblocks(m * 32, 256), 256, 0, s>>>(A.p, A.j, B.p,
-            M ? M->p : nullptr, mask_bounds, m, ncols, flops, capv);
-    cudaMemsetAsync(bins, 0, 64 * sizeof(int), s);
+            M ? M->p : nullptr, mask_bounds, m, ncols, P->flops, P->slot_off);
+    cudaMemsetAsync(P->bins, 0, 64 * sizeof(int), s);
+    BinLimits lim;
+    lim.nb = P->cfg.nb;
+    for (int q = 0; q < P->cfg.nb; q++) lim.limit[q] = P->cfg.bin[q].limit;
     if (m > 0)
-        k_bin_rows<<<nblocks(m, 256), 256, 0, s>>>(flops, M ? M->p : nullptr,
-            M != nullptr, m, bins, nullptr, row_bin);
-    // capacities -> slot offsets
-    cudaMemsetAsync(capv + m, 0, 8, s);
-    int info = scan_exclusive_i64(capv, capv, m + 1, s);
-    if (info != SUCCESS) return info;
-    int h_bins[NB_SMEM + 2] = {0};
+        k_bin_rows<<<nblocks(m, 256), 256, 0, s>>>(P->flops, M ? M->p : nullptr,
+            M != nullptr, m, lim, P->bins, P->row_bin);
+    cudaMemsetAsync(P->slot_off + m, 0, 8, s);
+    scan_exclusive_i64_ws(P->slot_off, P->slot_off, m + 1, P->scan_ws, s);
+    const int nb = P->cfg.nb;
     int64_t total_cap = 0;
-    cudaMemcpyAsync(h_bins, bins, sizeof(h_bins), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&total_cap, capv + m, 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(P->h_bins, P->bins, sizeof(int) * (nb + 2), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&total_cap, P->slot_off + m, 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_to_info(e);
-    // per-bin row lists
-    int h_start[NB_SMEM + 2] = {0};
-    for (int b = 1; b < NB_SMEM + 2; b++) h_start[b] = h_start[b - 1] + h_bins[b - 1];
-    int *d_start = bins + 16, *d_fill = bins + 32;
-    cudaMemcpyAsync(d_start, h_start, sizeof(h_start), cudaMemcpyHostToDevice, s);
+    P->total_cap = total_cap;
+    P->h_start[0] = 0;
+    for (int b = 1; b < nb + 2; b++) P->h_start[b] = P->h_start[b - 1] + P->h_bins[b - 1];
+    int *d_start = P->bins + 16, *d_fill = P->bins + 32;
+    cudaMemcpyAsync(d_start, P->h_start, sizeof(int) * (nb + 2), cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(d_fill, 0, 16 * sizeof(int), s);
     if (m > 0)
-        k_fill_bins<<<nblocks(m, 256), 256, 0, s>>>(row_bin, m, d_fill, d_start, bin_rows);
-    int32_t *Tj = ws.get<int32_t>(total_cap + 1);
-    Z *Tx = ws.get<Z>(total_cap + 1);
-    if (ws.failed) return OUT_OF_MEMORY;
-    cudaMemsetAsync(row_cnt, 0, (size_t)(m + 1) * 4, s);
-    const int ps = prof_begin("saxpy3_numeric", s);
-    launch_hash_bin<SR, 8, 128>(bin_rows + h_start[1], h_bins[1], A, B, M, mask_comp, capv, Tj, Tx, row_cnt, s);
-    launch_hash_bin<SR, 32, 512>(bin_rows + h_start[2], h_bins[2], A, B, M, mask_comp, capv, Tj, Tx, row_cnt, s);
-    launch_hash_bin<SR, 32, 2048>(bin_rows + h_start[3], h_bins[3], A, B, M, mask_comp, capv, Tj, Tx, row_cnt, s);
-    launch_hash_bin<SR, 256, 8192>(bin_rows + h_start[4], h_bins[4], A, B, M, mask_comp, capv, Tj, Tx, row_cnt, s);
-    const int heavy = NB_SMEM + 1;
-    const int nheavy = h_bins[heavy];
+        k_fill_bins<<<nblocks(m, 256), 256, 0, s>>>(P->row_bin, m, d_fill, d_start, P->bin_rows);
+    P->Tj = (int32_t *)dalloc((size_t)(total_cap + 1) * 4, s);
+    P->Tx = dalloc((size_t)(total_cap + 1) * sizeof(Z), s);
+    if (!P->Tj || !P->Tx) return OUT_OF_MEMORY;
+    const int nheavy = P->h_bins[nb + 1];
     if (nheavy > 0) {
-        const int32_t *hrows = bin_rows + h_start[heavy];
-        if constexpr (SR::order_free) {
-            // all heavy rows at once, one workspace row each (chunks bound memory)
+        if (SR::order_free) {
             int64_t chunk = nheavy;
-            int64_t per_row = ncols * (8 + (int64_t)sizeof(Z));
-            int64_t budget = (int64_t)4 << 30;
+            const int64_t per_row = ncols * (8 + (int64_t)sizeof(Z));
+            const int64_t budget = (int64_t)4 << 30;
             if (chunk * per_row > budget) chunk = budget / per_row > 0 ? budget / per_row : 1;
-            int64_t *flag = ws.get<int64_t>(chunk * ncols);
-            Z *val = ws.get<Z>(chunk * ncols);
-            if (ws.failed) return OUT_OF_MEMORY;
+            P->heavy_chunk = chunk;
+            P->flag = (int64_t *)dalloc((size_t)(chunk * ncols + 1) * 8, s);
+            P->val = dalloc((size_t)(chunk * ncols + 1) * sizeof(Z), s);
+            const int64_t cblocks = (ncols + DG_CHUNK - 1) / DG_CHUNK;
+            const int64_t ncnt = chunk * cblocks + 1;
+            P->dg_cnt = (int64_t *)dalloc((size_t)(ncnt + 1) * 8, s);
+            P->dg_ws = (int64_t *)dalloc(scan_ws_elems(ncnt) * 8, s);
+            if (!P->dg_cnt || !P->dg_ws) return OUT_OF_MEMORY;
+        } else {
+            const int nbk = nheavy < runtime().num_sms * 2 ? nheavy : runtime().num_sms * 2;
+            P->heavy_chunk = nbk;
+            P->flag = (int64_t *)dalloc((size_t)((int64_t)nbk * ncols + 1) * 8, s);
+            P->val = dalloc((size_t)((int64_t)nbk * ncols + 1) * sizeof(Z), s);
+        }
+        if (!P->flag || !P->val) return OUT_OF_MEMORY;
+    }
+    return cuda_to_info(cudaGetLastError());
+}
+
+template <class SR>
+static void launch_bin(const SaxpyPlan *P, int q, const DevCSR &A, const DevCSR &B,
+                       const DevCSR *M, cudaStream_t s)
+{
+    using Z = typename SR::z_t;
+    const BinSpec &b = P->cfg.bin[q];
+    const int cnt = P->h_bins[q + 1];
+    if (cnt == 0) return;
+    const int32_t *rows = P->bin_rows + P->h_start[q + 1];
+    const size_t smem = bin_smem(b, sizeof(Z));
+    const int cap_blocks = runtime().num_sms * P->cfg.blocks_per_sm;
+    if (b.tpr >= 256) {
+        static bool attr = false;
+        if (!attr) {
+            allow_dynamic_smem((const void *)k_saxpy_hash<SR, true>);
+            attr = true;
+        }
+        int blocks = cnt < cap_blocks ? cnt : cap_blocks;
+        k_saxpy_hash<SR, true><<<blocks, 256, smem, s>>>(rows, cnt, 8, b.cap,
+            A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
+            M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, P->mask_comp,
+            P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
+    } else {
+        static bool attr = false;
+        if (!attr) {
+            allow_dynamic_smem((const void *)k_saxpy_hash<SR, false>);
+            attr = true;
+        }
+        const int lg = b.tpr == 4 ? 2 : b.tpr == 8 ? 3 : b.tpr == 16 ? 4 : 5;
+        const int groups = 128 / b.tpr;
+        int blocks = (cnt + groups - 1) / groups;
+        if (blocks > cap_blocks) blocks = cap_blocks;
+        k_saxpy_hash<SR, false><<<blocks, 128, smem, s>>>(rows, cnt, lg, b.cap,
+            A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
+            M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, P->mask_comp,
+            P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
+    }
+}
+
+template <class SR>
+static int exec_t(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &B,
+                  int32_t *Cp, int32_t *Cj, void *Cx, int64_t *Cnnz64, cudaStream_t s)
+{
+    using Z = typename SR::z_t;
+    const int64_t m = P->m, ncols = P->ncols;
+    const int nb = P->cfg.nb;
+    cudaMemsetAsync(P->row_cnt, 0, (size_t)(m + 1) * 4, s);
+    const int ps = prof_begin("saxpy3_numeric", s);
+    for (int q = 0; q < nb; q++) launch_bin<SR>(P, q, A, B, M, s);
+    const int nheavy = P->h_bins[nb + 1];
+    if (nheavy > 0) {
+        const int32_t *hrows = P->bin_rows + P->h_start[nb + 1];
+        int64_t *flag = P->flag;
+        Z *val = (Z *)P->val;
+        if constexpr (SR::order_free) {
+            const int64_t chunk = P->heavy_chunk;
             for (int64_t c0 = 0; c0 < nheavy; c0 += chunk) {
-                int nr = (int)((nheavy - c0 < chunk) ? nheavy - c0 : chunk);
+                const int nr = (int)((nheavy - c0 < chunk) ? nheavy - c0 : chunk);
                 dim3 g1(nblocks(ncols, 256, 4), nr > 65535 ? 65535 : nr);
                 k_dense_init<SR><<<g1, 256, 0, s>>>(hrows + c0, nr, ncols, flag, val);
                 if (M) {
                     dim3 g2(8, nr > 65535 ? 65535 : nr);
-                    k_dense_mask<<<g2, 256, 0, s>>>(hrows + c0, nr, M->p, M->j, mask_comp, ncols, flag);
+                    k_dense_mask<<<g2, 256, 0, s>>>(hrows + c0, nr, M->p, M->j, P->mask_comp,
+                                                    ncols, flag);
                 }
-                dim3 g3((unsigned)runtime().num_sms * 8 / (nr < 8 ? nr : 8) + 1, nr > 65535 ? 65535 : nr);
+                dim3 g3((unsigned)runtime().num_sms * 8 / (nr < 8 ? nr : 8) + 1,
+                        nr > 65535 ? 65535 : nr);
                 k_dense_atomic<SR><<<g3, 256, 0, s>>>(hrows + c0, nr, A.p, A.j, A.x, A.iso,
-                    B.p, B.j, B.x, B.iso, M != nullptr, mask_comp, ncols, flag, val);
-                k_dense_gather<SR><<<nr < 1024 ? nr : 1024, 256, 0, s>>>(hrows + c0, nr, ncols,
-                    flag, val, capv, Tj, Tx, row_cnt);
+                    B.p, B.j, B.x, B.iso, M != nullptr, P->mask_comp, ncols, flag, val);
+                const int cblocks = (int)((ncols + DG_CHUNK - 1) / DG_CHUNK);
+                dim3 g4(cblocks, nr > 65535 ? 65535 : nr);
+                k_dense_count<<<g4, DG_THREADS, 0, s>>>(nr, ncols, cblocks, flag, P->dg_cnt);
+                const int64_t ncnt = (int64_t)nr * cblocks;
+                cudaMemsetAsync(P->dg_cnt + ncnt, 0, 8, s);
+                scan_exclusive_i64_ws(P->dg_cnt, P->dg_cnt, ncnt + 1, P->dg_ws, s);
+                k_dense_write<SR><<<g4, DG_THREADS, 0, s>>>(hrows + c0, nr, ncols, cblocks,
+                    flag, val, P->dg_cnt, P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
             }
         } else {
-            int nb = nheavy < runtime().num_sms * 2 ? nheavy : runtime().num_sms * 2;
-            int64_t *flag = ws.get<int64_t>((int64_t)nb * ncols);
-            Z *val = ws.get<Z>((int64_t)nb * ncols);
-            if (ws.failed) return OUT_OF_MEMORY;
-            cudaMemsetAsync(flag, 0, (size_t)nb * ncols * 8, s);
-            k_saxpy_dense_seq<SR><<<nb, 256, 0, s>>>(hrows, nheavy, A.p, A.j, A.x, A.iso,
+            const int nbk = (int)P->heavy_chunk;
+            cudaMemsetAsync(flag, 0, (size_t)nbk * ncols * 8, s);
+            k_saxpy_dense_seq<SR><<<nbk, 256, 0, s>>>(hrows, nheavy, A.p, A.j, A.x, A.iso,
                 B.p, B.j, B.x, B.iso, M ? M->p : nullptr, M ? M->j : nullptr,
-                M != nullptr, mask_comp, ncols, flag, val, capv, Tj, Tx, row_cnt);
+                M != nullptr, P->mask_comp, ncols, flag, val, P->slot_off, P->Tj,
+                (Z *)P->Tx, P->row_cnt);
         }
     }
     prof_end(ps, s);
-    // exact row counts -> C row pointers
-    int64_t *Cp64 = ws.get<int64_t>(m + 1);
-    if (ws.failed) return OUT_OF_MEMORY;
-    if (m > 0) k_cnt_to_i64<<<nblocks(m, 256), 256, 0, s>>>(row_cnt, row_bin, m, Cp64);
-    cudaMemsetAsync(Cp64 + m, 0, 8, s);
-    info = scan_exclusive_i64(Cp64, Cp64, m + 1, s);
-    if (info != SUCCESS) return info;
-    int64_t nnz = 0;
-    cudaMemcpyAsync(&nnz, Cp64 + m, 8, cudaMemcpyDeviceToHost, s);
-    e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cuda_to_info(e);
-    if (nnz >= INT32_MAX) return OUT_OF_MEMORY;
-    C.nrows = m; C.ncols = ncols; C.nnz = nnz; C.iso = false; C.nzombies = 0;
-    C.p = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
-    C.j = (int32_t *)dalloc((size_t)(nnz ? nnz : 1) * 4, s);
-    C.x = dalloc((size_t)(nnz ? nnz : 1) * sizeof(Z), s);
-    if (!C.p || !C.j || !C.x) { dev_free(C, s); return OUT_OF_MEMORY; }
-    k_i64_to_i32_p<<<nblocks(m + 1, 256), 256, 0, s>>>(Cp64, C.p, m + 1);
-    if (m > 0 && nnz > 0)
-        k_pack<Z><<<nblocks(m * 32, 256), 256, 0, s>>>(m, capv, Tj, Tx, row_cnt,
-            Cp64, C.j, (Z *)C.x);
-    e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) { dev_free(C, s); return cuda_to_info(e); }
+    // exact row counts -> C row pointers, then pack the slots
+    if (m > 0) k_cnt_to_i64<<<nblocks(m, 256), 256, 0, s>>>(P->row_cnt, P->row_bin, m, P->Cp64);
+    cudaMemsetAsync(P->Cp64 + m, 0, 8, s);
+    scan_exclusive_i64_ws(P->Cp64, P->Cp64, m + 1, P->scan_ws, s);
+    k_i64_to_i32_p<<<nblocks(m + 1, 256), 256, 0, s>>>(P->Cp64, Cp, m + 1, nullptr);
+    if (Cnnz64) k_copy_i64<<<1, 32, 0, s>>>(P->Cp64 + m, Cnnz64);
+    if (m > 0)
+        k_pack<Z><<<nblocks(m * 32, 256), 256, 0, s>>>(m, P->slot_off, P->Tj, (Z *)P->Tx,
+            P->row_cnt, P->Cp64, Cj, (Z *)Cx);
+    return cuda_to_info(cudaGetLastError());
+}
+
+int saxpy_plan_create(SaxpyPlan **Pout, const DevCSR *M, bool mask_comp,
+                      const DevCSR &A, const DevCSR &B, SemiringCode sr,
+                      const SaxpyConfig &cfg, cudaStream_t s)
+{
+    if (A.ncols != B.nrows) return DIMENSION_MISMATCH;
+    if (M && (M->nrows != A.nrows || M->ncols != B.ncols)) return DIMENSION_MISMATCH;
+    SaxpyPlan *P = new SaxpyPlan();
+    P->sr = sr;
+    P->cfg = cfg;
+    int info = NO_VALUE;
+#define GRB_PLAN_CASE(ADD, MULT, TC, CT)                                        \
+    if (sr.add == ADD && sr.mult == MULT && sr.type == TC) {                    \
+        if (!saxpy_config_valid(cfg, sizeof(CT))) info = INVALID_VALUE;         \
+        else info = plan_t<Semiring<ADD, MULT, CT>>(P, M, mask_comp, A, B, s);  \
+    } else
+    GRB_FOR_EACH_SEMIRING(GRB_PLAN_CASE) { info = NO_VALUE; }
+#undef GRB_PLAN_CASE
+    if (info != SUCCESS) { saxpy_plan_free(P, s); return info; }
+    *Pout = P;
     return SUCCESS;
 }
 
+int saxpy_plan_exec(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &B,
+                    int32_t *Cp, int32_t *Cj, void *Cx, int64_t *Cnnz64, cudaStream_t s)
+{
+    const SemiringCode sr = P->sr;
+#define GRB_EXEC_CASE(ADD, MULT, TC, CT)                                        \
+    if (sr.add == ADD && sr.mult == MULT && sr.type == TC)                      \
+        return exec_t<Semiring<ADD, MULT, CT>>(P, M, A, B, Cp, Cj, Cx, Cnnz64, s);
+    GRB_FOR_EACH_SEMIRING(GRB_EXEC_CASE)
+#undef GRB_EXEC_CASE
+    return NO_VALUE;
+}
+
+// one-shot C<M> = A*B: plan, execute, then trim the output to its exact size
 int saxpy3(DevCSR &C, const DevCSR *M, bool mask_comp, bool mask_struct,
            const DevCSR &A, const DevCSR &B, SemiringCode sr, cudaStream_t s)
 {
     if (A.ncols != B.nrows) return DIMENSION_MISMATCH;
     if (M && (M->nrows != A.nrows || M->ncols != B.ncols)) return DIMENSION_MISMATCH;
+    if (!semiring_supported(sr)) return NO_VALUE;
     DevCSR Ms;
     bool own_mask = false;
     if (M && !mask_struct && M->x) {
@@ -819,18 +1055,50 @@ int saxpy3(DevCSR &C, const DevCSR *M, bool mask_comp, bool mask_struct,
         if (info != SUCCESS) return info;
         M = &Ms;
         own_mask = true;
+    } else if (M && M->nzombies > 0) {
+        return NO_VALUE;
     }
     struct Guard { DevCSR *m; bool own; cudaStream_t s;
         ~Guard() { if (own) dev_free(*m, s); } } guard{&Ms, own_mask, s};
-#define GRB_SAXPY_CASE(ADD, MULT, TC, CT)                                      \
-    if (sr.add == ADD && sr.mult == MULT && sr.type == TC) {                   \
-        int info = saxpy3_t<Semiring<ADD, MULT, CT>>(C, M, mask_comp, A, B, s); \
-        if (info == SUCCESS) C.type = TC;                                      \
-        return info;                                                           \
+    SaxpyPlan *P = nullptr;
+    int info = saxpy_plan_create(&P, M, mask_comp, A, B, sr, saxpy_default_config(), s);
+    if (info != SUCCESS) return info;
+    const size_t zs = P->zsize;
+    const int64_t cap = P->total_cap, m = A.nrows;
+    DevCSR T;
+    T.nrows = m; T.ncols = B.ncols; T.type = sr.type; T.iso = false;
+    T.p = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
+    T.j = (int32_t *)dalloc((size_t)(cap + 1) * 4, s);
+    T.x = dalloc((size_t)(cap + 1) * zs, s);
+    int64_t *nnz_d = (int64_t *)dalloc(8, s);
+    if (!T.p || !T.j || !T.x || !nnz_d) {
+        dev_free(T, s); dfree(nnz_d, s); saxpy_plan_free(P, s); return OUT_OF_MEMORY;
     }
-    GRB_FOR_EACH_SEMIRING(GRB_SAXPY_CASE)
-#undef GRB_SAXPY_CASE
-    return NO_VALUE;
+    info = saxpy_plan_exec(P, M, A, B, T.p, T.j, T.x, nnz_d, s);
+    int64_t nnz = 0;
+    cudaMemcpyAsync(&nnz, nnz_d, 8, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    saxpy_plan_free(P, s);
+    dfree(nnz_d, s);
+    if (info == SUCCESS && e != cudaSuccess) info = cuda_to_info(e);
+    if (info != SUCCESS) { dev_free(T, s); return info; }
+    if (nnz >= INT32_MAX) { dev_free(T, s); return OUT_OF_MEMORY; }
+    T.nnz = nnz;
+    if (cap > 2 * nnz + 1024) {
+        // the flop bound overestimated the output a lot: keep exact arrays
+        int32_t *j2 = (int32_t *)dalloc((size_t)(nnz + 1) * 4, s);
+        void *x2 = dalloc((size_t)(nnz + 1) * zs, s);
+        if (j2 && x2) {
+            cudaMemcpyAsync(j2, T.j, (size_t)nnz * 4, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(x2, T.x, (size_t)nnz * zs, cudaMemcpyDeviceToDevice, s);
+            dfree(T.j, s); dfree(T.x, s);
+            T.j = j2; T.x = x2;
+        } else {
+            dfree(j2, s); dfree(x2, s);
+        }
+    }
+    C = T;
+    return cuda_to_info(cudaStreamSynchronize(s));
 }
 
 }  // namespace grb

@@ -1,0 +1,227 @@
+"""The request server (grb_b200_server_*, include/grb_b200.h) from Python.
+
+``Server`` wraps a server handle; ``make_trace`` builds the serving workload:
+an open-loop Poisson stream of mixed requests on device-resident graphs -
+triangle counts on R-MAT graphs of scale 10-16 (plus_pair, dot3), SSSP
+relaxation steps (min_plus fp32 vxm) and products C = A*A (plus_times fp64) on
+Erdos-Renyi matrices with n log-uniform in [1024, 65536] and 4-16 entries per
+row.  ``BenchServe`` is bench.py --config serve.
+"""
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import lib as _lib, check, workloads as W
+
+vp = ctypes.c_void_p
+K_TRICOUNT, K_SSSP, K_MXM = 1, 2, 3
+
+
+def _bind(L):
+    if getattr(L, "_serve_bound", False):
+        return L
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    L.grb_b200_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int64,
+                                         ctypes.c_bool]
+    L.grb_b200_server_add_graph.argtypes = [vp, ctypes.c_int, ctypes.c_int64, vp, vp, vp,
+                                            ctypes.POINTER(ctypes.c_int)]
+    L.grb_b200_server_replay.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp, vp, vp]
+    L.grb_b200_server_request.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int),
+                                          i64p, ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_double)]
+    L.grb_b200_server_result.argtypes = [vp, ctypes.c_int64, vp, vp, vp, i64p, i64p]
+    L.grb_b200_server_stats.argtypes = [vp, i64p, i64p, i64p, i64p, i64p,
+                                        ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_double)]
+    L.grb_b200_server_free.argtypes = [ctypes.POINTER(vp)]
+    for n in ("create", "add_graph", "replay", "request", "result", "stats", "free"):
+        getattr(L, "grb_b200_server_" + n).restype = ctypes.c_int
+    L._serve_bound = True
+    return L
+
+
+class Server:
+    def __init__(self, nslots=8, budget_bytes=40 << 30, keep_results=True):
+        self.L = _bind(_lib())
+        h = vp()
+        check(self.L.grb_b200_server_create(ctypes.byref(h), nslots, budget_bytes,
+                                            keep_results), "server_create")
+        self.h = h
+        self.kinds = []
+
+    def add_graph(self, kind, csr):
+        gid = ctypes.c_int()
+        x = None
+        if kind == K_SSSP:
+            x = np.ascontiguousarray(csr.x, np.float32)
+        elif kind == K_MXM:
+            x = np.ascontiguousarray(csr.x, np.float64)
+        p = np.ascontiguousarray(csr.p, np.int64)
+        i = np.ascontiguousarray(csr.i, np.int64)
+        check(self.L.grb_b200_server_add_graph(self.h, kind, csr.nrows, p.ctypes.data,
+                                               i.ctypes.data,
+                                               None if x is None else x.ctypes.data,
+                                               ctypes.byref(gid)), "server_add_graph")
+        self.kinds.append(kind)
+        return gid.value
+
+    def replay(self, trace):
+        kind = np.ascontiguousarray(trace["kind"], np.int32)
+        graph = np.ascontiguousarray(trace["graph"], np.int32)
+        t = np.ascontiguousarray(trace["t"], np.float64)
+        fp = np.ascontiguousarray(trace["fp"], np.int64)
+        fi = np.ascontiguousarray(trace["fi"], np.int64)
+        fx = np.ascontiguousarray(trace["fx"], np.float32)
+        check(self.L.grb_b200_server_replay(self.h, len(kind), kind.ctypes.data,
+                                            graph.ctypes.data, t.ctypes.data, fp.ctypes.data,
+                                            fi.ctypes.data, fx.ctypes.data), "server_replay")
+
+    def request(self, k):
+        st = ctypes.c_int()
+        cnt = ctypes.c_int64()
+        lat, wait = ctypes.c_double(), ctypes.c_double()
+        check(self.L.grb_b200_server_request(self.h, k, ctypes.byref(st), ctypes.byref(cnt),
+                                             ctypes.byref(lat), ctypes.byref(wait)))
+        return dict(status=st.value, count=cnt.value, latency=lat.value, wait=wait.value)
+
+    def result(self, k, kind):
+        npp, ni = ctypes.c_int64(), ctypes.c_int64()
+        check(self.L.grb_b200_server_result(self.h, k, None, None, None, ctypes.byref(npp),
+                                            ctypes.byref(ni)))
+        p = np.zeros(npp.value, np.int64)
+        i = np.zeros(ni.value, np.int64)
+        x = np.zeros(ni.value, np.float32 if kind == K_SSSP else np.float64)
+        check(self.L.grb_b200_server_result(self.h, k, p.ctypes.data, i.ctypes.data,
+                                            x.ctypes.data, ctypes.byref(npp),
+                                            ctypes.byref(ni)))
+        return p, i, x
+
+    def stats(self):
+        v = [ctypes.c_int64() for _ in range(5)]
+        pa = ctypes.c_int()
+        mk = ctypes.c_double()
+        check(self.L.grb_b200_server_stats(self.h, *[ctypes.byref(a) for a in v],
+                                           ctypes.byref(pa), ctypes.byref(mk)))
+        return dict(admitted=v[0].value, rejected=v[1].value, completed=v[2].value,
+                    failed=v[3].value, peak_bytes=v[4].value, peak_active=pa.value,
+                    makespan_s=mk.value)
+
+    def free(self):
+        if self.h and self.h.value:
+            self.L.grb_b200_server_free(ctypes.byref(self.h))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def make_graphs(seed=1, tc_scales=range(10, 17), n_sssp=3, n_mxm=6, mxm_nmax=65536):
+    """The resident graph set of the serving workload."""
+    graphs = []
+    for s in tc_scales:
+        graphs.append((K_TRICOUNT, W.rmat(s, 16, seed=seed + s)))
+    rng = np.random.default_rng(seed)
+    for k in range(n_sssp):
+        S = W.rmat(12 + 2 * k, 16, seed=seed + 100 + k)
+        w = (0.1 + 9.9 * rng.random(S.nnz)).astype(np.float32)
+        graphs.append((K_SSSP, W.Csr(S.nrows, S.ncols, S.p, S.i, w)))
+    lo, hi = math.log(1024), math.log(mxm_nmax)
+    for k in range(n_mxm):
+        n = int(round(math.exp(lo + (hi - lo) * W.unif01(seed + 7, k))))
+        graphs.append((K_MXM, W.er_range(n, 4, 16, seed=seed + 200 + k)))
+    return graphs
+
+
+def make_trace(graphs, nreq=4000, rate=2000.0, seed=3):
+    """Open-loop Poisson arrivals (mean `rate` per second), kinds uniform,
+    graphs uniform within a kind; SSSP frontiers are random vertex subsets
+    with fp32 distances."""
+    rng = np.random.default_rng(seed)
+    by_kind = {k: [g for g, (kk, _) in enumerate(graphs) if kk == k] for k in (1, 2, 3)}
+    t = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    kind = rng.integers(1, 4, nreq).astype(np.int32)
+    graph = np.array([by_kind[int(k)][rng.integers(len(by_kind[int(k)]))] for k in kind],
+                     np.int32)
+    fp = [0]
+    fi, fx = [], []
+    for k in range(nreq):
+        if kind[k] == K_SSSP:
+            n = graphs[graph[k]][1].nrows
+            m = int(min(n, max(16, rng.integers(16, 4096))))
+            idx = np.sort(rng.choice(n, m, replace=False)).astype(np.int64)
+            fi.append(idx)
+            fx.append((rng.random(m) * 50).astype(np.float32))
+            fp.append(fp[-1] + m)
+        else:
+            fp.append(fp[-1])
+    fi = np.concatenate(fi) if fi else np.zeros(1, np.int64)
+    fx = np.concatenate(fx) if fx else np.zeros(1, np.float32)
+    return {"t": t, "kind": kind, "graph": graph, "fp": np.array(fp, np.int64),
+            "fi": fi, "fx": fx}
+
+
+class BenchServe:
+    """bench.py --config serve: req/s with p50/p99 latency."""
+    metric, unit, dtype, kernel = "req/s", "req/s", "mixed", "dot3"
+
+    def __init__(self, args):
+        self.graphs = make_graphs(seed=args.seed)
+        self.nreq = 4000
+        self.trace = make_trace(self.graphs, nreq=self.nreq, rate=2000.0, seed=args.seed + 2)
+        self.workload = "serve_poisson2000_tc_rmat10-16_sssp_minplus_fp32_mxm_er_fp64"
+        self.alg_bytes = 0.0
+
+    def config(self):
+        return dict(requests=self.nreq, rate_req_s=2000.0, slots=8,
+                    hbm_budget_gb=40, **getattr(self, "lat", {}))
+
+    def _server(self):
+        S = Server(nslots=8, budget_bytes=40 << 30, keep_results=True)
+        for kind, g in self.graphs:
+            S.add_graph(kind, g)
+        return S
+
+    def dev_setup(self, gb):
+        self.S = self._server()
+
+    def _latencies(self, S):
+        lat = np.array([S.request(k)["latency"] for k in range(self.nreq)])
+        st = S.stats()
+        self.lat = {"p50_ms": float(np.percentile(lat, 50) * 1e3),
+                    "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                    "admitted": st["admitted"], "rejected": st["rejected"],
+                    "failed": st["failed"], "peak_hbm_gb": st["peak_bytes"] / 2**30,
+                    "peak_concurrent": st["peak_active"],
+                    "makespan_s": st["makespan_s"]}
+        return st
+
+    def step_dev(self):
+        self.S.replay(self.trace)
+        st = self._latencies(self.S)
+        return st["completed"]
+
+    def e2e_setup(self, torch):
+        return 0, 0
+
+    def step_e2e(self):
+        S = self._server()
+        S.replay(self.trace)
+        st = S.stats()
+        S.free()
+        return st["completed"]
+
+    def launches_per_step(self):
+        return 8 * self.nreq
+
+    def cpu_baseline(self, R, ncores):
+        return None, "not measured for the request stream"
+
+    def reference_steps(self, R, steps, warmup):
+        raise NotImplementedError
+
+    def free(self):
+        self.S.free()

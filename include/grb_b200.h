@@ -195,6 +195,98 @@ int grb_b200_dmxv(grb_b200_dmatrix *w, grb_b200_dmatrix mask, bool mask_comp,
                   const grb_b200_semiring *sr);
 
 /* ------------------------------------------------------------------------ */
+/* Batches of independent products                                          */
+/* ------------------------------------------------------------------------ */
+
+/* A batch of `count` independent products C_k = A_k * B_k (B_k = A_k when
+ * Bp is NULL).  No counterpart in the reference, where the caller loops over
+ * GrB_mxm (one GB_AxB_saxpy3 each, Source/mxm/GB_AxB_saxpy3.c:119).
+ *
+ * Inputs are concatenated CSR: instance k is a_nrows[k]-by-a_ncols[k]; its
+ * a_nrows[k]+1 row offsets follow instance k-1's in Ap and index the shared
+ * Aj/Ax arrays (Ap[0] = 0, offsets continue across instances).  B_k is
+ * a_ncols[k]-by-b_ncols[k], laid out the same way in Bp/Bj/Bx.  Ax/Bx NULL:
+ * pattern (iso one).  The batch is uploaded once as one block-diagonal
+ * matrix; its symbolic phase runs at creation. */
+typedef struct grb_b200_batch_s *grb_b200_batch;
+
+int grb_b200_batch_create(grb_b200_batch *B, int count, const int64_t *a_nrows,
+                          const int64_t *a_ncols, const int64_t *Ap,
+                          const int64_t *Aj, const void *Ax,
+                          const int64_t *b_ncols, const int64_t *Bp,
+                          const int64_t *Bj, const void *Bx,
+                          const grb_b200_semiring *semiring);
+
+/* Pick bin thresholds, hash-table sizes and threads per row by timing a set
+ * of candidate configurations on this batch (or reuse the cached choice for
+ * its size class when use_cache); *best_ms gets the numeric time. */
+int grb_b200_batch_tune(grb_b200_batch B, bool use_cache, double *best_ms);
+
+/* Numeric phase for every instance; use_graph replays it as one captured
+ * CUDA graph.  Synchronises before returning. */
+int grb_b200_batch_run(grb_b200_batch B, bool use_graph);
+
+/* Enqueue the captured graph on a caller's stream (NULL: the batch's own)
+ * without waiting for it. */
+int grb_b200_batch_enqueue(grb_b200_batch B, void *stream);
+
+/* Sizes of the batch, its shared-memory bin count, the tuned numeric time
+ * and the number of kernel launches in the captured graph (0 before the
+ * first graph run). */
+int grb_b200_batch_info(grb_b200_batch B, int64_t *total_rows, int64_t *nnz_c,
+                        int64_t *capacity, int *nbins, double *tuned_ms,
+                        int *graph_kernels);
+
+/* Results, concatenated like the inputs (malloc'd, owned by the caller): Cp
+ * holds a_nrows[k]+1 offsets per instance into Cj/Cx. */
+int grb_b200_batch_result(grb_b200_batch B, int64_t **Cp, int64_t **Cj,
+                          void **Cx, int64_t *nnz_per_instance);
+
+int grb_b200_batch_free(grb_b200_batch *B);
+
+/* ------------------------------------------------------------------------ */
+/* Request server over device-resident graphs                               */
+/* ------------------------------------------------------------------------ */
+
+/* No counterpart in the reference.  Request kinds: 1 = triangle count
+ * (C<L> = L*U' plus_pair int64, then sum), 2 = SSSP relaxation step
+ * (w = u' min.+ A, fp32, u a sparse frontier), 3 = product C = A*A
+ * (plus_times fp64).  nslots worker streams run admitted requests
+ * concurrently; a request is admitted when its estimated HBM footprint fits
+ * in hbm_budget_bytes next to the running ones, and rejected
+ * (GrB_OUT_OF_MEMORY status) if it never can. */
+typedef struct grb_b200_server_s *grb_b200_server;
+
+int grb_b200_server_create(grb_b200_server *S, int nslots,
+                           int64_t hbm_budget_bytes, bool keep_results);
+
+/* Upload a graph once: kind 1 takes a symmetric pattern (split into L, U),
+ * kind 2 fp32 weights, kind 3 fp64 values; square n-by-n CSR. */
+int grb_b200_server_add_graph(grb_b200_server S, int kind, int64_t n,
+                              const int64_t *p, const int64_t *i, const void *x,
+                              int *graph_id);
+
+/* Open-loop replay: request k of kind[k] on graph[k] arrives t_arrival[k]
+ * seconds after the call; SSSP frontiers are fi/fx[fp[k] .. fp[k+1]). */
+int grb_b200_server_replay(grb_b200_server S, int64_t nreq, const int *kind,
+                           const int *graph, const double *t_arrival,
+                           const int64_t *fp, const int64_t *fi,
+                           const float *fx);
+
+int grb_b200_server_request(grb_b200_server S, int64_t k, int *status,
+                            int64_t *count, double *latency_s, double *wait_s);
+
+int grb_b200_server_result(grb_b200_server S, int64_t k, int64_t *p,
+                           int64_t *i, void *x, int64_t *np, int64_t *ni);
+
+int grb_b200_server_stats(grb_b200_server S, int64_t *admitted,
+                          int64_t *rejected, int64_t *completed,
+                          int64_t *failed, int64_t *peak_bytes,
+                          int *peak_active, double *makespan_s);
+
+int grb_b200_server_free(grb_b200_server *S);
+
+/* ------------------------------------------------------------------------ */
 /* Masked dot products without any allocation                               */
 /* ------------------------------------------------------------------------ */
 

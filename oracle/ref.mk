@@ -39,3 +39,29 @@ $(OUT)/libgraphblas_ref.so: $(OBJS)
 	$(CC) -shared -fopenmp -o $@ $(OBJS) -lm -ldl -Wl,-soname,libgraphblas_ref.so
 
 .PHONY: all
+
+# The same reference library with its GB_AxB_dot3 / GB_AxB_saxpy3 calls routed
+# to libgrb_b200.so by the maintainer's shim (graphblas_b200/integration/
+# gb_b200_gateway.c) through link-time wrapping: the drop-in, demonstrated on
+# the real library.  GB_B200=1 in the environment switches the GPU on.
+GW      := graphblas_b200/integration/gb_b200_gateway.c
+GRBLIB  := graphblas_b200/lib
+WRAPPED := $(OUT)/libgraphblas_b200wrap.so
+
+wrap: $(WRAPPED) $(OUT)/libref_runner_wrap.so
+
+$(OBJ)/gb_b200_gateway.o: $(GW) include/grb_b200.h
+	@mkdir -p $(dir $@)
+	$(CC) $(CFLAGS) $(INCS) -Iinclude -c $< -o $@
+
+$(WRAPPED): $(OBJS) $(OBJ)/gb_b200_gateway.o $(GRBLIB)/libgrb_b200.so
+	$(CC) -shared -fopenmp -o $@ $(OBJS) $(OBJ)/gb_b200_gateway.o \
+	    -Wl,--wrap=GB_AxB_dot3 -Wl,--wrap=GB_AxB_saxpy3 \
+	    -L$(GRBLIB) -lgrb_b200 -Wl,-rpath,'$$ORIGIN/../../$(GRBLIB)' \
+	    -lm -ldl -Wl,-soname,libgraphblas_b200wrap.so
+
+$(OUT)/libref_runner_wrap.so: oracle/ref_runner.c $(WRAPPED)
+	$(CC) -O2 -fopenmp -fPIC -shared -std=gnu11 -I$(REF)/Include -o $@ $< \
+	    -L$(OUT) -lgraphblas_b200wrap -Wl,-rpath,'$$ORIGIN'
+
+.PHONY: wrap

@@ -1,0 +1,188 @@
+"""The GraphBLAS C API of the path (include/GraphBLAS_b200.h) end to end on
+the GPU, written the way the reference's own demos and tests call it:
+triangle counting (LAGraph's C<L> = L*U' plus_pair + reduce), BFS parents
+(vxm any_secondi with a complemented structural mask and replace, then
+assign), mxm with accumulators, masks, replace and transposes, mxv, and the
+error codes of the API.  Checked against the oracle (oracle/oracle.c).
+"""
+
+import numpy as np
+import pytest
+
+from graphblas_b200 import workloads as W
+from tests.helpers import assert_exact, random_csr, transpose_csr
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def api(gpu):
+    from graphblas_b200.grb import API
+    return API()
+
+
+def test_tricount_through_grb_mxm(api, oracle):
+    S = W.rmat(13, 16, seed=4)
+    Lc, Uc = W.tril_triu(S)
+    L = api.matrix_from_csr(Lc, 1)
+    U = api.matrix_from_csr(Uc, 1)
+    C = api.matrix_new(8, S.nrows, S.ncols)
+    api.mxm(C, L, None, "GxB_PLUS_PAIR_INT64", L, U, "GrB_DESC_ST1")
+    ntri = api.reduce(C, "GrB_PLUS_MONOID_INT64", 8)
+    assert ntri == oracle.tricount(S.nrows, Lc.p, Lc.i, Uc.p, Uc.i)
+    want = oracle.dot3(S.nrows, S.ncols, (Lc.p, Lc.i, None, 1), (Uc.p, Uc.i, None, 1),
+                       (Lc.p, Lc.i, None, 1), "PLUS", "PAIR", 8)
+    assert api.nvals(C) == len(want[1])          # zombies are not counted
+    got = api.matrix_to_csr(C, 8, S.nrows)
+    assert_exact(got, want, "C<L>=L*U'")
+    for A in (L, U, C):
+        api.free(A)
+
+
+def test_bfs_parents_through_grb_vxm(api, oracle):
+    S = W.rmat(14, 16, seed=8)
+    n = S.nrows
+    A = api.matrix_from_csr(S, 1)
+    src = 3
+    q = api.vector_from([src], [src], 8, n)
+    p = api.vector_from([src], [src], 8, n)
+    levels = 0
+    while True:
+        levels += 1
+        api.vxm(q, p, None, "GxB_ANY_SECONDI_INT64", q, A, "GrB_DESC_RSC")
+        if api.vnvals(q) == 0:
+            break
+        api.assign_all(p, q, None, q, n, "GrB_DESC_S")
+    idx, par = api.vector_to(p, 8)
+    parent = np.full(n, -1, np.int64)
+    parent[idx] = par
+    want, _ = oracle.bfs(n, S.p, S.i, src)
+    assert np.array_equal(parent, want)
+    for v in (q, p):
+        api.vfree(v)
+    api.free(A)
+
+
+# (replace, complement, structural) of each predefined descriptor
+DESC_FLAGS = {None: (False, False, False), "GrB_DESC_R": (True, False, False),
+              "GrB_DESC_S": (False, False, True), "GrB_DESC_RS": (True, False, True),
+              "GrB_DESC_SC": (False, True, True), "GrB_DESC_RSC": (True, True, True),
+              "GrB_DESC_C": (False, True, False), "GrB_DESC_RC": (True, True, False)}
+
+
+@pytest.mark.parametrize("accum", [None, "GrB_PLUS_FP64", "GrB_MIN_FP64",
+                                   "GrB_SECOND_FP64"])
+@pytest.mark.parametrize("desc", [None, "GrB_DESC_R", "GrB_DESC_S", "GrB_DESC_RS",
+                                  "GrB_DESC_SC", "GrB_DESC_RSC", "GrB_DESC_C",
+                                  "GrB_DESC_RC"])
+def test_mxm_accum_mask_replace(api, oracle, accum, desc):
+    m, k, n = 70, 60, 80
+    Ac = random_csr(m, k, 0.1, 1)
+    Bc = random_csr(k, n, 0.1, 2)
+    Mc = random_csr(m, n, 0.3, 3)
+    Mc.x = (np.arange(Mc.nnz) % 3).astype(np.float64)      # a third are false
+    Cc = random_csr(m, n, 0.2, 4)
+    A, B = api.matrix_from_csr(Ac), api.matrix_from_csr(Bc)
+    use_mask = desc is not None and desc != "GrB_DESC_R"
+    M = api.matrix_from_csr(Mc) if use_mask else None
+    C = api.matrix_from_csr(Cc)
+    api.mxm(C, M, accum, "GrB_PLUS_TIMES_SEMIRING_FP64", A, B, desc)
+    got = api.matrix_to_csr(C, 11, m)
+    T = oracle.saxpy(m, n, (Ac.p, Ac.i, Ac.x, 11), (Bc.p, Bc.i, Bc.x, 11), "PLUS",
+                     "TIMES", 11)
+    replace, comp, strct = DESC_FLAGS[desc]
+    acc = {None: None, "GrB_PLUS_FP64": "PLUS", "GrB_MIN_FP64": "MIN",
+           "GrB_SECOND_FP64": "SECOND"}[accum]
+    want = oracle.accum_mask(m, n, (Cc.p, Cc.i, Cc.x), T, 11,
+                             M=(Mc.p, Mc.i, Mc.x, 11) if use_mask else None,
+                             mask_struct=strct, mask_comp=comp, replace=replace,
+                             accum=acc)
+    assert_exact(got, want, "accum=%s desc=%s" % (accum, desc))
+    for X in (A, B, M, C):
+        if X is not None:
+            api.free(X)
+
+
+@pytest.mark.parametrize("desc", ["GrB_DESC_T0", "GrB_DESC_T1", "GrB_DESC_T0T1"])
+def test_mxm_transposes(api, oracle, desc):
+    m, k, n = 50, 65, 45
+    Ac = random_csr(m, k, 0.1, 5)
+    Bc = random_csr(k, n, 0.1, 6)
+    At, Bt = transpose_csr(Ac), transpose_csr(Bc)
+    A = api.matrix_from_csr(At if "T0" in desc else Ac)
+    B = api.matrix_from_csr(Bt if "T1" in desc else Bc)
+    C = api.matrix_new(11, m, n)
+    api.mxm(C, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", A, B, desc)
+    got = api.matrix_to_csr(C, 11, m)
+    want = oracle.saxpy(m, n, (Ac.p, Ac.i, Ac.x, 11), (Bc.p, Bc.i, Bc.x, 11), "PLUS",
+                        "TIMES", 11)
+    assert_exact(got, want, desc)
+    for X in (A, B, C):
+        api.free(X)
+
+
+def test_mxv_and_vxm_transposed(api, oracle):
+    m, n = 90, 70
+    Ac = random_csr(m, n, 0.1, 7)
+    rng = np.random.default_rng(8)
+    ui = np.sort(rng.choice(n, 30, replace=False)).astype(np.int64)
+    ux = rng.random(30)
+    A = api.matrix_from_csr(Ac)
+    u = api.vector_from(ui, ux, 11, n)
+    w = api.vector_new(11, m)
+    api.mxv(w, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", A, u, None)
+    wi, wx = api.vector_to(w, 11)
+    # oracle: dot of each row of A with u, ascending k (rows of M = all rows)
+    U1 = (np.array([0, 30], np.int64), ui, ux, 11)
+    Mall = (np.arange(m + 1, dtype=np.int64), np.zeros(m, np.int64), None, 1)
+    want = oracle.dot3(m, 1, (Ac.p, Ac.i, Ac.x, 11), U1, Mall, "PLUS", "TIMES", 11)
+    rows = np.repeat(np.arange(m), np.diff(want[0]))
+    assert np.array_equal(wi, rows)
+    assert np.array_equal(wx, want[2])
+    # w' = u'*A' equals A*u
+    w2 = api.vector_new(11, m)
+    api.vxm(w2, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", u, A, "GrB_DESC_T1")
+    wi2, wx2 = api.vector_to(w2, 11)
+    assert np.array_equal(wi2, wi) and np.array_equal(wx2, wx)
+    for v in (u, w, w2):
+        api.vfree(v)
+    api.free(A)
+
+
+def test_api_error_codes(api):
+    from graphblas_b200.grb import GrBError
+    A = api.matrix_from_csr(random_csr(10, 12, 0.3, 1))
+    B = api.matrix_from_csr(random_csr(10, 12, 0.3, 2))
+    C = api.matrix_new(11, 10, 12)
+    with pytest.raises(GrBError) as e:                 # 10x12 * 10x12
+        api.mxm(C, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", A, B, None)
+    assert e.value.info == -6                          # GrB_DIMENSION_MISMATCH
+    Ci = api.matrix_new(8, 10, 10)
+    with pytest.raises(GrBError) as e:
+        api.mxm(Ci, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", A, B, "GrB_DESC_T1")
+    assert e.value.info == -5                          # GrB_DOMAIN_MISMATCH
+    with pytest.raises(GrBError) as e:
+        api.call("GrB_mxm", C, None, None, None, A, B, None)
+    assert e.value.info == -2                          # GrB_NULL_POINTER
+    for X in (A, B, C, Ci):
+        api.free(X)
+
+
+def test_api_out_of_memory_injection(api, gpu):
+    """Host-side fault injection (the reference's malloc_debug idea): the next
+    device allocation fails and the call returns GrB_OUT_OF_MEMORY cleanly;
+    the following call succeeds."""
+    from graphblas_b200.grb import GrBError
+    Ac = random_csr(40, 40, 0.2, 9)
+    A = api.matrix_from_csr(Ac)
+    C = api.matrix_new(11, 40, 40)
+    api.mxm(C, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", A, A, None)   # warm
+    gpu.lib().grb_b200_debug_fail_alloc(1)
+    with pytest.raises(GrBError) as e:
+        api.mxm(C, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", A, A, None)
+    assert e.value.info == -102
+    gpu.lib().grb_b200_debug_fail_alloc(0)
+    api.mxm(C, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", A, A, None)
+    assert api.nvals(C) > 0
+    api.free(A)
+    api.free(C)

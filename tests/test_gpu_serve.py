@@ -1,0 +1,111 @@
+"""The request server: continuous batching over device-resident graphs.
+
+* In the mix (8 slots, requests arriving faster than they finish, kernels of
+  several requests overlapping on the device) every result equals the same
+  request run alone (1 slot, no overlap), bit for bit, and matches the
+  oracle (oracle/oracle.c).
+* Admission: a request whose HBM footprint exceeds the budget is rejected
+  with GrB_OUT_OF_MEMORY and the others still complete; the running set never
+  holds more than the budget.
+* Failure injection on the host: a device allocation that fails makes its
+  request fail cleanly (GrB_OUT_OF_MEMORY) and the server carries on.
+"""
+
+import numpy as np
+import pytest
+
+from graphblas_b200 import workloads as W
+from tests.helpers import assert_exact
+
+pytestmark = pytest.mark.gpu
+
+
+def _graphs():
+    from graphblas_b200.serve import make_graphs
+    return make_graphs(seed=5, tc_scales=range(8, 11), n_sssp=1, n_mxm=2, mxm_nmax=3000)
+
+
+def test_mixed_results_equal_alone_and_oracle(gpu, oracle):
+    from graphblas_b200.serve import Server, make_trace, K_TRICOUNT, K_SSSP, K_MXM
+    graphs = _graphs()
+    trace = make_trace(graphs, nreq=180, rate=50000.0, seed=7)
+    mix = Server(nslots=8, budget_bytes=8 << 30)
+    for kind, g in graphs:
+        mix.add_graph(kind, g)
+    mix.replay(trace)
+    st = mix.stats()
+    assert st["completed"] == 180 and st["failed"] == 0 and st["rejected"] == 0
+    assert st["peak_active"] > 1                     # requests overlapped
+    alone = Server(nslots=1, budget_bytes=8 << 30)
+    for kind, g in graphs:
+        alone.add_graph(kind, g)
+    slow = dict(trace)
+    slow["t"] = np.arange(len(trace["t"])) * 1e-4    # one at a time, in order
+    alone.replay(slow)
+    assert alone.stats()["peak_active"] == 1
+    tri_cache = {}
+    for k in range(180):
+        kind = int(trace["kind"][k])
+        g = graphs[int(trace["graph"][k])][1]
+        a, b = mix.request(k), alone.request(k)
+        assert a["status"] == 0 and b["status"] == 0
+        assert a["count"] == b["count"]
+        if kind == K_TRICOUNT:
+            gid = int(trace["graph"][k])
+            if gid not in tri_cache:
+                L, U = W.tril_triu(g)
+                tri_cache[gid] = oracle.tricount(g.nrows, L.p, L.i, U.p, U.i)
+            assert a["count"] == tri_cache[gid]
+        else:
+            ra, rb = mix.result(k, kind), alone.result(k, kind)
+            assert_exact(ra, rb, "request %d mixed vs alone" % k)
+            if k % 7 == 0:
+                if kind == K_SSSP:
+                    lo, hi = trace["fp"][k], trace["fp"][k + 1]
+                    ui, ux = trace["fi"][lo:hi], trace["fx"][lo:hi]
+                    u = (np.array([0, len(ui)], np.int64), ui, ux, 10)
+                    want = oracle.saxpy(1, g.ncols, u, (g.p, g.i, g.x, 10), "MIN", "PLUS", 10)
+                else:
+                    want = oracle.saxpy(g.nrows, g.ncols, (g.p, g.i, g.x, 11),
+                                        (g.p, g.i, g.x, 11), "PLUS", "TIMES", 11)
+                assert_exact(ra, want, "request %d vs oracle" % k)
+    mix.free()
+    alone.free()
+
+
+def test_admission_rejects_oversize_and_bounds_memory(gpu):
+    from graphblas_b200.serve import Server, make_trace
+    graphs = _graphs()
+    trace = make_trace(graphs, nreq=60, rate=20000.0, seed=9)
+    budget = 4 << 20                                  # 4 MiB: the big ones never fit
+    S = Server(nslots=4, budget_bytes=budget)
+    for kind, g in graphs:
+        S.add_graph(kind, g)
+    S.replay(trace)
+    st = S.stats()
+    assert st["rejected"] > 0
+    assert st["completed"] + st["rejected"] + st["failed"] == 60
+    assert st["completed"] > 0
+    assert st["peak_bytes"] <= budget
+    for k in range(60):
+        r = S.request(k)
+        assert r["status"] in (0, -102)
+    S.free()
+
+
+def test_injected_allocation_failure_is_isolated(gpu):
+    from graphblas_b200.serve import Server, make_trace
+    graphs = _graphs()
+    trace = make_trace(graphs, nreq=40, rate=2000.0, seed=11)
+    S = Server(nslots=1, budget_bytes=8 << 30)
+    for kind, g in graphs:
+        S.add_graph(kind, g)
+    gpu.lib().grb_b200_debug_fail_alloc(3)            # the 3rd allocation fails
+    S.replay(trace)
+    gpu.lib().grb_b200_debug_fail_alloc(0)
+    st = S.stats()
+    assert st["failed"] == 1
+    assert st["completed"] == 39
+    statuses = [S.request(k)["status"] for k in range(40)]
+    assert statuses.count(-102) == 1
+    S.free()
