@@ -115,6 +115,13 @@ class ClockSampler:
 # workloads
 # ---------------------------------------------------------------------------
 
+def scan_launches(n, tile=4096):
+    """Kernel launches of the library's device scan of n values (two per
+    level of the tile tree)."""
+    nb = (n + tile - 1) // tile
+    return 2 + (scan_launches(nb, tile) if nb > 1 else 0)
+
+
 class TriCount:
     metric, unit, dtype, kernel = "triangles/s", "triangles/s", "int64", "dot3"
 
@@ -171,7 +178,12 @@ class TriCount:
         return n
 
     def launches_per_step(self):
-        return 4            # classify, intersect, reduce partial, reduce final
+        # classify, intersect, reduce partial + final; with the bitmap path
+        # (masks of 65536+ entries) also group sizes, two scans over the
+        # group keys, route, item count, item fill and the bitmap kernel
+        if self.L.nnz < (1 << 16):
+            return 4
+        return 4 + 5 + 2 * scan_launches(self.S.nrows + self.U.nrows + 1)
 
     def cpu_baseline(self, R, ncores):
         ntri, times = R.tricount(self.S.nrows, self.L.p, self.L.i, self.U.p, self.U.i, reps=1)

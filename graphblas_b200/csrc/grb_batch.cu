@@ -159,28 +159,26 @@ int build_blockdiag(DevCSR &D, int count, const std::vector<int64_t> &rows,
 std::vector<SaxpyConfig> candidates()
 {
     std::vector<SaxpyConfig> v;
-    SaxpyConfig c = saxpy_default_config();
-    v.push_back(c);                                            // 64/8, 256/32, ...
-    SaxpyConfig a;
-    a.nb = 4;
-    a.bin[0] = {32, 4, 64}; a.bin[1] = {128, 16, 256};
-    a.bin[2] = {512, 32, 1024}; a.bin[3] = {4096, 256, 8192};
-    v.push_back(a);
-    SaxpyConfig b = c;
-    b.bin[0] = {64, 16, 128};
-    v.push_back(b);
-    SaxpyConfig d = c;
-    d.bin[0] = {64, 4, 128};
-    d.bin[1] = {256, 16, 512};
-    v.push_back(d);
-    SaxpyConfig e;
-    e.nb = 5;
-    e.bin[0] = {16, 4, 32}; e.bin[1] = {64, 8, 128}; e.bin[2] = {256, 32, 512};
-    e.bin[3] = {1024, 32, 2048}; e.bin[4] = {4096, 256, 8192};
-    v.push_back(e);
-    SaxpyConfig f = c;
-    f.bin[0] = {128, 8, 256};
-    v.push_back(f);
+    SaxpyConfig c = saxpy_default_config();           // ESC <= 256, hash above
+    v.push_back(c);
+    SaxpyConfig e1;                                    // ESC <= 128 only
+    e1.nb = 4;
+    e1.bin[0] = {128, 1, 128}; e1.bin[1] = {256, 32, 512};
+    e1.bin[2] = {1024, 32, 2048}; e1.bin[3] = {4096, 256, 8192};
+    v.push_back(e1);
+    SaxpyConfig e2 = c;                                // ESC <= 512
+    e2.bin[0] = {512, 1, 512};
+    v.push_back(e2);
+    SaxpyConfig h;                                     // hash only
+    h.nb = 4;
+    h.bin[0] = {64, 8, 128}; h.bin[1] = {256, 32, 512};
+    h.bin[2] = {1024, 32, 2048}; h.bin[3] = {4096, 256, 8192};
+    v.push_back(h);
+    SaxpyConfig h2;                                    // hash, finer classes
+    h2.nb = 5;
+    h2.bin[0] = {16, 4, 32}; h2.bin[1] = {64, 8, 128}; h2.bin[2] = {256, 32, 512};
+    h2.bin[3] = {1024, 32, 2048}; h2.bin[4] = {4096, 256, 8192};
+    v.push_back(h2);
     for (int bps : {8, 32}) {
         SaxpyConfig g = c;
         g.blocks_per_sm = bps;

@@ -31,9 +31,11 @@
 // counted in C.nzombies; C keeps M's row pointers, as the reference's dot3
 // does (GB_AxB_dot3.c:172-197).
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include "../../include/grb_b200.h"
 #include "grb_runtime.h"
 #include "grb_semirings.h"
@@ -85,7 +87,8 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
                 const void *__restrict__ Bx, bool b_iso,
                 int32_t *__restrict__ Cj, typename SR::z_t *__restrict__ Cx,
                 D3Work *__restrict__ queue, int *__restrict__ qlen,
-                unsigned long long *__restrict__ nzombies)
+                unsigned long long *__restrict__ nzombies,
+                int32_t *__restrict__ gcnt, uint32_t bm_bits)
 {
     using Z = typename SR::z_t;
     const int lane = threadIdx.x & 31;
@@ -101,7 +104,7 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
         r0 = __shfl_sync(0xffffffffu, r0, 0);
         int32_t i = r0;
         if (valid) while (Mp[i + 1] <= pm) i++;
-        int32_t j = 0, a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+        int32_t j = 0, a0 = 0, a1 = 0, b0 = 0, b1 = 0, key = -1;
         bool coop = false, exists = false;
         Z cij = Z();
         if (valid) {
@@ -137,6 +140,17 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
                             }
                         } else {
                             coop = true;
+                            if (bm_bits && min(a1 - a0, b1 - b0) <= (1 << 20)) {
+                                // bitmap of the longer list's whole row, if
+                                // its column span fits the bitmap (probed
+                                // lists of at most 2^20 keep the bitmap
+                                // kernel's per-round probe sums in int32)
+                                if ((a1 - a0) > (b1 - b0)) {
+                                    if ((uint32_t)(Aj[pa1 - 1] - Aj[pa0]) < bm_bits) key = i;
+                                } else if ((uint32_t)(bhi - blo) < bm_bits) {
+                                    key = (int32_t)nrows + j;
+                                }
+                            }
                         }
                     }
                 }
@@ -154,7 +168,16 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
             qbase = __shfl_sync(0xffffffffu, qbase, 0);
             if (coop) {
                 const int slot = qbase + __popc(q & ((1u << lane) - 1));
-                queue[slot] = D3Work{(int32_t)pm, i, j, a0, a1, b0, b1, 0};
+                queue[slot] = D3Work{(int32_t)pm, i, j, a0, a1, b0, b1, key};
+            }
+        }
+        if (bm_bits) {
+            // group sizes, one atomic per distinct key in the warp
+            const bool grouped = coop && key >= 0;
+            const unsigned gm = __ballot_sync(0xffffffffu, grouped);
+            if (grouped) {
+                const unsigned same = __match_any_sync(gm, key);
+                if ((int)(__ffs(same) - 1) == lane) atomicAdd(&gcnt[key], __popc(same));
             }
         }
     }
@@ -190,8 +213,8 @@ __device__ __forceinline__ void fold_matches(unsigned mm, bool match,
 
 template <class SR>
 __global__ void __launch_bounds__(256)
-k_dot3_intersect(const D3Work *__restrict__ queue, const int *__restrict__ qlen_p,
-                 int *__restrict__ qnext,
+k_dot3_intersect(const D3Work *__restrict__ queue, const int32_t *__restrict__ sel,
+                 const int *__restrict__ qlen_p, int *__restrict__ qnext,
                  const int32_t *__restrict__ Aj, const void *__restrict__ Ax, bool a_iso,
                  const int32_t *__restrict__ Bj, const void *__restrict__ Bx, bool b_iso,
                  int32_t *__restrict__ Cj, typename SR::z_t *__restrict__ Cx,
@@ -208,7 +231,7 @@ k_dot3_intersect(const D3Work *__restrict__ queue, const int *__restrict__ qlen_
         if (w0 >= qlen) break;
         const int w1 = min(w0 + D3_BATCH, qlen);
         for (int w = w0; w < w1; w++) {
-            const D3Work e = queue[w];
+            const D3Work e = queue[sel ? sel[w] : w];
             const int32_t nA = e.a1 - e.a0, nB = e.b1 - e.b0;
             const int32_t nS = nA < nB ? nA : nB, nL = nA < nB ? nB : nA;
             Part<Z> part{Z(), false};
@@ -311,6 +334,300 @@ k_dot3_intersect(const D3Work *__restrict__ queue, const int *__restrict__ qlen_
     if (lane == 0 && zcount) atomicAdd(nzombies, zcount);
 }
 
+// ---------------------------------------------------------------------------
+// bitmap path for counting semirings (PLUS_PAIR on integers: triangle and
+// support counts)
+//
+// A long entry is intersected by probing the elements of its shorter list in
+// a shared-memory bitmap of its longer list's whole row, so the longer list
+// is read once per group of entries sharing it instead of once per entry:
+// entries whose A(i,:) is longer are grouped by i, those whose B(j,:) is
+// longer by j (key nrows + j).  The result of PLUS_PAIR is the number of
+// matches, which needs neither values nor an order.  Groups with fewer than
+// D3_GMIN entries, and rows whose column span does not fit the bitmap, stay
+// on the merge path.
+// ---------------------------------------------------------------------------
+
+static constexpr int D3_GMIN = 16;             // smallest group worth a bitmap
+static constexpr int64_t D3_WCHUNK = 1 << 20;  // probes per work item
+static constexpr int D3_BM_THREADS = 1024;
+
+struct D3Item { int32_t key, t, nit, pad; };
+
+template <class SR> struct IsCount {
+    static constexpr bool value = SR::add_op == OP_PLUS && SR::mult_op == OP_PAIR &&
+        std::is_integral<typename SR::z_t>::value &&
+        !std::is_same<typename SR::z_t, bool>::value;
+};
+
+// group size kept (0 below D3_GMIN), as int64 for the offsets scan
+__global__ void k_d3_gsize(const int32_t *__restrict__ gcnt, int64_t nkeys,
+                           int64_t *__restrict__ gsz)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; t < nkeys; t += stride) {
+        const int32_t c = gcnt[t];
+        gsz[t] = c >= D3_GMIN ? c : 0;
+    }
+}
+
+// route every queued entry to its group's bucket or to the merge list
+__global__ void __launch_bounds__(256)
+k_d3_route(const D3Work *__restrict__ queue, const int *__restrict__ qlen_p,
+           const int64_t *__restrict__ gsz, const int64_t *__restrict__ goff,
+           int32_t *__restrict__ gfill, unsigned long long *__restrict__ gwork,
+           int32_t *__restrict__ bucket, int32_t *__restrict__ merge_sel,
+           int *__restrict__ merge_len)
+{
+    const int lane = threadIdx.x & 31;
+    const int qlen = *qlen_p;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+         base < qlen; base += nw * 32) {
+        const int w = (int)(base + lane);
+        bool grouped = false, merge = false;
+        int32_t key = -1;
+        unsigned long long work = 0;
+        if (w < qlen) {
+            const D3Work e = queue[w];
+            key = e.pad;
+            grouped = key >= 0 && gsz[key] > 0;
+            merge = !grouped;
+            // probes: the shorter list's elements
+            work = (unsigned long long)min(e.a1 - e.a0, e.b1 - e.b0);
+        }
+        const unsigned gm = __ballot_sync(0xffffffffu, grouped);
+        if (grouped) {
+            const unsigned same = __match_any_sync(gm, key);
+            const int leader = __ffs(same) - 1;
+            // the leader reserves slots and adds the work of its lanes (the
+            // work only balances items: each lane's share is capped at 2^26)
+            const unsigned wsum = __reduce_add_sync(same, (unsigned)min(work, 1ull << 26));
+            int slot0 = 0;
+            if (lane == leader) {
+                slot0 = atomicAdd(&gfill[key], __popc(same));
+                atomicAdd(&gwork[key], (unsigned long long)wsum);
+            }
+            slot0 = __shfl_sync(same, slot0, leader);
+            bucket[goff[key] + slot0 + __popc(same & ((1u << lane) - 1))] = w;
+        }
+        const unsigned mm = __ballot_sync(0xffffffffu, merge);
+        if (mm) {
+            int mbase = 0;
+            if (lane == 0) mbase = atomicAdd(merge_len, __popc(mm));
+            mbase = __shfl_sync(0xffffffffu, mbase, 0);
+            if (merge) merge_sel[mbase + __popc(mm & ((1u << lane) - 1))] = w;
+        }
+    }
+}
+
+// work items per group: about one per D3_WCHUNK probes, at most one per 32
+// entries (so the items never outnumber nkeys + entries / 32)
+__global__ void k_d3_item_count(const int64_t *__restrict__ gsz,
+                                const unsigned long long *__restrict__ gwork,
+                                int64_t nkeys, int64_t *__restrict__ nit)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; t < nkeys; t += stride) {
+        const int64_t g = gsz[t];
+        int64_t n = 0;
+        if (g > 0) {
+            n = 1 + (int64_t)(gwork[t] / D3_WCHUNK);
+            const int64_t mx = g / 32 > 1 ? g / 32 : 1;
+            if (n > mx) n = mx;
+        }
+        nit[t] = n;
+    }
+}
+
+__global__ void k_d3_item_fill(const int64_t *__restrict__ ioff, int64_t nkeys,
+                               D3Item *__restrict__ items)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; t < nkeys; t += stride) {
+        const int64_t o = ioff[t], n = ioff[t + 1] - o;
+        for (int64_t q = 0; q < n; q++) items[o + q] = D3Item{(int32_t)t, (int32_t)q, (int32_t)n, 0};
+    }
+}
+
+// One block per SM, persistent: take an item, set the bits of its key row
+// (A(i,:) or B(j,:), relative to the row's first column) in shared memory,
+// then count, for every entry of the item, the elements of its other
+// (trimmed) list that hit the bitmap.  The item's entries are flattened into
+// one sequence of probes split evenly over the block's warps; each warp walks
+// its share in steps of 32 probes and adds each run of lanes that belongs to
+// one entry into that entry's shared counter.  The bits are cleared again
+// from the row before the next item.
+template <class SR>
+__global__ void __launch_bounds__(D3_BM_THREADS, 1)
+k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict__ nitems_p,
+                    int *__restrict__ inext, const int64_t *__restrict__ goff,
+                    const int32_t *__restrict__ bucket, const D3Work *__restrict__ queue,
+                    int32_t nrows,
+                    const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+                    const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
+                    uint32_t bm_words, int32_t *__restrict__ Cj,
+                    typename SR::z_t *__restrict__ Cx,
+                    unsigned long long *__restrict__ nzombies)
+{
+    using Z = typename SR::z_t;
+    extern __shared__ uint32_t bm[];
+    __shared__ int s_item;
+    __shared__ int32_t s_pre[D3_BM_THREADS];    // inclusive probe counts
+    __shared__ int32_t s_cnt[D3_BM_THREADS];    // matches per entry
+    __shared__ int32_t s_s0[D3_BM_THREADS];     // start of each probed list
+    __shared__ int32_t s_wsum[D3_BM_THREADS / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nwarps = blockDim.x >> 5;
+    for (uint32_t q = tid; q < bm_words; q += blockDim.x) bm[q] = 0;
+    const int64_t nitems = *nitems_p;
+    unsigned long long zc = 0;
+    while (true) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(inext, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) break;
+        const D3Item I = items[it];
+        const bool by_row = I.key < nrows;
+        const int32_t r = by_row ? I.key : I.key - nrows;
+        const int32_t *P = by_row ? Ap : Bp;
+        const int32_t *J = by_row ? Aj : Bj;
+        const int32_t *S = by_row ? Bj : Aj;     // the probed lists
+        const int32_t rp0 = P[r], rp1 = P[r + 1];
+        const int32_t lo = J[rp0];
+        for (int32_t q = rp0 + tid; q < rp1; q += blockDim.x) {
+            const uint32_t k = (uint32_t)(J[q] - lo);
+            atomicOr(&bm[k >> 5], 1u << (k & 31));
+        }
+        const int64_t g0 = goff[I.key];
+        const int32_t gn = (int32_t)(goff[I.key + 1] - g0);
+        const int32_t m_item = (gn - I.t + I.nit - 1) / I.nit;
+        // rounds of up to one entry per thread
+        for (int32_t rb = 0; rb < m_item; rb += blockDim.x) {
+            const int32_t rr = rb + tid;
+            int32_t s0 = 0, len = 0, pm = 0, j = 0;
+            if (rr < m_item) {
+                const D3Work e = queue[bucket[g0 + I.t + (int64_t)I.nit * rr]];
+                s0 = by_row ? e.b0 : e.a0;
+                len = by_row ? e.b1 - e.b0 : e.a1 - e.a0;
+                pm = e.pm;
+                j = e.j;
+            }
+            // block inclusive scan of len
+            int v = len;
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += y;
+            }
+            if (lane == 31) s_wsum[warp] = v;
+            __syncthreads();                 // also orders the bitmap build
+            if (warp == 0) {
+                int ws = lane < nwarps ? s_wsum[lane] : 0;
+                #pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, ws, o);
+                    if (lane >= o) ws += y;
+                }
+                if (lane < nwarps) s_wsum[lane] = ws;
+            }
+            __syncthreads();
+            const int incl = v + (warp > 0 ? s_wsum[warp - 1] : 0);
+            s_pre[tid] = incl;
+            s_s0[tid] = s0;
+            s_cnt[tid] = 0;
+            const int nr = min((int)blockDim.x, m_item - rb);
+            const int total = s_wsum[nwarps - 1];
+            __syncthreads();
+            // this warp's share of the probes [q_begin, q_end)
+            const int q_begin = (int)((int64_t)total * warp / nwarps);
+            const int q_end = (int)((int64_t)total * (warp + 1) / nwarps);
+            // entry holding probe q_begin: first e with s_pre[e] > q_begin
+            int e_lane = 0;
+            {
+                int lo2 = 0, hi2 = nr;
+                while (lo2 < hi2) {
+                    const int mid = (lo2 + hi2) >> 1;
+                    if (s_pre[mid] <= q_begin) lo2 = mid + 1; else hi2 = mid;
+                }
+                e_lane = lo2;
+            }
+            for (int q0 = q_begin; q0 < q_end; q0 += 32) {
+                const int q = q0 + lane;
+                const bool act = q < q_end;
+                bool hit = false;
+                if (act) {
+                    while (s_pre[e_lane] <= q) e_lane++;
+                    const int ex = e_lane > 0 ? s_pre[e_lane - 1] : 0;
+                    const uint32_t k = (uint32_t)(S[s_s0[e_lane] + (q - ex)] - lo);
+                    hit = k < bm_words * 32u && ((bm[k >> 5] >> (k & 31)) & 1u);
+                }
+                const unsigned hits = __ballot_sync(0xffffffffu, hit);
+                // lanes of one entry are consecutive: the first lane of each
+                // run adds the run's hits
+                const int e_prev = __shfl_up_sync(0xffffffffu, e_lane, 1);
+                const bool head = act && (lane == 0 || e_prev != e_lane);
+                const unsigned heads = __ballot_sync(0xffffffffu, head);
+                if (head) {
+                    const unsigned higher = heads & ~((2u << lane) - 1u);
+                    const int end = higher ? __ffs(higher) - 1 : 32;
+                    const unsigned seg = (end == 32 ? 0xffffffffu : ((1u << end) - 1u)) &
+                                         ~((1u << lane) - 1u);
+                    const int c = __popc(hits & seg);
+                    if (c) atomicAdd(&s_cnt[e_lane], c);
+                }
+            }
+            __syncthreads();
+            if (rr < m_item) {
+                const int c = s_cnt[tid];
+                if (c) { Cj[pm] = j; Cx[pm] = (Z)c; }
+                else { Cj[pm] = flip(j); zc++; }
+            }
+            __syncthreads();
+        }
+        __syncthreads();
+        for (int32_t q = rp0 + tid; q < rp1; q += blockDim.x) {
+            const uint32_t k = (uint32_t)(J[q] - lo);
+            bm[k >> 5] = 0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) zc += __shfl_down_sync(0xffffffffu, zc, o);
+    if (lane == 0 && zc) atomicAdd(nzombies, zc);
+}
+
+static constexpr int64_t D3_BM_MIN_ENTRIES = 1 << 16;   // mask entries
+
+// Words of the shared-memory bitmap: enough for every column index (plus one
+// word of slack) when that fits beside the kernel's static shared memory,
+// else the most that fits (rows spanning more columns stay on the merge
+// path).  0 disables the bitmap path.
+template <class SR>
+static uint32_t bitmap_words(int64_t ncols)
+{
+    static int64_t avail = -1;
+    if (avail < 0) {
+        const void *fn = (const void *)k_dot3_bitmap_count<SR>;
+        cudaFuncAttributes fa;
+        int64_t a = 0;
+        if (cudaFuncGetAttributes(&fa, fn) == cudaSuccess) {
+            a = (int64_t)runtime().smem_optin - (int64_t)fa.sharedSizeBytes - 1024;
+            if (a < 0 ||
+                cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)a) != cudaSuccess)
+                a = 0;
+        }
+        cudaGetLastError();
+        avail = a / 4;
+    }
+    const int64_t need = (ncols + 31) / 32 + 1;
+    const int64_t w = need < avail ? need : avail;
+    return w >= 1024 || w == need ? (uint32_t)w : 0;
+}
+
 template <class SR>
 static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
                        const DevCSR &A, const DevCSR &B, cudaStream_t s)
@@ -328,20 +645,73 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
     }
     cudaMemcpyAsync(C.p, M.p, (size_t)(M.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
     cudaMemsetAsync(counter, 0, 64, s);
-    int *qlen = counter, *qnext = counter + 1;
+    int *qlen = counter, *qnext = counter + 1, *merge_len = counter + 2, *inext = counter + 3;
     unsigned long long *zc = (unsigned long long *)((char *)counter + 32);
+    // the bitmap path: counting semirings on masks large enough to pay for it
+    const int64_t nkeys = M.nrows + B.nrows;
+    uint32_t bm_words = 0;
+    if constexpr (IsCount<SR>::value) {
+        if (mnz >= D3_BM_MIN_ENTRIES && nkeys < INT32_MAX) bm_words = bitmap_words<SR>(A.ncols);
+    }
+    Scratch bm_scratch(s);
+    int32_t *gcnt = nullptr, *gfill = nullptr, *bucket = nullptr, *merge_sel = nullptr;
+    int64_t *gsz = nullptr, *goff = nullptr, *nit = nullptr, *ioff = nullptr, *ws = nullptr;
+    unsigned long long *gwork = nullptr;
+    D3Item *items = nullptr;
+    if (bm_words) {
+        gcnt = bm_scratch.get<int32_t>(nkeys);
+        gfill = bm_scratch.get<int32_t>(nkeys);
+        gsz = bm_scratch.get<int64_t>(nkeys + 1);
+        goff = bm_scratch.get<int64_t>(nkeys + 1);
+        nit = bm_scratch.get<int64_t>(nkeys + 1);
+        ioff = bm_scratch.get<int64_t>(nkeys + 1);
+        gwork = bm_scratch.get<unsigned long long>(nkeys);
+        items = bm_scratch.get<D3Item>(nkeys + mnz / 32 + 1);
+        bucket = bm_scratch.get<int32_t>(mnz);
+        merge_sel = bm_scratch.get<int32_t>(mnz);
+        ws = bm_scratch.get<int64_t>((int64_t)scan_ws_elems(nkeys + 1));
+        if (bm_scratch.failed) {
+            dev_free(C, s); dfree(counter, s); dfree(queue, s); return OUT_OF_MEMORY;
+        }
+    }
     if (mnz > 0 && M.nrows > 0) {
         const int nsm = runtime().num_sms;
         int64_t warps_needed = (mnz + 31) / 32;
         int64_t blocks = (warps_needed + 7) / 8;
         if (blocks > (int64_t)nsm * 16) blocks = (int64_t)nsm * 16;
         const int ps = prof_begin("dot3", s);
+        if (bm_words) {
+            cudaMemsetAsync(gcnt, 0, (size_t)nkeys * 4, s);
+            cudaMemsetAsync(gfill, 0, (size_t)nkeys * 4, s);
+            cudaMemsetAsync(gwork, 0, (size_t)nkeys * 8, s);
+            cudaMemsetAsync(gsz + nkeys, 0, 8, s);
+            cudaMemsetAsync(nit + nkeys, 0, 8, s);
+        }
         k_dot3_classify<SR><<<(unsigned)blocks, 256, 0, s>>>(
             M.p, M.j, mask_struct ? nullptr : M.x, M.type, mask_struct, mnz, M.nrows,
             A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso, C.j, (Z *)C.x,
-            queue, qlen, zc);
-        k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
-            queue, qlen, qnext, A.j, A.x, A.iso, B.j, B.x, B.iso, C.j, (Z *)C.x, zc);
+            queue, qlen, zc, gcnt, bm_words * 32u);
+        if (bm_words) {
+            const int kb = (int)std::min<int64_t>((nkeys + 255) / 256, (int64_t)nsm * 8);
+            k_d3_gsize<<<kb, 256, 0, s>>>(gcnt, nkeys, gsz);
+            scan_exclusive_i64_ws(gsz, goff, nkeys + 1, ws, s);
+            k_d3_route<<<(unsigned)blocks, 256, 0, s>>>(queue, qlen, gsz, goff, gfill, gwork,
+                                                       bucket, merge_sel, merge_len);
+            k_d3_item_count<<<kb, 256, 0, s>>>(gsz, gwork, nkeys, nit);
+            scan_exclusive_i64_ws(nit, ioff, nkeys + 1, ws, s);
+            k_d3_item_fill<<<kb, 256, 0, s>>>(ioff, nkeys, items);
+            if constexpr (IsCount<SR>::value)
+                k_dot3_bitmap_count<SR><<<nsm, D3_BM_THREADS, (size_t)bm_words * 4, s>>>(
+                    items, ioff + nkeys, inext, goff, bucket, queue, (int32_t)M.nrows,
+                    A.p, A.j, B.p, B.j, bm_words, C.j, (Z *)C.x, zc);
+            k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
+                queue, merge_sel, merge_len, qnext, A.j, A.x, A.iso, B.j, B.x, B.iso,
+                C.j, (Z *)C.x, zc);
+        } else {
+            k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
+                queue, nullptr, qlen, qnext, A.j, A.x, A.iso, B.j, B.x, B.iso, C.j,
+                (Z *)C.x, zc);
+        }
         prof_end(ps, s);
     }
     unsigned long long hz = 0;
@@ -490,9 +860,9 @@ static int dot3_noalloc_launch(int64_t nrows, int64_t mnz, const int32_t *Mp,
         if (blocks > (int64_t)nsm * 16) blocks = (int64_t)nsm * 16;
         k_dot3_classify<SR><<<(unsigned)blocks, 256, 0, s>>>(
             Mp, Mj, nullptr, T_BOOL, true, mnz, nrows, Ap, Aj, Ax, a_iso,
-            Bp, Bj, Bx, b_iso, Cj, (Z *)Cx, queue, qlen, zc);
+            Bp, Bj, Bx, b_iso, Cj, (Z *)Cx, queue, qlen, zc, nullptr, 0u);
         k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
-            queue, qlen, qnext, Aj, Ax, a_iso, Bj, Bx, b_iso, Cj, (Z *)Cx, zc);
+            queue, nullptr, qlen, qnext, Aj, Ax, a_iso, Bj, Bx, b_iso, Cj, (Z *)Cx, zc);
     }
     unsigned long long hz = 0;
     e = cudaMemcpyAsync(&hz, zc, sizeof(hz), cudaMemcpyDeviceToHost, s);

@@ -11,7 +11,10 @@
 //   2. device exclusive scan of the row capacities -> offsets of each row's
 //      slot in a temporary output (capacity = min(flops, ncols, |M(i,:)|)).
 //   3. numeric, one kernel per bin:
-//        tiny/small/medium rows: a group of TPR threads owns one row and a
+//        short rows (<= 256 products by default): one warp expands the row's
+//        products into shared memory, sorts them by (column, position) and
+//        folds equal columns in ascending k (expand-sort-compress);
+//        medium rows: a group of TPR threads owns one row and a
 //        shared-memory open-addressing hash table of CAP slots (the
 //        reference's coarse hash task, GB_AxB_saxpy3_coarseHash_phase5.c,
 //        with linear probing on GB_HASHF-style keys, math/include/GB_hash.h);
@@ -47,34 +50,41 @@ static constexpr uint8_t S_EMPTY = 0, S_ALLOWED = 1, S_SET = 2, S_FORBID = 3;
 // phase 1: flops and capacity per row
 // ---------------------------------------------------------------------------
 
-__global__ void k_flops(const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
-                        const int32_t *__restrict__ Bp,
-                        const int32_t *__restrict__ Mp, bool mask_bounds,
-                        int64_t nrows, int64_t ncols,
-                        int64_t *__restrict__ flops, int64_t *__restrict__ cap)
+// Flat over A's entries, so a row of any length is spread over the whole
+// grid (a one-row A, as in vxm, would otherwise run on one warp): each lane
+// takes one entry A(i,k) and adds nnz(B(k,:)); a segmented scan over the
+// warp's lanes (rows are contiguous in lane order) leaves one atomic per row
+// segment.  flops[] must be zero on entry.
+__global__ void __launch_bounds__(256)
+k_flops_flat(const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+             const int32_t *__restrict__ Bp, int64_t nrows, int64_t nnz,
+             unsigned long long *__restrict__ flops)
 {
-    // one warp per row
-    int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    int lane = threadIdx.x & 31;
-    for (int64_t r = warp; r < nrows; r += nw) {
-        int32_t lo = Ap[r], hi = Ap[r + 1];
-        int64_t f = 0;
-        for (int32_t p = lo + lane; p < hi; p += 32) {
-            int32_t k = Aj[p];
-            f += Bp[k + 1] - Bp[k];
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+         base < nnz; base += nw * 32) {
+        // row of the warp's first entry, then each lane walks to its own
+        int32_t r0 = 0;
+        if (lane == 0) r0 = upper_bound(Ap, 0, (int32_t)nrows + 1, (int32_t)base) - 1;
+        r0 = __shfl_sync(0xffffffffu, r0, 0);
+        const int64_t e = base + lane;
+        int32_t r = -1;
+        unsigned long long f = 0;
+        if (e < nnz) {
+            r = r0;
+            while (Ap[r + 1] <= e) r++;
+            const int32_t k = Aj[e];
+            f = (unsigned long long)(Bp[k + 1] - Bp[k]);
         }
-        for (int o = 16; o > 0; o >>= 1) f += __shfl_down_sync(0xffffffffu, f, o);
-        if (lane == 0) {
-            int64_t c = f < ncols ? f : ncols;
-            if (mask_bounds) {
-                int64_t mc = Mp[r + 1] - Mp[r];
-                if (mc < c) c = mc;
-            }
-            if (f == 0) c = 0;
-            flops[r] = f;
-            cap[r] = c;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, f, o);
+            const int32_t ry = __shfl_up_sync(0xffffffffu, r, o);
+            if (lane >= o && ry == r) f += y;
         }
+        const int32_t rn = __shfl_down_sync(0xffffffffu, r, 1);
+        if (r >= 0 && (lane == 31 || rn != r)) atomicAdd(&flops[r], f);
     }
 }
 
@@ -82,15 +92,24 @@ __global__ void k_flops(const int32_t *__restrict__ Ap, const int32_t *__restric
 // limits on flops + mask entries), nb+1 heavy (dense accumulator)
 struct BinLimits { int nb; int64_t limit[MAX_SMEM_BINS]; };
 
+// The same pass writes each row's slot capacity, min(flops, ncols,
+// |M(i,:)| when a plain mask bounds the row), 0 for an empty row.
 __global__ void k_bin_rows(const int64_t *__restrict__ flops,
                            const int32_t *__restrict__ Mp, bool has_mask,
+                           bool mask_bounds, int64_t ncols,
                            int64_t nrows, BinLimits lim, int *__restrict__ bin_count,
-                           int8_t *__restrict__ row_bin)
+                           int8_t *__restrict__ row_bin, int64_t *__restrict__ cap)
 {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r = t; r < nrows; r += stride) {
         int64_t f = flops[r];
+        int64_t c = f < ncols ? f : ncols;
+        if (mask_bounds) {
+            const int64_t mc = Mp[r + 1] - Mp[r];
+            if (mc < c) c = mc;
+        }
+        cap[r] = f == 0 ? 0 : c;
         int b;
         if (f == 0) b = 0;
         else {
@@ -285,6 +304,151 @@ k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin, int tpr_log2, int 
         for (int q = t; q < cnt; q += TPR) { Tj[off + q] = keys[q]; Tx[off + q] = vals[q]; }
         if (t == 0) row_cnt[i] = cnt;
         gsync();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// phase 3a': expand-sort-compress rows, one warp per row
+// ---------------------------------------------------------------------------
+
+// For rows with at most `cap` products.  The warp expands the row's products
+// in order (A(i,:) in ascending k, each B(k,:) in order) into shared memory,
+// keyed by (column j, position): the loads of all of the row's products are
+// issued at once, with no per-k synchronisation and no hash probing.  A
+// bitonic sort by that key groups equal columns with their terms still in
+// ascending k, and each group is folded in that order with the monoid's
+// UPDATE (first term written, later terms folded), as in the hash kernels,
+// so every semiring, floating PLUS included, gives the same bits.
+static constexpr int ESC_WARPS = 8;
+
+template <class SR>
+__global__ void __launch_bounds__(ESC_WARPS * 32)
+k_saxpy_esc(const int32_t *__restrict__ rows, int nrows_bin, int cap,
+            const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+            const void *__restrict__ Ax, bool a_iso,
+            const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
+            const void *__restrict__ Bx, bool b_iso,
+            const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
+            bool has_mask, bool mask_comp,
+            const int64_t *__restrict__ slot_off,
+            int32_t *__restrict__ Tj, typename SR::z_t *__restrict__ Tx,
+            int32_t *__restrict__ row_cnt)
+{
+    using Z = typename SR::z_t;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    // key = column << 20 | position (positions < cap <= 2^16)
+    uint64_t *key = (uint64_t *)(smem + (size_t)w * cap * (8 + sizeof(Z)));
+    Z *val = (Z *)((unsigned char *)key + (size_t)cap * 8);
+    const unsigned below = (1u << lane) - 1u;
+
+    for (int64_t rb = (int64_t)blockIdx.x * ESC_WARPS + w; rb < nrows_bin;
+         rb += (int64_t)gridDim.x * ESC_WARPS) {
+        const int32_t i = rows[rb];
+        const int32_t pa0 = Ap[i], pa1 = Ap[i + 1];
+        int32_t m0 = 0, m1 = 0;
+        if (has_mask) { m0 = Mp[i]; m1 = Mp[i + 1]; }
+        int n = 0;                                   // products kept so far
+        for (int32_t c0 = pa0; c0 < pa1; c0 += 32) {
+            // 32 entries of A(i,:) at a time: lane l holds k and nnz(B(k,:))
+            const int32_t pa = c0 + lane;
+            int32_t k = 0, b0 = 0, len = 0;
+            Z a = Z();
+            if (pa < pa1) {
+                k = Aj[pa];
+                b0 = Bp[k];
+                len = Bp[k + 1] - b0;
+                if (SR::needs_a) a = ld_val<Z>(Ax, pa, a_iso);
+            }
+            int incl = len;
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int q0 = 0; q0 < total; q0 += 32) {
+                // product q of this chunk belongs to the first lane src whose
+                // inclusive count exceeds q
+                const int q = q0 + lane;
+                int src = 0;
+                #pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int v = __shfl_sync(0xffffffffu, incl, src + step - 1);
+                    if (v <= q) src += step;
+                }
+                const int excl = __shfl_sync(0xffffffffu, incl - len, src);
+                const int32_t kk = __shfl_sync(0xffffffffu, k, src);
+                const int32_t bb = __shfl_sync(0xffffffffu, b0, src);
+                const Z aa = shfl<Z>(a, src);
+                bool keep = q < total;
+                int32_t j = 0, pb = 0;
+                if (keep) {
+                    pb = bb + (q - excl);
+                    j = Bj[pb];
+                    if (has_mask) {
+                        const int32_t f = lower_bound(Mj, m0, m1, j);
+                        const bool present = f < m1 && Mj[f] == j;
+                        keep = mask_comp ? !present : present;
+                    }
+                }
+                const unsigned km = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int pos = n + __popc(km & below);
+                    Z b = Z();
+                    if (SR::needs_b) b = ld_val<Z>(Bx, pb, b_iso);
+                    key[pos] = ((uint64_t)(uint32_t)j << 20) | (uint64_t)pos;
+                    val[pos] = SR::F::f(aa, b, i, kk, j);
+                }
+                n += __popc(km);
+            }
+        }
+        __syncwarp();
+        int n2 = 1;
+        while (n2 < n) n2 <<= 1;
+        for (int q = n + lane; q < n2; q += 32) key[q] = ~0ull;
+        __syncwarp();
+        for (int size = 2; size <= n2; size <<= 1) {
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int q = lane; q < n2; q += 32) {
+                    const int partner = q ^ stride;
+                    if (partner > q) {
+                        const bool up = ((q & size) == 0);
+                        const uint64_t ka = key[q], kb = key[partner];
+                        if ((ka > kb) == up) {
+                            key[q] = kb; key[partner] = ka;
+                            const Z va = val[q]; val[q] = val[partner]; val[partner] = va;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        // the first entry of each run of equal columns folds the run in
+        // ascending k and writes one output entry
+        const int64_t off = slot_off[i];
+        int out = 0;
+        for (int c0 = 0; c0 < n; c0 += 32) {
+            const int p = c0 + lane;
+            bool head = false;
+            uint32_t j = 0;
+            if (p < n) {
+                j = (uint32_t)(key[p] >> 20);
+                head = (p == 0) || ((uint32_t)(key[p - 1] >> 20) != j);
+            }
+            const unsigned hm = __ballot_sync(0xffffffffu, head);
+            if (head) {
+                Z z = val[p];
+                for (int r = p + 1; r < n && (uint32_t)(key[r] >> 20) == j; r++)
+                    z = SR::M::update(z, val[r]);
+                const int64_t dst = off + out + __popc(hm & below);
+                Tj[dst] = (int32_t)j;
+                Tx[dst] = z;
+            }
+            out += __popc(hm);
+        }
+        if (lane == 0) row_cnt[i] = out;
+        __syncwarp();
     }
 }
 
@@ -700,20 +864,40 @@ k_dense_write(const int32_t *__restrict__ rows, int nrows_bin, int64_t ncols, in
 // phase 4: pack each row's (sorted) slot into CSR
 // ---------------------------------------------------------------------------
 
+// Flat over C's entries: entry e of C lies in the row r with
+// Cp64[r] <= e < Cp64[r+1] and comes from position e - Cp64[r] of that row's
+// slot.  One binary search per warp finds the row of its first entry; lanes
+// walk forward from there.  A long row (vxm's single row) is copied by the
+// whole grid.
 template <typename Z>
 __global__ void __launch_bounds__(256)
 k_pack(int64_t nrows, const int64_t *__restrict__ slot_off,
        const int32_t *__restrict__ Tj, const Z *__restrict__ Tx,
-       const int32_t *__restrict__ row_cnt, const int64_t *__restrict__ Cp64,
-       int32_t *__restrict__ Cj, Z *__restrict__ Cx)
+       const int64_t *__restrict__ Cp64, int32_t *__restrict__ Cj, Z *__restrict__ Cx)
 {
     const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nnz = Cp64[nrows];
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t r = warp; r < nrows; r += nw) {
-        const int cnt = row_cnt[r];
-        const int64_t src = slot_off[r], dst = Cp64[r];
-        for (int q = lane; q < cnt; q += 32) { Cj[dst + q] = Tj[src + q]; Cx[dst + q] = Tx[src + q]; }
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+         base < nnz; base += nw * 32) {
+        int64_t r0 = 0;
+        if (lane == 0) {
+            int64_t lo = 0, hi = nrows + 1;          // first r with Cp64[r] > base
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (Cp64[mid] <= base) lo = mid + 1; else hi = mid;
+            }
+            r0 = lo - 1;
+        }
+        r0 = __shfl_sync(0xffffffffu, r0, 0);
+        const int64_t e = base + lane;
+        if (e < nnz) {
+            int64_t r = r0;
+            while (Cp64[r + 1] <= e) r++;
+            const int64_t src = slot_off[r] + (e - Cp64[r]);
+            Cj[e] = Tj[src];
+            Cx[e] = Tx[src];
+        }
     }
 }
 
@@ -746,11 +930,10 @@ __global__ void k_copy_i64(const int64_t *__restrict__ in, int64_t *__restrict__
 SaxpyConfig saxpy_default_config()
 {
     SaxpyConfig c;
-    c.nb = 4;
-    c.bin[0] = {64, 8, 128};
-    c.bin[1] = {256, 32, 512};
-    c.bin[2] = {1024, 32, 2048};
-    c.bin[3] = {4096, 256, 8192};
+    c.nb = 3;
+    c.bin[0] = {256, 1, 256};          // expand-sort-compress, warp per row
+    c.bin[1] = {1024, 32, 2048};       // shared-memory hash, warp per row
+    c.bin[2] = {4096, 256, 8192};      // shared-memory hash, block per row
     c.blocks_per_sm = 16;
     return c;
 }
@@ -768,6 +951,7 @@ static void allow_dynamic_smem(const void *fn)
 
 static size_t bin_smem(const BinSpec &b, size_t zsize)
 {
+    if (b.tpr == 1) return (size_t)ESC_WARPS * b.cap * (8 + zsize);
     const size_t gb = ((size_t)b.cap * (4 + zsize + 1) + 15) / 16 * 16;
     return b.tpr >= 256 ? gb : gb * (128 / b.tpr);
 }
@@ -778,9 +962,15 @@ bool saxpy_config_valid(const SaxpyConfig &cfg, size_t zsize)
     int64_t prev = 0;
     for (int q = 0; q < cfg.nb; q++) {
         const BinSpec &b = cfg.bin[q];
-        if (b.limit <= prev || (int64_t)b.cap < 2 * b.limit) return false;
-        if ((b.cap & (b.cap - 1)) != 0) return false;
-        if (!(b.tpr == 4 || b.tpr == 8 || b.tpr == 16 || b.tpr == 32 || b.tpr == 256)) return false;
+        if (b.limit <= prev || (b.cap & (b.cap - 1)) != 0) return false;
+        if (b.tpr == 1) {
+            // expand-sort-compress: one slot per product of the row
+            if ((int64_t)b.cap < b.limit || b.cap < 8 || b.cap > (1 << 16)) return false;
+        } else {
+            if ((int64_t)b.cap < 2 * b.limit) return false;
+            if (!(b.tpr == 4 || b.tpr == 8 || b.tpr == 16 || b.tpr == 32 || b.tpr == 256))
+                return false;
+        }
         if (bin_smem(b, zsize) + 256 > runtime().smem_optin) return false;
         prev = b.limit;
     }
@@ -851,16 +1041,17 @@ static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A
         !P->bin_rows || !P->row_cnt || !P->bins)
         return OUT_OF_MEMORY;
     const bool mask_bounds = (M != nullptr) && !mask_comp;
-    if (m > 0)
-        k_flops<<<nblocks(m * 32, 256), 256, 0, s>>>(A.p, A.j, B.p,
-            M ? M->p : nullptr, mask_bounds, m, ncols, P->flops, P->slot_off);
+    cudaMemsetAsync(P->flops, 0, (size_t)(m + 1) * 8, s);
+    if (m > 0 && A.nnz > 0)
+        k_flops_flat<<<nblocks(A.nnz, 256, 16), 256, 0, s>>>(A.p, A.j, B.p, m, A.nnz,
+            (unsigned long long *)P->flops);
     cudaMemsetAsync(P->bins, 0, 64 * sizeof(int), s);
     BinLimits lim;
     lim.nb = P->cfg.nb;
     for (int q = 0; q < P->cfg.nb; q++) lim.limit[q] = P->cfg.bin[q].limit;
     if (m > 0)
         k_bin_rows<<<nblocks(m, 256), 256, 0, s>>>(P->flops, M ? M->p : nullptr,
-            M != nullptr, m, lim, P->bins, P->row_bin);
+            M != nullptr, mask_bounds, ncols, m, lim, P->bins, P->row_bin, P->slot_off);
     cudaMemsetAsync(P->slot_off + m, 0, 8, s);
     scan_exclusive_i64_ws(P->slot_off, P->slot_off, m + 1, P->scan_ws, s);
     const int nb = P->cfg.nb;
@@ -917,7 +1108,19 @@ static void launch_bin(const SaxpyPlan *P, int q, const DevCSR &A, const DevCSR 
     const int32_t *rows = P->bin_rows + P->h_start[q + 1];
     const size_t smem = bin_smem(b, sizeof(Z));
     const int cap_blocks = runtime().num_sms * P->cfg.blocks_per_sm;
-    if (b.tpr >= 256) {
+    if (b.tpr == 1) {
+        static bool attr = false;
+        if (!attr) {
+            allow_dynamic_smem((const void *)k_saxpy_esc<SR>);
+            attr = true;
+        }
+        int blocks = (cnt + ESC_WARPS - 1) / ESC_WARPS;
+        if (blocks > cap_blocks) blocks = cap_blocks;
+        k_saxpy_esc<SR><<<blocks, ESC_WARPS * 32, smem, s>>>(rows, cnt, b.cap,
+            A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
+            M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, P->mask_comp,
+            P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
+    } else if (b.tpr >= 256) {
         static bool attr = false;
         if (!attr) {
             allow_dynamic_smem((const void *)k_saxpy_hash<SR, true>);
@@ -1000,9 +1203,9 @@ static int exec_t(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &
     scan_exclusive_i64_ws(P->Cp64, P->Cp64, m + 1, P->scan_ws, s);
     k_i64_to_i32_p<<<nblocks(m + 1, 256), 256, 0, s>>>(P->Cp64, Cp, m + 1, nullptr);
     if (Cnnz64) k_copy_i64<<<1, 32, 0, s>>>(P->Cp64 + m, Cnnz64);
-    if (m > 0)
-        k_pack<Z><<<nblocks(m * 32, 256), 256, 0, s>>>(m, P->slot_off, P->Tj, (Z *)P->Tx,
-            P->row_cnt, P->Cp64, Cj, (Z *)Cx);
+    if (m > 0 && P->total_cap > 0)
+        k_pack<Z><<<nblocks(P->total_cap, 256, 16), 256, 0, s>>>(m, P->slot_off, P->Tj,
+            (Z *)P->Tx, P->Cp64, Cj, (Z *)Cx);
     return cuda_to_info(cudaGetLastError());
 }
 

@@ -11,8 +11,9 @@
 namespace grb {
 
 // one shared-memory bin: rows whose flops (+ mask entries) are <= limit go to
-// a group of tpr threads (4..32, or 256 for a whole block) with a hash table
-// of cap slots (a power of two, at least twice the limit)
+// either an expand-sort-compress warp (tpr = 1, cap >= limit product slots)
+// or a group of tpr threads (4..32, or 256 for a whole block) with a hash
+// table of cap slots (a power of two, at least twice the limit)
 struct BinSpec { int64_t limit; int tpr; int cap; };
 
 struct SaxpyConfig {

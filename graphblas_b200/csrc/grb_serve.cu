@@ -39,7 +39,6 @@ struct Graph {
     int kind;                 // what it serves
     DevCSR S;                 // the matrix (weights for SSSP / values for MXM)
     DevCSR L, U;              // triangle counting: strict lower / upper
-    std::vector<int64_t> flops_row_sum;   // unused placeholder for extensions
     int64_t mxm_cap = 0;      // symbolic output capacity of S*S (entries)
 };
 
@@ -55,6 +54,7 @@ struct Req {
     int status = 0;
     // results
     int64_t count = 0;                // triangles, or nnz of the result
+    double checksum = 0;              // sum of the result's values (device)
     std::vector<int64_t> rp, ri;      // result pattern (SSSP: 1-row; MXM: CSR)
     std::vector<uint8_t> rx;          // result values (raw bytes)
 };
@@ -114,6 +114,7 @@ int run_request(grb_b200_server_s *S, Req *r, cudaStream_t s)
             int64_t n = 0;
             info = reduce_scalar(&n, C, OP_PLUS, s);
             r->count = n;
+            r->checksum = (double)n;
         }
         dev_free(C, s);
     } else if (r->kind == K_SSSP) {
@@ -129,6 +130,11 @@ int run_request(grb_b200_server_s *S, Req *r, cudaStream_t s)
         }
         if (info == SUCCESS) {
             r->count = w.nnz;
+            float sum = 0;
+            info = reduce_scalar(&sum, w, OP_PLUS, s);
+            r->checksum = sum;
+        }
+        if (info == SUCCESS) {
             if (S->keep_results) {
                 int64_t *p = nullptr, *i = nullptr;
                 void *x = nullptr;
@@ -149,6 +155,11 @@ int run_request(grb_b200_server_s *S, Req *r, cudaStream_t s)
         info = saxpy3(C, nullptr, false, true, g.S, g.S, sr, s);
         if (info == SUCCESS) {
             r->count = C.nnz;
+            double sum = 0;
+            info = reduce_scalar(&sum, C, OP_PLUS, s);
+            r->checksum = sum;
+        }
+        if (info == SUCCESS) {
             if (S->keep_results) {
                 int64_t *p = nullptr, *i = nullptr;
                 void *x = nullptr;
@@ -346,10 +357,12 @@ int grb_b200_server_replay(grb_b200_server S, int64_t nreq, const int *kind,
     return SUCCESS;
 }
 
-// Per-request outcome: status, count (triangles or result nnz), latency
-// (done - arrival), queueing delay (start - arrival).
+// Per-request outcome: status, count (triangles or result nnz), checksum (sum
+// of the result's values, reduced on the device, so it is there whether or
+// not results are kept), latency (done - arrival), queueing delay (start -
+// arrival).
 int grb_b200_server_request(grb_b200_server S, int64_t k, int *status, int64_t *count,
-                            double *latency_s, double *wait_s)
+                            double *checksum, double *latency_s, double *wait_s)
 {
     if (!S) return NULL_POINTER;
     if (k < 0 || k >= (int64_t)S->all.size()) return INVALID_VALUE;
@@ -358,6 +371,7 @@ int grb_b200_server_request(grb_b200_server S, int64_t k, int *status, int64_t *
     if (!r) return INVALID_VALUE;
     if (status) *status = r->status;
     if (count) *count = r->count;
+    if (checksum) *checksum = r->checksum;
     if (latency_s) *latency_s = r->t_done - r->t_arrival;
     if (wait_s) *wait_s = r->t_start - r->t_arrival;
     return SUCCESS;

@@ -30,6 +30,7 @@ def _bind(L):
     L.grb_b200_server_replay.argtypes = [vp, ctypes.c_int64, vp, vp, vp, vp, vp, vp]
     L.grb_b200_server_request.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int),
                                           i64p, ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_double),
                                           ctypes.POINTER(ctypes.c_double)]
     L.grb_b200_server_result.argtypes = [vp, ctypes.c_int64, vp, vp, vp, i64p, i64p]
     L.grb_b200_server_stats.argtypes = [vp, i64p, i64p, i64p, i64p, i64p,
@@ -81,10 +82,12 @@ class Server:
     def request(self, k):
         st = ctypes.c_int()
         cnt = ctypes.c_int64()
-        lat, wait = ctypes.c_double(), ctypes.c_double()
+        lat, wait, cs = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         check(self.L.grb_b200_server_request(self.h, k, ctypes.byref(st), ctypes.byref(cnt),
-                                             ctypes.byref(lat), ctypes.byref(wait)))
-        return dict(status=st.value, count=cnt.value, latency=lat.value, wait=wait.value)
+                                             ctypes.byref(cs), ctypes.byref(lat),
+                                             ctypes.byref(wait)))
+        return dict(status=st.value, count=cnt.value, checksum=cs.value,
+                    latency=lat.value, wait=wait.value)
 
     def result(self, k, kind):
         npp, ni = ctypes.c_int64(), ctypes.c_int64()
@@ -180,7 +183,9 @@ class BenchServe:
                     hbm_budget_gb=40, **getattr(self, "lat", {}))
 
     def _server(self):
-        S = Server(nslots=8, budget_bytes=40 << 30, keep_results=True)
+        # results stay on the device (counts and checksums come back), as a
+        # caller chaining requests would use them
+        S = Server(nslots=8, budget_bytes=40 << 30, keep_results=False)
         for kind, g in self.graphs:
             S.add_graph(kind, g)
         return S

@@ -7,7 +7,7 @@
  *     length vlen, int64 offsets/indices, GB_Type_code, GB_Opcode) and return
  *     results allocated with the library's own allocator, so a maintainer can
  *     call them from the library's method selectors in place of the CPU
- *     kernels (see INTEGRATION.md for the shim).
+ *     kernels (graphblas_b200/integration/gb_b200_gateway.c is that shim).
  *
  *  2. Device-resident matrices (grb_b200_dmatrix), used by the by-row host API
  *     in GraphBLAS_b200.h, by the batched kernel and by the request server:
@@ -273,8 +273,12 @@ int grb_b200_server_replay(grb_b200_server S, int64_t nreq, const int *kind,
                            const int64_t *fp, const int64_t *fi,
                            const float *fx);
 
+/* Outcome of request k: status (GrB_Info), count (triangles, or entries of
+ * the result), checksum (sum of the result's values), latency (completion -
+ * arrival) and queueing delay (start - arrival), in seconds. */
 int grb_b200_server_request(grb_b200_server S, int64_t k, int *status,
-                            int64_t *count, double *latency_s, double *wait_s);
+                            int64_t *count, double *checksum, double *latency_s,
+                            double *wait_s);
 
 int grb_b200_server_result(grb_b200_server S, int64_t k, int64_t *p,
                            int64_t *i, void *x, int64_t *np, int64_t *ni);

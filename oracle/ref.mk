@@ -3,7 +3,10 @@
 # only to oracle/_ref/.  The configuration matches a stock release build with
 # the CPU JIT off (-DNJIT), OpenMP on and the factory kernels compiled in.
 # The cpu_features helper is disabled (-DGBNCPUFEAT); the library then picks
-# its AVX paths from compiler macros instead of a run-time probe.
+# its AVX paths from compiler macros instead of a run-time probe.  The two
+# files cmake would configure (Config/GB_config.h, whose strings only the
+# disabled JIT reads, and the no-JIT JITpackage/GB_JITpackage.c) are generated
+# from their templates into oracle/_ref/gen when the tree does not hold them.
 #
 #   make -f oracle/ref.mk REF=/root/reference -j8
 #
@@ -13,8 +16,9 @@
 REF    ?= /root/reference
 OUT    := oracle/_ref
 OBJ    := $(OUT)/obj
+GEN    := $(OUT)/gen
 CC     := /usr/bin/gcc
-INCS   := -I$(REF) -I$(REF)/Source -I$(REF)/Include -I$(REF)/Config \
+INCS   := -I$(GEN) -I$(REF) -I$(REF)/Source -I$(REF)/Include -I$(REF)/Config \
           -I$(REF)/xxHash -I$(REF)/lz4 -I$(REF)/zstd -I$(REF)/zstd/zstd_subset \
           -I$(REF)/JITpackage -I$(REF)/Demo/Include \
           $(foreach d,apply assign builder builtin callback concat convert ewise \
@@ -25,13 +29,33 @@ CFLAGS := -O3 -DNDEBUG -fPIC -fopenmp -std=c11 -Wno-pragmas -Wundef -w \
           -DNJIT -DGBNCPUFEAT
 
 SRCS := $(wildcard $(REF)/PreJIT/*.c) $(wildcard $(REF)/Config/*.c) \
-        $(wildcard $(REF)/Source/*/*.c) $(REF)/JITpackage/GB_JITpackage.c \
-        $(wildcard $(REF)/FactoryKernels/*.c)
+        $(wildcard $(REF)/Source/*/*.c) $(wildcard $(REF)/FactoryKernels/*.c)
 OBJS := $(patsubst $(REF)/%.c,$(OBJ)/%.o,$(SRCS))
+
+# JIT package: the tree's own file when cmake made one, else the no-JIT one
+ifneq ($(wildcard $(REF)/JITpackage/GB_JITpackage.c),)
+OBJS += $(OBJ)/JITpackage/GB_JITpackage.o
+else
+OBJS += $(OBJ)/gen/GB_JITpackage.o
+endif
+CONFIG_H := $(if $(wildcard $(REF)/Config/GB_config.h),,$(GEN)/GB_config.h)
 
 all: $(OUT)/libgraphblas_ref.so
 
-$(OBJ)/%.o: $(REF)/%.c
+$(GEN)/GB_config.h: $(REF)/Config/GB_config.h.in
+	@mkdir -p $(GEN)
+	sed -e 's/@GB_LIB_PREFIX@/lib/' -e 's/@GB_LIB_SUFFIX@/.so/' \
+	    -e 's/@GB_OBJ_SUFFIX@/.o/' -e 's/@[A-Z_]*@//g' $< > $@
+
+$(GEN)/GB_JITpackage.c: $(REF)/Config/GB_JITpackage_NJIT.c.in
+	@mkdir -p $(GEN)
+	cp $< $@
+
+$(OBJ)/gen/GB_JITpackage.o: $(GEN)/GB_JITpackage.c
+	@mkdir -p $(dir $@)
+	@$(CC) $(CFLAGS) $(INCS) -c $< -o $@
+
+$(OBJ)/%.o: $(REF)/%.c | $(CONFIG_H)
 	@mkdir -p $(dir $@)
 	@$(CC) $(CFLAGS) $(INCS) -c $< -o $@
 

@@ -24,7 +24,7 @@ def _dot3_dev(gb, M, A, B, sr, mask_struct=True, type_name=None):
     return out, info
 
 
-@pytest.mark.parametrize("scale", [6, 8, 10, 12, 14])
+@pytest.mark.parametrize("scale", [6, 8, 10, 12, 14, 16])
 def test_tricount_rmat(gpu, oracle, scale):
     S = W.rmat(scale, 16, seed=scale)
     L, U = W.tril_triu(S)
@@ -94,6 +94,38 @@ def test_dot3_long_rows(gpu, oracle):
     want = oracle.dot3(S.nrows, S.ncols, (L.p, L.i, L.x, 11), (U.p, U.i, U.x, 11),
                        (L.p, L.i, None, 1), "PLUS", "TIMES", 11)
     assert_exact(got, want, "dot3 long rows")
+
+
+@pytest.mark.parametrize("tname,np_t", [("int64", np.int64), ("int32", np.int32)])
+def test_dot3_count_bitmap_and_merge_mix(gpu, oracle, tname, np_t):
+    """PLUS_PAIR on a mask large enough for the bitmap path, with rows whose
+    column span fits the shared-memory bitmap (grouped) and rows spanning
+    4M columns (left on the merge path), long and short lists, empty rows."""
+    gb = gpu
+    m, n, k = 3000, 2500, 4_000_000
+
+    def rows(nr, seed):
+        r = np.random.default_rng(seed)
+        p = [0]
+        idx = []
+        for q in range(nr):
+            ln = int(r.integers(0, 400)) if q % 11 else 0
+            hi = k if q % 2 else 60_000          # wide or narrow column span
+            c = np.unique(r.integers(0, hi, ln))
+            idx.append(c)
+            p.append(p[-1] + len(c))
+        return W.Csr(nr, k, np.array(p, np.int64), np.concatenate(idx).astype(np.int64),
+                     np.ones(p[-1], np_t))
+    A, B = rows(m, 1), rows(n, 2)
+    M = random_csr(m, n, 0.03, 3, np.bool_)
+    M.x = None
+    assert M.nnz >= 1 << 16
+    sr = gb.semiring("PLUS", "PAIR", tname)
+    got, _ = _dot3_dev(gb, M, A, B, sr)
+    tc = gb.TYPES[tname]
+    want = oracle.dot3(m, n, (A.p, A.i, A.x, tc), (B.p, B.i, B.x, tc),
+                       (M.p, M.i, None, 1), "PLUS", "PAIR", tc)
+    assert_exact(got, want, "plus_pair bitmap/merge mix")
 
 
 def test_dot3_valued_mask(gpu, oracle):

@@ -50,6 +50,7 @@ def test_mixed_results_equal_alone_and_oracle(gpu, oracle):
         a, b = mix.request(k), alone.request(k)
         assert a["status"] == 0 and b["status"] == 0
         assert a["count"] == b["count"]
+        assert a["checksum"] == b["checksum"]
         if kind == K_TRICOUNT:
             gid = int(trace["graph"][k])
             if gid not in tri_cache:
