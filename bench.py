@@ -239,19 +239,33 @@ class Saxpy:
         return self.flops / 1e9
 
     def e2e_setup(self, torch):
-        self.hbytes = 2 * (8 * (self.n + 1) + 16 * self.A.nnz)
-        return self.hbytes, 8 * (self.n + 1) + 16 * self.nnz_c
+        # the caller's arrays live in page-locked host memory; GrB_Matrix_import
+        # copies them to HBM and GrB_Matrix_export copies C back
+        def pin(a):
+            return torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        n, nc = self.n, self.nnz_c
+        self.pin = {"Ap": pin(self.A.p), "Ai": pin(self.A.i), "Ax": pin(self.A.x),
+                    "Bp": pin(self.B.p), "Bi": pin(self.B.i), "Bx": pin(self.B.x),
+                    "Cp": torch.empty(n + 1, dtype=torch.int64).pin_memory(),
+                    "Ci": torch.empty(nc, dtype=torch.int64).pin_memory(),
+                    "Cx": torch.empty(nc, dtype=torch.float64).pin_memory()}
+        nb = lambda k: int(self.pin[k].numel() * self.pin[k].element_size())
+        return (sum(nb(k) for k in ("Ap", "Ai", "Ax", "Bp", "Bi", "Bx")),
+                sum(nb(k) for k in ("Cp", "Ci", "Cx")))
 
     def step_e2e(self):
-        api = self.api
-        A = api.matrix_from_csr(self.A)
-        B = api.matrix_from_csr(self.B)
-        C = api.matrix_new(11, self.n, self.n)
+        api, P, n = self.api, self.pin, self.n
+        A = api.matrix_import(11, n, n, P["Ap"].data_ptr(), P["Ai"].data_ptr(),
+                              P["Ax"].data_ptr(), self.A.nnz)
+        B = api.matrix_import(11, n, n, P["Bp"].data_ptr(), P["Bi"].data_ptr(),
+                              P["Bx"].data_ptr(), self.B.nnz)
+        C = api.matrix_new(11, n, n)
         api.mxm(C, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", A, B)
-        p, i, x = api.matrix_to_csr(C, 11, self.n)
+        nv = api.matrix_export(C, 11, P["Cp"].data_ptr(), P["Ci"].data_ptr(),
+                               P["Cx"].data_ptr(), n + 1, self.nnz_c)
         for X in (A, B, C):
             api.free(X)
-        assert int(p[-1]) == self.nnz_c
+        assert nv == self.nnz_c
         return self.flops / 1e9
 
     def launches_per_step(self):
@@ -338,16 +352,28 @@ class Bfs:
         return self.edges
 
     def e2e_setup(self, torch):
-        return 8 * (self.n + 1) + 8 * self.S.nnz, 16 * self.n
+        # S arrives from page-locked host memory through GrB_Matrix_import
+        # (pattern values as bool ones); the parent vector goes back through
+        # GrB_Vector_extractTuples
+        def pin(a):
+            return torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+        self.pin = {"Sp": pin(self.S.p), "Si": pin(self.S.i),
+                    "Sx": pin(np.ones(self.S.nnz, np.bool_)),
+                    "Pi": torch.empty(self.n, dtype=torch.int64).pin_memory(),
+                    "Px": torch.empty(self.n, dtype=torch.int64).pin_memory()}
+        nb = lambda k: int(self.pin[k].numel() * self.pin[k].element_size())
+        return nb("Sp") + nb("Si") + nb("Sx"), 16 * int(getattr(self, "reached", self.n))
 
     def step_e2e(self):
-        api = self.api
-        Sg = api.matrix_from_csr(self.S, 1)
+        api, P = self.api, self.pin
+        Sg = api.matrix_import(1, self.n, self.n, P["Sp"].data_ptr(), P["Si"].data_ptr(),
+                               P["Sx"].data_ptr(), self.S.nnz)
         q, p = self.bfs(Sg)
-        idx, par = api.vector_to(p, 8)
+        nv = api.vector_extract(p, 8, P["Pi"].data_ptr(), P["Px"].data_ptr(), self.n)
         for v in (q, p):
             api.vfree(v)
         api.free(Sg)
+        assert nv == self.reached
         return self.edges
 
     def launches_per_step(self):

@@ -319,6 +319,29 @@ int grb_b200_dmatrix_download(grb_b200_dmatrix D, int64_t **p, int64_t **i,
     return dev_download(D->A, p, i, x, !prune, g_malloc, g.s);
 }
 
+int grb_b200_dmatrix_import(grb_b200_dmatrix *D, int64_t nrows, int64_t ncols,
+                            const int64_t *p, const int64_t *i, const void *x, int type)
+{
+    if (!D || !p || !i || !x) return NULL_POINTER;
+    *D = nullptr;
+    int info = init_device();
+    if (info != SUCCESS) return info;
+    if (type_size(type) == 0) return INVALID_VALUE;
+    StreamGuard g;
+    grb_b200_dmatrix h = new grb_b200_dmatrix_s();
+    info = dev_import(h->A, nrows, ncols, p, i, x, type, g.s);
+    if (info != SUCCESS) { delete h; return info; }
+    *D = h;
+    return SUCCESS;
+}
+
+int grb_b200_dmatrix_export(grb_b200_dmatrix D, int64_t *p, int64_t *i, void *x)
+{
+    if (!D || !p || !i) return NULL_POINTER;
+    StreamGuard g;
+    return dev_download_to(D->A, p, i, x, g.s);
+}
+
 int grb_b200_dmatrix_free(grb_b200_dmatrix *D)
 {
     if (!D || !*D) return SUCCESS;

@@ -618,6 +618,110 @@ EXTRACT(FP64, double, 11)
 #undef EXTRACT
 
 //------------------------------------------------------------------------------
+// import / export: copies between the caller's CSR arrays and the device
+// (GrB_Matrix_import.c:28-205, GrB_Matrix_export.c:38-215,
+// GrB_Matrix_exportSize.c).  Only GrB_CSR_FORMAT is supported here; the
+// arrays go straight to or from HBM (no host copy is kept), and the import
+// is checked on the device as the reference's secure import checks it.
+//------------------------------------------------------------------------------
+
+static GrB_Info import_any(GrB_Matrix *A, GrB_Type type, int code, GrB_Index nrows,
+                           GrB_Index ncols, const GrB_Index *Ap, const GrB_Index *Ai,
+                           const void *Ax, GrB_Index Ap_len, GrB_Index Ai_len,
+                           GrB_Index Ax_len, GrB_Format format)
+{
+    CHECK_INIT;
+    if (!A) return GrB_NULL_POINTER;
+    *A = NULL;
+    if (!type || !Ax || !Ap || !Ai) return GrB_NULL_POINTER;
+    if (type->code != code) return GrB_DOMAIN_MISMATCH;
+    if (format == GrB_CSC_FORMAT || format == GrB_COO_FORMAT) return GrB_NOT_IMPLEMENTED;
+    if (format != GrB_CSR_FORMAT) return GrB_INVALID_VALUE;
+    if (Ap_len < nrows + 1) return GrB_INVALID_VALUE;
+    const GrB_Index nvals = Ap[nrows];
+    if (Ai_len < nvals || Ax_len < nvals) return GrB_INVALID_VALUE;
+    GrB_Matrix M = NULL;
+    CHECK(GrB_Matrix_new(&M, type, nrows, ncols));
+    int info = grb_b200_dmatrix_import(&M->dev, (int64_t)nrows, (int64_t)ncols,
+                                       (const int64_t *)Ap, (const int64_t *)Ai, Ax,
+                                       type->code);
+    if (info != 0) { M->dev = NULL; GrB_Matrix_free(&M); return (GrB_Info)info; }
+    M->dev_ok = true;
+    *A = M;
+    return GrB_SUCCESS;
+}
+
+static GrB_Info export_any(GrB_Index *Ap, GrB_Index *Ai, void *Ax, int code,
+                           GrB_Index *Ap_len, GrB_Index *Ai_len, GrB_Index *Ax_len,
+                           GrB_Format format, GrB_Matrix A)
+{
+    if (!Ap || !Ai || !Ax || !Ap_len || !Ai_len || !Ax_len) return GrB_NULL_POINTER;
+    if (!OBJ_OK(A)) return GrB_UNINITIALIZED_OBJECT;
+    if (A->type->code != code) return GrB_DOMAIN_MISMATCH;
+    if (format == GrB_CSC_FORMAT || format == GrB_COO_FORMAT) return GrB_NOT_IMPLEMENTED;
+    if (format != GrB_CSR_FORMAT) return GrB_INVALID_VALUE;
+    const GrB_Index nvals = (GrB_Index)nvals_of(A);
+    const GrB_Index plen = (GrB_Index)A->nrows + 1;
+    if (plen > *Ap_len || nvals > *Ai_len || nvals > *Ax_len) return GrB_INSUFFICIENT_SPACE;
+    if (A->dev_ok)
+    {
+        // straight from HBM into the caller's arrays
+        int info = grb_b200_dmatrix_export(A->dev, (int64_t *)Ap, (int64_t *)Ai, Ax);
+        if (info != 0) return (GrB_Info)info;
+    }
+    else
+    {
+        if (!A->host_ok) CHECK(host_empty(A));
+        memcpy(Ap, A->hp, plen * sizeof(int64_t));
+        memcpy(Ai, A->hi, nvals * sizeof(int64_t));
+        for (GrB_Index k = 0; k < nvals; k++)
+            memcpy((char *)Ax + k * A->type->size,
+                   (char *)A->hx + (A->hiso ? 0 : k) * A->type->size, A->type->size);
+    }
+    *Ap_len = plen;
+    *Ai_len = nvals;
+    *Ax_len = nvals;
+    return GrB_SUCCESS;
+}
+
+#define IMPORT_EXPORT(T, CT, CODE) \
+GrB_Info GrB_Matrix_import_##T(GrB_Matrix *A, GrB_Type type, GrB_Index nrows, \
+    GrB_Index ncols, const GrB_Index *Ap, const GrB_Index *Ai, const CT *Ax, \
+    GrB_Index Ap_len, GrB_Index Ai_len, GrB_Index Ax_len, GrB_Format format) \
+{ \
+    return import_any(A, type, CODE, nrows, ncols, Ap, Ai, Ax, Ap_len, Ai_len, \
+                      Ax_len, format); \
+} \
+GrB_Info GrB_Matrix_export_##T(GrB_Index *Ap, GrB_Index *Ai, CT *Ax, \
+    GrB_Index *Ap_len, GrB_Index *Ai_len, GrB_Index *Ax_len, GrB_Format format, \
+    GrB_Matrix A) \
+{ \
+    return export_any(Ap, Ai, Ax, CODE, Ap_len, Ai_len, Ax_len, format, A); \
+}
+IMPORT_EXPORT(BOOL, bool, 1)
+IMPORT_EXPORT(INT32, int32_t, 6)
+IMPORT_EXPORT(UINT32, uint32_t, 7)
+IMPORT_EXPORT(INT64, int64_t, 8)
+IMPORT_EXPORT(UINT64, uint64_t, 9)
+IMPORT_EXPORT(FP32, float, 10)
+IMPORT_EXPORT(FP64, double, 11)
+#undef IMPORT_EXPORT
+
+GrB_Info GrB_Matrix_exportSize(GrB_Index *Ap_len, GrB_Index *Ai_len,
+                               GrB_Index *Ax_len, GrB_Format format, GrB_Matrix A)
+{
+    if (!Ap_len || !Ai_len || !Ax_len) return GrB_NULL_POINTER;
+    if (!OBJ_OK(A)) return GrB_UNINITIALIZED_OBJECT;
+    if (format == GrB_CSC_FORMAT || format == GrB_COO_FORMAT) return GrB_NOT_IMPLEMENTED;
+    if (format != GrB_CSR_FORMAT) return GrB_INVALID_VALUE;
+    const GrB_Index nvals = (GrB_Index)nvals_of(A);
+    *Ap_len = (GrB_Index)A->nrows + 1;
+    *Ai_len = nvals;
+    *Ax_len = nvals;
+    return GrB_SUCCESS;
+}
+
+//------------------------------------------------------------------------------
 // vectors (1-by-n rows inside)
 //------------------------------------------------------------------------------
 
@@ -779,18 +883,45 @@ GrB_Info GxB_Vector_unpack_CSC(GrB_Vector v, GrB_Index **vi, void **vx,
     return GrB_SUCCESS;
 }
 
-#define VEXTRACT(T, CT) \
+// a vector held on the device goes straight into the caller's I and X (its
+// one row's indices and values), with no host copy in between
+static GrB_Info vector_extract_dev(GrB_Index *I, void *X, GrB_Index *nvals, GrB_Vector v)
+{
+    GrB_Matrix A = VM(v);
+    const int64_t nv = nvals_of(A);
+    if (*nvals < (GrB_Index)nv) return GrB_INSUFFICIENT_SPACE;
+    int64_t p2[2];
+    int64_t *ii = (int64_t *)I;
+    void *xx = X;
+    int64_t *tmp_i = NULL;
+    if (!ii)
+    {
+        tmp_i = malloc((size_t)(nv ? nv : 1) * sizeof(int64_t));
+        if (!tmp_i) return GrB_OUT_OF_MEMORY;
+        ii = tmp_i;
+    }
+    int info = grb_b200_dmatrix_export(A->dev, p2, ii, xx);
+    free(tmp_i);
+    if (info != 0) return (GrB_Info)info;
+    *nvals = (GrB_Index)nv;
+    return GrB_SUCCESS;
+}
+
+#define VEXTRACT(T, CT, CODE) \
 GrB_Info GrB_Vector_extractTuples_##T(GrB_Index *I, CT *X, GrB_Index *nvals, \
                                       const GrB_Vector v) \
 { \
+    if (!nvals) return GrB_NULL_POINTER; \
     if (!VOK(v)) return GrB_UNINITIALIZED_OBJECT; \
+    if (X && VM(v)->type->code != CODE) return GrB_DOMAIN_MISMATCH; \
+    if (VM(v)->dev_ok && !VM(v)->host_ok) return vector_extract_dev(I, X, nvals, v); \
     return GrB_Matrix_extractTuples_##T(NULL, I, X, nvals, VM(v)); \
 }
-VEXTRACT(BOOL, bool)
-VEXTRACT(INT32, int32_t)
-VEXTRACT(INT64, int64_t)
-VEXTRACT(FP32, float)
-VEXTRACT(FP64, double)
+VEXTRACT(BOOL, bool, 1)
+VEXTRACT(INT32, int32_t, 6)
+VEXTRACT(INT64, int64_t, 8)
+VEXTRACT(FP32, float, 10)
+VEXTRACT(FP64, double, 11)
 #undef VEXTRACT
 
 //------------------------------------------------------------------------------

@@ -351,6 +351,9 @@ k_dot3_intersect(const D3Work *__restrict__ queue, const int32_t *__restrict__ s
 static constexpr int D3_GMIN = 16;             // smallest group worth a bitmap
 static constexpr int64_t D3_WCHUNK = 1 << 20;  // probes per work item
 static constexpr int D3_BM_THREADS = 1024;
+static constexpr int D3_LONG = 2048;          // longer lists go to the shared table
+static constexpr int D3_SEG = 512;            // probes per shared long-list segment
+static constexpr int D3_TABLE = 1024;         // long lists registered per item
 
 struct D3Item { int32_t key, t, nit, pad; };
 
@@ -456,15 +459,23 @@ __global__ void k_d3_item_fill(const int64_t *__restrict__ ioff, int64_t nkeys,
 // One block per SM, persistent: take an item, set the bits of its key row
 // (A(i,:) or B(j,:), relative to the row's first column) in shared memory,
 // then count, for every entry of the item, the elements of its other
-// (trimmed) list that hit the bitmap.  The item's entries are flattened into
-// one sequence of probes split evenly over the block's warps; each warp walks
-// its share in steps of 32 probes and adds each run of lanes that belongs to
-// one entry into that entry's shared counter.  The bits are cleared again
-// from the row before the next item.
+// (trimmed) list that hit the bitmap, in two phases:
+//   A. each warp splits into groups of G lanes (G a power of two near half
+//      the group's mean probes per entry, so short lists do not waste
+//      lanes); groups take the item's entries one at a time from a shared
+//      counter and stride over their list; a list longer than D3_LONG is
+//      instead registered in a shared table (up to D3_TABLE entries) as
+//      segments of D3_SEG probes;
+//   B. all warps take the segments from a shared counter, 32 probes per step,
+//      and add their hits to the entry's shared count; then the table's
+//      entries are written.
+// If the table is full, the group that owns the entry finishes it itself.
+// The bits are cleared again from the row before the next item.
 template <class SR>
 __global__ void __launch_bounds__(D3_BM_THREADS, 1)
 k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict__ nitems_p,
                     int *__restrict__ inext, const int64_t *__restrict__ goff,
+                    const unsigned long long *__restrict__ gwork,
                     const int32_t *__restrict__ bucket, const D3Work *__restrict__ queue,
                     int32_t nrows,
                     const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
@@ -475,19 +486,39 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
 {
     using Z = typename SR::z_t;
     extern __shared__ uint32_t bm[];
-    __shared__ int s_item;
-    __shared__ int32_t s_pre[D3_BM_THREADS];    // inclusive probe counts
-    __shared__ int32_t s_cnt[D3_BM_THREADS];    // matches per entry
-    __shared__ int32_t s_s0[D3_BM_THREADS];     // start of each probed list
-    __shared__ int32_t s_wsum[D3_BM_THREADS / 32];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nwarps = blockDim.x >> 5;
+    __shared__ int s_item, s_next, s_gnext;
+    __shared__ unsigned long long s_tbl;          // (segments << 32) | entries
+    __shared__ int32_t t_start[D3_TABLE], t_rem[D3_TABLE], t_seg0[D3_TABLE];
+    __shared__ int32_t t_cnt[D3_TABLE], t_pm[D3_TABLE], t_j[D3_TABLE];
+    const int tid = threadIdx.x, lane = tid & 31;
+    const uint32_t nbits = bm_words * 32u;
     for (uint32_t q = tid; q < bm_words; q += blockDim.x) bm[q] = 0;
     const int64_t nitems = *nitems_p;
     unsigned long long zc = 0;
+    // hits among S[b0 + t] for t = first, first + step, ... < n
+    auto probes = [&](const int32_t *S, int32_t b0, int32_t first, int32_t step, int32_t n,
+                      int32_t lo) -> int {
+        int c = 0;
+        int32_t t = first;
+        for (; t + 3 * step < n; t += 4 * step) {
+            const int32_t x0 = S[b0 + t], x1 = S[b0 + t + step];
+            const int32_t x2 = S[b0 + t + 2 * step], x3 = S[b0 + t + 3 * step];
+            const uint32_t k0 = (uint32_t)(x0 - lo), k1 = (uint32_t)(x1 - lo);
+            const uint32_t k2 = (uint32_t)(x2 - lo), k3 = (uint32_t)(x3 - lo);
+            c += (k0 < nbits) ? (int)((bm[k0 >> 5] >> (k0 & 31)) & 1u) : 0;
+            c += (k1 < nbits) ? (int)((bm[k1 >> 5] >> (k1 & 31)) & 1u) : 0;
+            c += (k2 < nbits) ? (int)((bm[k2 >> 5] >> (k2 & 31)) & 1u) : 0;
+            c += (k3 < nbits) ? (int)((bm[k3 >> 5] >> (k3 & 31)) & 1u) : 0;
+        }
+        for (; t < n; t += step) {
+            const uint32_t k = (uint32_t)(S[b0 + t] - lo);
+            c += (k < nbits) ? (int)((bm[k >> 5] >> (k & 31)) & 1u) : 0;
+        }
+        return c;
+    };
     while (true) {
         __syncthreads();
-        if (tid == 0) s_item = atomicAdd(inext, 1);
+        if (tid == 0) { s_item = atomicAdd(inext, 1); s_next = 0; s_gnext = 0; s_tbl = 0; }
         __syncthreads();
         const int it = s_item;
         if (it >= nitems) break;
@@ -506,9 +537,20 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
         const int64_t g0 = goff[I.key];
         const int32_t gn = (int32_t)(goff[I.key + 1] - g0);
         const int32_t m_item = (gn - I.t + I.nit - 1) / I.nit;
-        // rounds of up to one entry per thread
-        for (int32_t rb = 0; rb < m_item; rb += blockDim.x) {
-            const int32_t rr = rb + tid;
+        // lanes per entry
+        const unsigned long long mean = gwork[I.key] / (unsigned long long)gn;
+        int lg = 0;
+        while (lg < 5 && (2ull << lg) < mean) lg++;
+        const int G = 1 << lg, gi = lane >> lg, gl = lane & (G - 1);
+        const int groups = 32 >> lg;
+        __syncthreads();
+        // phase A
+        while (true) {
+            int c0 = 0;
+            if (lane == 0) c0 = atomicAdd(&s_next, groups);
+            c0 = __shfl_sync(0xffffffffu, c0, 0);
+            if (c0 >= m_item) break;
+            const int32_t rr = c0 + gi;
             int32_t s0 = 0, len = 0, pm = 0, j = 0;
             if (rr < m_item) {
                 const D3Work e = queue[bucket[g0 + I.t + (int64_t)I.nit * rr]];
@@ -517,77 +559,62 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
                 pm = e.pm;
                 j = e.j;
             }
-            // block inclusive scan of len
-            int v = len;
-            #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, v, o);
-                if (lane >= o) v += y;
-            }
-            if (lane == 31) s_wsum[warp] = v;
-            __syncthreads();                 // also orders the bitmap build
-            if (warp == 0) {
-                int ws = lane < nwarps ? s_wsum[lane] : 0;
-                #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, ws, o);
-                    if (lane >= o) ws += y;
-                }
-                if (lane < nwarps) s_wsum[lane] = ws;
-            }
-            __syncthreads();
-            const int incl = v + (warp > 0 ? s_wsum[warp - 1] : 0);
-            s_pre[tid] = incl;
-            s_s0[tid] = s0;
-            s_cnt[tid] = 0;
-            const int nr = min((int)blockDim.x, m_item - rb);
-            const int total = s_wsum[nwarps - 1];
-            __syncthreads();
-            // this warp's share of the probes [q_begin, q_end)
-            const int q_begin = (int)((int64_t)total * warp / nwarps);
-            const int q_end = (int)((int64_t)total * (warp + 1) / nwarps);
-            // entry holding probe q_begin: first e with s_pre[e] > q_begin
-            int e_lane = 0;
-            {
-                int lo2 = 0, hi2 = nr;
-                while (lo2 < hi2) {
-                    const int mid = (lo2 + hi2) >> 1;
-                    if (s_pre[mid] <= q_begin) lo2 = mid + 1; else hi2 = mid;
-                }
-                e_lane = lo2;
-            }
-            for (int q0 = q_begin; q0 < q_end; q0 += 32) {
-                const int q = q0 + lane;
-                const bool act = q < q_end;
-                bool hit = false;
-                if (act) {
-                    while (s_pre[e_lane] <= q) e_lane++;
-                    const int ex = e_lane > 0 ? s_pre[e_lane - 1] : 0;
-                    const uint32_t k = (uint32_t)(S[s_s0[e_lane] + (q - ex)] - lo);
-                    hit = k < bm_words * 32u && ((bm[k >> 5] >> (k & 31)) & 1u);
-                }
-                const unsigned hits = __ballot_sync(0xffffffffu, hit);
-                // lanes of one entry are consecutive: the first lane of each
-                // run adds the run's hits
-                const int e_prev = __shfl_up_sync(0xffffffffu, e_lane, 1);
-                const bool head = act && (lane == 0 || e_prev != e_lane);
-                const unsigned heads = __ballot_sync(0xffffffffu, head);
-                if (head) {
-                    const unsigned higher = heads & ~((2u << lane) - 1u);
-                    const int end = higher ? __ffs(higher) - 1 : 32;
-                    const unsigned seg = (end == 32 ? 0xffffffffu : ((1u << end) - 1u)) &
-                                         ~((1u << lane) - 1u);
-                    const int c = __popc(hits & seg);
-                    if (c) atomicAdd(&s_cnt[e_lane], c);
+            // a long list goes to the table (its group's first lane registers
+            // it); the group keeps it only if the table is full
+            unsigned slot = 0xffffffffu;
+            if (len > D3_LONG && gl == 0) {
+                const unsigned long long nseg =
+                    (unsigned long long)((len + D3_SEG - 1) / D3_SEG);
+                const unsigned long long old = atomicAdd(&s_tbl, (nseg << 32) | 1ull);
+                slot = (unsigned)(old & 0xffffffffull);
+                if (slot < (unsigned)D3_TABLE) {
+                    t_start[slot] = s0;
+                    t_rem[slot] = len;
+                    t_seg0[slot] = (int32_t)(old >> 32);
+                    t_cnt[slot] = 0;
+                    t_pm[slot] = pm;
+                    t_j[slot] = j;
                 }
             }
-            __syncthreads();
-            if (rr < m_item) {
-                const int c = s_cnt[tid];
-                if (c) { Cj[pm] = j; Cx[pm] = (Z)c; }
+            slot = __shfl_sync(0xffffffffu, slot, gi << lg);
+            const bool own = rr < m_item && slot >= (unsigned)D3_TABLE;
+            int cnt = own ? probes(S, s0, gl, G, len, lo) : 0;
+            for (int o = G >> 1; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o, G);
+            if (own && gl == 0) {
+                if (cnt) { Cj[pm] = j; Cx[pm] = (Z)cnt; }
                 else { Cj[pm] = flip(j); zc++; }
             }
-            __syncthreads();
+        }
+        __syncthreads();
+        // phase B
+        const unsigned long long tb = s_tbl;
+        const int ntab = (int)min((unsigned long long)D3_TABLE, tb & 0xffffffffull);
+        if (ntab > 0) {
+            const int total = t_seg0[ntab - 1] + (t_rem[ntab - 1] + D3_SEG - 1) / D3_SEG;
+            while (true) {
+                int g = 0;
+                if (lane == 0) g = atomicAdd(&s_gnext, 1);
+                g = __shfl_sync(0xffffffffu, g, 0);
+                if (g >= total) break;
+                // table entry holding segment g: last with t_seg0 <= g
+                int a = 0, b = ntab;
+                while (b - a > 1) {
+                    const int mid = (a + b) >> 1;
+                    if (t_seg0[mid] <= g) a = mid; else b = mid;
+                }
+                const int32_t off = (g - t_seg0[a]) * D3_SEG;
+                const int32_t n = min(D3_SEG, t_rem[a] - off);
+                const int c = (int)__reduce_add_sync(
+                    0xffffffffu, (unsigned)probes(S, t_start[a] + off, lane, 32, n, lo));
+                if (lane == 0 && c) atomicAdd(&t_cnt[a], c);
+            }
+        }
+        __syncthreads();
+        for (int q = tid; q < ntab; q += blockDim.x) {
+            const int c = t_cnt[q];
+            const int32_t pm = t_pm[q], j = t_j[q];
+            if (c) { Cj[pm] = j; Cx[pm] = (Z)c; }
+            else { Cj[pm] = flip(j); zc++; }
         }
         __syncthreads();
         for (int32_t q = rp0 + tid; q < rp1; q += blockDim.x) {
@@ -702,7 +729,7 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
             k_d3_item_fill<<<kb, 256, 0, s>>>(ioff, nkeys, items);
             if constexpr (IsCount<SR>::value)
                 k_dot3_bitmap_count<SR><<<nsm, D3_BM_THREADS, (size_t)bm_words * 4, s>>>(
-                    items, ioff + nkeys, inext, goff, bucket, queue, (int32_t)M.nrows,
+                    items, ioff + nkeys, inext, goff, gwork, bucket, queue, (int32_t)M.nrows,
                     A.p, A.j, B.p, B.j, bm_words, C.j, (Z *)C.x, zc);
             k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
                 queue, merge_sel, merge_len, qnext, A.j, A.x, A.iso, B.j, B.x, B.iso,

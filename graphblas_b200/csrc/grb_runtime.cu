@@ -232,6 +232,173 @@ int dev_upload(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
 }
 
 // ---------------------------------------------------------------------------
+// import with checks, and export into the caller's arrays
+// ---------------------------------------------------------------------------
+
+// narrow with a range check: flag |= bit for a value outside [lo, hi], or,
+// for offsets (monotone), a value above its successor
+__global__ void k_narrow_check(const int64_t *__restrict__ in, int32_t *__restrict__ out,
+                               int64_t n, int64_t lo, int64_t hi, bool monotone,
+                               unsigned *__restrict__ flag, unsigned bit)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    bool bad = false;
+    for (; t < n; t += stride) {
+        const int64_t v = in[t];
+        bad |= v < lo || v > hi || (monotone && t + 1 < n && in[t + 1] < v);
+        out[t] = (int32_t)v;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, bit);
+}
+
+// flag |= bit when some row's indices are not strictly increasing (flat over
+// the entries: one binary search per warp for its first entry's row)
+__global__ void k_check_rows(const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+                             int64_t nrows, int64_t nnz, unsigned *__restrict__ flag,
+                             unsigned bit)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    bool bad = false;
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+         base < nnz; base += nw * 32) {
+        int32_t r0 = 0;
+        if (lane == 0) r0 = upper_bound(Ap, 0, (int32_t)nrows + 1, (int32_t)base) - 1;
+        r0 = __shfl_sync(0xffffffffu, r0, 0);
+        const int64_t e = base + lane;
+        if (e < nnz) {
+            int32_t r = r0;
+            while (Ap[r + 1] <= e) r++;
+            if (e > Ap[r]) bad |= Aj[e - 1] >= Aj[e];
+        }
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(flag, bit);
+}
+
+int dev_import(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
+               const int64_t *i, const void *x, int type, cudaStream_t s)
+{
+    if (nrows < 0 || ncols < 0) return INVALID_VALUE;
+    const int64_t nnz = p[nrows];
+    if (p[0] != 0 || nnz < 0) return INVALID_OBJECT;
+    if (nrows >= INT32_MAX || ncols >= INT32_MAX || nnz >= INT32_MAX) return NO_VALUE;
+    A = DevCSR();
+    A.nrows = nrows; A.ncols = ncols; A.nnz = nnz; A.type = type; A.iso = false;
+    const size_t ts = type_size(type);
+    Scratch ws(s);
+    int64_t *stage = ws.get<int64_t>((nrows + 1 > nnz) ? nrows + 1 : nnz);
+    unsigned *flag = ws.get<unsigned>(1);
+    A.p = (int32_t *)dalloc((size_t)(nrows + 1) * 4, s);
+    A.j = (int32_t *)dalloc((size_t)(nnz ? nnz : 1) * 4, s);
+    A.x = dalloc((size_t)(nnz ? nnz : 1) * ts, s);
+    if (ws.failed || !A.p || !A.j || !A.x) { dev_free(A, s); return OUT_OF_MEMORY; }
+    cudaMemsetAsync(flag, 0, 4, s);
+    cudaMemcpyAsync(stage, p, (size_t)(nrows + 1) * 8, cudaMemcpyHostToDevice, s);
+    k_narrow_check<<<grid_for(nrows + 1, 256), 256, 0, s>>>(stage, A.p, nrows + 1, 0, nnz,
+                                                            true, flag, 1u);
+    if (nnz > 0) {
+        cudaMemcpyAsync(stage, i, (size_t)nnz * 8, cudaMemcpyHostToDevice, s);
+        k_narrow_check<<<grid_for(nnz, 256), 256, 0, s>>>(stage, A.j, nnz, 0, ncols - 1,
+                                                          false, flag, 2u);
+        cudaMemcpyAsync(A.x, x, (size_t)nnz * ts, cudaMemcpyHostToDevice, s);
+    }
+    unsigned hflag = 0;
+    cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { dev_free(A, s); return cuda_to_info(e); }
+    if (hflag) { dev_free(A, s); return INVALID_OBJECT; }
+    if (nnz == 0) return SUCCESS;
+    k_check_rows<<<grid_for(nnz, 256), 256, 0, s>>>(A.p, A.j, nrows, nnz, flag, 4u);
+    cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { dev_free(A, s); return cuda_to_info(e); }
+    if (hflag == 0) return SUCCESS;
+    // rows given out of order: (A')' has every row sorted
+    DevCSR T, B;
+    int info = transpose(T, A, s);
+    if (info == SUCCESS) info = transpose(B, T, s);
+    dev_free(T, s);
+    dev_free(A, s);
+    if (info != SUCCESS) { dev_free(B, s); return info; }
+    A = B;
+    // a sorted row with two equal indices holds a duplicate: not a matrix
+    cudaMemsetAsync(flag, 0, 4, s);
+    k_check_rows<<<grid_for(nnz, 256), 256, 0, s>>>(A.p, A.j, nrows, nnz, flag, 4u);
+    cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess || hflag) {
+        dev_free(A, s);
+        return e != cudaSuccess ? cuda_to_info(e) : INVALID_OBJECT;
+    }
+    return SUCCESS;
+}
+
+template <typename T>
+__global__ void k_fill_value(T *__restrict__ out, const T *__restrict__ v, int64_t n)
+{
+    const T x = *v;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x)
+        out[t] = x;
+}
+
+static int download_to_t(const DevCSR &A, int64_t *p, int64_t *i, void *x, cudaStream_t s)
+{
+    Scratch ws(s);
+    const size_t ts = type_size(A.type);
+    const int64_t nnz = A.nnz;
+    int64_t *stage = ws.get<int64_t>((A.nrows + 1 > nnz) ? A.nrows + 1 : nnz);
+    char *ex = (x && A.x && A.iso && nnz > 0) ? ws.get<char>((size_t)nnz * ts) : nullptr;
+    if (ws.failed) return OUT_OF_MEMORY;
+    k_widen<<<grid_for(A.nrows + 1, 256), 256, 0, s>>>(A.p, stage, A.nrows + 1);
+    cudaMemcpyAsync(p, stage, (size_t)(A.nrows + 1) * 8, cudaMemcpyDeviceToHost, s);
+    if (nnz > 0) {
+        k_widen<<<grid_for(nnz, 256), 256, 0, s>>>(A.j, stage, nnz);
+        cudaMemcpyAsync(i, stage, (size_t)nnz * 8, cudaMemcpyDeviceToHost, s);
+        if (x && A.x) {
+            if (ex) {
+                // iso values are expanded, one per entry
+                switch (ts) {
+                    case 1: k_fill_value<uint8_t><<<grid_for(nnz, 256), 256, 0, s>>>(
+                                (uint8_t *)ex, (const uint8_t *)A.x, nnz); break;
+                    case 4: k_fill_value<uint32_t><<<grid_for(nnz, 256), 256, 0, s>>>(
+                                (uint32_t *)ex, (const uint32_t *)A.x, nnz); break;
+                    default: k_fill_value<uint64_t><<<grid_for(nnz, 256), 256, 0, s>>>(
+                                (uint64_t *)ex, (const uint64_t *)A.x, nnz); break;
+                }
+                cudaMemcpyAsync(x, ex, (size_t)nnz * ts, cudaMemcpyDeviceToHost, s);
+            } else {
+                cudaMemcpyAsync(x, A.x, (size_t)nnz * ts, cudaMemcpyDeviceToHost, s);
+            }
+        }
+    }
+    return cuda_to_info(cudaStreamSynchronize(s));
+}
+
+int dev_download_to(const DevCSR &A0, int64_t *p, int64_t *i, void *x, cudaStream_t s)
+{
+    if (A0.nzombies == 0) return download_to_t(A0, p, i, x, s);
+    // prune a private copy so the caller's matrix is untouched
+    DevCSR B = A0;
+    const size_t ts = type_size(A0.type);
+    B.p = (int32_t *)dalloc((size_t)(A0.nrows + 1) * 4, s);
+    B.j = (int32_t *)dalloc((size_t)(A0.nnz ? A0.nnz : 1) * 4, s);
+    B.x = nullptr;
+    if (A0.x) B.x = dalloc(A0.iso ? ts : (size_t)(A0.nnz ? A0.nnz : 1) * ts, s);
+    if (!B.p || !B.j || (A0.x && !B.x)) { dev_free(B, s); return OUT_OF_MEMORY; }
+    cudaMemcpyAsync(B.p, A0.p, (size_t)(A0.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(B.j, A0.j, (size_t)A0.nnz * 4, cudaMemcpyDeviceToDevice, s);
+    if (A0.x) cudaMemcpyAsync(B.x, A0.x, A0.iso ? ts : (size_t)A0.nnz * ts,
+                              cudaMemcpyDeviceToDevice, s);
+    int info = dev_prune_zombies(B, s);
+    if (info == SUCCESS) info = download_to_t(B, p, i, x, s);
+    dev_free(B, s);
+    cudaStreamSynchronize(s);
+    return info;
+}
+
+// ---------------------------------------------------------------------------
 // exclusive scans (three passes: block totals, scan of totals, block scans)
 // ---------------------------------------------------------------------------
 

@@ -96,6 +96,17 @@ int dev_mask_to_struct(DevCSR &out, const DevCSR &M, cudaStream_t s);
 // remove zombies in place (GB_wait's zombie pruning), producing a clean CSR
 int dev_prune_zombies(DevCSR &A, cudaStream_t s);
 
+// upload from the caller's int64 CSR with checks on the device (offsets from
+// 0 to nnz, never decreasing; indices in [0, ncols); rows given out of order
+// are sorted, duplicates rejected): INVALID_OBJECT when the arrays are not a
+// matrix (GrB_Matrix_import's secure import)
+int dev_import(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
+               const int64_t *i, const void *x, int type, cudaStream_t s);
+
+// copy the live entries into the caller's arrays (nrows+1 offsets, then the
+// live indices and values; iso values expanded); synchronises s
+int dev_download_to(const DevCSR &A, int64_t *p, int64_t *i, void *x, cudaStream_t s);
+
 // ---- scans ----
 // exclusive scan of n int64 values in place; out[n] receives the total when
 // `with_total`.  `in` and `out` may alias.

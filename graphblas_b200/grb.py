@@ -23,6 +23,7 @@ U64 = ctypes.c_uint64
 TYPE_NAMES = {1: "GrB_BOOL", 6: "GrB_INT32", 7: "GrB_UINT32", 8: "GrB_INT64",
               9: "GrB_UINT64", 10: "GrB_FP32", 11: "GrB_FP64"}
 SUFFIX = {1: "BOOL", 6: "INT32", 8: "INT64", 10: "FP32", 11: "FP64"}
+SUFFIX_ALL = {**SUFFIX, 7: "UINT32", 9: "UINT64"}
 CTYPE = {1: ctypes.c_bool, 6: ctypes.c_int32, 8: ctypes.c_int64,
          10: ctypes.c_float, 11: ctypes.c_double}
 
@@ -81,6 +82,22 @@ class API:
         L.GrB_Vector_setElement_INT64.argtypes = [vp, ctypes.c_int64, U64]
         L.GrB_Matrix_dup.argtypes = [ctypes.POINTER(vp), vp]
         L.GrB_Matrix_clear.argtypes = [vp]
+        for suf in set(SUFFIX.values()) | {"UINT32", "UINT64"}:
+            f = getattr(L, "GrB_Matrix_import_" + suf)
+            f.restype = ctypes.c_int
+            f.argtypes = [ctypes.POINTER(vp), vp, U64, U64, vp, vp, vp, U64, U64, U64,
+                          ctypes.c_int]
+            f = getattr(L, "GrB_Matrix_export_" + suf)
+            f.restype = ctypes.c_int
+            f.argtypes = [vp, vp, vp, ctypes.POINTER(U64), ctypes.POINTER(U64),
+                          ctypes.POINTER(U64), ctypes.c_int, vp]
+        L.GrB_Matrix_exportSize.restype = ctypes.c_int
+        L.GrB_Matrix_exportSize.argtypes = [ctypes.POINTER(U64), ctypes.POINTER(U64),
+                                            ctypes.POINTER(U64), ctypes.c_int, vp]
+        for suf in SUFFIX.values():
+            f = getattr(L, "GrB_Vector_extractTuples_" + suf)
+            f.restype = ctypes.c_int
+            f.argtypes = [vp, vp, ctypes.POINTER(U64), vp]
         for t, suf in SUFFIX.items():
             f = getattr(L, "GrB_Matrix_reduce_" + suf)
             f.restype = ctypes.c_int
@@ -136,6 +153,34 @@ class API:
                   ctypes.byref(xp), (csr.nrows + 1) * 8, max(nnz, 1) * 8, xs, iso,
                   False, None)
         return A
+
+    def matrix_import(self, type_code, nrows, ncols, p, i, x, nvals):
+        """GrB_Matrix_import (CSR) from raw host addresses (numpy or pinned
+        buffers): int64 offsets p, int64 indices i, nvals values x."""
+        A = vp()
+        self.call("GrB_Matrix_import_" + SUFFIX_ALL[type_code], ctypes.byref(A),
+                  self.obj(TYPE_NAMES[type_code]), nrows, ncols, p, i, x, nrows + 1,
+                  nvals, nvals, 0)
+        return A
+
+    def matrix_export(self, A, type_code, p, i, x, plen, nvals):
+        """GrB_Matrix_export (CSR) into raw host addresses; returns nvals."""
+        a, b, c = U64(plen), U64(nvals), U64(nvals)
+        self.call("GrB_Matrix_export_" + SUFFIX_ALL[type_code], p, i, x, ctypes.byref(a),
+                  ctypes.byref(b), ctypes.byref(c), 0, A)
+        return b.value
+
+    def export_size(self, A):
+        a, b, c = U64(), U64(), U64()
+        self.call("GrB_Matrix_exportSize", ctypes.byref(a), ctypes.byref(b),
+                  ctypes.byref(c), 0, A)
+        return a.value, b.value
+
+    def vector_extract(self, v, type_code, i, x, cap):
+        """GrB_Vector_extractTuples into raw host addresses; returns nvals."""
+        n = U64(cap)
+        self.call("GrB_Vector_extractTuples_" + SUFFIX[type_code], i, x, ctypes.byref(n), v)
+        return n.value
 
     def matrix_to_csr(self, A, type_code, nrows):
         """GxB_Matrix_unpack_CSR into numpy (the matrix becomes empty)."""

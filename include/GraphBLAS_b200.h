@@ -181,6 +181,26 @@ GRB_B200_EXTRACT(FP32, float)
 GRB_B200_EXTRACT(FP64, double)
 #undef GRB_B200_EXTRACT
 
+/* ---- import / export (copies; GrB_CSR_FORMAT) ---- */
+typedef enum { GrB_CSR_FORMAT = 0, GrB_CSC_FORMAT = 1, GrB_COO_FORMAT = 2 } GrB_Format;
+#define GRB_B200_IMPORT(T, CT) \
+    GrB_Info GrB_Matrix_import_##T(GrB_Matrix *A, GrB_Type type, GrB_Index nrows, \
+        GrB_Index ncols, const GrB_Index *Ap, const GrB_Index *Ai, const CT *Ax, \
+        GrB_Index Ap_len, GrB_Index Ai_len, GrB_Index Ax_len, GrB_Format format); \
+    GrB_Info GrB_Matrix_export_##T(GrB_Index *Ap, GrB_Index *Ai, CT *Ax, \
+        GrB_Index *Ap_len, GrB_Index *Ai_len, GrB_Index *Ax_len, GrB_Format format, \
+        GrB_Matrix A);
+GRB_B200_IMPORT(BOOL, bool)
+GRB_B200_IMPORT(INT32, int32_t)
+GRB_B200_IMPORT(UINT32, uint32_t)
+GRB_B200_IMPORT(INT64, int64_t)
+GRB_B200_IMPORT(UINT64, uint64_t)
+GRB_B200_IMPORT(FP32, float)
+GRB_B200_IMPORT(FP64, double)
+#undef GRB_B200_IMPORT
+GrB_Info GrB_Matrix_exportSize(GrB_Index *Ap_len, GrB_Index *Ai_len,
+                               GrB_Index *Ax_len, GrB_Format format, GrB_Matrix A);
+
 /* ---- vectors (sparse) ---- */
 GrB_Info GrB_Vector_new(GrB_Vector *v, GrB_Type type, GrB_Index n);
 GrB_Info GrB_Vector_free(GrB_Vector *v);

@@ -148,6 +148,23 @@ int grb_b200_dmatrix_upload(grb_b200_dmatrix *D, int64_t nrows, int64_t ncols,
 int grb_b200_dmatrix_download(grb_b200_dmatrix D, int64_t **p, int64_t **i,
                               void **x, bool prune);
 
+/* Copy a CSR matrix from the caller's arrays (host memory; page-locked
+ * memory goes by DMA) and check it on the device: offsets start at 0, never
+ * decrease and end at nnz = p[nrows], indices lie in [0, ncols), and no row
+ * holds an index twice (rows given out of order are sorted on the device).
+ * x holds nnz values of `type`.  GrB_INVALID_OBJECT when the arrays are not a
+ * matrix.  The device half of GrB_Matrix_import's copy-and-check
+ * (Source/import_export/GrB_Matrix_import.c:28-205, GB_import.c:330-367). */
+int grb_b200_dmatrix_import(grb_b200_dmatrix *D, int64_t nrows, int64_t ncols,
+                            const int64_t *p, const int64_t *i, const void *x,
+                            int type);
+
+/* Copy the live entries of D into the caller's arrays: nrows+1 offsets, then
+ * nvals indices and nvals values (iso values expanded; x may be NULL).
+ * nvals = stored entries - zombies (grb_b200_dmatrix_info).  The copy of
+ * GrB_Matrix_export (Source/import_export/GrB_Matrix_export.c:38-215). */
+int grb_b200_dmatrix_export(grb_b200_dmatrix D, int64_t *p, int64_t *i, void *x);
+
 int grb_b200_dmatrix_free(grb_b200_dmatrix *D);
 
 /* nrows, ncols, stored entries (zombies included), zombies, type, iso */

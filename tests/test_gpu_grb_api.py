@@ -186,3 +186,103 @@ def test_api_out_of_memory_injection(api, gpu):
     assert api.nvals(C) > 0
     api.free(A)
     api.free(C)
+
+
+def _addr(a):
+    return a.ctypes.data
+
+
+def test_import_export_round_trip_and_product(api, oracle):
+    """GrB_Matrix_import copies the caller's CSR arrays straight to HBM (checked
+    on the device), GrB_Matrix_export copies a result straight back."""
+    Ac = random_csr(300, 280, 0.05, 11)
+    Bc = random_csr(280, 260, 0.05, 12)
+    A = api.matrix_import(11, 300, 280, _addr(Ac.p), _addr(Ac.i), _addr(Ac.x), Ac.nnz)
+    B = api.matrix_import(11, 280, 260, _addr(Bc.p), _addr(Bc.i), _addr(Bc.x), Bc.nnz)
+    assert api.export_size(A) == (301, Ac.nnz)
+    p = np.zeros(301, np.int64)
+    i = np.zeros(Ac.nnz, np.int64)
+    x = np.zeros(Ac.nnz)
+    assert api.matrix_export(A, 11, _addr(p), _addr(i), _addr(x), 301, Ac.nnz) == Ac.nnz
+    assert_exact((p, i, x), (Ac.p, Ac.i, Ac.x), "import/export round trip")
+    C = api.matrix_new(11, 300, 260)
+    api.mxm(C, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", A, B)
+    plen, nv = api.export_size(C)
+    cp = np.zeros(plen, np.int64)
+    ci = np.zeros(nv, np.int64)
+    cx = np.zeros(nv)
+    api.matrix_export(C, 11, _addr(cp), _addr(ci), _addr(cx), plen, nv)
+    want = oracle.saxpy(300, 260, (Ac.p, Ac.i, Ac.x, 11), (Bc.p, Bc.i, Bc.x, 11),
+                        "PLUS", "TIMES", 11)
+    assert_exact((cp, ci, cx), want, "mxm of imported matrices")
+    for X in (A, B, C):
+        api.free(X)
+
+
+def test_import_sorts_jumbled_rows_and_rejects_bad_arrays(api):
+    from graphblas_b200.grb import GrBError
+    rng = np.random.default_rng(5)
+    Ac = random_csr(200, 150, 0.1, 13)
+    jp, ji, jx = Ac.p.copy(), Ac.i.copy(), Ac.x.copy()
+    for r in range(200):                      # shuffle every row
+        lo, hi = jp[r], jp[r + 1]
+        perm = lo + rng.permutation(hi - lo)
+        ji[lo:hi], jx[lo:hi] = ji[perm], jx[perm]
+    A = api.matrix_import(11, 200, 150, _addr(jp), _addr(ji), _addr(jx), Ac.nnz)
+    p = np.zeros(201, np.int64)
+    i = np.zeros(Ac.nnz, np.int64)
+    x = np.zeros(Ac.nnz)
+    api.matrix_export(A, 11, _addr(p), _addr(i), _addr(x), 201, Ac.nnz)
+    assert_exact((p, i, x), (Ac.p, Ac.i, Ac.x), "jumbled rows come back sorted")
+    # export into arrays that are too small
+    with pytest.raises(GrBError) as e:
+        api.matrix_export(A, 11, _addr(p), _addr(i), _addr(x), 201, Ac.nnz - 1)
+    assert e.value.info == -103                   # GrB_INSUFFICIENT_SPACE
+    api.free(A)
+
+    def bad(p_, i_, x_, what):
+        with pytest.raises(GrBError) as e:
+            api.matrix_import(11, 200, 150, _addr(p_), _addr(i_), _addr(x_), len(i_))
+        assert e.value.info == -104, what         # GrB_INVALID_OBJECT
+    i2 = Ac.i.copy()
+    i2[7] = 150                                   # column out of range
+    bad(Ac.p, i2, Ac.x, "index out of range")
+    p2 = Ac.p.copy()
+    p2[50] = p2[51] + 1                           # offsets decrease
+    bad(p2, Ac.i, Ac.x, "decreasing offsets")
+    r = int(np.argmax(np.diff(Ac.p) >= 2))        # a row with two entries
+    i3 = Ac.i.copy()
+    i3[Ac.p[r] + 1] = i3[Ac.p[r]]                 # duplicate index in a row
+    bad(Ac.p, i3, Ac.x, "duplicate")
+    import ctypes
+    h = ctypes.c_void_p()
+    with pytest.raises(GrBError) as e:            # only GrB_CSR_FORMAT is built
+        api.call("GrB_Matrix_import_FP64", ctypes.byref(h), api.obj("GrB_FP64"), 200, 150,
+                 _addr(Ac.p), _addr(Ac.i), _addr(Ac.x), 201, Ac.nnz, Ac.nnz, 1)
+    assert e.value.info == -8                     # GrB_NOT_IMPLEMENTED
+    with pytest.raises(GrBError) as e:            # Ap shorter than nrows+1
+        api.call("GrB_Matrix_import_FP64", ctypes.byref(h), api.obj("GrB_FP64"), 200, 150,
+                 _addr(Ac.p), _addr(Ac.i), _addr(Ac.x), 200, Ac.nnz, Ac.nnz, 0)
+    assert e.value.info == -3                     # GrB_INVALID_VALUE
+
+
+def test_vector_extract_from_device(api):
+    """GrB_Vector_extractTuples of a vector computed on the device copies its
+    indices and values straight from HBM."""
+    S = W.rmat(10, 8, seed=2)
+    A = api.matrix_from_csr(S, 1)
+    n = S.nrows
+    v0 = int(np.argmax(np.diff(S.p)))
+    q = api.vector_from([v0], [v0], 8, n)
+    w = api.vector_new(8, n)
+    api.vxm(w, None, None, "GxB_ANY_SECONDI_INT64", q, A, None)
+    nv = api.vnvals(w)
+    i = np.zeros(nv, np.int64)
+    x = np.zeros(nv, np.int64)
+    assert api.vector_extract(w, 8, _addr(i), _addr(x), nv) == nv
+    lo, hi = S.p[v0], S.p[v0 + 1]
+    assert np.array_equal(i, S.i[lo:hi])
+    assert np.array_equal(x, np.full(hi - lo, v0))  # any_secondi: row index of q's entry
+    for v in (q, w):
+        api.vfree(v)
+    api.free(A)
