@@ -355,7 +355,13 @@ static constexpr int D3_LONG = 2048;          // longer lists go to the shared t
 static constexpr int D3_SEG = 512;            // probes per shared long-list segment
 static constexpr int D3_TABLE = 1024;         // long lists registered per item
 
-struct D3Item { int32_t key, t, nit, pad; };
+// a grouped entry as the bitmap kernel reads it: its probed list and where
+// its result goes
+struct __align__(16) D3Rec { int32_t s0, len, pm, j; };
+
+// a work item: every nit-th entry of key's group, from the t-th; its key row
+// (offsets rp0..rp1, first column lo) and lanes per entry 2^lg
+struct __align__(16) D3Item { int32_t key, t, nit, m_item, rp0, rp1, lo, lg; int64_t g0, pad; };
 
 template <class SR> struct IsCount {
     static constexpr bool value = SR::add_op == OP_PLUS && SR::mult_op == OP_PAIR &&
@@ -380,7 +386,7 @@ __global__ void __launch_bounds__(256)
 k_d3_route(const D3Work *__restrict__ queue, const int *__restrict__ qlen_p,
            const int64_t *__restrict__ gsz, const int64_t *__restrict__ goff,
            int32_t *__restrict__ gfill, unsigned long long *__restrict__ gwork,
-           int32_t *__restrict__ bucket, int32_t *__restrict__ merge_sel,
+           D3Rec *__restrict__ bucket, int32_t nrows, int32_t *__restrict__ merge_sel,
            int *__restrict__ merge_len)
 {
     const int lane = threadIdx.x & 31;
@@ -392,13 +398,17 @@ k_d3_route(const D3Work *__restrict__ queue, const int *__restrict__ qlen_p,
         bool grouped = false, merge = false;
         int32_t key = -1;
         unsigned long long work = 0;
+        D3Rec rec{0, 0, 0, 0};
         if (w < qlen) {
             const D3Work e = queue[w];
             key = e.pad;
             grouped = key >= 0 && gsz[key] > 0;
             merge = !grouped;
-            // probes: the shorter list's elements
-            work = (unsigned long long)min(e.a1 - e.a0, e.b1 - e.b0);
+            // probes: the other list's elements (the shorter one)
+            const bool by_row = key < nrows;
+            rec = by_row ? D3Rec{e.b0, e.b1 - e.b0, e.pm, e.j}
+                         : D3Rec{e.a0, e.a1 - e.a0, e.pm, e.j};
+            work = (unsigned long long)rec.len;
         }
         const unsigned gm = __ballot_sync(0xffffffffu, grouped);
         if (grouped) {
@@ -413,7 +423,7 @@ k_d3_route(const D3Work *__restrict__ queue, const int *__restrict__ qlen_p,
                 atomicAdd(&gwork[key], (unsigned long long)wsum);
             }
             slot0 = __shfl_sync(same, slot0, leader);
-            bucket[goff[key] + slot0 + __popc(same & ((1u << lane) - 1))] = w;
+            bucket[goff[key] + slot0 + __popc(same & ((1u << lane) - 1))] = rec;
         }
         const unsigned mm = __ballot_sync(0xffffffffu, merge);
         if (mm) {
@@ -446,13 +456,29 @@ __global__ void k_d3_item_count(const int64_t *__restrict__ gsz,
 }
 
 __global__ void k_d3_item_fill(const int64_t *__restrict__ ioff, int64_t nkeys,
+                               const int64_t *__restrict__ goff,
+                               const unsigned long long *__restrict__ gwork, int32_t nrows,
+                               const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+                               const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
                                D3Item *__restrict__ items)
 {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; t < nkeys; t += stride) {
         const int64_t o = ioff[t], n = ioff[t + 1] - o;
-        for (int64_t q = 0; q < n; q++) items[o + q] = D3Item{(int32_t)t, (int32_t)q, (int32_t)n, 0};
+        if (n == 0) continue;
+        const bool by_row = t < nrows;
+        const int32_t r = by_row ? (int32_t)t : (int32_t)(t - nrows);
+        const int32_t rp0 = by_row ? Ap[r] : Bp[r], rp1 = by_row ? Ap[r + 1] : Bp[r + 1];
+        const int32_t lo = by_row ? Aj[rp0] : Bj[rp0];
+        const int64_t g0 = goff[t], gn = goff[t + 1] - g0;
+        // lanes per entry: a power of two near half the mean list length
+        const unsigned long long mean = gwork[t] / (unsigned long long)gn;
+        int lg = 0;
+        while (lg < 5 && (2ull << lg) < mean) lg++;
+        for (int64_t q = 0; q < n; q++)
+            items[o + q] = D3Item{(int32_t)t, (int32_t)q, (int32_t)n,
+                                  (int32_t)((gn - q + n - 1) / n), rp0, rp1, lo, lg, g0, 0};
     }
 }
 
@@ -474,12 +500,9 @@ __global__ void k_d3_item_fill(const int64_t *__restrict__ ioff, int64_t nkeys,
 template <class SR>
 __global__ void __launch_bounds__(D3_BM_THREADS, 1)
 k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict__ nitems_p,
-                    int *__restrict__ inext, const int64_t *__restrict__ goff,
-                    const unsigned long long *__restrict__ gwork,
-                    const int32_t *__restrict__ bucket, const D3Work *__restrict__ queue,
-                    int32_t nrows,
-                    const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
-                    const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
+                    int *__restrict__ inext, const D3Rec *__restrict__ bucket,
+                    int32_t nrows, const int32_t *__restrict__ Aj,
+                    const int32_t *__restrict__ Bj,
                     uint32_t bm_words, int32_t *__restrict__ Cj,
                     typename SR::z_t *__restrict__ Cx,
                     unsigned long long *__restrict__ nzombies)
@@ -487,6 +510,7 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
     using Z = typename SR::z_t;
     extern __shared__ uint32_t bm[];
     __shared__ int s_item, s_next, s_gnext;
+    __shared__ D3Item s_I;                        // the next item, fetched ahead
     __shared__ unsigned long long s_tbl;          // (segments << 32) | entries
     __shared__ int32_t t_start[D3_TABLE], t_rem[D3_TABLE], t_seg0[D3_TABLE];
     __shared__ int32_t t_cnt[D3_TABLE], t_pm[D3_TABLE], t_j[D3_TABLE];
@@ -516,34 +540,36 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
         }
         return c;
     };
+    if (tid == 0) {
+        s_item = atomicAdd(inext, 1);
+        if (s_item < nitems) s_I = items[s_item];
+    }
     while (true) {
-        __syncthreads();
-        if (tid == 0) { s_item = atomicAdd(inext, 1); s_next = 0; s_gnext = 0; s_tbl = 0; }
         __syncthreads();
         const int it = s_item;
         if (it >= nitems) break;
-        const D3Item I = items[it];
+        const D3Item I = s_I;
+        __syncthreads();
+        if (tid == 0) { s_next = 0; s_gnext = 0; s_tbl = 0; }
         const bool by_row = I.key < nrows;
-        const int32_t r = by_row ? I.key : I.key - nrows;
-        const int32_t *P = by_row ? Ap : Bp;
         const int32_t *J = by_row ? Aj : Bj;
         const int32_t *S = by_row ? Bj : Aj;     // the probed lists
-        const int32_t rp0 = P[r], rp1 = P[r + 1];
-        const int32_t lo = J[rp0];
+        const int32_t rp0 = I.rp0, rp1 = I.rp1, lo = I.lo;
         for (int32_t q = rp0 + tid; q < rp1; q += blockDim.x) {
             const uint32_t k = (uint32_t)(J[q] - lo);
             atomicOr(&bm[k >> 5], 1u << (k & 31));
         }
-        const int64_t g0 = goff[I.key];
-        const int32_t gn = (int32_t)(goff[I.key + 1] - g0);
-        const int32_t m_item = (gn - I.t + I.nit - 1) / I.nit;
-        // lanes per entry
-        const unsigned long long mean = gwork[I.key] / (unsigned long long)gn;
-        int lg = 0;
-        while (lg < 5 && (2ull << lg) < mean) lg++;
+        const int64_t g0 = I.g0;
+        const int32_t m_item = I.m_item;
+        const int lg = I.lg;
         const int G = 1 << lg, gi = lane >> lg, gl = lane & (G - 1);
         const int groups = 32 >> lg;
         __syncthreads();
+        // fetch the next item while this one runs
+        if (tid == 0) {
+            s_item = atomicAdd(inext, 1);
+            if (s_item < nitems) s_I = items[s_item];
+        }
         // phase A
         while (true) {
             int c0 = 0;
@@ -553,9 +579,9 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
             const int32_t rr = c0 + gi;
             int32_t s0 = 0, len = 0, pm = 0, j = 0;
             if (rr < m_item) {
-                const D3Work e = queue[bucket[g0 + I.t + (int64_t)I.nit * rr]];
-                s0 = by_row ? e.b0 : e.a0;
-                len = by_row ? e.b1 - e.b0 : e.a1 - e.a0;
+                const D3Rec e = bucket[g0 + I.t + (int64_t)I.nit * rr];
+                s0 = e.s0;
+                len = e.len;
                 pm = e.pm;
                 j = e.j;
             }
@@ -681,7 +707,8 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
         if (mnz >= D3_BM_MIN_ENTRIES && nkeys < INT32_MAX) bm_words = bitmap_words<SR>(A.ncols);
     }
     Scratch bm_scratch(s);
-    int32_t *gcnt = nullptr, *gfill = nullptr, *bucket = nullptr, *merge_sel = nullptr;
+    int32_t *gcnt = nullptr, *gfill = nullptr, *merge_sel = nullptr;
+    D3Rec *bucket = nullptr;
     int64_t *gsz = nullptr, *goff = nullptr, *nit = nullptr, *ioff = nullptr, *ws = nullptr;
     unsigned long long *gwork = nullptr;
     D3Item *items = nullptr;
@@ -694,7 +721,7 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
         ioff = bm_scratch.get<int64_t>(nkeys + 1);
         gwork = bm_scratch.get<unsigned long long>(nkeys);
         items = bm_scratch.get<D3Item>(nkeys + mnz / 32 + 1);
-        bucket = bm_scratch.get<int32_t>(mnz);
+        bucket = bm_scratch.get<D3Rec>(mnz);
         merge_sel = bm_scratch.get<int32_t>(mnz);
         ws = bm_scratch.get<int64_t>((int64_t)scan_ws_elems(nkeys + 1));
         if (bm_scratch.failed) {
@@ -723,14 +750,16 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
             k_d3_gsize<<<kb, 256, 0, s>>>(gcnt, nkeys, gsz);
             scan_exclusive_i64_ws(gsz, goff, nkeys + 1, ws, s);
             k_d3_route<<<(unsigned)blocks, 256, 0, s>>>(queue, qlen, gsz, goff, gfill, gwork,
-                                                       bucket, merge_sel, merge_len);
+                                                       bucket, (int32_t)M.nrows, merge_sel,
+                                                       merge_len);
             k_d3_item_count<<<kb, 256, 0, s>>>(gsz, gwork, nkeys, nit);
             scan_exclusive_i64_ws(nit, ioff, nkeys + 1, ws, s);
-            k_d3_item_fill<<<kb, 256, 0, s>>>(ioff, nkeys, items);
+            k_d3_item_fill<<<kb, 256, 0, s>>>(ioff, nkeys, goff, gwork, (int32_t)M.nrows,
+                                              A.p, A.j, B.p, B.j, items);
             if constexpr (IsCount<SR>::value)
                 k_dot3_bitmap_count<SR><<<nsm, D3_BM_THREADS, (size_t)bm_words * 4, s>>>(
-                    items, ioff + nkeys, inext, goff, gwork, bucket, queue, (int32_t)M.nrows,
-                    A.p, A.j, B.p, B.j, bm_words, C.j, (Z *)C.x, zc);
+                    items, ioff + nkeys, inext, bucket, (int32_t)M.nrows, A.j, B.j,
+                    bm_words, C.j, (Z *)C.x, zc);
             k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
                 queue, merge_sel, merge_len, qnext, A.j, A.x, A.iso, B.j, B.x, B.iso,
                 C.j, (Z *)C.x, zc);
