@@ -350,6 +350,11 @@ int batch_capture(grb_b200_batch_s *B)
     return SUCCESS;
 }
 
+int ensure_prepared(grb_b200_batch_s *B)
+{
+    return B->plan ? SUCCESS : batch_prepare(B, saxpy_default_config());
+}
+
 double time_exec(grb_b200_batch_s *B, int reps)
 {
     cudaEvent_t a, b;
@@ -416,7 +421,8 @@ int grb_b200_batch_create(grb_b200_batch *Bout, int count, const int64_t *a_nrow
     }
     B->nnz_d = (int64_t *)dalloc(8, B->s);
     if (info == SUCCESS && !B->nnz_d) info = OUT_OF_MEMORY;
-    if (info == SUCCESS) info = batch_prepare(B, saxpy_default_config());
+    // the symbolic phase waits for the first tune or run, so that a tuned
+    // (or cached) configuration is prepared once
     if (info != SUCCESS) { grb_b200_batch_free(&B); return info; }
     *Bout = B;
     return SUCCESS;
@@ -461,6 +467,8 @@ int grb_b200_batch_run(grb_b200_batch B, bool use_graph)
     int info = SUCCESS;
     // the caller's stream for this thread (grb_b200_set_stream), else the batch's
     cudaStream_t st = thread_stream() ? thread_stream() : B->s;
+    info = ensure_prepared(B);
+    if (info != SUCCESS) return info;
     if (st != B->s) {
         // order the batch's own stream (setup work) before the caller's
         cudaStreamSynchronize(B->s);
@@ -490,7 +498,8 @@ int grb_b200_batch_enqueue(grb_b200_batch B, void *stream)
     // graph replay on the caller's stream, no host synchronisation
     if (!B) return NULL_POINTER;
     if (!B->gexec) {
-        int info = batch_capture(B);
+        int info = ensure_prepared(B);
+        if (info == SUCCESS) info = batch_capture(B);
         if (info != SUCCESS) return info;
     }
     return cuda_to_info(cudaGraphLaunch(B->gexec, stream ? (cudaStream_t)stream : B->s));
@@ -517,52 +526,67 @@ int grb_b200_batch_info(grb_b200_batch B, int64_t *total_rows, int64_t *nnz_c,
     }
     if (total_rows) *total_rows = B->A.nrows;
     if (nnz_c) *nnz_c = B->last_nnz;
-    if (capacity) *capacity = saxpy_plan_capacity(B->plan);
+    if (capacity) *capacity = B->plan ? saxpy_plan_capacity(B->plan) : 0;
     if (nbins) *nbins = B->cfg.nb;
     if (tuned_ms) *tuned_ms = B->tuned ? B->tuned_ms : -1.0;
     return SUCCESS;
 }
 
-int grb_b200_batch_result(grb_b200_batch B, int64_t **Cp, int64_t **Cj, void **Cx,
-                          int64_t *nnz_per_instance)
+int grb_b200_batch_result_into(grb_b200_batch B, int64_t *Cp, int64_t *Cj, void *Cx,
+                               int64_t *nnz_per_instance)
 {
     if (!B || !Cp || !Cj || !Cx) return NULL_POINTER;
+    if (!B->plan) return INVALID_VALUE;            // nothing has run yet
     cudaStream_t s = B->s;
     const int count = B->count;
     const int64_t m = B->A.nrows;
-    int64_t nnz = 0;
-    cudaMemcpyAsync(&nnz, B->C.p + m, 4, cudaMemcpyDeviceToHost, s);   // int32
+    int32_t nnz32 = 0;
+    cudaMemcpyAsync(&nnz32, B->C.p + m, 4, cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
-    nnz = (int64_t)(int32_t)nnz;
+    const int64_t nnz = nnz32;
     std::vector<int64_t> pout(count + 1, 0);
     for (int k = 0; k < count; k++) pout[k + 1] = pout[k] + B->am[k] + 1;
     int64_t *dn = upload_vec(B->am, s), *dr = upload_vec(B->roff, s);
     int64_t *dc = upload_vec(B->bcoff, s), *dpo = upload_vec(pout, s);
     int64_t *dP = (int64_t *)dalloc((size_t)pout[count] * 8 + 8, s);
     int64_t *dJ = (int64_t *)dalloc((size_t)(nnz + 1) * 8, s);
-    *Cp = (int64_t *)malloc((size_t)pout[count] * 8 + 8);
-    *Cj = (int64_t *)malloc((size_t)(nnz + 1) * 8);
-    *Cx = malloc((size_t)(nnz + 1) * B->zsize);
     int info = SUCCESS;
-    if (!dn || !dr || !dc || !dpo || !dP || !dJ || !*Cp || !*Cj || !*Cx) info = OUT_OF_MEMORY;
+    if (!dn || !dr || !dc || !dpo || !dP || !dJ) info = OUT_OF_MEMORY;
     if (info == SUCCESS) {
         k_split<<<count < 65535 ? count : 65535, 128, 0, s>>>(count, dn, dr, dc, dpo,
             B->C.p, B->C.j, dP, dJ);
-        cudaMemcpyAsync(*Cp, dP, (size_t)pout[count] * 8, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(*Cj, dJ, (size_t)nnz * 8, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(*Cx, B->C.x, (size_t)nnz * B->zsize, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(Cp, dP, (size_t)pout[count] * 8, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(Cj, dJ, (size_t)nnz * 8, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(Cx, B->C.x, (size_t)nnz * B->zsize, cudaMemcpyDeviceToHost, s);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) info = cuda_to_info(e);
     }
     dfree(dn, s); dfree(dr, s); dfree(dc, s); dfree(dpo, s); dfree(dP, s); dfree(dJ, s);
     if (info == SUCCESS && nnz_per_instance)
         for (int k = 0; k < count; k++)
-            nnz_per_instance[k] = (*Cp)[pout[k] + B->am[k]] - (*Cp)[pout[k]];
-    if (info != SUCCESS) {
-        free(*Cp); free(*Cj); free(*Cx);
-        *Cp = nullptr; *Cj = nullptr; *Cx = nullptr;
-    }
+            nnz_per_instance[k] = Cp[pout[k] + B->am[k]] - Cp[pout[k]];
     return info;
+}
+
+int grb_b200_batch_result(grb_b200_batch B, int64_t **Cp, int64_t **Cj, void **Cx,
+                          int64_t *nnz_per_instance)
+{
+    if (!B || !Cp || !Cj || !Cx) return NULL_POINTER;
+    *Cp = nullptr; *Cj = nullptr; *Cx = nullptr;
+    if (!B->plan) return INVALID_VALUE;
+    int32_t nnz32 = 0;
+    cudaMemcpyAsync(&nnz32, B->C.p + B->A.nrows, 4, cudaMemcpyDeviceToHost, B->s);
+    cudaStreamSynchronize(B->s);
+    int64_t np = 0;
+    for (int k = 0; k < B->count; k++) np += B->am[k] + 1;
+    int64_t *P = (int64_t *)malloc((size_t)np * 8 + 8);
+    int64_t *J = (int64_t *)malloc((size_t)(nnz32 + 1) * 8);
+    void *X = malloc((size_t)(nnz32 + 1) * B->zsize);
+    int info = (P && J && X) ? grb_b200_batch_result_into(B, P, J, X, nnz_per_instance)
+                             : OUT_OF_MEMORY;
+    if (info != SUCCESS) { free(P); free(J); free(X); return info; }
+    *Cp = P; *Cj = J; *Cx = X;
+    return SUCCESS;
 }
 
 int grb_b200_batch_free(grb_b200_batch *Bp)

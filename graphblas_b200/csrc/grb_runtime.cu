@@ -252,8 +252,8 @@ __global__ void k_narrow_check(const int64_t *__restrict__ in, int32_t *__restri
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, bit);
 }
 
-// flag |= bit when some row's indices are not strictly increasing (flat over
-// the entries: one binary search per warp for its first entry's row)
+// flag |= bit when some row's indices are not strictly increasing (one warp
+// per row, coalesced)
 __global__ void k_check_rows(const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
                              int64_t nrows, int64_t nnz, unsigned *__restrict__ flag,
                              unsigned bit)
@@ -261,18 +261,11 @@ __global__ void k_check_rows(const int32_t *__restrict__ Ap, const int32_t *__re
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     bool bad = false;
-    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
-         base < nnz; base += nw * 32) {
-        int32_t r0 = 0;
-        if (lane == 0) r0 = upper_bound(Ap, 0, (int32_t)nrows + 1, (int32_t)base) - 1;
-        r0 = __shfl_sync(0xffffffffu, r0, 0);
-        const int64_t e = base + lane;
-        if (e < nnz) {
-            int32_t r = r0;
-            while (Ap[r + 1] <= e) r++;
-            if (e > Ap[r]) bad |= Aj[e - 1] >= Aj[e];
-        }
+    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nrows; r += nw) {
+        const int32_t p0 = Ap[r], p1 = Ap[r + 1];
+        for (int32_t q = p0 + 1 + lane; q < p1; q += 32) bad |= Aj[q - 1] >= Aj[q];
     }
+    (void)nnz;
     if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(flag, bit);
 }
 
@@ -309,7 +302,7 @@ int dev_import(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
     if (e != cudaSuccess) { dev_free(A, s); return cuda_to_info(e); }
     if (hflag) { dev_free(A, s); return INVALID_OBJECT; }
     if (nnz == 0) return SUCCESS;
-    k_check_rows<<<grid_for(nnz, 256), 256, 0, s>>>(A.p, A.j, nrows, nnz, flag, 4u);
+    k_check_rows<<<grid_for(nrows * 32, 256), 256, 0, s>>>(A.p, A.j, nrows, nnz, flag, 4u);
     cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, s);
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) { dev_free(A, s); return cuda_to_info(e); }
@@ -324,7 +317,7 @@ int dev_import(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
     A = B;
     // a sorted row with two equal indices holds a duplicate: not a matrix
     cudaMemsetAsync(flag, 0, 4, s);
-    k_check_rows<<<grid_for(nnz, 256), 256, 0, s>>>(A.p, A.j, nrows, nnz, flag, 4u);
+    k_check_rows<<<grid_for(nrows * 32, 256), 256, 0, s>>>(A.p, A.j, nrows, nnz, flag, 4u);
     cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, s);
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess || hflag) {

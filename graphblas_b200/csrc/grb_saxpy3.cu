@@ -98,28 +98,41 @@ __global__ void k_bin_rows(const int64_t *__restrict__ flops,
                            const int32_t *__restrict__ Mp, bool has_mask,
                            bool mask_bounds, int64_t ncols,
                            int64_t nrows, BinLimits lim, int *__restrict__ bin_count,
-                           int8_t *__restrict__ row_bin, int64_t *__restrict__ cap)
+                           int8_t *__restrict__ row_bin, int64_t *__restrict__ cap,
+                           const int32_t *__restrict__ Ap,
+                           unsigned long long *__restrict__ heavy_alen)
 {
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t r = t; r < nrows; r += stride) {
-        int64_t f = flops[r];
-        int64_t c = f < ncols ? f : ncols;
-        if (mask_bounds) {
-            const int64_t mc = Mp[r + 1] - Mp[r];
-            if (mc < c) c = mc;
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    // warp-uniform loop: the bin counters take one atomic per bin per warp
+    for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); r0 < nrows;
+         r0 += stride) {
+        const int64_t r = r0 + lane;
+        int b = -1;
+        if (r < nrows) {
+            const int64_t f = flops[r];
+            int64_t c = f < ncols ? f : ncols;
+            if (mask_bounds) {
+                const int64_t mc = Mp[r + 1] - Mp[r];
+                if (mc < c) c = mc;
+            }
+            cap[r] = f == 0 ? 0 : c;
+            if (f == 0) b = 0;
+            else {
+                const int64_t need = f + (has_mask ? (int64_t)(Mp[r + 1] - Mp[r]) : 0);
+                b = lim.nb + 1;
+                for (int q = 0; q < lim.nb; q++)
+                    if (need <= lim.limit[q]) { b = q + 1; break; }
+            }
+            row_bin[r] = (int8_t)b;
+            // entries of A in the heavy rows (sizes the flat product index)
+            if (b == lim.nb + 1) atomicAdd(heavy_alen, (unsigned long long)(Ap[r + 1] - Ap[r]));
         }
-        cap[r] = f == 0 ? 0 : c;
-        int b;
-        if (f == 0) b = 0;
-        else {
-            int64_t need = f + (has_mask ? (int64_t)(Mp[r + 1] - Mp[r]) : 0);
-            b = lim.nb + 1;
-            for (int q = 0; q < lim.nb; q++)
-                if (need <= lim.limit[q]) { b = q + 1; break; }
+        const unsigned counted = __ballot_sync(0xffffffffu, b > 0);
+        if (b > 0) {
+            const unsigned same = __match_any_sync(counted, b);
+            if ((int)(__ffs(same) - 1) == lane) atomicAdd(&bin_count[b], __popc(same));
         }
-        row_bin[r] = (int8_t)b;
-        if (b > 0) atomicAdd(&bin_count[b], 1);
     }
 }
 
@@ -129,13 +142,20 @@ __global__ void k_fill_bins(const int8_t *__restrict__ row_bin, int64_t nrows,
                             const int *__restrict__ bin_start,
                             int32_t *__restrict__ bin_rows)
 {
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t r = t; r < nrows; r += stride) {
-        int b = row_bin[r];
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); r0 < nrows;
+         r0 += stride) {
+        const int64_t r = r0 + lane;
+        const int b = r < nrows ? row_bin[r] : 0;
+        const unsigned placed = __ballot_sync(0xffffffffu, b > 0);
         if (b > 0) {
-            int pos = atomicAdd(&bin_fill[b], 1);
-            bin_rows[bin_start[b] + pos] = (int32_t)r;
+            const unsigned same = __match_any_sync(placed, b);
+            const int leader = __ffs(same) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&bin_fill[b], __popc(same));
+            base = __shfl_sync(same, base, leader);
+            bin_rows[bin_start[b] + base + __popc(same & ((1u << lane) - 1))] = (int32_t)r;
         }
     }
 }
@@ -175,7 +195,7 @@ template <typename Z> __host__ __device__ inline size_t group_bytes(int cap)
 // A group of TPR threads (TPR = 4..32 inside a 128-thread block, or the whole
 // 256-thread block when BLOCK) owns one row and one hash table of cap slots.
 template <class SR, bool BLOCK>
-__global__ void __launch_bounds__(BLOCK ? 256 : 128)
+__global__ void __launch_bounds__(BLOCK ? 256 : 128, BLOCK ? 4 : 8)
 k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin, int tpr_log2, int cap,
              const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
              const void *__restrict__ Ax, bool a_iso,
@@ -321,9 +341,12 @@ k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin, int tpr_log2, int 
 // so every semiring, floating PLUS included, gives the same bits.
 static constexpr int ESC_WARPS = 8;
 
-template <class SR>
-__global__ void __launch_bounds__(ESC_WARPS * 32)
-k_saxpy_esc(const int32_t *__restrict__ rows, int nrows_bin, int cap,
+// KT: 32-bit keys when (column << posb) fits, else 64-bit; posb = log2(cap)
+// bits hold the product's position, so only the keys move in the sort and
+// the values stay where the expansion wrote them.
+template <class SR, typename KT>
+__global__ void __launch_bounds__(ESC_WARPS * 32, 4)
+k_saxpy_esc(const int32_t *__restrict__ rows, int nrows_bin, int cap, int posb,
             const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
             const void *__restrict__ Ax, bool a_iso,
             const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
@@ -337,10 +360,10 @@ k_saxpy_esc(const int32_t *__restrict__ rows, int nrows_bin, int cap,
     using Z = typename SR::z_t;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    // key = column << 20 | position (positions < cap <= 2^16)
-    uint64_t *key = (uint64_t *)(smem + (size_t)w * cap * (8 + sizeof(Z)));
-    Z *val = (Z *)((unsigned char *)key + (size_t)cap * 8);
+    KT *key = (KT *)(smem + (size_t)w * cap * (sizeof(KT) + sizeof(Z)));
+    Z *val = (Z *)((unsigned char *)key + (size_t)cap * sizeof(KT));
     const unsigned below = (1u << lane) - 1u;
+    const KT posmask = ((KT)1 << posb) - 1;
 
     for (int64_t rb = (int64_t)blockIdx.x * ESC_WARPS + w; rb < nrows_bin;
          rb += (int64_t)gridDim.x * ESC_WARPS) {
@@ -397,7 +420,7 @@ k_saxpy_esc(const int32_t *__restrict__ rows, int nrows_bin, int cap,
                     const int pos = n + __popc(km & below);
                     Z b = Z();
                     if (SR::needs_b) b = ld_val<Z>(Bx, pb, b_iso);
-                    key[pos] = ((uint64_t)(uint32_t)j << 20) | (uint64_t)pos;
+                    key[pos] = ((KT)(uint32_t)j << posb) | (KT)pos;
                     val[pos] = SR::F::f(aa, b, i, kk, j);
                 }
                 n += __popc(km);
@@ -406,43 +429,45 @@ k_saxpy_esc(const int32_t *__restrict__ rows, int nrows_bin, int cap,
         __syncwarp();
         int n2 = 1;
         while (n2 < n) n2 <<= 1;
-        for (int q = n + lane; q < n2; q += 32) key[q] = ~0ull;
+        for (int q = n + lane; q < n2; q += 32) key[q] = ~(KT)0;
         __syncwarp();
+        // bitonic sort of the keys; a lane owns every 32nd compare-exchange
         for (int size = 2; size <= n2; size <<= 1) {
             for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                for (int q = lane; q < n2; q += 32) {
-                    const int partner = q ^ stride;
-                    if (partner > q) {
-                        const bool up = ((q & size) == 0);
-                        const uint64_t ka = key[q], kb = key[partner];
-                        if ((ka > kb) == up) {
-                            key[q] = kb; key[partner] = ka;
-                            const Z va = val[q]; val[q] = val[partner]; val[partner] = va;
-                        }
-                    }
+                for (int q = lane; q < (n2 >> 1); q += 32) {
+                    // q-th pair of this pass: lower index a, partner a + stride
+                    const int a = ((q & ~(stride - 1)) << 1) | (q & (stride - 1));
+                    const int b = a + stride;
+                    const bool up = ((a & size) == 0);
+                    const KT ka = key[a], kb = key[b];
+                    if ((ka > kb) == up) { key[a] = kb; key[b] = ka; }
                 }
                 __syncwarp();
             }
         }
         // the first entry of each run of equal columns folds the run in
-        // ascending k and writes one output entry
+        // ascending k (its positions ascend) and writes one output entry
         const int64_t off = slot_off[i];
         int out = 0;
         for (int c0 = 0; c0 < n; c0 += 32) {
             const int p = c0 + lane;
             bool head = false;
-            uint32_t j = 0;
+            KT kp = 0;
             if (p < n) {
-                j = (uint32_t)(key[p] >> 20);
-                head = (p == 0) || ((uint32_t)(key[p - 1] >> 20) != j);
+                kp = key[p];
+                head = (p == 0) || ((key[p - 1] >> posb) != (kp >> posb));
             }
             const unsigned hm = __ballot_sync(0xffffffffu, head);
             if (head) {
-                Z z = val[p];
-                for (int r = p + 1; r < n && (uint32_t)(key[r] >> 20) == j; r++)
-                    z = SR::M::update(z, val[r]);
+                const KT jcol = kp >> posb;
+                Z z = val[kp & posmask];
+                for (int r = p + 1; r < n; r++) {
+                    const KT kr = key[r];
+                    if ((kr >> posb) != jcol) break;
+                    z = SR::M::update(z, val[kr & posmask]);
+                }
                 const int64_t dst = off + out + __popc(hm & below);
-                Tj[dst] = (int32_t)j;
+                Tj[dst] = (int32_t)jcol;
                 Tx[dst] = z;
             }
             out += __popc(hm);
@@ -668,12 +693,12 @@ template <class SR> __device__ __forceinline__ typename SR::z_t dense_init()
 
 template <class SR>
 __global__ void k_dense_init(const int32_t *__restrict__ rows, int nrows_bin,
-                             int64_t ncols, int64_t *__restrict__ flag_all,
+                             int64_t ncols, uint8_t *__restrict__ flag_all,
                              typename SR::z_t *__restrict__ val_all)
 {
     // one block-row of workspace per heavy row (rows are few)
     for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
-        int64_t *flag = flag_all + rb * ncols;
+        uint8_t *flag = flag_all + rb * ncols;
         typename SR::z_t *val = val_all + rb * ncols;
         for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < ncols;
              j += (int64_t)gridDim.x * blockDim.x) {
@@ -687,101 +712,111 @@ __global__ void k_dense_init(const int32_t *__restrict__ rows, int nrows_bin,
 __global__ void k_dense_mask(const int32_t *__restrict__ rows, int nrows_bin,
                              const int32_t *__restrict__ Mp,
                              const int32_t *__restrict__ Mj, bool mask_comp,
-                             int64_t ncols, int64_t *__restrict__ flag_all)
+                             int64_t ncols, uint8_t *__restrict__ flag_all)
 {
     for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
         const int32_t i = rows[rb];
-        int64_t *flag = flag_all + rb * ncols;
+        uint8_t *flag = flag_all + rb * ncols;
         for (int32_t pm = Mp[i] + blockIdx.x * blockDim.x + threadIdx.x; pm < Mp[i + 1];
              pm += gridDim.x * blockDim.x)
             flag[Mj[pm]] = mask_comp ? 2 : 1;
     }
 }
 
-// every product (i,k,j) of the heavy rows, spread over the grid: a warp takes
-// one A entry (i,k) at a time and its lanes split B(k,:)
-template <class SR>
-__global__ void k_dense_atomic(const int32_t *__restrict__ rows, int nrows_bin,
-                               const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
-                               const void *__restrict__ Ax, bool a_iso,
-                               const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
-                               const void *__restrict__ Bx, bool b_iso,
-                               bool has_mask, bool mask_comp, int64_t ncols,
-                               int64_t *__restrict__ flag_all,
-                               typename SR::z_t *__restrict__ val_all)
+// Flat product index of a chunk of heavy rows: hlen[rb] = nnz(A(i,:)) for the
+// chunk's rows (scanned into hoff), then wlen[e] = nnz(B(k,:)) for the e-th
+// A entry of the chunk (scanned into wprefix), so product t lies in entry e
+// with wprefix[e] <= t < wprefix[e+1].
+__global__ void k_heavy_alen(const int32_t *__restrict__ rows, int nr,
+                             const int32_t *__restrict__ Ap, int64_t *__restrict__ hlen)
 {
-    using Z = typename SR::z_t;
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
-        const int32_t i = rows[rb];
-        int64_t *flag = flag_all + rb * ncols;
-        Z *val = val_all + rb * ncols;
-        const int32_t pa0 = Ap[i], pa1 = Ap[i + 1];
-        for (int64_t pa = pa0 + warp; pa < pa1; pa += nw) {
-            const int32_t k = Aj[pa];
-            Z a = Z();
-            if (SR::needs_a) a = ld_val<Z>(Ax, pa, a_iso);
-            for (int32_t pb = Bp[k] + lane; pb < Bp[k + 1]; pb += 32) {
-                const int32_t j = Bj[pb];
-                if (has_mask) {
-                    const int64_t f = flag[j];
-                    if (!mask_comp && f == 0) continue;
-                    if (mask_comp && f == 2) continue;
-                }
-                Z b = Z();
-                if (SR::needs_b) b = ld_val<Z>(Bx, pb, b_iso);
-                const Z tv = SR::F::f(a, b, i, k, j);
-                AtomicUpd<SR::add_op, Z>::run(&val[j], tv);
-                flag[j] = 3;
-            }
-        }
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nr; t += gridDim.x * blockDim.x) {
+        const int32_t i = rows[t];
+        hlen[t] = Ap[i + 1] - Ap[i];
     }
 }
 
-// ordered compaction of the dense rows (one block per heavy row)
+__device__ __forceinline__ int64_t upper_bound64(const int64_t *a, int64_t lo, int64_t hi,
+                                                 int64_t key)
+{
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (a[mid] <= key) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_heavy_blen(const int32_t *__restrict__ rows, int nr,
+                             const int64_t *__restrict__ hoff,
+                             const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+                             const int32_t *__restrict__ Bp, int64_t *__restrict__ wlen)
+{
+    const int64_t ne = hoff[nr];
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ne;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int rb = nr == 1 ? 0 : (int)(upper_bound64(hoff, 0, nr + 1, e) - 1);
+        const int32_t k = Aj[Ap[rows[rb]] + (e - hoff[rb])];
+        wlen[e] = Bp[k + 1] - Bp[k];
+    }
+}
+
+// Every product of the chunk's heavy rows, flat over the product index: a
+// warp takes 32 consecutive products (one binary search for the first one's
+// A entry; lanes walk forward), so a hub column of B is spread over many
+// warps instead of one.
 template <class SR>
 __global__ void __launch_bounds__(256)
-k_dense_gather(const int32_t *__restrict__ rows, int nrows_bin, int64_t ncols,
-               const int64_t *__restrict__ flag_all,
-               const typename SR::z_t *__restrict__ val_all,
-               const int64_t *__restrict__ slot_off, int32_t *__restrict__ Tj,
-               typename SR::z_t *__restrict__ Tx, int32_t *__restrict__ row_cnt)
+k_dense_atomic_flat(const int32_t *__restrict__ rows, int nr,
+                    const int64_t *__restrict__ hoff, const int64_t *__restrict__ wprefix,
+                    const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+                    const void *__restrict__ Ax, bool a_iso,
+                    const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
+                    const void *__restrict__ Bx, bool b_iso,
+                    bool has_mask, bool mask_comp, int64_t ncols,
+                    uint8_t *__restrict__ flag_all, typename SR::z_t *__restrict__ val_all)
 {
-    __shared__ int s_warp[8];
-    __shared__ int s_base;
-    for (int64_t rb = blockIdx.x; rb < nrows_bin; rb += gridDim.x) {
+    using Z = typename SR::z_t;
+    constexpr bool idem = SR::M::any || SR::add_op == OP_MIN || SR::add_op == OP_MAX ||
+                          SR::add_op == OP_LOR || SR::add_op == OP_LAND;
+    const int lane = threadIdx.x & 31;
+    const int64_t ne = hoff[nr];
+    const int64_t total = wprefix[ne];
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
+         base < total; base += nw * 32) {
+        int64_t e0 = 0;
+        if (lane == 0) e0 = upper_bound64(wprefix, 0, ne + 1, base) - 1;
+        e0 = __shfl_sync(0xffffffffu, e0, 0);
+        const int64_t t = base + lane;
+        if (t >= total) continue;
+        int64_t e = e0;
+        while (wprefix[e + 1] <= t) e++;
+        const int rb = nr == 1 ? 0 : (int)(upper_bound64(hoff, 0, nr + 1, e) - 1);
         const int32_t i = rows[rb];
-        const int64_t *flag = flag_all + rb * ncols;
-        const typename SR::z_t *val = val_all + rb * ncols;
-        const int64_t off = slot_off[i];
-        int total = 0;
-        for (int64_t c0 = 0; c0 < ncols; c0 += blockDim.x) {
-            const int64_t j = c0 + threadIdx.x;
-            const bool on = (j < ncols) && (flag[j] == 3);
-            const unsigned m = __ballot_sync(0xffffffffu, on);
-            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-            if (lane == 0) s_warp[w] = __popc(m);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                int acc = 0;
-                for (int q = 0; q < (int)(blockDim.x >> 5); q++) {
-                    int c = s_warp[q]; s_warp[q] = acc; acc += c;
-                }
-                s_base = acc;
-            }
-            __syncthreads();
-            if (on) {
-                const int64_t q = off + total + s_warp[w] + __popc(m & ((1u << lane) - 1));
-                Tj[q] = (int32_t)j;
-                Tx[q] = val[j];
-            }
-            total += s_base;
-            __syncthreads();
+        const int32_t pa = Ap[i] + (int32_t)(e - hoff[rb]);
+        const int32_t k = Aj[pa];
+        const int32_t pb = Bp[k] + (int32_t)(t - wprefix[e]);
+        const int32_t j = Bj[pb];
+        uint8_t *flag = flag_all + (int64_t)rb * ncols;
+        Z *val = val_all + (int64_t)rb * ncols;
+        const uint8_t f = flag[j];
+        if (has_mask) {
+            if (!mask_comp && f == 0) continue;
+            if (mask_comp && f == 2) continue;
         }
-        if (threadIdx.x == 0) row_cnt[i] = total;
-        __syncthreads();
+        Z a = Z(), b = Z();
+        if (SR::needs_a) a = ld_val<Z>(Ax, pa, a_iso);
+        if (SR::needs_b) b = ld_val<Z>(Bx, pb, b_iso);
+        const Z tv = SR::F::f(a, b, i, k, j);
+        if constexpr (idem) {
+            if (f == 3) {
+                if (SR::any_const) continue;
+                const Z cur = val[j];
+                if (SR::M::any ? !(tv > cur) : (SR::M::update(cur, tv) == cur)) continue;
+            }
+        }
+        AtomicUpd<SR::add_op, Z>::run(&val[j], tv);
+        if (f != 3) flag[j] = 3;
     }
 }
 
@@ -791,12 +826,12 @@ k_dense_gather(const int32_t *__restrict__ rows, int nrows_bin, int64_t ncols,
 static constexpr int DG_THREADS = 256, DG_ITEMS = 16, DG_CHUNK = DG_THREADS * DG_ITEMS;
 
 __global__ void __launch_bounds__(DG_THREADS)
-k_dense_count(int nrows_bin, int64_t ncols, int cblocks, const int64_t *__restrict__ flag_all,
+k_dense_count(int nrows_bin, int64_t ncols, int cblocks, const uint8_t *__restrict__ flag_all,
               int64_t *__restrict__ cnt)
 {
     __shared__ int s_w[DG_THREADS / 32];
     for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
-        const int64_t *flag = flag_all + rb * ncols;
+        const uint8_t *flag = flag_all + rb * ncols;
         const int64_t c0 = (int64_t)blockIdx.x * DG_CHUNK;
         int c = 0;
         for (int it = 0; it < DG_ITEMS; it++) {
@@ -818,7 +853,7 @@ k_dense_count(int nrows_bin, int64_t ncols, int cblocks, const int64_t *__restri
 template <class SR>
 __global__ void __launch_bounds__(DG_THREADS)
 k_dense_write(const int32_t *__restrict__ rows, int nrows_bin, int64_t ncols, int cblocks,
-              const int64_t *__restrict__ flag_all,
+              const uint8_t *__restrict__ flag_all,
               const typename SR::z_t *__restrict__ val_all,
               const int64_t *__restrict__ off /* scanned counts */,
               const int64_t *__restrict__ slot_off, int32_t *__restrict__ Tj,
@@ -829,7 +864,7 @@ k_dense_write(const int32_t *__restrict__ rows, int nrows_bin, int64_t ncols, in
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
         const int32_t i = rows[rb];
-        const int64_t *flag = flag_all + rb * ncols;
+        const uint8_t *flag = flag_all + rb * ncols;
         const typename SR::z_t *val = val_all + rb * ncols;
         const int64_t row0 = off[rb * cblocks];
         int64_t pos = slot_off[i] + (off[rb * cblocks + blockIdx.x] - row0);
@@ -994,9 +1029,13 @@ struct SaxpyPlan {
     void *Tx = nullptr;
     int *bins = nullptr;
     int64_t heavy_chunk = 0;
-    int64_t *flag = nullptr;
+    int64_t *flag = nullptr;                       // order-dependent rows: row marks
+    uint8_t *flag8 = nullptr;                      // order-free rows: 0/1/2/3 states
     void *val = nullptr;
     int64_t *dg_cnt = nullptr, *dg_ws = nullptr;   // dense-row compaction
+    int64_t heavy_alen = 0;                         // A entries in the heavy rows
+    int64_t *hlen = nullptr, *hoff = nullptr;       // flat product index (per chunk)
+    int64_t *wlen = nullptr, *wprefix = nullptr, *hw_ws = nullptr;
 };
 
 void saxpy_plan_free(SaxpyPlan *P, cudaStream_t s)
@@ -1004,8 +1043,10 @@ void saxpy_plan_free(SaxpyPlan *P, cudaStream_t s)
     if (!P) return;
     dfree(P->flops, s); dfree(P->slot_off, s); dfree(P->Cp64, s); dfree(P->scan_ws, s);
     dfree(P->row_bin, s); dfree(P->bin_rows, s); dfree(P->row_cnt, s); dfree(P->Tj, s);
-    dfree(P->Tx, s); dfree(P->bins, s); dfree(P->flag, s); dfree(P->val, s);
+    dfree(P->Tx, s); dfree(P->bins, s); dfree(P->flag, s); dfree(P->flag8, s); dfree(P->val, s);
     dfree(P->dg_cnt, s); dfree(P->dg_ws, s);
+    dfree(P->hlen, s); dfree(P->hoff, s); dfree(P->wlen, s); dfree(P->wprefix, s);
+    dfree(P->hw_ws, s);
     delete P;
 }
 
@@ -1051,13 +1092,15 @@ static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A
     for (int q = 0; q < P->cfg.nb; q++) lim.limit[q] = P->cfg.bin[q].limit;
     if (m > 0)
         k_bin_rows<<<nblocks(m, 256), 256, 0, s>>>(P->flops, M ? M->p : nullptr,
-            M != nullptr, mask_bounds, ncols, m, lim, P->bins, P->row_bin, P->slot_off);
+            M != nullptr, mask_bounds, ncols, m, lim, P->bins, P->row_bin, P->slot_off,
+            A.p, (unsigned long long *)(P->bins + 48));
     cudaMemsetAsync(P->slot_off + m, 0, 8, s);
     scan_exclusive_i64_ws(P->slot_off, P->slot_off, m + 1, P->scan_ws, s);
     const int nb = P->cfg.nb;
     int64_t total_cap = 0;
     cudaMemcpyAsync(P->h_bins, P->bins, sizeof(int) * (nb + 2), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&total_cap, P->slot_off + m, 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&P->heavy_alen, P->bins + 48, 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_to_info(e);
     P->total_cap = total_cap;
@@ -1075,24 +1118,32 @@ static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A
     if (nheavy > 0) {
         if (SR::order_free) {
             int64_t chunk = nheavy;
-            const int64_t per_row = ncols * (8 + (int64_t)sizeof(Z));
+            const int64_t per_row = ncols * (1 + (int64_t)sizeof(Z));
             const int64_t budget = (int64_t)4 << 30;
             if (chunk * per_row > budget) chunk = budget / per_row > 0 ? budget / per_row : 1;
             P->heavy_chunk = chunk;
-            P->flag = (int64_t *)dalloc((size_t)(chunk * ncols + 1) * 8, s);
+            P->flag8 = (uint8_t *)dalloc((size_t)(chunk * ncols + 1), s);
             P->val = dalloc((size_t)(chunk * ncols + 1) * sizeof(Z), s);
             const int64_t cblocks = (ncols + DG_CHUNK - 1) / DG_CHUNK;
             const int64_t ncnt = chunk * cblocks + 1;
             P->dg_cnt = (int64_t *)dalloc((size_t)(ncnt + 1) * 8, s);
             P->dg_ws = (int64_t *)dalloc(scan_ws_elems(ncnt) * 8, s);
             if (!P->dg_cnt || !P->dg_ws) return OUT_OF_MEMORY;
+            const int64_t hmax = (chunk + 1) > (P->heavy_alen + 1) ? chunk + 1 : P->heavy_alen + 1;
+            P->hlen = (int64_t *)dalloc((size_t)(chunk + 1) * 8, s);
+            P->hoff = (int64_t *)dalloc((size_t)(chunk + 1) * 8, s);
+            P->wlen = (int64_t *)dalloc((size_t)(P->heavy_alen + 1) * 8, s);
+            P->wprefix = (int64_t *)dalloc((size_t)(P->heavy_alen + 1) * 8, s);
+            P->hw_ws = (int64_t *)dalloc(scan_ws_elems(hmax) * 8, s);
+            if (!P->hlen || !P->hoff || !P->wlen || !P->wprefix || !P->hw_ws)
+                return OUT_OF_MEMORY;
         } else {
             const int nbk = nheavy < runtime().num_sms * 2 ? nheavy : runtime().num_sms * 2;
             P->heavy_chunk = nbk;
             P->flag = (int64_t *)dalloc((size_t)((int64_t)nbk * ncols + 1) * 8, s);
             P->val = dalloc((size_t)((int64_t)nbk * ncols + 1) * sizeof(Z), s);
         }
-        if (!P->flag || !P->val) return OUT_OF_MEMORY;
+        if ((!P->flag && !P->flag8) || !P->val) return OUT_OF_MEMORY;
     }
     return cuda_to_info(cudaGetLastError());
 }
@@ -1111,15 +1162,27 @@ static void launch_bin(const SaxpyPlan *P, int q, const DevCSR &A, const DevCSR 
     if (b.tpr == 1) {
         static bool attr = false;
         if (!attr) {
-            allow_dynamic_smem((const void *)k_saxpy_esc<SR>);
+            allow_dynamic_smem((const void *)k_saxpy_esc<SR, uint32_t>);
+            allow_dynamic_smem((const void *)k_saxpy_esc<SR, uint64_t>);
             attr = true;
         }
+        int posb = 0;
+        while ((1 << posb) < b.cap) posb++;
         int blocks = (cnt + ESC_WARPS - 1) / ESC_WARPS;
         if (blocks > cap_blocks) blocks = cap_blocks;
-        k_saxpy_esc<SR><<<blocks, ESC_WARPS * 32, smem, s>>>(rows, cnt, b.cap,
-            A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
-            M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, P->mask_comp,
-            P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
+        // 32-bit keys when every (column << posb) and the padding fit
+        if (((uint64_t)B.ncols << posb) < 0xffffffffull) {
+            const size_t sm32 = (size_t)ESC_WARPS * b.cap * (4 + sizeof(Z));
+            k_saxpy_esc<SR, uint32_t><<<blocks, ESC_WARPS * 32, sm32, s>>>(rows, cnt, b.cap,
+                posb, A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
+                M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, P->mask_comp,
+                P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
+        } else {
+            k_saxpy_esc<SR, uint64_t><<<blocks, ESC_WARPS * 32, smem, s>>>(rows, cnt, b.cap,
+                posb, A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
+                M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, P->mask_comp,
+                P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
+        }
     } else if (b.tpr >= 256) {
         static bool attr = false;
         if (!attr) {
@@ -1162,30 +1225,39 @@ static int exec_t(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &
     if (nheavy > 0) {
         const int32_t *hrows = P->bin_rows + P->h_start[nb + 1];
         int64_t *flag = P->flag;
+        uint8_t *flag8 = P->flag8;
         Z *val = (Z *)P->val;
         if constexpr (SR::order_free) {
             const int64_t chunk = P->heavy_chunk;
             for (int64_t c0 = 0; c0 < nheavy; c0 += chunk) {
                 const int nr = (int)((nheavy - c0 < chunk) ? nheavy - c0 : chunk);
                 dim3 g1(nblocks(ncols, 256, 4), nr > 65535 ? 65535 : nr);
-                k_dense_init<SR><<<g1, 256, 0, s>>>(hrows + c0, nr, ncols, flag, val);
+                k_dense_init<SR><<<g1, 256, 0, s>>>(hrows + c0, nr, ncols, flag8, val);
                 if (M) {
-                    dim3 g2(8, nr > 65535 ? 65535 : nr);
+                    dim3 g2(runtime().num_sms * 2 / (nr < 8 ? nr : 8) + 1, nr > 65535 ? 65535 : nr);
                     k_dense_mask<<<g2, 256, 0, s>>>(hrows + c0, nr, M->p, M->j, P->mask_comp,
-                                                    ncols, flag);
+                                                    ncols, flag8);
                 }
-                dim3 g3((unsigned)runtime().num_sms * 8 / (nr < 8 ? nr : 8) + 1,
-                        nr > 65535 ? 65535 : nr);
-                k_dense_atomic<SR><<<g3, 256, 0, s>>>(hrows + c0, nr, A.p, A.j, A.x, A.iso,
-                    B.p, B.j, B.x, B.iso, M != nullptr, P->mask_comp, ncols, flag, val);
+                // flat product index of the chunk, then every product over the grid
+                k_heavy_alen<<<(nr + 255) / 256, 256, 0, s>>>(hrows + c0, nr, A.p, P->hlen);
+                cudaMemsetAsync(P->hlen + nr, 0, 8, s);
+                scan_exclusive_i64_ws(P->hlen, P->hoff, nr + 1, P->hw_ws, s);
+                // entries past this chunk's count stay 0 (wprefix[ne] is the total)
+                cudaMemsetAsync(P->wlen, 0, (size_t)(P->heavy_alen + 1) * 8, s);
+                k_heavy_blen<<<nblocks(P->heavy_alen, 256, 8), 256, 0, s>>>(hrows + c0, nr,
+                    P->hoff, A.p, A.j, B.p, P->wlen);
+                scan_exclusive_i64_ws(P->wlen, P->wprefix, P->heavy_alen + 1, P->hw_ws, s);
+                k_dense_atomic_flat<SR><<<runtime().num_sms * 16, 256, 0, s>>>(hrows + c0, nr,
+                    P->hoff, P->wprefix, A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
+                    M != nullptr, P->mask_comp, ncols, flag8, val);
                 const int cblocks = (int)((ncols + DG_CHUNK - 1) / DG_CHUNK);
                 dim3 g4(cblocks, nr > 65535 ? 65535 : nr);
-                k_dense_count<<<g4, DG_THREADS, 0, s>>>(nr, ncols, cblocks, flag, P->dg_cnt);
+                k_dense_count<<<g4, DG_THREADS, 0, s>>>(nr, ncols, cblocks, flag8, P->dg_cnt);
                 const int64_t ncnt = (int64_t)nr * cblocks;
                 cudaMemsetAsync(P->dg_cnt + ncnt, 0, 8, s);
                 scan_exclusive_i64_ws(P->dg_cnt, P->dg_cnt, ncnt + 1, P->dg_ws, s);
                 k_dense_write<SR><<<g4, DG_THREADS, 0, s>>>(hrows + c0, nr, ncols, cblocks,
-                    flag, val, P->dg_cnt, P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
+                    flag8, val, P->dg_cnt, P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
             }
         } else {
             const int nbk = (int)P->heavy_chunk;

@@ -224,7 +224,7 @@ int grb_b200_dmxv(grb_b200_dmatrix *w, grb_b200_dmatrix mask, bool mask_comp,
  * Aj/Ax arrays (Ap[0] = 0, offsets continue across instances).  B_k is
  * a_ncols[k]-by-b_ncols[k], laid out the same way in Bp/Bj/Bx.  Ax/Bx NULL:
  * pattern (iso one).  The batch is uploaded once as one block-diagonal
- * matrix; its symbolic phase runs at creation. */
+ * matrix; its symbolic phase runs at the first tune or run. */
 typedef struct grb_b200_batch_s *grb_b200_batch;
 
 int grb_b200_batch_create(grb_b200_batch *B, int count, const int64_t *a_nrows,
@@ -258,6 +258,12 @@ int grb_b200_batch_info(grb_b200_batch B, int64_t *total_rows, int64_t *nnz_c,
  * holds a_nrows[k]+1 offsets per instance into Cj/Cx. */
 int grb_b200_batch_result(grb_b200_batch B, int64_t **Cp, int64_t **Cj,
                           void **Cx, int64_t *nnz_per_instance);
+
+/* The same results written into the caller's arrays (host memory; page-
+ * locked memory is copied by DMA): Cp holds sum(a_nrows[k]+1) offsets, Cj and
+ * Cx nnz_c entries (grb_b200_batch_info after a run). */
+int grb_b200_batch_result_into(grb_b200_batch B, int64_t *Cp, int64_t *Cj, void *Cx,
+                               int64_t *nnz_per_instance);
 
 int grb_b200_batch_free(grb_b200_batch *B);
 

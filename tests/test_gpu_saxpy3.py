@@ -164,3 +164,28 @@ def test_saxpy_edge_cases(gpu, oracle):
     want = oracle.saxpy(20, 25, (A.p, A.i, A.x, 11), (B.p, B.i, B.x, 11), "PLUS",
                         "TIMES", 11)
     assert_exact(got, want, "complement of empty mask")
+
+
+@pytest.mark.parametrize("add,mult,tname,np_t", [("PLUS", "TIMES", "fp64", np.float64),
+                                                 ("MIN", "PLUS", "fp32", np.float32)])
+def test_saxpy_short_rows_wide_columns(gpu, oracle, add, mult, tname, np_t):
+    """Short rows (expand-sort-compress bin) over 2^24 + 5 columns: the sort
+    keys (column, position) no longer fit 32 bits and take the 64-bit form;
+    columns repeat inside a row so the runs are folded in ascending k."""
+    gb = gpu
+    tc = gb.TYPES[tname]
+    rng = np.random.default_rng(17)
+    m, k, n = 64, 300, (1 << 24) + 5
+    A = random_csr(m, k, 0.05, 18, np_t, lo=0.5, hi=2.0)
+    hot = rng.integers(0, n, 40)                 # columns shared by many rows of B
+    bp, bi = [0], []
+    for _ in range(k):
+        c = np.unique(np.concatenate([rng.integers(0, n, 5), rng.choice(hot, 3)]))
+        bi.append(c)
+        bp.append(bp[-1] + len(c))
+    bi = np.concatenate(bi).astype(np.int64)
+    B = W.Csr(k, n, np.array(bp, np.int64), bi,
+              (0.5 + 1.5 * rng.random(len(bi))).astype(np_t))
+    got = _saxpy_dev(gb, A, B, gb.semiring(add, mult, tname))
+    want = oracle.saxpy(m, n, (A.p, A.i, A.x, tc), (B.p, B.i, B.x, tc), add, mult, tc)
+    assert_exact(got, want, "wide columns %s_%s" % (add, mult))
