@@ -252,21 +252,38 @@ __global__ void k_narrow_check(const int64_t *__restrict__ in, int32_t *__restri
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, bit);
 }
 
-// flag |= bit when some row's indices are not strictly increasing (one warp
-// per row, coalesced)
-__global__ void k_check_rows(const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
-                             int64_t nrows, int64_t nnz, unsigned *__restrict__ flag,
-                             unsigned bit)
+// bit p[r] of `starts` marks the first entry of every non-empty row r
+__global__ void k_row_starts(const int32_t *__restrict__ Ap, int64_t nrows,
+                             unsigned *__restrict__ starts)
 {
-    const int lane = threadIdx.x & 31;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    bool bad = false;
-    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nrows; r += nw) {
-        const int32_t p0 = Ap[r], p1 = Ap[r + 1];
-        for (int32_t q = p0 + 1 + lane; q < p1; q += 32) bad |= Aj[q - 1] >= Aj[q];
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t q = Ap[r];
+        if (q < Ap[r + 1]) atomicOr(&starts[q >> 5], 1u << (q & 31));
     }
-    (void)nnz;
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(flag, bit);
+}
+
+// flag |= bit when an entry that does not start a row is not above the one
+// before it (rows not strictly increasing), flat and coalesced over entries
+__global__ void k_check_rows(const int32_t *__restrict__ Aj, int64_t nnz,
+                             const unsigned *__restrict__ starts,
+                             unsigned *__restrict__ flag, unsigned bit)
+{
+    bool bad = false;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; q < nnz;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        if (!((starts[q >> 5] >> (q & 31)) & 1u)) bad |= Aj[q - 1] >= Aj[q];
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, bit);
+}
+
+// are the rows of A strictly increasing?  (flag bit set when not)
+static void check_rows(const DevCSR &A, unsigned *starts, unsigned *flag, unsigned bit,
+                       cudaStream_t s)
+{
+    cudaMemsetAsync(starts, 0, (size_t)((A.nnz + 31) / 32) * 4, s);
+    k_row_starts<<<grid_for(A.nrows, 256), 256, 0, s>>>(A.p, A.nrows, starts);
+    k_check_rows<<<grid_for(A.nnz, 256), 256, 0, s>>>(A.j, A.nnz, starts, flag, bit);
 }
 
 int dev_import(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
@@ -282,6 +299,7 @@ int dev_import(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
     Scratch ws(s);
     int64_t *stage = ws.get<int64_t>((nrows + 1 > nnz) ? nrows + 1 : nnz);
     unsigned *flag = ws.get<unsigned>(1);
+    unsigned *starts = ws.get<unsigned>((nnz + 31) / 32 + 1);
     A.p = (int32_t *)dalloc((size_t)(nrows + 1) * 4, s);
     A.j = (int32_t *)dalloc((size_t)(nnz ? nnz : 1) * 4, s);
     A.x = dalloc((size_t)(nnz ? nnz : 1) * ts, s);
@@ -302,7 +320,7 @@ int dev_import(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
     if (e != cudaSuccess) { dev_free(A, s); return cuda_to_info(e); }
     if (hflag) { dev_free(A, s); return INVALID_OBJECT; }
     if (nnz == 0) return SUCCESS;
-    k_check_rows<<<grid_for(nrows * 32, 256), 256, 0, s>>>(A.p, A.j, nrows, nnz, flag, 4u);
+    check_rows(A, starts, flag, 4u, s);
     cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, s);
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) { dev_free(A, s); return cuda_to_info(e); }
@@ -317,7 +335,7 @@ int dev_import(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
     A = B;
     // a sorted row with two equal indices holds a duplicate: not a matrix
     cudaMemsetAsync(flag, 0, 4, s);
-    k_check_rows<<<grid_for(nrows * 32, 256), 256, 0, s>>>(A.p, A.j, nrows, nnz, flag, 4u);
+    check_rows(A, starts, flag, 4u, s);
     cudaMemcpyAsync(&hflag, flag, 4, cudaMemcpyDeviceToHost, s);
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess || hflag) {

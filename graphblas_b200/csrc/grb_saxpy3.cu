@@ -57,34 +57,42 @@ static constexpr uint8_t S_EMPTY = 0, S_ALLOWED = 1, S_SET = 2, S_FORBID = 3;
 // segment.  flops[] must be zero on entry.
 __global__ void __launch_bounds__(256)
 k_flops_flat(const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
-             const int32_t *__restrict__ Bp, int64_t nrows, int64_t nnz,
+             const int32_t *__restrict__ Bp, int64_t nrows, int64_t nnz, int span,
              unsigned long long *__restrict__ flops)
 {
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
-         base < nnz; base += nw * 32) {
-        // row of the warp's first entry, then each lane walks to its own
+    // each warp owns spans of `span` consecutive entries (a multiple of 32):
+    // one binary search per span, then the row carries over from one 32-entry
+    // step to the next
+    for (int64_t s0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * span;
+         s0 < nnz; s0 += nw * span) {
         int32_t r0 = 0;
-        if (lane == 0) r0 = upper_bound(Ap, 0, (int32_t)nrows + 1, (int32_t)base) - 1;
+        if (lane == 0) r0 = upper_bound(Ap, 0, (int32_t)nrows + 1, (int32_t)s0) - 1;
         r0 = __shfl_sync(0xffffffffu, r0, 0);
-        const int64_t e = base + lane;
-        int32_t r = -1;
-        unsigned long long f = 0;
-        if (e < nnz) {
-            r = r0;
-            while (Ap[r + 1] <= e) r++;
-            const int32_t k = Aj[e];
-            f = (unsigned long long)(Bp[k + 1] - Bp[k]);
+        const int64_t s1 = s0 + span < nnz ? s0 + span : nnz;
+        for (int64_t base = s0; base < s1; base += 32) {
+            const int64_t e = base + lane;
+            int32_t r = -1;
+            unsigned long long f = 0;
+            if (e < s1) {
+                r = r0;
+                while (Ap[r + 1] <= e) r++;
+                const int32_t k = Aj[e];
+                f = (unsigned long long)(Bp[k + 1] - Bp[k]);
+            }
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(0xffffffffu, f, o);
+                const int32_t ry = __shfl_up_sync(0xffffffffu, r, o);
+                if (lane >= o && ry == r) f += y;
+            }
+            const int32_t rn = __shfl_down_sync(0xffffffffu, r, 1);
+            if (r >= 0 && (lane == 31 || rn != r)) atomicAdd(&flops[r], f);
+            // the next step starts in the row of this step's last entry
+            const int32_t rl = __shfl_sync(0xffffffffu, r, 31);
+            r0 = rl >= 0 ? rl : r0;
         }
-        #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long y = __shfl_up_sync(0xffffffffu, f, o);
-            const int32_t ry = __shfl_up_sync(0xffffffffu, r, o);
-            if (lane >= o && ry == r) f += y;
-        }
-        const int32_t rn = __shfl_down_sync(0xffffffffu, r, 1);
-        if (r >= 0 && (lane == 31 || rn != r)) atomicAdd(&flops[r], f);
     }
 }
 
@@ -429,6 +437,22 @@ k_saxpy_esc(const int32_t *__restrict__ rows, int nrows_bin, int cap, int posb,
         __syncwarp();
         int n2 = 1;
         while (n2 < n) n2 <<= 1;
+        if (n <= 32) {
+            // one key per lane: bitonic network over the lanes in registers
+            KT kk = lane < n ? key[lane] : ~(KT)0;
+            #pragma unroll
+            for (int size = 2; size <= 32; size <<= 1) {
+                #pragma unroll
+                for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                    const KT other = __shfl_xor_sync(0xffffffffu, kk, stride);
+                    const bool up = (lane & size) == 0;
+                    const bool lower = (lane & stride) == 0;
+                    kk = (lower == up) ? (kk < other ? kk : other) : (kk < other ? other : kk);
+                }
+            }
+            if (lane < n) key[lane] = kk;
+            n2 = 0;                                  // the shared-memory network is skipped
+        }
         for (int q = n + lane; q < n2; q += 32) key[q] = ~(KT)0;
         __syncwarp();
         // bitonic sort of the keys; a lane owns every 32nd compare-exchange
@@ -906,32 +930,36 @@ k_dense_write(const int32_t *__restrict__ rows, int nrows_bin, int64_t ncols, in
 // whole grid.
 template <typename Z>
 __global__ void __launch_bounds__(256)
-k_pack(int64_t nrows, const int64_t *__restrict__ slot_off,
+k_pack(int64_t nrows, int span, const int64_t *__restrict__ slot_off,
        const int32_t *__restrict__ Tj, const Z *__restrict__ Tx,
        const int64_t *__restrict__ Cp64, int32_t *__restrict__ Cj, Z *__restrict__ Cx)
 {
     const int lane = threadIdx.x & 31;
     const int64_t nnz = Cp64[nrows];
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
-         base < nnz; base += nw * 32) {
+    for (int64_t s0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * span;
+         s0 < nnz; s0 += nw * span) {
         int64_t r0 = 0;
         if (lane == 0) {
-            int64_t lo = 0, hi = nrows + 1;          // first r with Cp64[r] > base
+            int64_t lo = 0, hi = nrows + 1;          // first r with Cp64[r] > s0
             while (lo < hi) {
                 const int64_t mid = (lo + hi) >> 1;
-                if (Cp64[mid] <= base) lo = mid + 1; else hi = mid;
+                if (Cp64[mid] <= s0) lo = mid + 1; else hi = mid;
             }
             r0 = lo - 1;
         }
         r0 = __shfl_sync(0xffffffffu, r0, 0);
-        const int64_t e = base + lane;
-        if (e < nnz) {
+        const int64_t s1 = s0 + span < nnz ? s0 + span : nnz;
+        for (int64_t base = s0; base < s1; base += 32) {
+            const int64_t e = base + lane;
             int64_t r = r0;
-            while (Cp64[r + 1] <= e) r++;
-            const int64_t src = slot_off[r] + (e - Cp64[r]);
-            Cj[e] = Tj[src];
-            Cx[e] = Tx[src];
+            if (e < s1) {
+                while (Cp64[r + 1] <= e) r++;
+                const int64_t src = slot_off[r] + (e - Cp64[r]);
+                Cj[e] = Tj[src];
+                Cx[e] = Tx[src];
+            }
+            r0 = __shfl_sync(0xffffffffu, r, 31);
         }
     }
 }
@@ -1052,6 +1080,16 @@ void saxpy_plan_free(SaxpyPlan *P, cudaStream_t s)
 
 int64_t saxpy_plan_capacity(const SaxpyPlan *P) { return P->total_cap; }
 
+// entries per warp work unit of the flat kernels: one 32-entry step for
+// small inputs (many warps, no walking), up to 1024 for large ones (one
+// binary search per span instead of per step)
+static inline int flat_span(int64_t n)
+{
+    const int64_t target = (int64_t)runtime().num_sms * 64;     // warps to fill
+    int64_t sp = (n / target + 31) / 32 * 32;
+    return (int)(sp < 32 ? 32 : sp > 1024 ? 1024 : sp);
+}
+
 static inline int nblocks(int64_t n, int threads, int per_sm = 8)
 {
     int64_t b = (n + threads - 1) / threads;
@@ -1085,6 +1123,7 @@ static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A
     cudaMemsetAsync(P->flops, 0, (size_t)(m + 1) * 8, s);
     if (m > 0 && A.nnz > 0)
         k_flops_flat<<<nblocks(A.nnz, 256, 16), 256, 0, s>>>(A.p, A.j, B.p, m, A.nnz,
+            flat_span(A.nnz),
             (unsigned long long *)P->flops);
     cudaMemsetAsync(P->bins, 0, 64 * sizeof(int), s);
     BinLimits lim;
@@ -1276,7 +1315,8 @@ static int exec_t(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &
     k_i64_to_i32_p<<<nblocks(m + 1, 256), 256, 0, s>>>(P->Cp64, Cp, m + 1, nullptr);
     if (Cnnz64) k_copy_i64<<<1, 32, 0, s>>>(P->Cp64 + m, Cnnz64);
     if (m > 0 && P->total_cap > 0)
-        k_pack<Z><<<nblocks(P->total_cap, 256, 16), 256, 0, s>>>(m, P->slot_off, P->Tj,
+        k_pack<Z><<<nblocks(P->total_cap, 256, 16), 256, 0, s>>>(m, flat_span(P->total_cap),
+            P->slot_off, P->Tj,
             (Z *)P->Tx, P->Cp64, Cj, (Z *)Cx);
     return cuda_to_info(cudaGetLastError());
 }
