@@ -349,7 +349,11 @@ k_dot3_intersect(const D3Work *__restrict__ queue, const int32_t *__restrict__ s
 // ---------------------------------------------------------------------------
 
 static constexpr int D3_GMIN = 16;             // smallest group worth a bitmap
-static constexpr int64_t D3_WCHUNK = 1 << 20;  // probes per work item
+static constexpr int64_t D3_WCHUNK = 1 << 20;  // probes per bitmap work item
+static constexpr int D3_HKEY = 256;             // key rows up to this long: warp hash
+static constexpr int D3_HSLOTS = 512;           // slots of a warp's hash table
+static constexpr int64_t D3_HCHUNK = 1 << 16;   // probes per warp-hash work item
+static constexpr int D3_HWARPS = 8;             // warps (tables) per hash block
 static constexpr int D3_BM_THREADS = 1024;
 static constexpr int D3_LONG = 2048;          // longer lists go to the shared table
 static constexpr int D3_SEG = 512;            // probes per shared long-list segment
@@ -435,23 +439,34 @@ k_d3_route(const D3Work *__restrict__ queue, const int *__restrict__ qlen_p,
     }
 }
 
-// work items per group: about one per D3_WCHUNK probes, at most one per 32
-// entries (so the items never outnumber nkeys + entries / 32)
+// work items per group.  A group whose key row has at most D3_HKEY entries
+// goes to the warp-hash kernel (items of about D3_HCHUNK probes), a longer
+// key row to the block-bitmap kernel (items of about D3_WCHUNK probes); at
+// most one item per 32 entries, so items never outnumber nkeys + entries/32.
 __global__ void k_d3_item_count(const int64_t *__restrict__ gsz,
                                 const unsigned long long *__restrict__ gwork,
-                                int64_t nkeys, int64_t *__restrict__ nit)
+                                int64_t nkeys, int32_t nrows,
+                                const int32_t *__restrict__ Ap,
+                                const int32_t *__restrict__ Bp,
+                                int64_t *__restrict__ nit_big, int64_t *__restrict__ nit_small)
 {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; t < nkeys; t += stride) {
         const int64_t g = gsz[t];
-        int64_t n = 0;
+        int64_t nb = 0, ns = 0;
         if (g > 0) {
-            n = 1 + (int64_t)(gwork[t] / D3_WCHUNK);
+            const bool by_row = t < nrows;
+            const int32_t r = by_row ? (int32_t)t : (int32_t)(t - nrows);
+            const int32_t klen = by_row ? Ap[r + 1] - Ap[r] : Bp[r + 1] - Bp[r];
+            const bool small = klen <= D3_HKEY;
+            int64_t n = 1 + (int64_t)(gwork[t] / (small ? D3_HCHUNK : D3_WCHUNK));
             const int64_t mx = g / 32 > 1 ? g / 32 : 1;
             if (n > mx) n = mx;
+            if (small) ns = n; else nb = n;
         }
-        nit[t] = n;
+        nit_big[t] = nb;
+        nit_small[t] = ns;
     }
 }
 
@@ -652,6 +667,89 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
     if (lane == 0 && zc) atomicAdd(nzombies, zc);
 }
 
+// One warp per work item whose key row is short (at most D3_HKEY entries):
+// the key row's columns go into the warp's own shared-memory hash table
+// (D3_HSLOTS slots, open addressing, at most half full), then the warp's
+// lanes, in groups of 2^lg per entry, probe the item's entries' other lists
+// against it.  No block-wide barrier: the many small groups of a skewed
+// graph run side by side, 8 tables (16 KB) per block.
+__device__ __forceinline__ uint32_t d3_hash(int32_t k)
+{
+    return ((uint32_t)k * 0x9E3779B1u) >> (32 - 9);       // 2^9 = D3_HSLOTS
+}
+
+template <class SR>
+__global__ void __launch_bounds__(D3_HWARPS * 32)
+k_dot3_hash_count(const D3Item *__restrict__ items, const int64_t *__restrict__ nitems_p,
+                  int *__restrict__ inext, const D3Rec *__restrict__ bucket,
+                  int32_t nrows, const int32_t *__restrict__ Aj,
+                  const int32_t *__restrict__ Bj, int32_t *__restrict__ Cj,
+                  typename SR::z_t *__restrict__ Cx,
+                  unsigned long long *__restrict__ nzombies)
+{
+    using Z = typename SR::z_t;
+    __shared__ int32_t tab_all[D3_HWARPS][D3_HSLOTS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int32_t *tab = tab_all[w];
+    for (int q = lane; q < D3_HSLOTS; q += 32) tab[q] = -1;
+    __syncwarp();
+    const int64_t nitems = *nitems_p;
+    unsigned long long zc = 0;
+    auto has = [&](int32_t k) -> int {
+        uint32_t h = d3_hash(k);
+        while (true) {
+            const int32_t v = tab[h];
+            if (v == k) return 1;
+            if (v < 0) return 0;
+            h = (h + 1) & (D3_HSLOTS - 1);
+        }
+    };
+    while (true) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(inext, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= nitems) break;
+        const D3Item I = items[it];
+        const bool by_row = I.key < nrows;
+        const int32_t *J = by_row ? Aj : Bj;
+        const int32_t *S = by_row ? Bj : Aj;
+        for (int32_t q = I.rp0 + lane; q < I.rp1; q += 32) {
+            const int32_t k = J[q];
+            uint32_t h = d3_hash(k);
+            while (atomicCAS(&tab[h], -1, k) != -1) h = (h + 1) & (D3_HSLOTS - 1);
+        }
+        __syncwarp();
+        const int lg = I.lg, G = 1 << lg, gi = lane >> lg, gl = lane & (G - 1);
+        const int groups = 32 >> lg;
+        for (int32_t c0 = 0; c0 < I.m_item; c0 += groups) {
+            const int32_t rr = c0 + gi;
+            int32_t s0 = 0, len = 0, pm = 0, j = 0;
+            if (rr < I.m_item) {
+                const D3Rec e = bucket[I.g0 + I.t + (int64_t)I.nit * rr];
+                s0 = e.s0; len = e.len; pm = e.pm; j = e.j;
+            }
+            int cnt = 0;
+            int32_t t = gl;
+            for (; t + 3 * G < len; t += 4 * G) {
+                const int32_t x0 = S[s0 + t], x1 = S[s0 + t + G];
+                const int32_t x2 = S[s0 + t + 2 * G], x3 = S[s0 + t + 3 * G];
+                cnt += has(x0) + has(x1) + has(x2) + has(x3);
+            }
+            for (; t < len; t += G) cnt += has(S[s0 + t]);
+            for (int o = G >> 1; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o, G);
+            if (rr < I.m_item && gl == 0) {
+                if (cnt) { Cj[pm] = j; Cx[pm] = (Z)cnt; }
+                else { Cj[pm] = flip(j); zc++; }
+            }
+        }
+        __syncwarp();
+        for (int q = lane; q < D3_HSLOTS; q += 32) tab[q] = -1;
+        __syncwarp();
+    }
+    for (int o = 16; o > 0; o >>= 1) zc += __shfl_down_sync(0xffffffffu, zc, o);
+    if (lane == 0 && zc) atomicAdd(nzombies, zc);
+}
+
 static constexpr int64_t D3_BM_MIN_ENTRIES = 1 << 16;   // mask entries
 
 // Words of the shared-memory bitmap: enough for every column index (plus one
@@ -710,6 +808,8 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
     int32_t *gcnt = nullptr, *gfill = nullptr, *merge_sel = nullptr;
     D3Rec *bucket = nullptr;
     int64_t *gsz = nullptr, *goff = nullptr, *nit = nullptr, *ioff = nullptr, *ws = nullptr;
+    int64_t *nit_s = nullptr, *ioff_s = nullptr;
+    D3Item *items_s = nullptr;
     unsigned long long *gwork = nullptr;
     D3Item *items = nullptr;
     if (bm_words) {
@@ -719,6 +819,9 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
         goff = bm_scratch.get<int64_t>(nkeys + 1);
         nit = bm_scratch.get<int64_t>(nkeys + 1);
         ioff = bm_scratch.get<int64_t>(nkeys + 1);
+        nit_s = bm_scratch.get<int64_t>(nkeys + 1);
+        ioff_s = bm_scratch.get<int64_t>(nkeys + 1);
+        items_s = bm_scratch.get<D3Item>(nkeys + mnz / 32 + 1);
         gwork = bm_scratch.get<unsigned long long>(nkeys);
         items = bm_scratch.get<D3Item>(nkeys + mnz / 32 + 1);
         bucket = bm_scratch.get<D3Rec>(mnz);
@@ -740,6 +843,7 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
             cudaMemsetAsync(gwork, 0, (size_t)nkeys * 8, s);
             cudaMemsetAsync(gsz + nkeys, 0, 8, s);
             cudaMemsetAsync(nit + nkeys, 0, 8, s);
+            cudaMemsetAsync(nit_s + nkeys, 0, 8, s);
         }
         k_dot3_classify<SR><<<(unsigned)blocks, 256, 0, s>>>(
             M.p, M.j, mask_struct ? nullptr : M.x, M.type, mask_struct, mnz, M.nrows,
@@ -752,10 +856,18 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
             k_d3_route<<<(unsigned)blocks, 256, 0, s>>>(queue, qlen, gsz, goff, gfill, gwork,
                                                        bucket, (int32_t)M.nrows, merge_sel,
                                                        merge_len);
-            k_d3_item_count<<<kb, 256, 0, s>>>(gsz, gwork, nkeys, nit);
+            k_d3_item_count<<<kb, 256, 0, s>>>(gsz, gwork, nkeys, (int32_t)M.nrows, A.p, B.p,
+                                               nit, nit_s);
             scan_exclusive_i64_ws(nit, ioff, nkeys + 1, ws, s);
             k_d3_item_fill<<<kb, 256, 0, s>>>(ioff, nkeys, goff, gwork, (int32_t)M.nrows,
                                               A.p, A.j, B.p, B.j, items);
+            scan_exclusive_i64_ws(nit_s, ioff_s, nkeys + 1, ws, s);
+            k_d3_item_fill<<<kb, 256, 0, s>>>(ioff_s, nkeys, goff, gwork, (int32_t)M.nrows,
+                                              A.p, A.j, B.p, B.j, items_s);
+            if constexpr (IsCount<SR>::value)
+                k_dot3_hash_count<SR><<<nsm * 8, D3_HWARPS * 32, 0, s>>>(
+                    items_s, ioff_s + nkeys, inext + 1, bucket, (int32_t)M.nrows, A.j, B.j,
+                    C.j, (Z *)C.x, zc);
             if constexpr (IsCount<SR>::value)
                 k_dot3_bitmap_count<SR><<<nsm, D3_BM_THREADS, (size_t)bm_words * 4, s>>>(
                     items, ioff + nkeys, inext, bucket, (int32_t)M.nrows, A.j, B.j,
