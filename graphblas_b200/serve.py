@@ -10,6 +10,7 @@ row.  ``BenchServe`` is bench.py --config serve.
 
 import ctypes
 import math
+import os
 
 import numpy as np
 
@@ -222,11 +223,41 @@ class BenchServe:
     def launches_per_step(self):
         return 8 * self.nreq
 
+    # the reference replays a bounded sample of the trace: its first requests,
+    # with the same arrival times, through 8 host workers
+    REF_SAMPLE = 400
+
+    def _ref_trace(self):
+        k = self.REF_SAMPLE
+        t = self.trace
+        return {"t": t["t"][:k], "kind": t["kind"][:k], "graph": t["graph"][:k],
+                "fp": t["fp"][:k + 1], "fi": t["fi"], "fx": t["fx"]}
+
+    def _ref_run(self, R, ncores):
+        tr = self._ref_trace()
+        per = max(1, ncores // 8)
+        status, count, cs, lat, mk = R.serve(self.graphs, tr, 8, per)
+        done = int((status == 0).sum())
+        desc = ("first %d requests of the trace (same arrivals), 8 host workers x %d "
+                "threads, p50 %.2f ms, p99 %.2f ms" %
+                (self.REF_SAMPLE, per, 1e3 * np.percentile(lat, 50),
+                 1e3 * np.percentile(lat, 99)))
+        return done, mk, desc
+
     def cpu_baseline(self, R, ncores):
-        return None, "not measured for the request stream"
+        done, mk, desc = self._ref_run(R, ncores)
+        return done / mk, desc
 
     def reference_steps(self, R, steps, warmup):
-        raise NotImplementedError
+        ncores = os.cpu_count() or 1
+        for _ in range(warmup):
+            self._ref_run(R, ncores)
+        units, secs, desc = 0, 0.0, ""
+        for _ in range(steps):
+            done, mk, desc = self._ref_run(R, ncores)
+            units += done
+            secs += mk
+        return units, secs, desc
 
     def free(self):
         self.S.free()

@@ -173,6 +173,10 @@ class Reference:
         L.ref_tricount.argtypes = [ctypes.c_int64, vp, vp, vp, vp, ctypes.c_int,
                                    vp, vp]
         L.ref_bfs.argtypes = [ctypes.c_int64, vp, vp, ctypes.c_int64, vp, vp, vp]
+        L.ref_serve_add_graph.argtypes = [ctypes.c_int, ctypes.c_int64, vp, vp, vp]
+        L.ref_serve_clear.restype = None
+        L.ref_serve_replay.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64] + [vp] * 10 \
+            + [vp]
         L.ref_batch_square.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp,
                                        ctypes.c_int, ctypes.c_int, vp, vp]
         self.nthreads = nthreads or os.cpu_count()
@@ -253,6 +257,43 @@ class Reference:
         if info != 0:
             raise RuntimeError("reference batch failed: %d" % info)
         return nnz_out, float(secs[0])
+
+
+    def serve(self, graphs, trace, nworkers, nthreads_per_call):
+        """Replay a request trace (graphblas_b200.serve.make_trace) through a
+        pool of host threads running the reference library; graphs are the
+        (kind, Csr) list of graphblas_b200.serve.make_graphs.  Returns
+        (status, count, checksum, latency, makespan)."""
+        L = self.lib
+        L.ref_serve_clear()
+        keep = []
+        for kind, g in graphs:
+            x = None
+            if kind == 2:
+                x = np.ascontiguousarray(g.x, np.float32)
+            elif kind == 3:
+                x = np.ascontiguousarray(g.x, np.float64)
+            p, i = _i64(g.p), _i64(g.i)
+            keep += [p, i, x]
+            info = L.ref_serve_add_graph(kind, g.nrows, _ptr(p), _ptr(i), _ptr(x))
+            if info != 0:
+                raise RuntimeError("reference serve graph failed: %d" % info)
+        kind = np.ascontiguousarray(trace["kind"], np.int32)
+        graph = np.ascontiguousarray(trace["graph"], np.int32)
+        t = np.ascontiguousarray(trace["t"], np.float64)
+        fp, fi = _i64(trace["fp"]), _i64(trace["fi"])
+        fx = np.ascontiguousarray(trace["fx"], np.float32)
+        n = len(kind)
+        status = np.zeros(n, np.int32)
+        count = np.zeros(n, np.int64)
+        checksum = np.zeros(n, np.float64)
+        latency = np.zeros(n, np.float64)
+        makespan = np.zeros(1, np.float64)
+        L.ref_serve_replay(nworkers, nthreads_per_call, n, _ptr(kind), _ptr(graph),
+                           _ptr(t), _ptr(fp), _ptr(fi), _ptr(fx), _ptr(status),
+                           _ptr(count), _ptr(checksum), _ptr(latency), _ptr(makespan))
+        L.ref_serve_clear()
+        return status, count, checksum, latency, float(makespan[0])
 
 
 def reference_available():

@@ -404,3 +404,216 @@ done:
     return (int)info;
     #undef TRY
 }
+
+//------------------------------------------------------------------------------
+// The serving workload on the reference: the same open-loop request trace
+// replayed through a pool of host threads over graphs held in CPU memory.
+// Request kinds: 1 triangle count (C<L> = L*U' plus_pair int64, then sum),
+// 2 SSSP relaxation step (w = u min.+ S, fp32, u a sparse frontier),
+// 3 product C = S*S (plus_times fp64).  Each worker runs one request at a
+// time with GxB_NTHREADS = nthreads_per_call; latency = completion - arrival.
+//------------------------------------------------------------------------------
+
+#include <pthread.h>
+#include <time.h>
+
+#define REF_SERVE_MAX_GRAPHS 64
+
+static struct
+{
+    int ngraphs;
+    int kind[REF_SERVE_MAX_GRAPHS];
+    int64_t n[REF_SERVE_MAX_GRAPHS];
+    GrB_Matrix S[REF_SERVE_MAX_GRAPHS], L[REF_SERVE_MAX_GRAPHS], U[REF_SERVE_MAX_GRAPHS];
+} g_serve;
+
+static double now_s(const struct timespec *t0)
+{
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return (double)(t.tv_sec - t0->tv_sec) + 1e-9 * (double)(t.tv_nsec - t0->tv_nsec);
+}
+
+// Add a resident graph: kind 1 takes a symmetric pattern (split into strict
+// lower / upper triangles here), kind 2 fp32 weights, kind 3 fp64 values.
+int ref_serve_add_graph(int kind, int64_t n, const int64_t *p, const int64_t *i,
+                        const void *x)
+{
+    if (g_serve.ngraphs >= REF_SERVE_MAX_GRAPHS) return (int)GrB_INVALID_VALUE;
+    const int g = g_serve.ngraphs;
+    GrB_Info info = GrB_SUCCESS;
+    g_serve.S[g] = g_serve.L[g] = g_serve.U[g] = NULL;
+    if (kind == 1)
+    {
+        int64_t *Lp = malloc((n + 1) * sizeof(int64_t)), *Up = malloc((n + 1) * sizeof(int64_t));
+        int64_t *Li = malloc((p[n] / 2 + 1) * sizeof(int64_t));
+        int64_t *Ui = malloc((p[n] / 2 + 1) * sizeof(int64_t));
+        int64_t nl = 0, nu = 0;
+        for (int64_t r = 0; r < n; r++)
+        {
+            Lp[r] = nl; Up[r] = nu;
+            for (int64_t q = p[r]; q < p[r + 1]; q++)
+            {
+                if (i[q] < r) Li[nl++] = i[q];
+                else if (i[q] > r) Ui[nu++] = i[q];
+            }
+        }
+        Lp[n] = nl; Up[n] = nu;
+        info = make_csr(&g_serve.L[g], T_BOOL, n, n, Lp, Li, NULL);
+        if (info == GrB_SUCCESS) info = make_csr(&g_serve.U[g], T_BOOL, n, n, Up, Ui, NULL);
+        free(Lp); free(Up); free(Li); free(Ui);
+    }
+    else
+    {
+        info = make_csr(&g_serve.S[g], kind == 2 ? T_FP32 : T_FP64, n, n, p, i, x);
+    }
+    if (info != GrB_SUCCESS) return (int)info;
+    g_serve.kind[g] = kind;
+    g_serve.n[g] = n;
+    g_serve.ngraphs++;
+    return (int)GrB_SUCCESS;
+}
+
+void ref_serve_clear(void)
+{
+    for (int g = 0; g < g_serve.ngraphs; g++)
+    {
+        GrB_Matrix_free(&g_serve.S[g]);
+        GrB_Matrix_free(&g_serve.L[g]);
+        GrB_Matrix_free(&g_serve.U[g]);
+    }
+    g_serve.ngraphs = 0;
+}
+
+typedef struct
+{
+    int64_t nreq;
+    const int *kind, *graph;
+    const double *t_arrival;
+    const int64_t *fp, *fi;
+    const float *fx;
+    struct timespec t0;
+    pthread_mutex_t mu;
+    pthread_cond_t cv;
+    int64_t submitted, next;
+    // outputs
+    int *status;
+    int64_t *count;
+    double *checksum, *latency;
+} serve_run;
+
+static int serve_one(serve_run *R, int64_t k)
+{
+    const int g = R->graph[k];
+    const int64_t n = g_serve.n[g];
+    GrB_Info info = GrB_SUCCESS;
+    #define TRY(x) { info = (x); if (info != GrB_SUCCESS) goto done; }
+    GrB_Matrix C = NULL;
+    GrB_Vector u = NULL, w = NULL;
+    GrB_Index *ui = NULL;
+    if (R->kind[k] == 1)
+    {
+        int64_t s = 0;
+        TRY(GrB_Matrix_new(&C, GrB_INT64, n, n));
+        TRY(GrB_mxm(C, g_serve.L[g], NULL, GxB_PLUS_PAIR_INT64, g_serve.L[g], g_serve.U[g],
+                    GrB_DESC_ST1));
+        TRY(GrB_Matrix_reduce_INT64(&s, NULL, GrB_PLUS_MONOID_INT64, C, NULL));
+        R->count[k] = s;
+        R->checksum[k] = (double)s;
+    }
+    else if (R->kind[k] == 2)
+    {
+        const int64_t lo = R->fp[k], nu = R->fp[k + 1] - lo;
+        ui = malloc((nu ? nu : 1) * sizeof(GrB_Index));
+        for (int64_t t = 0; t < nu; t++) ui[t] = (GrB_Index)R->fi[lo + t];
+        TRY(GrB_Vector_new(&u, GrB_FP32, n));
+        TRY(GrB_Vector_build_FP32(u, ui, R->fx + lo, nu, GrB_FIRST_FP32));
+        TRY(GrB_Vector_new(&w, GrB_FP32, n));
+        TRY(GrB_vxm(w, NULL, NULL, GrB_MIN_PLUS_SEMIRING_FP32, u, g_serve.S[g], NULL));
+        GrB_Index nv = 0;
+        float sum = 0;
+        TRY(GrB_Vector_nvals(&nv, w));
+        TRY(GrB_Vector_reduce_FP32(&sum, NULL, GrB_PLUS_MONOID_FP32, w, NULL));
+        R->count[k] = (int64_t)nv;
+        R->checksum[k] = sum;
+    }
+    else
+    {
+        TRY(GrB_Matrix_new(&C, GrB_FP64, n, n));
+        TRY(GrB_mxm(C, NULL, NULL, GrB_PLUS_TIMES_SEMIRING_FP64, g_serve.S[g], g_serve.S[g],
+                    NULL));
+        GrB_Index nv = 0;
+        double sum = 0;
+        TRY(GrB_Matrix_nvals(&nv, C));
+        TRY(GrB_Matrix_reduce_FP64(&sum, NULL, GrB_PLUS_MONOID_FP64, C, NULL));
+        R->count[k] = (int64_t)nv;
+        R->checksum[k] = sum;
+    }
+done:
+    GrB_Matrix_free(&C);
+    GrB_Vector_free(&u);
+    GrB_Vector_free(&w);
+    free(ui);
+    return (int)info;
+    #undef TRY
+}
+
+static void *serve_worker(void *arg)
+{
+    serve_run *R = (serve_run *)arg;
+    while (true)
+    {
+        pthread_mutex_lock(&R->mu);
+        while (R->next >= R->submitted && R->submitted < R->nreq)
+            pthread_cond_wait(&R->cv, &R->mu);
+        if (R->next >= R->nreq) { pthread_mutex_unlock(&R->mu); break; }
+        const int64_t k = R->next++;
+        pthread_mutex_unlock(&R->mu);
+        R->status[k] = serve_one(R, k);
+        R->latency[k] = now_s(&R->t0) - R->t_arrival[k];
+    }
+    return NULL;
+}
+
+// Replay: request k arrives t_arrival[k] seconds after the call and is taken
+// by the first free worker (FIFO).  Returns GrB_Info; *makespan gets the time
+// to the last completion.
+int ref_serve_replay(int nworkers, int nthreads_per_call, int64_t nreq, const int *kind,
+                     const int *graph, const double *t_arrival, const int64_t *fp,
+                     const int64_t *fi, const float *fx, int *status, int64_t *count,
+                     double *checksum, double *latency, double *makespan)
+{
+    GxB_Global_Option_set_INT32(GxB_GLOBAL_NTHREADS, nthreads_per_call);
+    serve_run R;
+    memset(&R, 0, sizeof(R));
+    R.nreq = nreq; R.kind = kind; R.graph = graph; R.t_arrival = t_arrival;
+    R.fp = fp; R.fi = fi; R.fx = fx;
+    R.status = status; R.count = count; R.checksum = checksum; R.latency = latency;
+    pthread_mutex_init(&R.mu, NULL);
+    pthread_cond_init(&R.cv, NULL);
+    pthread_t *th = malloc(nworkers * sizeof(pthread_t));
+    clock_gettime(CLOCK_MONOTONIC, &R.t0);
+    for (int w = 0; w < nworkers; w++) pthread_create(&th[w], NULL, serve_worker, &R);
+    for (int64_t k = 0; k < nreq; k++)
+    {
+        // open loop: wait for the arrival time, never for the workers
+        const double wait = t_arrival[k] - now_s(&R.t0);
+        if (wait > 0)
+        {
+            struct timespec ts = {(time_t)wait, (long)((wait - (double)(time_t)wait) * 1e9)};
+            nanosleep(&ts, NULL);
+        }
+        pthread_mutex_lock(&R.mu);
+        R.submitted = k + 1;
+        pthread_cond_broadcast(&R.cv);
+        pthread_mutex_unlock(&R.mu);
+    }
+    for (int w = 0; w < nworkers; w++) pthread_join(th[w], NULL);
+    *makespan = now_s(&R.t0);
+    free(th);
+    pthread_mutex_destroy(&R.mu);
+    pthread_cond_destroy(&R.cv);
+    int info = 0;
+    for (int64_t k = 0; k < nreq; k++) if (status[k] != 0) info = status[k];
+    return info;
+}

@@ -171,3 +171,30 @@ def test_oracle_vs_reference_batch(O, R):
         C = O.saxpy(a.nrows, a.ncols, (a.p, a.i, a.x, 10), (a.p, a.i, a.x, 10),
                     "MIN", "PLUS", 10)
         assert C[0][-1] == nnz_ref[k]
+
+
+def test_reference_serve_replay_matches_oracle(O, R):
+    """The reference arm of the serving workload: the request trace replayed
+    through a thread pool on the reference library gives, request by request,
+    the triangle counts and result sizes the oracle computes."""
+    from graphblas_b200.serve import make_graphs, make_trace, K_TRICOUNT, K_SSSP
+    graphs = make_graphs(seed=3, tc_scales=range(6, 9), n_sssp=1, n_mxm=2, mxm_nmax=2000)
+    trace = make_trace(graphs, nreq=40, rate=4000.0, seed=5)
+    status, count, checksum, latency, makespan = R.serve(graphs, trace, 4, 1)
+    assert (status == 0).all()
+    assert makespan > 0 and (latency > 0).all()
+    for k in range(40):
+        kind = int(trace["kind"][k])
+        g = graphs[int(trace["graph"][k])][1]
+        if kind == K_TRICOUNT:
+            L, U = W.tril_triu(g)
+            assert count[k] == O.tricount(g.nrows, L.p, L.i, U.p, U.i)
+        elif kind == K_SSSP:
+            lo, hi = trace["fp"][k], trace["fp"][k + 1]
+            u = (np.array([0, hi - lo], np.int64), trace["fi"][lo:hi], trace["fx"][lo:hi], 10)
+            want = O.saxpy(1, g.ncols, u, (g.p, g.i, g.x, 10), "MIN", "PLUS", 10)
+            assert count[k] == len(want[1])
+        else:
+            want = O.saxpy(g.nrows, g.ncols, (g.p, g.i, g.x, 11), (g.p, g.i, g.x, 11),
+                           "PLUS", "TIMES", 11)
+            assert count[k] == len(want[1])
