@@ -135,6 +135,10 @@ class TriCount:
         # merge reads of every (i,j) in L plus mask read and C write
         self.alg_bytes = 4.0 * (np.sum(dL * dL) + np.sum(dU * dU)) + 16.0 * self.L.nnz
         self.workload = "tricount_rmat%d_ef16_dot3_plus_pair" % self.scale
+        # DRAM bytes of one dot3 call (dram__bytes_read.sum + dram__bytes_write.sum
+        # over its kernels, ncu on R-MAT scale 18: 431.6 MB for 3,805,187 mask
+        # entries), scaled by mask entries
+        self.traffic_per_launch = 431.6e6 / 3805187 * self.L.nnz
 
     def config(self):
         return {"n": int(self.S.nrows), "nnz_L": int(self.L.nnz),
@@ -179,11 +183,12 @@ class TriCount:
 
     def launches_per_step(self):
         # classify, intersect, reduce partial + final; with the bitmap path
-        # (masks of 65536+ entries) also group sizes, two scans over the
-        # group keys, route, item count, item fill and the bitmap kernel
+        # (masks of 65536+ entries) also group sizes, route, item count, two
+        # item fills, the bitmap and warp-hash kernels, and three scans over
+        # the group keys
         if self.L.nnz < (1 << 16):
             return 4
-        return 4 + 5 + 2 * scan_launches(self.S.nrows + self.U.nrows + 1)
+        return 4 + 7 + 3 * scan_launches(self.S.nrows + self.U.nrows + 1)
 
     def cpu_baseline(self, R, ncores):
         ntri, times = R.tricount(self.S.nrows, self.L.p, self.L.i, self.U.p, self.U.i, reps=1)
@@ -216,6 +221,9 @@ class Saxpy:
         self.products = int(np.sum(deg[self.A.i]))
         self.flops = 2.0 * self.products
         self.workload = "saxpy3_er16384_d8_plus_times_fp64"
+        # DRAM bytes of the numeric kernel per launch (ncu capture of this
+        # workload: the inputs come from L2, the written slots stay there)
+        self.traffic_per_launch = 3.49e6
 
     def config(self):
         return {"n": self.n, "nnz_A": int(self.A.nnz), "products": self.products,
@@ -561,7 +569,8 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                          "unit": "GB/s",
                          "frac": (achieved / hbm_peak) if achieved else None,
-                         "peak_kind": peak_kind, "traffic": None,
+                         "peak_kind": peak_kind,
+                         "traffic": getattr(work, "traffic_per_launch", None),
                          "kernel": work.kernel, "kernel_ms_per_launch": kernel_ms,
                          "algorithmic_bytes_per_launch": alg_per_launch},
             "clocks": clocks,
