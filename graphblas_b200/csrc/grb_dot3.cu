@@ -365,7 +365,8 @@ struct __align__(16) D3Rec { int32_t s0, len, pm, j; };
 
 // a work item: every nit-th entry of key's group, from the t-th; its key row
 // (offsets rp0..rp1, first column lo) and lanes per entry 2^lg
-struct __align__(16) D3Item { int32_t key, t, nit, m_item, rp0, rp1, lo, lg; int64_t g0, pad; };
+struct __align__(16) D3Item { int32_t key, t, nit, m_item, rp0, rp1, lo, lg; int64_t g0;
+                               int32_t hi, pad; };
 
 template <class SR> struct IsCount {
     static constexpr bool value = SR::add_op == OP_PLUS && SR::mult_op == OP_PAIR &&
@@ -486,6 +487,7 @@ __global__ void k_d3_item_fill(const int64_t *__restrict__ ioff, int64_t nkeys,
         const int32_t r = by_row ? (int32_t)t : (int32_t)(t - nrows);
         const int32_t rp0 = by_row ? Ap[r] : Bp[r], rp1 = by_row ? Ap[r + 1] : Bp[r + 1];
         const int32_t lo = by_row ? Aj[rp0] : Bj[rp0];
+        const int32_t hi = by_row ? Aj[rp1 - 1] : Bj[rp1 - 1];
         const int64_t g0 = goff[t], gn = goff[t + 1] - g0;
         // lanes per entry: a power of two near half the mean list length
         const unsigned long long mean = gwork[t] / (unsigned long long)gn;
@@ -493,7 +495,8 @@ __global__ void k_d3_item_fill(const int64_t *__restrict__ ioff, int64_t nkeys,
         while (lg < 5 && (2ull << lg) < mean) lg++;
         for (int64_t q = 0; q < n; q++)
             items[o + q] = D3Item{(int32_t)t, (int32_t)q, (int32_t)n,
-                                  (int32_t)((gn - q + n - 1) / n), rp0, rp1, lo, lg, g0, 0};
+                                  (int32_t)((gn - q + n - 1) / n), rp0, rp1, lo, lg, g0,
+                                  hi, 0};
     }
 }
 
@@ -523,7 +526,7 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
                     unsigned long long *__restrict__ nzombies)
 {
     using Z = typename SR::z_t;
-    extern __shared__ uint32_t bm[];
+    extern __shared__ __align__(16) uint32_t bm[];
     __shared__ int s_item, s_next, s_gnext;
     __shared__ D3Item s_I;                        // the next item, fetched ahead
     __shared__ unsigned long long s_tbl;          // (segments << 32) | entries
@@ -535,23 +538,23 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
     const int64_t nitems = *nitems_p;
     unsigned long long zc = 0;
     // hits among S[b0 + t] for t = first, first + step, ... < n
+    // (four predicated loads issued together per step, the tail included;
+    // a skipped slot reads as lo - 1, which is never a bit of the row)
     auto probes = [&](const int32_t *S, int32_t b0, int32_t first, int32_t step, int32_t n,
                       int32_t lo) -> int {
         int c = 0;
-        int32_t t = first;
-        for (; t + 3 * step < n; t += 4 * step) {
-            const int32_t x0 = S[b0 + t], x1 = S[b0 + t + step];
-            const int32_t x2 = S[b0 + t + 2 * step], x3 = S[b0 + t + 3 * step];
-            const uint32_t k0 = (uint32_t)(x0 - lo), k1 = (uint32_t)(x1 - lo);
-            const uint32_t k2 = (uint32_t)(x2 - lo), k3 = (uint32_t)(x3 - lo);
-            c += (k0 < nbits) ? (int)((bm[k0 >> 5] >> (k0 & 31)) & 1u) : 0;
-            c += (k1 < nbits) ? (int)((bm[k1 >> 5] >> (k1 & 31)) & 1u) : 0;
-            c += (k2 < nbits) ? (int)((bm[k2 >> 5] >> (k2 & 31)) & 1u) : 0;
-            c += (k3 < nbits) ? (int)((bm[k3 >> 5] >> (k3 & 31)) & 1u) : 0;
-        }
-        for (; t < n; t += step) {
-            const uint32_t k = (uint32_t)(S[b0 + t] - lo);
-            c += (k < nbits) ? (int)((bm[k >> 5] >> (k & 31)) & 1u) : 0;
+        for (int32_t t = first; t < n; t += 4 * step) {
+            int32_t x[4];
+            #pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int32_t q = t + u * step;
+                x[u] = q < n ? S[b0 + q] : lo - 1;
+            }
+            #pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint32_t k = (uint32_t)(x[u] - lo);
+                c += (k < nbits) ? (int)((bm[k >> 5] >> (k & 31)) & 1u) : 0;
+            }
         }
         return c;
     };
@@ -570,9 +573,23 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
         const int32_t *J = by_row ? Aj : Bj;
         const int32_t *S = by_row ? Bj : Aj;     // the probed lists
         const int32_t rp0 = I.rp0, rp1 = I.rp1, lo = I.lo;
-        for (int32_t q = rp0 + tid; q < rp1; q += blockDim.x) {
-            const uint32_t k = (uint32_t)(J[q] - lo);
-            atomicOr(&bm[k >> 5], 1u << (k & 31));
+        // set the key row's bits: four loads in flight per thread
+        {
+            const int32_t nt = (int32_t)blockDim.x;
+            int32_t q = rp0 + tid;
+            for (; q + 3 * nt < rp1; q += 4 * nt) {
+                const uint32_t k0 = (uint32_t)(J[q] - lo), k1 = (uint32_t)(J[q + nt] - lo);
+                const uint32_t k2 = (uint32_t)(J[q + 2 * nt] - lo);
+                const uint32_t k3 = (uint32_t)(J[q + 3 * nt] - lo);
+                atomicOr(&bm[k0 >> 5], 1u << (k0 & 31));
+                atomicOr(&bm[k1 >> 5], 1u << (k1 & 31));
+                atomicOr(&bm[k2 >> 5], 1u << (k2 & 31));
+                atomicOr(&bm[k3 >> 5], 1u << (k3 & 31));
+            }
+            for (; q < rp1; q += nt) {
+                const uint32_t k = (uint32_t)(J[q] - lo);
+                atomicOr(&bm[k >> 5], 1u << (k & 31));
+            }
         }
         const int64_t g0 = I.g0;
         const int32_t m_item = I.m_item;
@@ -585,21 +602,22 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
             s_item = atomicAdd(inext, 1);
             if (s_item < nitems) s_I = items[s_item];
         }
-        // phase A
+        // phase A: the next chunk's records are fetched while this chunk
+        // probes, so their load latency overlaps the probes'
+        int c_next = 0;
+        if (lane == 0) c_next = atomicAdd(&s_next, groups);
+        c_next = __shfl_sync(0xffffffffu, c_next, 0);
+        D3Rec e_next{0, 0, 0, 0};
+        if (c_next + gi < m_item) e_next = bucket[g0 + I.t + (int64_t)I.nit * (c_next + gi)];
         while (true) {
-            int c0 = 0;
-            if (lane == 0) c0 = atomicAdd(&s_next, groups);
-            c0 = __shfl_sync(0xffffffffu, c0, 0);
+            const int c0 = c_next;
             if (c0 >= m_item) break;
             const int32_t rr = c0 + gi;
-            int32_t s0 = 0, len = 0, pm = 0, j = 0;
-            if (rr < m_item) {
-                const D3Rec e = bucket[g0 + I.t + (int64_t)I.nit * rr];
-                s0 = e.s0;
-                len = e.len;
-                pm = e.pm;
-                j = e.j;
-            }
+            const int32_t s0 = e_next.s0, len = rr < m_item ? e_next.len : 0;
+            const int32_t pm = e_next.pm, j = e_next.j;
+            if (lane == 0) c_next = atomicAdd(&s_next, groups);
+            c_next = __shfl_sync(0xffffffffu, c_next, 0);
+            if (c_next + gi < m_item) e_next = bucket[g0 + I.t + (int64_t)I.nit * (c_next + gi)];
             // a long list goes to the table (its group's first lane registers
             // it); the group keeps it only if the table is full
             unsigned slot = 0xffffffffu;
@@ -658,9 +676,18 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
             else { Cj[pm] = flip(j); zc++; }
         }
         __syncthreads();
-        for (int32_t q = rp0 + tid; q < rp1; q += blockDim.x) {
-            const uint32_t k = (uint32_t)(J[q] - lo);
-            bm[k >> 5] = 0;
+        // clear: zero the row's word range with 16-byte stores when that is
+        // cheaper than revisiting the row's entries
+        const uint32_t span_words = (uint32_t)(I.hi - lo) / 32u + 1u;
+        if (span_words <= 4u * (uint32_t)(rp1 - rp0)) {
+            uint4 *b4 = reinterpret_cast<uint4 *>(bm);
+            const uint32_t n4 = (span_words + 3u) / 4u;
+            for (uint32_t q = tid; q < n4; q += blockDim.x) b4[q] = make_uint4(0, 0, 0, 0);
+        } else {
+            for (int32_t q = rp0 + tid; q < rp1; q += blockDim.x) {
+                const uint32_t k = (uint32_t)(J[q] - lo);
+                bm[k >> 5] = 0;
+            }
         }
     }
     for (int o = 16; o > 0; o >>= 1) zc += __shfl_down_sync(0xffffffffu, zc, o);
@@ -774,8 +801,10 @@ static uint32_t bitmap_words(int64_t ncols)
         cudaGetLastError();
         avail = a / 4;
     }
-    const int64_t need = (ncols + 31) / 32 + 1;
-    const int64_t w = need < avail ? need : avail;
+    // a multiple of 4 words: the clear writes 16-byte blocks
+    const int64_t need = ((ncols + 31) / 32 + 1 + 3) & ~(int64_t)3;
+    const int64_t cap = avail & ~(int64_t)3;
+    const int64_t w = need < cap ? need : cap;
     return w >= 1024 || w == need ? (uint32_t)w : 0;
 }
 
