@@ -748,21 +748,27 @@ k_dot3_hash_count(const D3Item *__restrict__ items, const int64_t *__restrict__ 
         __syncwarp();
         const int lg = I.lg, G = 1 << lg, gi = lane >> lg, gl = lane & (G - 1);
         const int groups = 32 >> lg;
+        // the next chunk's records load while this chunk probes; four
+        // predicated loads per step (a skipped slot looks up -2, never a key)
+        D3Rec e_next{0, 0, 0, 0};
+        if (gi < I.m_item) e_next = bucket[I.g0 + I.t + (int64_t)I.nit * gi];
         for (int32_t c0 = 0; c0 < I.m_item; c0 += groups) {
             const int32_t rr = c0 + gi;
-            int32_t s0 = 0, len = 0, pm = 0, j = 0;
-            if (rr < I.m_item) {
-                const D3Rec e = bucket[I.g0 + I.t + (int64_t)I.nit * rr];
-                s0 = e.s0; len = e.len; pm = e.pm; j = e.j;
-            }
+            const int32_t s0 = e_next.s0, len = rr < I.m_item ? e_next.len : 0;
+            const int32_t pm = e_next.pm, j = e_next.j;
+            if (rr + groups < I.m_item)
+                e_next = bucket[I.g0 + I.t + (int64_t)I.nit * (rr + groups)];
             int cnt = 0;
-            int32_t t = gl;
-            for (; t + 3 * G < len; t += 4 * G) {
-                const int32_t x0 = S[s0 + t], x1 = S[s0 + t + G];
-                const int32_t x2 = S[s0 + t + 2 * G], x3 = S[s0 + t + 3 * G];
-                cnt += has(x0) + has(x1) + has(x2) + has(x3);
+            for (int32_t t = gl; t < len; t += 4 * G) {
+                int32_t x[4];
+                #pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int32_t q = t + u * G;
+                    x[u] = q < len ? S[s0 + q] : -2;
+                }
+                #pragma unroll
+                for (int u = 0; u < 4; u++) cnt += x[u] >= 0 ? has(x[u]) : 0;
             }
-            for (; t < len; t += G) cnt += has(S[s0 + t]);
             for (int o = G >> 1; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o, G);
             if (rr < I.m_item && gl == 0) {
                 if (cnt) { Cj[pm] = j; Cx[pm] = (Z)cnt; }
