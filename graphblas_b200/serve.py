@@ -193,6 +193,37 @@ class BenchServe:
 
     def dev_setup(self, gb):
         self.S = self._server()
+        # per-graph sizes for the bytes each request must move (4-byte
+        # indices; fp32 / fp64 values): triangle count reads L, U and the
+        # mask once and writes C; SSSP reads u and the rows of S it touches
+        # and writes w; A*A reads A, the B rows of every product and writes C
+        self.gstat = []
+        for kind, g in self.graphs:
+            deg = np.diff(g.p)
+            if kind == K_TRICOUNT:
+                nl = int(np.sum(g.i < np.repeat(np.arange(g.nrows), deg)))
+                self.gstat.append({"tc": 8.0 * (g.nrows + 1) + 8.0 * nl + 16.0 * nl})
+            elif kind == K_SSSP:
+                self.gstat.append({"deg": deg})
+            else:
+                prods = float(np.sum(deg[g.i]))
+                self.gstat.append({"mxm": 8.0 * (g.nrows + 1) + 12.0 * g.nnz + 12.0 * prods})
+
+    def _request_bytes(self, S):
+        tot = 0.0
+        t = self.trace
+        for k in range(self.nreq):
+            g = int(t["graph"][k])
+            st = self.gstat[g]
+            cnt = S.request(k)["count"]
+            if "tc" in st:
+                tot += st["tc"]
+            elif "deg" in st:
+                lo, hi = t["fp"][k], t["fp"][k + 1]
+                tot += 8.0 * (hi - lo) + 8.0 * float(np.sum(st["deg"][t["fi"][lo:hi]])) + 8.0 * cnt
+            else:
+                tot += st["mxm"] + 12.0 * cnt
+        return tot
 
     def _latencies(self, S):
         lat = np.array([S.request(k)["latency"] for k in range(self.nreq)])
@@ -208,6 +239,10 @@ class BenchServe:
     def step_dev(self):
         self.S.replay(self.trace)
         st = self._latencies(self.S)
+        # roofline over the whole replay: every request's bytes over the
+        # makespan (idle gaps between arrivals included)
+        self.alg_bytes = self._request_bytes(self.S)
+        self.kernel_ms_override = 1e3 * st["makespan_s"]
         return st["completed"]
 
     def e2e_setup(self, torch):
