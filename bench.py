@@ -277,7 +277,9 @@ class Saxpy:
         return self.flops / 1e9
 
     def launches_per_step(self):
-        return 9
+        # flops, bins, fill, numeric, counts, pack, conversions and two scans of
+        # two levels each: 16 (counted on this workload's launch list)
+        return 16
 
     def cpu_baseline(self, R, ncores):
         t = 0.0
@@ -385,7 +387,10 @@ class Bfs:
         return self.edges
 
     def launches_per_step(self):
-        return 12 * max(getattr(self, "levels", 1), 1)
+        # per level, the vxm (symbolic phase, flat heavy-row product index and
+        # dense row, compaction, pack) and the parent assign: 35 on average
+        # (counted on this workload's launch list)
+        return 35 * max(getattr(self, "levels", 1), 1)
 
     def cpu_baseline(self, R, ncores):
         parent, secs, nlev = R.bfs(self.n, self.S.p, self.S.i, self.src)
