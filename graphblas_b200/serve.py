@@ -256,7 +256,10 @@ class BenchServe:
         return st["completed"]
 
     def launches_per_step(self):
-        return 8 * self.nreq
+        # about 18 per request: a saxpy3 product or vxm step ~16-20 (symbolic
+        # phase, numeric, compaction, pack), a triangle count 5 (small graphs)
+        # to 25 (bitmap path), plus the device checksum reduction
+        return 18 * self.nreq
 
     # the reference replays a bounded sample of the trace: its first requests,
     # with the same arrival times, through 8 host workers
