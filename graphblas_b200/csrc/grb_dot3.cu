@@ -356,6 +356,7 @@ static constexpr int64_t D3_HCHUNK = 1 << 16;   // probes per warp-hash work ite
 static constexpr int D3_HWARPS = 8;             // warps (tables) per hash block
 static constexpr int D3_BM_THREADS = 1024;
 static constexpr int D3_LONG = 2048;          // longer lists go to the shared table
+static constexpr int D3_PROBE_UNROLL = 4;     // probe loads in flight per lane
 static constexpr int D3_SEG = 512;            // probes per shared long-list segment
 static constexpr int D3_TABLE = 1024;         // long lists registered per item
 
@@ -538,20 +539,20 @@ k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict_
     const int64_t nitems = *nitems_p;
     unsigned long long zc = 0;
     // hits among S[b0 + t] for t = first, first + step, ... < n
-    // (four predicated loads issued together per step, the tail included;
+    // (D3_PROBE_UNROLL predicated loads issued together per step, the tail included;
     // a skipped slot reads as lo - 1, which is never a bit of the row)
     auto probes = [&](const int32_t *S, int32_t b0, int32_t first, int32_t step, int32_t n,
                       int32_t lo) -> int {
         int c = 0;
-        for (int32_t t = first; t < n; t += 4 * step) {
-            int32_t x[4];
+        for (int32_t t = first; t < n; t += D3_PROBE_UNROLL * step) {
+            int32_t x[D3_PROBE_UNROLL];
             #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < D3_PROBE_UNROLL; u++) {
                 const int32_t q = t + u * step;
                 x[u] = q < n ? S[b0 + q] : lo - 1;
             }
             #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < D3_PROBE_UNROLL; u++) {
                 const uint32_t k = (uint32_t)(x[u] - lo);
                 c += (k < nbits) ? (int)((bm[k >> 5] >> (k & 31)) & 1u) : 0;
             }
