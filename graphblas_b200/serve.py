@@ -181,7 +181,8 @@ class BenchServe:
 
     def config(self):
         return dict(requests=self.nreq, rate_req_s=2000.0, slots=8,
-                    hbm_budget_gb=40, **getattr(self, "lat", {}))
+                    hbm_budget_gb=40, **getattr(self, "lat", {}),
+                    **getattr(self, "capacity", {}))
 
     def _server(self):
         # results stay on the device (counts and checksums come back), as a
@@ -193,6 +194,14 @@ class BenchServe:
 
     def dev_setup(self, gb):
         self.S = self._server()
+        # capacity: the same requests all arriving at once (closed batch), so
+        # the replay runs as fast as the server can take them
+        burst = dict(self.trace)
+        burst["t"] = np.zeros(self.nreq)
+        self.S.replay(burst)
+        st = self.S.stats()
+        self.capacity = {"capacity_req_s": st["completed"] / max(st["makespan_s"], 1e-9),
+                         "capacity_peak_concurrent": st["peak_active"]}
         # per-graph sizes for the bytes each request must move (4-byte
         # indices; fp32 / fp64 values): triangle count reads L, U and the
         # mask once and writes C; SSSP reads u and the rows of S it touches
