@@ -22,6 +22,15 @@
 //     search window advancing chunk by chunk.  The queue spreads R-MAT's
 //     heavy entries over every warp of the GPU.
 //
+// Counting semirings (PLUS_PAIR on integers: triangle and support counts)
+// on masks of 65536+ entries take a third route for most queued entries:
+// entries sharing their longer list (row i of A, or row j of B) form a
+// group, the shared row is loaded once into a shared-memory bitmap (key rows
+// over 256 entries, one block per SM) or a per-warp hash table (shorter key
+// rows), and every entry's other list is probed against it; the count of
+// hits is C(i,j).  Entries of small groups, and rows too wide for the
+// bitmap, stay on the merge path above.
+//
 // Matches come out of __ballot_sync in ascending k, so order-dependent
 // monoids (floating PLUS/TIMES, ANY) fold them in exactly the reference's
 // sequential order, first match assigned and later ones added

@@ -26,13 +26,18 @@
 //      C(i,j) sees its terms in the reference's order: first term written,
 //      later terms folded with the monoid's UPDATE.  This makes floating
 //      PLUS bit-exact as well.  Order-free monoids on heavy rows instead
-//      spread all products over the grid with atomic updates.
+//      spread all products over the grid (a flat product index: the heavy
+//      rows' A entries and each one's B-row length, scanned) with atomic
+//      updates into a dense row of byte flags and values, skipping the atomic
+//      when an idempotent monoid's value cannot change.
 //   4. each row's entries are sorted by column in shared memory (bitonic) and
 //      written to its slot; a compaction kernel packs the slots into CSR.
 //
-// Masks: M (or !M) is scattered into the row's table first (the reference's
-// "scatter M" step, GB_AxB_saxpy3_symbolic.c), with a state per slot:
-// allowed-unset, set, or forbidden.
+// Masks: in the hash bins M (or !M) is scattered into the row's table first
+// (the reference's "scatter M" step, GB_AxB_saxpy3_symbolic.c), with a state
+// per slot: allowed-unset, set, or forbidden; the expand-sort-compress bin
+// checks each product's column against M(i,:) by binary search; heavy rows
+// mark the dense row's flags.
 
 #include <cstdio>
 #include <cstring>
