@@ -33,7 +33,7 @@ CC_FLAGS = ["-O3", "-fPIC", "-std=gnu11", "-fopenmp",
 
 CU_SOURCES = ["grb_runtime.cu", "grb_dot3.cu", "grb_saxpy3.cu", "grb_reduce.cu",
               "grb_ewise.cu", "grb_mxv.cu", "grb_batch.cu", "grb_serve.cu", "grb_abi.cu"]
-C_SOURCES = ["grb_api.c"]
+C_SOURCES = ["grb_api.c", "grb_serialize.c", "grb_zstd.c"]
 
 
 def _nvcc():

@@ -722,6 +722,126 @@ GrB_Info GrB_Matrix_exportSize(GrB_Index *Ap_len, GrB_Index *Ai_len,
 }
 
 //------------------------------------------------------------------------------
+// serialize / deserialize (Source/serialize/GrB_Matrix_serialize.c,
+// GxB_Matrix_serialize.c, GrB_Matrix_serializeSize.c, GxB_Matrix_deserialize.c,
+// GrB_Matrix_deserialize.c, GxB_Vector_serialize.c, GxB_Vector_deserialize.c).
+// A blob is written from the matrix's CSR arrays (one download from HBM when
+// the matrix lives there) in the reference's uncompressed format, and a blob
+// read is decoded on the host into the matrix's host copy, which goes to HBM
+// at its first use on the device.
+//------------------------------------------------------------------------------
+
+static GrB_Type type_of_code(int code)
+{
+    switch (code)
+    {
+        case 1: return GrB_BOOL;
+        case 6: return GrB_INT32;
+        case 7: return GrB_UINT32;
+        case 8: return GrB_INT64;
+        case 9: return GrB_UINT64;
+        case 10: return GrB_FP32;
+        case 11: return GrB_FP64;
+    }
+    return NULL;
+}
+
+// blob of A (a 1-by-n vector is written as the reference's n-by-1 column);
+// blob == NULL: *size gets the exact size
+static GrB_Info serialize_any(void *blob, size_t *size, GrB_Matrix A, bool vector)
+{
+    CHECK(to_host(A));
+    if (vector)
+        return (GrB_Info)grb_b200_blob_encode(blob, size, A->ncols, 1, A->type->code,
+                                              A->hp, A->hi, A->hx, A->hiso, true);
+    return (GrB_Info)grb_b200_blob_encode(blob, size, A->nrows, A->ncols, A->type->code,
+                                          A->hp, A->hi, A->hx, A->hiso, false);
+}
+
+GrB_Info GrB_Matrix_serializeSize(GrB_Index *blob_size_handle, GrB_Matrix A)
+{
+    if (!blob_size_handle) return GrB_NULL_POINTER;
+    if (!OBJ_OK(A)) return GrB_UNINITIALIZED_OBJECT;
+    size_t size = 0;
+    CHECK(serialize_any(NULL, &size, A, false));
+    *blob_size_handle = (GrB_Index)size;
+    return GrB_SUCCESS;
+}
+
+GrB_Info GrB_Matrix_serialize(void *blob, GrB_Index *blob_size_handle, GrB_Matrix A)
+{
+    if (!blob || !blob_size_handle) return GrB_NULL_POINTER;
+    if (!OBJ_OK(A)) return GrB_UNINITIALIZED_OBJECT;
+    size_t size = (size_t)*blob_size_handle;
+    CHECK(serialize_any(blob, &size, A, false));
+    *blob_size_handle = (GrB_Index)size;
+    return GrB_SUCCESS;
+}
+
+static GrB_Info serialize_alloc(void **blob_handle, GrB_Index *blob_size_handle,
+                                GrB_Matrix A, bool vector)
+{
+    size_t size = 0;
+    CHECK(serialize_any(NULL, &size, A, vector));
+    void *blob = malloc(size);
+    if (!blob) return GrB_OUT_OF_MEMORY;
+    GrB_Info info = serialize_any(blob, &size, A, vector);
+    if (info != GrB_SUCCESS) { free(blob); return info; }
+    *blob_handle = blob;
+    *blob_size_handle = (GrB_Index)size;
+    return GrB_SUCCESS;
+}
+
+GrB_Info GxB_Matrix_serialize(void **blob_handle, GrB_Index *blob_size_handle,
+                              GrB_Matrix A, const GrB_Descriptor desc)
+{
+    (void)desc;
+    if (!blob_handle || !blob_size_handle) return GrB_NULL_POINTER;
+    if (!OBJ_OK(A)) return GrB_UNINITIALIZED_OBJECT;
+    return serialize_alloc(blob_handle, blob_size_handle, A, false);
+}
+
+// decode a blob into a new matrix whose host copy holds the arrays
+static GrB_Info deserialize_any(GrB_Matrix *C, GrB_Type type, const void *blob,
+                                GrB_Index blob_size)
+{
+    CHECK_INIT;
+    if (!C || !blob) return GrB_NULL_POINTER;
+    *C = NULL;
+    int64_t nrows = 0, ncols = 0, *p = NULL, *i = NULL;
+    void *x = NULL;
+    int code = 0;
+    bool iso = false;
+    CHECK(grb_b200_blob_decode(blob, (size_t)blob_size, type ? type->code : 0, &nrows,
+                               &ncols, &code, &p, &i, &x, &iso));
+    GrB_Matrix M = NULL;
+    GrB_Info info = GrB_Matrix_new(&M, type_of_code(code), (GrB_Index)nrows,
+                                   (GrB_Index)ncols);
+    if (info != GrB_SUCCESS) { free(p); free(i); free(x); return info; }
+    if (!i) i = malloc(sizeof(int64_t));          // the host copy keeps non-NULL arrays
+    if (!x) x = calloc(1, M->type->size);
+    if (!i || !x) { free(p); free(i); free(x); GrB_Matrix_free(&M); return GrB_OUT_OF_MEMORY; }
+    M->hp = p; M->hi = i; M->hx = x;
+    M->hiso = iso;
+    M->host_ok = true;
+    *C = M;
+    return GrB_SUCCESS;
+}
+
+GrB_Info GrB_Matrix_deserialize(GrB_Matrix *C, GrB_Type type, const void *blob,
+                                GrB_Index blob_size)
+{
+    return deserialize_any(C, type, blob, blob_size);
+}
+
+GrB_Info GxB_Matrix_deserialize(GrB_Matrix *C, GrB_Type type, const void *blob,
+                                GrB_Index blob_size, const GrB_Descriptor desc)
+{
+    (void)desc;
+    return deserialize_any(C, type, blob, blob_size);
+}
+
+//------------------------------------------------------------------------------
 // vectors (1-by-n rows inside)
 //------------------------------------------------------------------------------
 
@@ -923,6 +1043,45 @@ VEXTRACT(INT64, int64_t, 8)
 VEXTRACT(FP32, float, 10)
 VEXTRACT(FP64, double, 11)
 #undef VEXTRACT
+
+GrB_Info GxB_Vector_serialize(void **blob_handle, GrB_Index *blob_size_handle,
+                              GrB_Vector u, const GrB_Descriptor desc)
+{
+    (void)desc;
+    if (!blob_handle || !blob_size_handle) return GrB_NULL_POINTER;
+    if (!VOK(u)) return GrB_UNINITIALIZED_OBJECT;
+    return serialize_alloc(blob_handle, blob_size_handle, VM(u), true);
+}
+
+// a vector blob holds an n-by-1 matrix; its entries become the one row here
+GrB_Info GxB_Vector_deserialize(GrB_Vector *w, GrB_Type type, const void *blob,
+                                GrB_Index blob_size, const GrB_Descriptor desc)
+{
+    (void)desc;
+    if (!w) return GrB_NULL_POINTER;
+    *w = NULL;
+    GrB_Matrix C = NULL;
+    CHECK(deserialize_any(&C, type, blob, blob_size));
+    if (C->ncols != 1) { GrB_Matrix_free(&C); return GrB_INVALID_OBJECT; }
+    const int64_t n = C->nrows, nnz = C->hp[n];
+    int64_t *p = malloc(2 * sizeof(int64_t));
+    int64_t *ii = malloc((size_t)(nnz ? nnz : 1) * sizeof(int64_t));
+    if (!p || !ii) { free(p); free(ii); GrB_Matrix_free(&C); return GrB_OUT_OF_MEMORY; }
+    for (int64_t r = 0; r < n; r++)
+        if (C->hp[r + 1] > C->hp[r]) ii[C->hp[r]] = r;   // the value order is kept
+    p[0] = 0;
+    p[1] = nnz;
+    GrB_Vector v = malloc(sizeof(*v));
+    if (!v) { free(p); free(ii); GrB_Matrix_free(&C); return GrB_OUT_OF_MEMORY; }
+    matrix_init(VM(v), C->type, 1, n);
+    v->m.hp = p; v->m.hi = ii; v->m.hx = C->hx;
+    v->m.hiso = C->hiso;
+    v->m.host_ok = true;
+    C->hx = NULL;
+    GrB_Matrix_free(&C);
+    *w = v;
+    return GrB_SUCCESS;
+}
 
 //------------------------------------------------------------------------------
 // the multiply path

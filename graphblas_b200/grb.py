@@ -91,6 +91,18 @@ class API:
             f.restype = ctypes.c_int
             f.argtypes = [vp, vp, vp, ctypes.POINTER(U64), ctypes.POINTER(U64),
                           ctypes.POINTER(U64), ctypes.c_int, vp]
+        for name in ("GrB_Matrix_serializeSize", "GrB_Matrix_serialize",
+                     "GxB_Matrix_serialize", "GrB_Matrix_deserialize",
+                     "GxB_Matrix_deserialize", "GxB_Vector_serialize",
+                     "GxB_Vector_deserialize"):
+            getattr(L, name).restype = ctypes.c_int
+        L.GrB_Matrix_serializeSize.argtypes = [ctypes.POINTER(U64), vp]
+        L.GrB_Matrix_serialize.argtypes = [vp, ctypes.POINTER(U64), vp]
+        L.GxB_Matrix_serialize.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(U64), vp, vp]
+        L.GxB_Vector_serialize.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(U64), vp, vp]
+        L.GrB_Matrix_deserialize.argtypes = [ctypes.POINTER(vp), vp, vp, U64]
+        L.GxB_Matrix_deserialize.argtypes = [ctypes.POINTER(vp), vp, vp, U64, vp]
+        L.GxB_Vector_deserialize.argtypes = [ctypes.POINTER(vp), vp, vp, U64, vp]
         L.GrB_Matrix_exportSize.restype = ctypes.c_int
         L.GrB_Matrix_exportSize.argtypes = [ctypes.POINTER(U64), ctypes.POINTER(U64),
                                             ctypes.POINTER(U64), ctypes.c_int, vp]
@@ -181,6 +193,47 @@ class API:
         n = U64(cap)
         self.call("GrB_Vector_extractTuples_" + SUFFIX[type_code], i, x, ctypes.byref(n), v)
         return n.value
+
+    # ---- serialize / deserialize ----
+    def matrix_serialize(self, A, preallocated=False):
+        """The blob of A as bytes: GxB_Matrix_serialize, or with preallocated
+        GrB_Matrix_serializeSize + GrB_Matrix_serialize into a caller buffer."""
+        if preallocated:
+            n = U64()
+            self.call("GrB_Matrix_serializeSize", ctypes.byref(n), A)
+            buf = ctypes.create_string_buffer(max(n.value, 1))
+            used = U64(n.value)
+            self.call("GrB_Matrix_serialize", buf, ctypes.byref(used), A)
+            return buf.raw[:used.value]
+        return self._take_blob("GxB_Matrix_serialize", A)
+
+    def vector_serialize(self, v):
+        return self._take_blob("GxB_Vector_serialize", v)
+
+    def _take_blob(self, name, obj):
+        bp, n = vp(), U64()
+        self.call(name, ctypes.byref(bp), ctypes.byref(n), obj, None)
+        out = ctypes.string_at(bp.value, n.value)
+        _libc.free(bp.value)
+        return out
+
+    def matrix_deserialize(self, blob, type_code=None, gxb=True):
+        """GxB_Matrix_deserialize (or GrB_Matrix_deserialize) of a bytes blob."""
+        A = vp()
+        t = None if type_code is None else self.obj(TYPE_NAMES[type_code])
+        buf = ctypes.create_string_buffer(blob, max(len(blob), 1))
+        if gxb:
+            self.call("GxB_Matrix_deserialize", ctypes.byref(A), t, buf, len(blob), None)
+        else:
+            self.call("GrB_Matrix_deserialize", ctypes.byref(A), t, buf, len(blob))
+        return A
+
+    def vector_deserialize(self, blob, type_code=None):
+        v = vp()
+        t = None if type_code is None else self.obj(TYPE_NAMES[type_code])
+        buf = ctypes.create_string_buffer(blob, max(len(blob), 1))
+        self.call("GxB_Vector_deserialize", ctypes.byref(v), t, buf, len(blob), None)
+        return v
 
     def matrix_to_csr(self, A, type_code, nrows):
         """GxB_Matrix_unpack_CSR into numpy (the matrix becomes empty)."""
@@ -285,6 +338,64 @@ class API:
         for k, v in fields.items():
             self.call("GrB_Descriptor_set", d, codes[k], v)
         return d
+
+
+def _blob_lib():
+    L = _lib_loader()
+    if not getattr(L, "_blob_bound", False):
+        L.grb_b200_blob_decode.restype = ctypes.c_int
+        L.grb_b200_blob_decode.argtypes = [vp, ctypes.c_size_t, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int64),
+                                           ctypes.POINTER(ctypes.c_int64),
+                                           ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                           ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_bool)]
+        L.grb_b200_blob_encode.restype = ctypes.c_int
+        L.grb_b200_blob_encode.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t),
+                                           ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                           vp, vp, vp, ctypes.c_bool, ctypes.c_bool]
+        L._blob_bound = True
+    return L
+
+
+def blob_decode(blob, expected_type=0):
+    """Read a serialized-matrix blob on the host (no GPU): returns
+    (nrows, ncols, type_code, p, i, x, iso), CSR by row; x holds one value
+    when iso.  Raises GrBError with the GrB_Info of a rejected blob."""
+    L = _blob_lib()
+    buf = ctypes.create_string_buffer(bytes(blob), max(len(blob), 1))
+    nr, nc, t = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int()
+    pp, ip, xp = vp(), vp(), vp()
+    iso = ctypes.c_bool()
+    info = L.grb_b200_blob_decode(buf, len(blob), expected_type, ctypes.byref(nr),
+                                  ctypes.byref(nc), ctypes.byref(t), ctypes.byref(pp),
+                                  ctypes.byref(ip), ctypes.byref(xp), ctypes.byref(iso))
+    if info != 0:
+        raise GrBError(info, "grb_b200_blob_decode")
+    p = _take(pp.value, nr.value + 1, np.int64)
+    nnz = int(p[-1])
+    i = _take(ip.value, nnz, np.int64)
+    x = _take(xp.value, 1 if iso.value else nnz, NP_OF[t.value])
+    return nr.value, nc.value, t.value, p, i, x, iso.value
+
+
+def blob_encode(nrows, ncols, type_code, p, i, x, iso=False, by_col=False):
+    """Write an uncompressed serialized-matrix blob on the host (no GPU)."""
+    L = _blob_lib()
+    p = np.ascontiguousarray(p, np.int64)
+    i = np.ascontiguousarray(i, np.int64)
+    x = np.ascontiguousarray(x, NP_OF[type_code])
+    n = ctypes.c_size_t()
+    args = (nrows, ncols, type_code, p.ctypes.data, i.ctypes.data if i.size else None,
+            x.ctypes.data if x.size else None, iso, by_col)
+    info = L.grb_b200_blob_encode(None, ctypes.byref(n), *args)
+    if info != 0:
+        raise GrBError(info, "grb_b200_blob_encode")
+    buf = ctypes.create_string_buffer(n.value)
+    info = L.grb_b200_blob_encode(buf, ctypes.byref(n), *args)
+    if info != 0:
+        raise GrBError(info, "grb_b200_blob_encode")
+    return buf.raw[:n.value]
 
 
 def _copy_to_malloc(a):

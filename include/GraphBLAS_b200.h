@@ -201,6 +201,23 @@ GRB_B200_IMPORT(FP64, double)
 GrB_Info GrB_Matrix_exportSize(GrB_Index *Ap_len, GrB_Index *Ai_len,
                                GrB_Index *Ax_len, GrB_Format format, GrB_Matrix A);
 
+/* ---- serialize / deserialize (the reference's blob format) ----
+ * Blobs written here are uncompressed (GxB_COMPRESSION_NONE); blobs read may
+ * also be LZ4 / LZ4HC compressed.  ZSTD blobs give GrB_NOT_IMPLEMENTED.  The
+ * descriptor arguments are accepted and ignored. */
+GrB_Info GrB_Matrix_serializeSize(GrB_Index *blob_size_handle, GrB_Matrix A);
+GrB_Info GrB_Matrix_serialize(void *blob, GrB_Index *blob_size_handle, GrB_Matrix A);
+GrB_Info GxB_Matrix_serialize(void **blob_handle, GrB_Index *blob_size_handle,
+                              GrB_Matrix A, const GrB_Descriptor desc);
+GrB_Info GrB_Matrix_deserialize(GrB_Matrix *C, GrB_Type type, const void *blob,
+                                GrB_Index blob_size);
+GrB_Info GxB_Matrix_deserialize(GrB_Matrix *C, GrB_Type type, const void *blob,
+                                GrB_Index blob_size, const GrB_Descriptor desc);
+GrB_Info GxB_Vector_serialize(void **blob_handle, GrB_Index *blob_size_handle,
+                              GrB_Vector u, const GrB_Descriptor desc);
+GrB_Info GxB_Vector_deserialize(GrB_Vector *w, GrB_Type type, const void *blob,
+                                GrB_Index blob_size, const GrB_Descriptor desc);
+
 /* ---- vectors (sparse) ---- */
 GrB_Info GrB_Vector_new(GrB_Vector *v, GrB_Type type, GrB_Index n);
 GrB_Info GrB_Vector_free(GrB_Vector *v);

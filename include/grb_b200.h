@@ -165,6 +165,35 @@ int grb_b200_dmatrix_import(grb_b200_dmatrix *D, int64_t nrows, int64_t ncols,
  * GrB_Matrix_export (Source/import_export/GrB_Matrix_export.c:38-215). */
 int grb_b200_dmatrix_export(grb_b200_dmatrix D, int64_t *p, int64_t *i, void *x);
 
+/* Serialized-matrix blobs in the reference's format (host code, no GPU).
+ *
+ * grb_b200_blob_decode reads a blob made by GxB_Matrix_serialize /
+ * GrB_Matrix_serialize (Source/serialize/GB_serialize.c:43) the way
+ * GB_deserialize reads it (Source/serialize/GB_deserialize.c:22): any of the
+ * four sparsity forms, by row or by column, stored raw or LZ4 / LZ4HC
+ * compressed.  The result is CSR by row with sorted rows: *Cp (nrows+1),
+ * *Ci (nnz) and *Cx (nnz values, or one value when *iso) are malloc'ed and
+ * the caller frees them.  expected_type 0 accepts any built-in type, else
+ * the blob's type code must equal it.  GrB_INVALID_OBJECT for a malformed
+ * blob, GrB_DOMAIN_MISMATCH for a type mismatch or a user-defined type,
+ * GrB_NOT_IMPLEMENTED for ZSTD blocks (the reference's default compression)
+ * and for built-in types outside bool/int32/uint32/int64/uint64/fp32/fp64.
+ *
+ * grb_b200_blob_encode writes an uncompressed sparse blob (the reference's
+ * GxB_COMPRESSION_NONE form, which its deserializer reads) of a matrix given
+ * compressed by row (p has nrows+1 entries, i column indices), or by column
+ * when by_col (p has ncols+1 entries, i row indices; vectors are n-by-1 by
+ * column).  x holds nnz values, or one value when iso.  blob_out NULL stores
+ * the exact size in *blob_size; otherwise *blob_size is the room in
+ * blob_out on input (GrB_INSUFFICIENT_SPACE when short) and the bytes
+ * written on output (GrB_Matrix_serialize's contract). */
+int grb_b200_blob_decode(const void *blob, size_t blob_size, int expected_type,
+                         int64_t *nrows, int64_t *ncols, int *type, int64_t **Cp,
+                         int64_t **Ci, void **Cx, bool *iso);
+int grb_b200_blob_encode(void *blob_out, size_t *blob_size, int64_t nrows,
+                         int64_t ncols, int type, const int64_t *p, const int64_t *i,
+                         const void *x, bool iso, bool by_col);
+
 int grb_b200_dmatrix_free(grb_b200_dmatrix *D);
 
 /* nrows, ncols, stored entries (zombies included), zombies, type, iso */

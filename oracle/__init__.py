@@ -179,6 +179,16 @@ class Reference:
             + [vp]
         L.ref_batch_square.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp,
                                        ctypes.c_int, ctypes.c_int, vp, vp]
+        L.ref_serialize.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, vp, vp,
+                                    vp, ctypes.c_int, ctypes.c_bool, ctypes.c_int,
+                                    ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_uint64)]
+        L.ref_blob_free.argtypes = [vp]
+        L.ref_blob_free.restype = None
+        L.ref_deserialize.restype = vp
+        L.ref_deserialize.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int64),
+                                      ctypes.POINTER(ctypes.c_int64),
+                                      ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int)]
         self.nthreads = nthreads or os.cpu_count()
         info = L.ref_init(self.nthreads)
         if info != 0:
@@ -223,6 +233,45 @@ class Reference:
         L.ref_export(h, _ptr(p), _ptr(i), _ptr(x))
         L.ref_free(h)
         return p, i[:nnz], x[:nnz]
+
+    def serialize(self, t, nrows, ncols, p, i, x, sparsity=2, by_col=False,
+                  method=-1):
+        """The reference's GxB_Matrix_serialize blob (bytes) of a CSR matrix
+        (x None: iso-true pattern) stored with GxB_SPARSITY_CONTROL
+        `sparsity`, by column when by_col, compressed with GxB_COMPRESSION
+        `method`."""
+        keep = [_i64(p), _i64(i)]
+        xx = None if x is None else np.ascontiguousarray(x, NP_TYPES[t])
+        bp, n = ctypes.c_void_p(), ctypes.c_uint64()
+        info = self.lib.ref_serialize(t, nrows, ncols, _ptr(keep[0]), _ptr(keep[1]),
+                                      _ptr(xx), sparsity, by_col, method,
+                                      ctypes.byref(bp), ctypes.byref(n))
+        if info != 0:
+            raise RuntimeError("reference GxB_Matrix_serialize failed: %d" % info)
+        out = ctypes.string_at(bp.value, n.value)
+        self.lib.ref_blob_free(bp)
+        return out
+
+    def deserialize(self, blob):
+        """The reference's GxB_Matrix_deserialize of a blob, as
+        (nrows, ncols, type, p, i, x) CSR by row; raises with the GrB_Info
+        of a rejected blob (attribute .info)."""
+        buf = ctypes.create_string_buffer(bytes(blob), max(len(blob), 1))
+        nr, nc, t, info = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int(), ctypes.c_int()
+        h = self.lib.ref_deserialize(buf, len(blob), ctypes.byref(nr), ctypes.byref(nc),
+                                     ctypes.byref(t), ctypes.byref(info))
+        if not h:
+            e = RuntimeError("reference GxB_Matrix_deserialize failed: %d" % info.value)
+            e.info = info.value
+            raise e
+        L = self.lib
+        nnz = L.ref_nnz(h)
+        p = np.empty(nr.value + 1, np.int64)
+        i = np.empty(max(nnz, 1), np.int64)
+        x = np.empty(max(nnz, 1), NP_TYPES[t.value])
+        L.ref_export(h, _ptr(p), _ptr(i), _ptr(x))
+        L.ref_free(h)
+        return nr.value, nc.value, t.value, p, i[:nnz], x[:nnz]
 
     def tricount(self, n, Lp, Li, Up, Ui, reps=1):
         keep = [_i64(a) for a in (Lp, Li, Up, Ui)]

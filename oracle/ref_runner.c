@@ -617,3 +617,89 @@ int ref_serve_replay(int nworkers, int nthreads_per_call, int64_t nreq, const in
     for (int64_t k = 0; k < nreq; k++) if (status[k] != 0) info = status[k];
     return info;
 }
+
+//------------------------------------------------------------------------------
+// serialize / deserialize with the reference (GxB_Matrix_serialize,
+// Include/GraphBLAS.h:10917; GxB_Matrix_deserialize, :10963), to pin the
+// library's blob reader and writer to the reference's own blobs.
+//------------------------------------------------------------------------------
+
+// Blob of a CSR matrix (x == NULL: iso-true pattern of type t) stored with
+// the given GxB_SPARSITY_CONTROL (1 hyper, 2 sparse, 4 bitmap, 8 full), by
+// column when by_col, compressed with `method` (a GxB_COMPRESSION_* value).
+// *blob is malloc'ed (the reference's default allocator); ref_blob_free.
+int ref_serialize(int t, int64_t nrows, int64_t ncols, const int64_t *p,
+                  const int64_t *i, const void *x, int sparsity, bool by_col,
+                  int method, void **blob, uint64_t *blob_size)
+{
+    GrB_Matrix A = NULL;
+    GrB_Descriptor D = NULL;
+    GrB_Info info;
+    GrB_Index size = 0;
+    *blob = NULL;
+    #define TRY(x) { info = (x); if (info != GrB_SUCCESS) goto done; }
+    TRY(make_csr(&A, t, nrows, ncols, p, i, x));
+    TRY(GxB_Matrix_Option_set_INT32(A, GxB_FORMAT, by_col ? GxB_BY_COL : GxB_BY_ROW));
+    TRY(GxB_Matrix_Option_set_INT32(A, GxB_SPARSITY_CONTROL, sparsity));
+    TRY(GrB_Matrix_wait(A, GrB_MATERIALIZE));
+    TRY(GrB_Descriptor_new(&D));
+    TRY(GxB_Desc_set_INT32(D, GxB_COMPRESSION, method));
+    TRY(GxB_Matrix_serialize(blob, &size, A, D));
+    *blob_size = (uint64_t)size;
+done:
+    GrB_Matrix_free(&A);
+    GrB_Descriptor_free(&D);
+    return (int)info;
+    #undef TRY
+}
+
+void ref_blob_free(void *blob) { free(blob); }
+
+// A blob read by the reference, returned as CSR by row with sorted rows
+// (iso values expanded); *nrows_out / *ncols_out / *type_out describe it.
+ref_csr *ref_deserialize(const void *blob, uint64_t blob_size, int64_t *nrows_out,
+                         int64_t *ncols_out, int *type_out, int *info_out)
+{
+    GrB_Matrix C = NULL;
+    GrB_Type type = NULL;
+    ref_csr *R = NULL;
+    GrB_Index nr = 0, nc = 0;
+    GrB_Info info;
+    #define TRY(x) { info = (x); if (info != GrB_SUCCESS) goto done; }
+    TRY(GxB_Matrix_deserialize(&C, NULL, blob, (GrB_Index)blob_size, NULL));
+    TRY(GrB_Matrix_nrows(&nr, C));
+    TRY(GrB_Matrix_ncols(&nc, C));
+    TRY(GxB_Matrix_type(&type, C));
+    int code = 0;
+    for (int t = 1; t <= 11 && !code; t++)
+        if (tsize(t) && type_of(t) == type) code = t;
+    if (!code) { info = GrB_DOMAIN_MISMATCH; goto done; }
+    TRY(GxB_Matrix_Option_set_INT32(C, GxB_FORMAT, GxB_BY_ROW));
+    TRY(GxB_Matrix_Option_set_INT32(C, GxB_SPARSITY_CONTROL, GxB_SPARSE));
+    TRY(GrB_Matrix_wait(C, GrB_MATERIALIZE));
+    R = calloc(1, sizeof(ref_csr));
+    R->nrows = (int64_t)nr; R->type = code;
+    GrB_Index psize, isize, xsize;
+    bool iso = false;
+    TRY(GxB_Matrix_unpack_CSR(C, &R->p, &R->i, &R->x, &psize, &isize, &xsize,
+                              &iso, NULL, NULL));
+    R->nnz = R->p[nr];
+    if (iso && R->nnz > 0)
+    {
+        size_t ts = tsize(code);
+        void *xx = malloc(R->nnz * ts);
+        for (int64_t k = 0; k < R->nnz; k++)
+            memcpy((char *)xx + k * ts, R->x, ts);
+        free(R->x);
+        R->x = xx;
+    }
+    *nrows_out = (int64_t)nr;
+    *ncols_out = (int64_t)nc;
+    *type_out = code;
+done:
+    GrB_Matrix_free(&C);
+    if (info_out) *info_out = (int)info;
+    if (info != GrB_SUCCESS) { ref_free(R); return NULL; }
+    return R;
+    #undef TRY
+}
