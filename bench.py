@@ -115,11 +115,14 @@ class ClockSampler:
 # workloads
 # ---------------------------------------------------------------------------
 
-def scan_launches(n, tile=4096):
-    """Kernel launches of the library's device scan of n values (two per
-    level of the tile tree)."""
+def scan_launches(n, tile=4096, single=32768):
+    """Kernel launches of the library's device scan of n values: one block
+    scans up to 32768 values in one launch; longer arrays take a tile-sum
+    launch and a tile-scan launch around the scan of the tile sums."""
+    if n <= single:
+        return 1
     nb = (n + tile - 1) // tile
-    return 2 + (scan_launches(nb, tile) if nb > 1 else 0)
+    return 2 + scan_launches(nb, tile, single)
 
 
 class TriCount:
@@ -277,9 +280,9 @@ class Saxpy:
         return self.flops / 1e9
 
     def launches_per_step(self):
-        # flops, bins, fill, numeric, counts, pack, conversions and two scans of
-        # two levels each: 16 (counted on this workload's launch list)
-        return 16
+        # flop counts, bins, slot scan, bin fill, numeric, row counts, row
+        # scan, pack: 8 (counted on this workload's launch list)
+        return 8
 
     def cpu_baseline(self, R, ncores):
         t = 0.0

@@ -394,6 +394,7 @@ __global__ void k_d3_gsize(const int32_t *__restrict__ gcnt, int64_t nkeys,
         const int32_t c = gcnt[t];
         gsz[t] = c >= D3_GMIN ? c : 0;
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) gsz[nkeys] = 0;    // the scan's last input
 }
 
 // route every queued entry to its group's bucket or to the merge list
@@ -463,6 +464,7 @@ __global__ void k_d3_item_count(const int64_t *__restrict__ gsz,
 {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    if (t == 0) { nit_big[nkeys] = 0; nit_small[nkeys] = 0; }    // the scans' last inputs
     for (; t < nkeys; t += stride) {
         const int64_t g = gsz[t];
         int64_t nb = 0, ns = 0;
@@ -834,22 +836,17 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
     C.p = (int32_t *)dalloc((size_t)(M.nrows + 1) * 4, s);
     C.j = (int32_t *)dalloc((size_t)(mnz ? mnz : 1) * 4, s);
     C.x = dalloc((size_t)(mnz ? mnz : 1) * sizeof(Z), s);
-    int *counter = (int *)dalloc(64, s);
-    D3Work *queue = (D3Work *)dalloc((size_t)(mnz ? mnz : 1) * sizeof(D3Work), s);
-    if (!C.p || !C.j || !C.x || !counter || !queue) {
-        dev_free(C, s); dfree(counter, s); dfree(queue, s); return OUT_OF_MEMORY;
-    }
-    cudaMemcpyAsync(C.p, M.p, (size_t)(M.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
-    cudaMemsetAsync(counter, 0, 64, s);
-    int *qlen = counter, *qnext = counter + 1, *merge_len = counter + 2, *inext = counter + 3;
-    unsigned long long *zc = (unsigned long long *)((char *)counter + 32);
     // the bitmap path: counting semirings on masks large enough to pay for it
     const int64_t nkeys = M.nrows + B.nrows;
     uint32_t bm_words = 0;
     if constexpr (IsCount<SR>::value) {
         if (mnz >= D3_BM_MIN_ENTRIES && nkeys < INT32_MAX) bm_words = bitmap_words<SR>(A.ncols);
     }
-    Scratch bm_scratch(s);
+    // the work queue, the counters and the bitmap path's arrays in one
+    // allocation; the counters, group sizes, fill cursors and work sums come
+    // first and adjacent, so that one memset clears them
+    int *counter = nullptr;
+    D3Work *queue = nullptr;
     int32_t *gcnt = nullptr, *gfill = nullptr, *merge_sel = nullptr;
     D3Rec *bucket = nullptr;
     int64_t *gsz = nullptr, *goff = nullptr, *nit = nullptr, *ioff = nullptr, *ws = nullptr;
@@ -857,39 +854,47 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
     D3Item *items_s = nullptr;
     unsigned long long *gwork = nullptr;
     D3Item *items = nullptr;
-    if (bm_words) {
-        gcnt = bm_scratch.get<int32_t>(nkeys);
-        gfill = bm_scratch.get<int32_t>(nkeys);
-        gsz = bm_scratch.get<int64_t>(nkeys + 1);
-        goff = bm_scratch.get<int64_t>(nkeys + 1);
-        nit = bm_scratch.get<int64_t>(nkeys + 1);
-        ioff = bm_scratch.get<int64_t>(nkeys + 1);
-        nit_s = bm_scratch.get<int64_t>(nkeys + 1);
-        ioff_s = bm_scratch.get<int64_t>(nkeys + 1);
-        items_s = bm_scratch.get<D3Item>(nkeys + mnz / 32 + 1);
-        gwork = bm_scratch.get<unsigned long long>(nkeys);
-        items = bm_scratch.get<D3Item>(nkeys + mnz / 32 + 1);
-        bucket = bm_scratch.get<D3Rec>(mnz);
-        merge_sel = bm_scratch.get<int32_t>(mnz);
-        ws = bm_scratch.get<int64_t>((int64_t)scan_ws_elems(nkeys + 1));
-        if (bm_scratch.failed) {
-            dev_free(C, s); dfree(counter, s); dfree(queue, s); return OUT_OF_MEMORY;
+    Carve cv(s);
+    auto layout = [&]() {
+        counter = cv.take<int>(16);
+        if (bm_words) {
+            gcnt = cv.take<int32_t>(nkeys);
+            gfill = cv.take<int32_t>(nkeys);
+            gwork = cv.take<unsigned long long>(nkeys);
         }
+        queue = cv.take<D3Work>(mnz ? mnz : 1);
+        if (bm_words) {
+            gsz = cv.take<int64_t>(nkeys + 1);
+            goff = cv.take<int64_t>(nkeys + 1);
+            nit = cv.take<int64_t>(nkeys + 1);
+            ioff = cv.take<int64_t>(nkeys + 1);
+            nit_s = cv.take<int64_t>(nkeys + 1);
+            ioff_s = cv.take<int64_t>(nkeys + 1);
+            items_s = cv.take<D3Item>(nkeys + mnz / 32 + 1);
+            items = cv.take<D3Item>(nkeys + mnz / 32 + 1);
+            bucket = cv.take<D3Rec>(mnz);
+            merge_sel = cv.take<int32_t>(mnz);
+            ws = cv.take<int64_t>((int64_t)scan_ws_elems(nkeys + 1));
+        }
+    };
+    layout();
+    const bool got = cv.alloc();
+    layout();
+    struct Release { Carve &c; ~Release() { dfree(c.base, c.s); } } release{cv};
+    if (!C.p || !C.j || !C.x || !got) {
+        dev_free(C, s); return OUT_OF_MEMORY;
     }
+    cudaMemcpyAsync(C.p, M.p, (size_t)(M.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
+    const char *zero_end = bm_words ? (const char *)(gwork + nkeys) : (const char *)(counter + 16);
+    cudaMemsetAsync(counter, 0, (size_t)(zero_end - (const char *)counter), s);
+    int *qlen = counter, *qnext = counter + 1, *merge_len = counter + 2, *inext = counter + 3;
+    unsigned long long *zc = (unsigned long long *)((char *)counter + 32);
     if (mnz > 0 && M.nrows > 0) {
         const int nsm = runtime().num_sms;
         int64_t warps_needed = (mnz + 31) / 32;
         int64_t blocks = (warps_needed + 7) / 8;
         if (blocks > (int64_t)nsm * 16) blocks = (int64_t)nsm * 16;
         const int ps = prof_begin("dot3", s);
-        if (bm_words) {
-            cudaMemsetAsync(gcnt, 0, (size_t)nkeys * 4, s);
-            cudaMemsetAsync(gfill, 0, (size_t)nkeys * 4, s);
-            cudaMemsetAsync(gwork, 0, (size_t)nkeys * 8, s);
-            cudaMemsetAsync(gsz + nkeys, 0, 8, s);
-            cudaMemsetAsync(nit + nkeys, 0, 8, s);
-            cudaMemsetAsync(nit_s + nkeys, 0, 8, s);
-        }
         k_dot3_classify<SR><<<(unsigned)blocks, 256, 0, s>>>(
             M.p, M.j, mask_struct ? nullptr : M.x, M.type, mask_struct, mnz, M.nrows,
             A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso, C.j, (Z *)C.x,
@@ -930,8 +935,6 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
     unsigned long long hz = 0;
     cudaMemcpyAsync(&hz, zc, 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
-    dfree(counter, s);
-    dfree(queue, s);
     if (e != cudaSuccess) { dev_free(C, s); return cuda_to_info(e); }
     C.nzombies = (int64_t)hz;
     return SUCCESS;

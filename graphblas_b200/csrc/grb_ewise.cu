@@ -80,6 +80,7 @@ __global__ void k_am_tside(int64_t m, const int32_t *__restrict__ Tp,
                            bool comp, int accum, int64_t *__restrict__ keepT,
                            Z *__restrict__ valT)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0) keepT[nT] = 0;       // the scan's last input
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nT;
          e += (int64_t)gridDim.x * blockDim.x) {
         const int32_t i = row_of(Tp, m, e), j = Tj[e];
@@ -102,6 +103,7 @@ __global__ void k_am_cside(int64_t m, const int32_t *__restrict__ Cp,
                            bool comp, bool replace, int accum,
                            int64_t *__restrict__ keepC)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0) keepC[nC] = 0;       // the scan's last input
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nC;
          e += (int64_t)gridDim.x * blockDim.x) {
         const int32_t i = row_of(Cp, m, e), j = Cj[e];
@@ -163,26 +165,32 @@ static int accum_mask_t(DevCSR &C, const DevCSR &T, const DevCSR *M, bool comp,
                         bool replace, int accum, cudaStream_t s)
 {
     const int64_t m = T.nrows, nT = T.nnz, nC = C.nnz;
-    Scratch ws(s);
-    int64_t *keepT = ws.get<int64_t>(nT + 1);
-    int64_t *keepC = ws.get<int64_t>(nC + 1);
-    Z *valT = ws.get<Z>(nT + 1);
-    if (ws.failed) return OUT_OF_MEMORY;
+    // the keep flags / offsets of both sides, T's values, the scan workspace
+    // and the two totals in one allocation
+    Carve cv(s);
+    int64_t *keepT = nullptr, *keepC = nullptr, *ws = nullptr, *tot_d = nullptr;
+    Z *valT = nullptr;
+    const int64_t nmax = nT > nC ? nT : nC;
+    auto layout = [&]() {
+        tot_d = cv.take<int64_t>(2);
+        keepT = cv.take<int64_t>(nT + 1);
+        keepC = cv.take<int64_t>(nC + 1);
+        valT = cv.take<Z>(nT + 1);
+        ws = cv.take<int64_t>(scan_ws_elems(nmax + 1));
+    };
+    layout();
+    if (!cv.alloc()) return OUT_OF_MEMORY;
+    layout();
+    struct Release { Carve &c; ~Release() { dfree(c.base, c.s); } } release{cv};
     const int32_t *Mp = M ? M->p : nullptr, *Mj = M ? M->j : nullptr;
-    if (nT > 0)
-        k_am_tside<Z><<<grid_n(nT), 256, 0, s>>>(m, T.p, T.j, (const Z *)T.x, T.iso, nT,
-            C.p, C.j, (const Z *)C.x, C.iso, Mp, Mj, comp, accum, keepT, valT);
-    if (nC > 0)
-        k_am_cside<Z><<<grid_n(nC), 256, 0, s>>>(m, C.p, C.j, nC, T.p, T.j, Mp, Mj,
-            comp, replace, accum, keepC);
-    cudaMemsetAsync(keepT + nT, 0, 8, s);
-    cudaMemsetAsync(keepC + nC, 0, 8, s);
-    int info = scan_exclusive_i64(keepT, keepT, nT + 1, s);
-    if (info == SUCCESS) info = scan_exclusive_i64(keepC, keepC, nC + 1, s);
-    if (info != SUCCESS) return info;
+    k_am_tside<Z><<<grid_n(nT), 256, 0, s>>>(m, T.p, T.j, (const Z *)T.x, T.iso, nT,
+        C.p, C.j, (const Z *)C.x, C.iso, Mp, Mj, comp, accum, keepT, valT);
+    k_am_cside<Z><<<grid_n(nC), 256, 0, s>>>(m, C.p, C.j, nC, T.p, T.j, Mp, Mj,
+        comp, replace, accum, keepC);
+    scan_exclusive_i64_ws(keepT, keepT, nT + 1, ws, s, tot_d);
+    scan_exclusive_i64_ws(keepC, keepC, nC + 1, ws, s, tot_d + 1);
     int64_t tot[2] = {0, 0};
-    cudaMemcpyAsync(&tot[0], keepT + nT, 8, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&tot[1], keepC + nC, 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(tot, tot_d, 16, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_to_info(e);
     const int64_t nR = tot[0] + tot[1];
@@ -200,7 +208,7 @@ static int accum_mask_t(DevCSR &C, const DevCSR &T, const DevCSR *M, bool comp,
     if (nC > 0)
         k_am_write<Z><<<grid_n(nC), 256, 0, s>>>(m, C.p, C.j, (const Z *)C.x, C.iso, nC,
             keepC, T.p, T.j, keepT, R.p, R.j, (Z *)R.x);
-    e = cudaStreamSynchronize(s);
+    e = cudaGetLastError();
     if (e != cudaSuccess) { dev_free(R, s); return cuda_to_info(e); }
     dev_free(C, s);
     C = R;

@@ -438,10 +438,13 @@ __global__ void k_scan_totals(const T *__restrict__ in, int64_t n,
     }
 }
 
-// scan one tile per block; offsets[b] is the exclusive prefix of the tile
+// scan one tile per block; offsets[b] is the exclusive prefix of the tile;
+// total / out32 as in scan_exclusive_i64_ws
 template <typename T>
 __global__ void k_scan_tiles(const T *__restrict__ in, int64_t *__restrict__ out,
-                             int64_t n, const int64_t *__restrict__ offsets)
+                             int64_t n, const int64_t *__restrict__ offsets,
+                             int64_t *__restrict__ total = nullptr,
+                             int32_t *__restrict__ out32 = nullptr)
 {
     __shared__ int64_t warp_sums[SCAN_THREADS / 32];
     int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
@@ -476,9 +479,80 @@ __global__ void k_scan_tiles(const T *__restrict__ in, int64_t *__restrict__ out
     #pragma unroll
     for (int it = 0; it < SCAN_ITEMS; it++) {
         int64_t idx = base + it;
-        if (idx < n) out[idx] = prefix;
+        if (idx < n) {
+            out[idx] = prefix;
+            if (out32) out32[idx] = (int32_t)prefix;
+        }
         prefix += v[it];
+        if (total && idx == n - 1) *total = prefix;
     }
+}
+
+// the whole scan in one block of 1024 threads, tile after tile with a running
+// carry (in may equal out: every tile is read before it is written).  A warp
+// owns 256 consecutive values as 8 rows of 32: loads and stores are
+// coalesced, each row is scanned with shuffles and carried into the next.
+static constexpr int SCAN1_THREADS = 1024;
+static constexpr int SCAN1_ROWS = 8;
+static constexpr int SCAN1_TILE = SCAN1_THREADS * SCAN1_ROWS;
+
+template <typename T>
+__global__ void __launch_bounds__(SCAN1_THREADS)
+k_scan_single(const T *in, int64_t *out, int64_t n, int64_t *__restrict__ total,
+              int32_t *__restrict__ out32)
+{
+    __shared__ int64_t warp_sums[SCAN1_THREADS / 32];
+    __shared__ int64_t tile_sum;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int64_t carry = 0;
+    for (int64_t tile = 0; tile < n; tile += SCAN1_TILE) {
+        const int64_t base = tile + (int64_t)warp * (32 * SCAN1_ROWS) + lane;
+        int64_t v[SCAN1_ROWS];
+        #pragma unroll
+        for (int r = 0; r < SCAN1_ROWS; r++) {
+            const int64_t idx = base + r * 32;
+            v[r] = idx < n ? (int64_t)in[idx] : 0;
+        }
+        // inclusive scan of the warp's 256 values, row by row
+        int64_t run = 0;
+        #pragma unroll
+        for (int r = 0; r < SCAN1_ROWS; r++) {
+            int64_t x = v[r];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            v[r] = run + x - v[r];                  // exclusive within the warp
+            run += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (lane == 0) warp_sums[warp] = run;
+        __syncthreads();
+        if (warp == 0) {
+            const int64_t own = warp_sums[lane];
+            int64_t w = own;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            warp_sums[lane] = w - own;              // exclusive prefix of each warp
+        }
+        __syncthreads();
+        const int64_t wbase = carry + warp_sums[warp];
+        #pragma unroll
+        for (int r = 0; r < SCAN1_ROWS; r++) {
+            const int64_t idx = base + r * 32;
+            if (idx < n) {
+                const int64_t o = wbase + v[r];
+                out[idx] = o;
+                if (out32) out32[idx] = (int32_t)o;
+            }
+        }
+        // the tile's sum: the last warp's prefix plus its own run
+        if (warp == SCAN1_THREADS / 32 - 1 && lane == 0) tile_sum = warp_sums[warp] + run;
+        __syncthreads();
+        carry += tile_sum;
+    }
+    if (total && threadIdx.x == 0) *total = carry;
 }
 
 template <typename T>
@@ -519,21 +593,25 @@ size_t scan_ws_elems(int64_t n)
 }
 
 template <typename T>
-static void scan_ws_impl(const T *in, int64_t *out, int64_t n, int64_t *ws, cudaStream_t s)
+static void scan_ws_impl(const T *in, int64_t *out, int64_t n, int64_t *ws, cudaStream_t s,
+                         int64_t *total = nullptr, int32_t *out32 = nullptr)
 {
     if (n <= 0) return;
+    if (n <= SCAN_SINGLE_MAX) {
+        k_scan_single<T><<<1, SCAN1_THREADS, 0, s>>>(in, out, n, total, out32);
+        return;
+    }
     int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
     int64_t *totals = ws;
     k_scan_totals<T><<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, totals);
-    if (nb > 1) scan_ws_impl<int64_t>(totals, totals, nb, ws + nb + 1, s);
-    else cudaMemsetAsync(totals, 0, 8, s);
-    k_scan_tiles<T><<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, totals);
+    scan_ws_impl<int64_t>(totals, totals, nb, ws + nb + 1, s);
+    k_scan_tiles<T><<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, totals, total, out32);
 }
 
 void scan_exclusive_i64_ws(const int64_t *in, int64_t *out, int64_t n, int64_t *ws,
-                           cudaStream_t s)
+                           cudaStream_t s, int64_t *total, int32_t *out32)
 {
-    scan_ws_impl<int64_t>(in, out, n, ws, s);
+    scan_ws_impl<int64_t>(in, out, n, ws, s, total, out32);
 }
 
 int scan_exclusive_i32_to_i64(const int32_t *in, int64_t *out, int64_t n,

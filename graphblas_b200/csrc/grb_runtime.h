@@ -59,6 +59,28 @@ void set_alloc_fail_countdown(int64_t n);
 // GB_cuda_error.hpp:22-35): out of memory -> OUT_OF_MEMORY, else PANIC
 int cuda_to_info(cudaError_t e);
 
+// One device allocation carved into 256-byte aligned pieces.  The caller
+// lays its buffers out twice with the same take() calls: a sizing pass
+// (take() returns null), then, after alloc(), the pass that hands out the
+// pieces.  One allocation and one free replace one pair per buffer: the
+// stream-ordered allocator's host cost dominates small calls.
+struct Carve {
+    cudaStream_t s;
+    char *base = nullptr;
+    size_t off = 0;
+    explicit Carve(cudaStream_t st) : s(st) {}
+    template <typename T> T *take(size_t count) {
+        const size_t o = (off + 255) & ~(size_t)255;
+        off = o + count * sizeof(T);
+        return base ? reinterpret_cast<T *>(base + o) : nullptr;
+    }
+    bool alloc() {
+        base = (char *)dalloc(off ? off : 16, s);
+        off = 0;
+        return base != nullptr;
+    }
+};
+
 // scratch buffers that live for one call on one stream
 struct Scratch {
     cudaStream_t s;
@@ -116,8 +138,13 @@ int scan_exclusive_i32_to_i64(const int32_t *in, int64_t *out, int64_t n,
                               cudaStream_t s);
 // allocation-free variant: ws holds scan_ws_elems(n) int64 values
 size_t scan_ws_elems(int64_t n);
+static constexpr int64_t SCAN_SINGLE_MAX = 32768;
+// Arrays of at most SCAN_SINGLE_MAX elements are scanned by one launch of one
+// block.  total (device, may be null) receives the sum of all n inputs;
+// out32 (may be null) receives the offsets narrowed to int32 as well.
 void scan_exclusive_i64_ws(const int64_t *in, int64_t *out, int64_t n, int64_t *ws,
-                           cudaStream_t s);
+                           cudaStream_t s, int64_t *total = nullptr,
+                           int32_t *out32 = nullptr);
 
 // ---- operations (device matrices) ----
 

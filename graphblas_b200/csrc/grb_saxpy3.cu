@@ -39,6 +39,7 @@
 // checks each product's column against M(i,:) by binary search; heavy rows
 // mark the dense row's flags.
 
+#include <functional>
 #include <cstdio>
 #include <cstring>
 #include "grb_saxpy3.h"
@@ -149,12 +150,22 @@ __global__ void k_bin_rows(const int64_t *__restrict__ flops,
     }
 }
 
-// scatter rows into per-bin lists (order within a bin does not matter)
+// scatter rows into per-bin lists (order within a bin does not matter); a
+// bin's list starts after the rows of the bins before it
 __global__ void k_fill_bins(const int8_t *__restrict__ row_bin, int64_t nrows,
                             int *__restrict__ bin_fill,
-                            const int *__restrict__ bin_start,
+                            const int *__restrict__ bin_count, int nbins,
                             int32_t *__restrict__ bin_rows)
 {
+    __shared__ int bin_start[16];
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int q = 0; q < 16; q++) {
+            bin_start[q] = acc;
+            if (q < nbins) acc += bin_count[q];
+        }
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t r0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); r0 < nrows;
@@ -763,6 +774,7 @@ __global__ void k_heavy_alen(const int32_t *__restrict__ rows, int nr,
         const int32_t i = rows[t];
         hlen[t] = Ap[i + 1] - Ap[i];
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) hlen[nr] = 0;
 }
 
 __device__ __forceinline__ int64_t upper_bound64(const int64_t *a, int64_t lo, int64_t hi,
@@ -859,6 +871,8 @@ k_dense_count(int nrows_bin, int64_t ncols, int cblocks, const uint8_t *__restri
               int64_t *__restrict__ cnt)
 {
     __shared__ int s_w[DG_THREADS / 32];
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
+        cnt[(int64_t)nrows_bin * cblocks] = 0;
     for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
         const uint8_t *flag = flag_all + rb * ncols;
         const int64_t c0 = (int64_t)blockIdx.x * DG_CHUNK;
@@ -969,27 +983,15 @@ k_pack(int64_t nrows, int span, const int64_t *__restrict__ slot_off,
     }
 }
 
+// out[0..n) the counts of the binned rows (0 for empty ones), out[n] = 0
 __global__ void k_cnt_to_i64(const int32_t *__restrict__ cnt, const int8_t *__restrict__ row_bin,
                              int64_t n, int64_t *__restrict__ out)
 {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (; t < n; t += stride) out[t] = row_bin[t] ? (int64_t)cnt[t] : 0;
+    for (; t <= n; t += stride) out[t] = (t < n && row_bin[t]) ? (int64_t)cnt[t] : 0;
 }
 
-__global__ void k_i64_to_i32_p(const int64_t *__restrict__ in, int32_t *__restrict__ out,
-                               int64_t n, int64_t *__restrict__ nnz64)
-{
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (; t < n; t += stride) out[t] = (int32_t)in[t];
-    if (nnz64 && t == 0) *nnz64 = in[n - 1];
-}
-
-__global__ void k_copy_i64(const int64_t *__restrict__ in, int64_t *__restrict__ out)
-{
-    if (threadIdx.x == 0 && blockIdx.x == 0) *out = *in;
-}
 
 // ---------------------------------------------------------------------------
 // configuration, plan, execution
@@ -1069,17 +1071,16 @@ struct SaxpyPlan {
     int64_t heavy_alen = 0;                         // A entries in the heavy rows
     int64_t *hlen = nullptr, *hoff = nullptr;       // flat product index (per chunk)
     int64_t *wlen = nullptr, *wprefix = nullptr, *hw_ws = nullptr;
+    int64_t *nnz_d = nullptr;                       // one-shot calls: nnz(C)
+    // the three allocations the buffers above are carved from: symbolic
+    // arrays, slots (Tj, Tx), heavy-row accumulators
+    void *block = nullptr, *tblock = nullptr, *hblock = nullptr;
 };
 
 void saxpy_plan_free(SaxpyPlan *P, cudaStream_t s)
 {
     if (!P) return;
-    dfree(P->flops, s); dfree(P->slot_off, s); dfree(P->Cp64, s); dfree(P->scan_ws, s);
-    dfree(P->row_bin, s); dfree(P->bin_rows, s); dfree(P->row_cnt, s); dfree(P->Tj, s);
-    dfree(P->Tx, s); dfree(P->bins, s); dfree(P->flag, s); dfree(P->flag8, s); dfree(P->val, s);
-    dfree(P->dg_cnt, s); dfree(P->dg_ws, s);
-    dfree(P->hlen, s); dfree(P->hoff, s); dfree(P->wlen, s); dfree(P->wprefix, s);
-    dfree(P->hw_ws, s);
+    dfree(P->block, s); dfree(P->tblock, s); dfree(P->hblock, s);
     delete P;
 }
 
@@ -1113,81 +1114,102 @@ static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A
     P->order_free = SR::order_free;
     P->m = m; P->ncols = ncols;
     P->has_mask = M != nullptr; P->mask_comp = mask_comp;
-    P->flops = (int64_t *)dalloc((size_t)(m + 1) * 8, s);
-    P->slot_off = (int64_t *)dalloc((size_t)(m + 1) * 8, s);
-    P->Cp64 = (int64_t *)dalloc((size_t)(m + 2) * 8, s);
-    P->scan_ws = (int64_t *)dalloc(scan_ws_elems(m + 1) * 8, s);
-    P->row_bin = (int8_t *)dalloc((size_t)(m + 1), s);
-    P->bin_rows = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
-    P->row_cnt = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
-    P->bins = (int *)dalloc(64 * sizeof(int), s);
-    if (!P->flops || !P->slot_off || !P->Cp64 || !P->scan_ws || !P->row_bin ||
-        !P->bin_rows || !P->row_cnt || !P->bins)
-        return OUT_OF_MEMORY;
+    // the symbolic arrays in one allocation: the bin counters (256 bytes),
+    // the flop counts and the slot offsets first and adjacent, so that one
+    // memset clears all three
+    Carve cv(s);
+    auto layout = [&]() {
+        P->bins = cv.take<int>(64);
+        P->flops = cv.take<int64_t>(m + 1);
+        P->slot_off = cv.take<int64_t>(m + 1);
+        P->Cp64 = cv.take<int64_t>(m + 2);
+        P->scan_ws = cv.take<int64_t>(scan_ws_elems(m + 1));
+        P->row_bin = cv.take<int8_t>(m + 1);
+        P->bin_rows = cv.take<int32_t>(m + 1);
+        P->row_cnt = cv.take<int32_t>(m + 1);
+        P->nnz_d = cv.take<int64_t>(1);
+    };
+    layout();
+    if (!cv.alloc()) return OUT_OF_MEMORY;
+    layout();
+    P->block = cv.base;
     const bool mask_bounds = (M != nullptr) && !mask_comp;
-    cudaMemsetAsync(P->flops, 0, (size_t)(m + 1) * 8, s);
+    cudaMemsetAsync(P->bins, 0, (size_t)((char *)(P->slot_off + m + 1) - (char *)P->bins), s);
     if (m > 0 && A.nnz > 0)
         k_flops_flat<<<nblocks(A.nnz, 256, 16), 256, 0, s>>>(A.p, A.j, B.p, m, A.nnz,
             flat_span(A.nnz),
             (unsigned long long *)P->flops);
-    cudaMemsetAsync(P->bins, 0, 64 * sizeof(int), s);
     BinLimits lim;
     lim.nb = P->cfg.nb;
     for (int q = 0; q < P->cfg.nb; q++) lim.limit[q] = P->cfg.bin[q].limit;
+    // bins[]: 0..15 row counts per bin, 32..47 fill cursors, 48-49 the A
+    // entries of heavy rows (u64), 50-51 the total slot count (i64)
     if (m > 0)
         k_bin_rows<<<nblocks(m, 256), 256, 0, s>>>(P->flops, M ? M->p : nullptr,
             M != nullptr, mask_bounds, ncols, m, lim, P->bins, P->row_bin, P->slot_off,
             A.p, (unsigned long long *)(P->bins + 48));
-    cudaMemsetAsync(P->slot_off + m, 0, 8, s);
-    scan_exclusive_i64_ws(P->slot_off, P->slot_off, m + 1, P->scan_ws, s);
+    scan_exclusive_i64_ws(P->slot_off, P->slot_off, m + 1, P->scan_ws, s,
+                          (int64_t *)(P->bins + 50));
     const int nb = P->cfg.nb;
-    int64_t total_cap = 0;
-    cudaMemcpyAsync(P->h_bins, P->bins, sizeof(int) * (nb + 2), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&total_cap, P->slot_off + m, 8, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&P->heavy_alen, P->bins + 48, 8, cudaMemcpyDeviceToHost, s);
+    int hb[52];
+    cudaMemcpyAsync(hb, P->bins, sizeof(hb), cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_to_info(e);
+    for (int b = 0; b < nb + 2; b++) P->h_bins[b] = hb[b];
+    int64_t total_cap = 0;
+    memcpy(&P->heavy_alen, hb + 48, 8);
+    memcpy(&total_cap, hb + 50, 8);
     P->total_cap = total_cap;
     P->h_start[0] = 0;
     for (int b = 1; b < nb + 2; b++) P->h_start[b] = P->h_start[b - 1] + P->h_bins[b - 1];
-    int *d_start = P->bins + 16, *d_fill = P->bins + 32;
-    cudaMemcpyAsync(d_start, P->h_start, sizeof(int) * (nb + 2), cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(d_fill, 0, 16 * sizeof(int), s);
     if (m > 0)
-        k_fill_bins<<<nblocks(m, 256), 256, 0, s>>>(P->row_bin, m, d_fill, d_start, P->bin_rows);
-    P->Tj = (int32_t *)dalloc((size_t)(total_cap + 1) * 4, s);
-    P->Tx = dalloc((size_t)(total_cap + 1) * sizeof(Z), s);
-    if (!P->Tj || !P->Tx) return OUT_OF_MEMORY;
+        k_fill_bins<<<nblocks(m, 256), 256, 0, s>>>(P->row_bin, m, P->bins + 32, P->bins,
+                                                   nb + 2, P->bin_rows);
+    Carve tv(s);
+    auto tlayout = [&]() {
+        P->Tj = tv.take<int32_t>(total_cap + 1);
+        P->Tx = tv.take<Z>(total_cap + 1);
+    };
+    tlayout();
+    if (!tv.alloc()) return OUT_OF_MEMORY;
+    tlayout();
+    P->tblock = tv.base;
     const int nheavy = P->h_bins[nb + 1];
     if (nheavy > 0) {
+        Carve hv(s);
+        std::function<void()> hlayout;
         if (SR::order_free) {
             int64_t chunk = nheavy;
             const int64_t per_row = ncols * (1 + (int64_t)sizeof(Z));
             const int64_t budget = (int64_t)4 << 30;
             if (chunk * per_row > budget) chunk = budget / per_row > 0 ? budget / per_row : 1;
             P->heavy_chunk = chunk;
-            P->flag8 = (uint8_t *)dalloc((size_t)(chunk * ncols + 1), s);
-            P->val = dalloc((size_t)(chunk * ncols + 1) * sizeof(Z), s);
             const int64_t cblocks = (ncols + DG_CHUNK - 1) / DG_CHUNK;
             const int64_t ncnt = chunk * cblocks + 1;
-            P->dg_cnt = (int64_t *)dalloc((size_t)(ncnt + 1) * 8, s);
-            P->dg_ws = (int64_t *)dalloc(scan_ws_elems(ncnt) * 8, s);
-            if (!P->dg_cnt || !P->dg_ws) return OUT_OF_MEMORY;
             const int64_t hmax = (chunk + 1) > (P->heavy_alen + 1) ? chunk + 1 : P->heavy_alen + 1;
-            P->hlen = (int64_t *)dalloc((size_t)(chunk + 1) * 8, s);
-            P->hoff = (int64_t *)dalloc((size_t)(chunk + 1) * 8, s);
-            P->wlen = (int64_t *)dalloc((size_t)(P->heavy_alen + 1) * 8, s);
-            P->wprefix = (int64_t *)dalloc((size_t)(P->heavy_alen + 1) * 8, s);
-            P->hw_ws = (int64_t *)dalloc(scan_ws_elems(hmax) * 8, s);
-            if (!P->hlen || !P->hoff || !P->wlen || !P->wprefix || !P->hw_ws)
-                return OUT_OF_MEMORY;
+            hlayout = [&, chunk, ncnt, hmax]() {
+                P->flag8 = hv.take<uint8_t>(chunk * ncols + 1);
+                P->val = hv.take<Z>(chunk * ncols + 1);
+                P->dg_cnt = hv.take<int64_t>(ncnt + 1);
+                P->dg_ws = hv.take<int64_t>(scan_ws_elems(ncnt));
+                P->hlen = hv.take<int64_t>(chunk + 1);
+                P->hoff = hv.take<int64_t>(chunk + 1);
+                P->wlen = hv.take<int64_t>(P->heavy_alen + 1);
+                P->wprefix = hv.take<int64_t>(P->heavy_alen + 1);
+                P->hw_ws = hv.take<int64_t>(scan_ws_elems(hmax));
+            };
         } else {
             const int nbk = nheavy < runtime().num_sms * 2 ? nheavy : runtime().num_sms * 2;
             P->heavy_chunk = nbk;
-            P->flag = (int64_t *)dalloc((size_t)((int64_t)nbk * ncols + 1) * 8, s);
-            P->val = dalloc((size_t)((int64_t)nbk * ncols + 1) * sizeof(Z), s);
+            hlayout = [&, nbk]() {
+                P->flag = hv.take<int64_t>((int64_t)nbk * ncols + 1);
+                P->val = hv.take<Z>((int64_t)nbk * ncols + 1);
+            };
         }
-        if ((!P->flag && !P->flag8) || !P->val) return OUT_OF_MEMORY;
+        hlayout();
+        if (!hv.alloc()) return OUT_OF_MEMORY;
+        hlayout();
+        P->hblock = hv.base;
     }
     return cuda_to_info(cudaGetLastError());
 }
@@ -1284,7 +1306,6 @@ static int exec_t(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &
                 }
                 // flat product index of the chunk, then every product over the grid
                 k_heavy_alen<<<(nr + 255) / 256, 256, 0, s>>>(hrows + c0, nr, A.p, P->hlen);
-                cudaMemsetAsync(P->hlen + nr, 0, 8, s);
                 scan_exclusive_i64_ws(P->hlen, P->hoff, nr + 1, P->hw_ws, s);
                 // entries past this chunk's count stay 0 (wprefix[ne] is the total)
                 cudaMemsetAsync(P->wlen, 0, (size_t)(P->heavy_alen + 1) * 8, s);
@@ -1298,7 +1319,6 @@ static int exec_t(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &
                 dim3 g4(cblocks, nr > 65535 ? 65535 : nr);
                 k_dense_count<<<g4, DG_THREADS, 0, s>>>(nr, ncols, cblocks, flag8, P->dg_cnt);
                 const int64_t ncnt = (int64_t)nr * cblocks;
-                cudaMemsetAsync(P->dg_cnt + ncnt, 0, 8, s);
                 scan_exclusive_i64_ws(P->dg_cnt, P->dg_cnt, ncnt + 1, P->dg_ws, s);
                 k_dense_write<SR><<<g4, DG_THREADS, 0, s>>>(hrows + c0, nr, ncols, cblocks,
                     flag8, val, P->dg_cnt, P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
@@ -1314,11 +1334,8 @@ static int exec_t(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &
     }
     prof_end(ps, s);
     // exact row counts -> C row pointers, then pack the slots
-    if (m > 0) k_cnt_to_i64<<<nblocks(m, 256), 256, 0, s>>>(P->row_cnt, P->row_bin, m, P->Cp64);
-    cudaMemsetAsync(P->Cp64 + m, 0, 8, s);
-    scan_exclusive_i64_ws(P->Cp64, P->Cp64, m + 1, P->scan_ws, s);
-    k_i64_to_i32_p<<<nblocks(m + 1, 256), 256, 0, s>>>(P->Cp64, Cp, m + 1, nullptr);
-    if (Cnnz64) k_copy_i64<<<1, 32, 0, s>>>(P->Cp64 + m, Cnnz64);
+    k_cnt_to_i64<<<nblocks(m + 1, 256), 256, 0, s>>>(P->row_cnt, P->row_bin, m, P->Cp64);
+    scan_exclusive_i64_ws(P->Cp64, P->Cp64, m + 1, P->scan_ws, s, Cnnz64, Cp);
     if (m > 0 && P->total_cap > 0)
         k_pack<Z><<<nblocks(P->total_cap, 256, 16), 256, 0, s>>>(m, flat_span(P->total_cap),
             P->slot_off, P->Tj,
@@ -1390,16 +1407,15 @@ int saxpy3(DevCSR &C, const DevCSR *M, bool mask_comp, bool mask_struct,
     T.p = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
     T.j = (int32_t *)dalloc((size_t)(cap + 1) * 4, s);
     T.x = dalloc((size_t)(cap + 1) * zs, s);
-    int64_t *nnz_d = (int64_t *)dalloc(8, s);
-    if (!T.p || !T.j || !T.x || !nnz_d) {
-        dev_free(T, s); dfree(nnz_d, s); saxpy_plan_free(P, s); return OUT_OF_MEMORY;
+    int64_t *nnz_d = P->nnz_d;
+    if (!T.p || !T.j || !T.x) {
+        dev_free(T, s); saxpy_plan_free(P, s); return OUT_OF_MEMORY;
     }
     info = saxpy_plan_exec(P, M, A, B, T.p, T.j, T.x, nnz_d, s);
     int64_t nnz = 0;
     cudaMemcpyAsync(&nnz, nnz_d, 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     saxpy_plan_free(P, s);
-    dfree(nnz_d, s);
     if (info == SUCCESS && e != cudaSuccess) info = cuda_to_info(e);
     if (info != SUCCESS) { dev_free(T, s); return info; }
     if (nnz >= INT32_MAX) { dev_free(T, s); return OUT_OF_MEMORY; }
