@@ -391,9 +391,10 @@ class Bfs:
 
     def launches_per_step(self):
         # per level, the vxm (symbolic phase, flat heavy-row product index and
-        # dense row, compaction, pack) and the parent assign: 35 on average
-        # (counted on this workload's launch list)
-        return 35 * max(getattr(self, "levels", 1), 1)
+        # dense row, compaction, pack: 12 kernels plus scans) and the parent
+        # assign (5 kernels plus two scans): 26 on average (this workload's
+        # launch list counts 157 for the 6-level traversal)
+        return 26 * max(getattr(self, "levels", 1), 1)
 
     def cpu_baseline(self, R, ncores):
         parent, secs, nlev = R.bfs(self.n, self.S.p, self.S.i, self.src)

@@ -365,6 +365,54 @@ k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin, int tpr_log2, int 
 // so every semiring, floating PLUS included, gives the same bits.
 static constexpr int ESC_WARPS = 8;
 
+// Bitonic sort of a warp's n <= 32*R keys in registers: element e = 32*r +
+// lane sits in k[r]; compare-exchanges with strides of 32 or more stay inside
+// a lane, shorter ones go through shuffles.  Keys past n sort as all ones.
+// The keys are read from and written back to key[0..n).
+template <int R, typename KT>
+__device__ __forceinline__ void warp_sort_regs(KT *key, int n, int lane)
+{
+    KT k[R];
+    #pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int e = r * 32 + lane;
+        k[r] = e < n ? key[e] : ~(KT)0;
+    }
+    #pragma unroll
+    for (int size = 2; size <= 32 * R; size <<= 1) {
+        #pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            if (stride >= 32) {
+                const int rs = stride >> 5;
+                #pragma unroll
+                for (int r = 0; r < R; r++) {
+                    if (r & rs) continue;
+                    const int r2 = r | rs;
+                    const bool up = ((r * 32 + lane) & size) == 0;
+                    const KT a = k[r], b = k[r2];
+                    const KT lo = a < b ? a : b, hi = a < b ? b : a;
+                    k[r] = up ? lo : hi;
+                    k[r2] = up ? hi : lo;
+                }
+            } else {
+                #pragma unroll
+                for (int r = 0; r < R; r++) {
+                    const KT other = __shfl_xor_sync(0xffffffffu, k[r], stride);
+                    const bool up = ((r * 32 + lane) & size) == 0;
+                    const bool lower = (lane & stride) == 0;
+                    k[r] = (lower == up) ? (k[r] < other ? k[r] : other)
+                                         : (k[r] < other ? other : k[r]);
+                }
+            }
+        }
+    }
+    #pragma unroll
+    for (int r = 0; r < R; r++) {
+        const int e = r * 32 + lane;
+        if (e < n) key[e] = k[r];
+    }
+}
+
 // KT: 32-bit keys when (column << posb) fits, else 64-bit; posb = log2(cap)
 // bits hold the product's position, so only the keys move in the sort and
 // the values stay where the expansion wrote them.
@@ -468,6 +516,15 @@ k_saxpy_esc(const int32_t *__restrict__ rows, int nrows_bin, int cap, int posb,
             }
             if (lane < n) key[lane] = kk;
             n2 = 0;                                  // the shared-memory network is skipped
+        } else if (n <= 64) {
+            warp_sort_regs<2>(key, n, lane);
+            n2 = 0;
+        } else if (n <= 128) {
+            warp_sort_regs<4>(key, n, lane);
+            n2 = 0;
+        } else if (n <= 256) {
+            warp_sort_regs<8>(key, n, lane);
+            n2 = 0;
         }
         for (int q = n + lane; q < n2; q += 32) key[q] = ~(KT)0;
         __syncwarp();
