@@ -417,7 +417,7 @@ __device__ __forceinline__ void warp_sort_regs(KT *key, int n, int lane)
 // bits hold the product's position, so only the keys move in the sort and
 // the values stay where the expansion wrote them.
 template <class SR, typename KT>
-__global__ void __launch_bounds__(ESC_WARPS * 32, 4)
+__global__ void __launch_bounds__(ESC_WARPS * 32, 6)
 k_saxpy_esc(const int32_t *__restrict__ rows, int nrows_bin, int cap, int posb,
             const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
             const void *__restrict__ Ax, bool a_iso,
