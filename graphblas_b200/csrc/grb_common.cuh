@@ -234,6 +234,27 @@ __device__ __forceinline__ int32_t lower_bound(const int32_t *a, int32_t lo,
     return lo;
 }
 
+// the largest r in [0, n] with a[r] <= key (a nondecreasing, a[0] <= key),
+// found by the 32 lanes of a warp together: each step probes 32 evenly
+// spaced entries at once and keeps the gap that holds key, so a million
+// entries take four dependent loads instead of twenty.  All lanes call it
+// with the same arguments and get the same result.
+template <typename T, typename I>
+__device__ __forceinline__ I warp_last_le(const T *__restrict__ a, I n, T key, int lane)
+{
+    I lo = 0, hi = n;                              // a[lo] <= key; the answer is in [lo, hi]
+    while (lo < hi) {
+        const I step = (hi - lo + 31) / 32;
+        const I p = lo + (I)(lane + 1) * step;
+        const bool le = p <= hi && a[p] <= key;
+        const int k = __popc(__ballot_sync(0xffffffffu, le));
+        const I nhi = lo + (I)(k + 1) * step - 1;
+        lo = lo + (I)k * step;
+        hi = nhi < hi ? nhi : hi;
+    }
+    return lo;
+}
+
 // first position p in [lo,hi) with a[p] > key
 __device__ __forceinline__ int32_t upper_bound(const int32_t *a, int32_t lo,
                                                int32_t hi, int32_t key)

@@ -85,27 +85,6 @@ struct __align__(32) D3Work { int32_t pm, i, j, a0, a1, b0, b1, pad; };
 // launch 1: classify
 // ---------------------------------------------------------------------------
 
-// the row r with Mp[r] <= e < Mp[r+1] (the last such r over empty rows),
-// found by all 32 lanes together: each step probes 32 evenly spaced row
-// pointers at once and keeps the gap that holds e, so a million rows take
-// four dependent loads instead of twenty
-__device__ __forceinline__ int32_t warp_row_of(const int32_t *__restrict__ Mp, int32_t nrows,
-                                               int32_t e, int lane)
-{
-    int32_t lo = 0, hi = nrows;                    // Mp[lo] <= e; the row is in [lo, hi]
-    while (lo < hi) {
-        const int32_t step = (hi - lo + 31) / 32;
-        const int32_t p = lo + (lane + 1) * step;
-        const bool le = p <= hi && Mp[p] <= e;
-        const int k = __popc(__ballot_sync(0xffffffffu, le));
-        const int32_t nlo = lo + k * step;
-        const int32_t nhi = lo + (k + 1) * step - 1;
-        lo = nlo;
-        hi = nhi < hi ? nhi : hi;
-    }
-    return lo;
-}
-
 template <class SR>
 __global__ void __launch_bounds__(256)
 k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
@@ -128,9 +107,10 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
     for (int64_t base = warp * 32; base < mnz; base += nwarps * 32) {
         const int64_t pm = base + lane;
         const bool valid = pm < mnz;
-        // row of the chunk's first entry (a 32-ary search by the whole warp),
-        // then each lane walks forward
-        const int32_t r0 = warp_row_of(Mp, (int32_t)nrows, (int32_t)base, lane);
+        // row of the chunk's first entry (the last r with Mp[r] <= base,
+        // searched by the whole warp), then each lane walks forward
+        const int32_t r0 = warp_last_le<int32_t, int32_t>(Mp, (int32_t)nrows, (int32_t)base,
+                                                          lane);
         int32_t i = r0;
         if (valid) while (Mp[i + 1] <= pm) i++;
         int32_t j = 0, a0 = 0, a1 = 0, b0 = 0, b1 = 0, key = -1;

@@ -880,41 +880,49 @@ k_dense_atomic_flat(const int32_t *__restrict__ rows, int nr,
     const int64_t ne = hoff[nr];
     const int64_t total = wprefix[ne];
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
-         base < total; base += nw * 32) {
-        int64_t e0 = 0;
-        if (lane == 0) e0 = upper_bound64(wprefix, 0, ne + 1, base) - 1;
-        e0 = __shfl_sync(0xffffffffu, e0, 0);
-        const int64_t t = base + lane;
-        if (t >= total) continue;
-        int64_t e = e0;
-        while (wprefix[e + 1] <= t) e++;
-        const int rb = nr == 1 ? 0 : (int)(upper_bound64(hoff, 0, nr + 1, e) - 1);
-        const int32_t i = rows[rb];
-        const int32_t pa = Ap[i] + (int32_t)(e - hoff[rb]);
-        const int32_t k = Aj[pa];
-        const int32_t pb = Bp[k] + (int32_t)(t - wprefix[e]);
-        const int32_t j = Bj[pb];
-        uint8_t *flag = flag_all + (int64_t)rb * ncols;
-        Z *val = val_all + (int64_t)rb * ncols;
-        const uint8_t f = flag[j];
-        if (has_mask) {
-            if (!mask_comp && f == 0) continue;
-            if (mask_comp && f == 2) continue;
-        }
-        Z a = Z(), b = Z();
-        if (SR::needs_a) a = ld_val<Z>(Ax, pa, a_iso);
-        if (SR::needs_b) b = ld_val<Z>(Bx, pb, b_iso);
-        const Z tv = SR::F::f(a, b, i, k, j);
-        if constexpr (idem) {
-            if (f == 3) {
-                if (SR::any_const) continue;
-                const Z cur = val[j];
-                if (SR::M::any ? !(tv > cur) : (SR::M::update(cur, tv) == cur)) continue;
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    // each warp takes spans of consecutive products (about two per warp,
+    // 32 to 1024 long): the A entry of a span's first product is searched
+    // once, and every later step of 32 starts from the previous step's last
+    int64_t span = (total + 2 * nw - 1) / (2 * nw);
+    span = (span + 31) & ~(int64_t)31;
+    span = span < 32 ? 32 : (span > 1024 ? 1024 : span);
+    for (int64_t s0 = wid * span; s0 < total; s0 += nw * span) {
+        const int64_t s1 = s0 + span < total ? s0 + span : total;
+        int64_t e0 = warp_last_le<int64_t, int64_t>(wprefix, ne, s0, lane);
+        for (int64_t base = s0; base < s1; base += 32) {
+            const int64_t t = base + lane;
+            int64_t e = e0;
+            if (t < s1) while (wprefix[e + 1] <= t) e++;
+            e0 = __shfl_sync(0xffffffffu, e, 31);      // the next step's first entry
+            if (t >= s1) continue;
+            const int rb = nr == 1 ? 0 : (int)(upper_bound64(hoff, 0, nr + 1, e) - 1);
+            const int32_t i = rows[rb];
+            const int32_t pa = Ap[i] + (int32_t)(e - hoff[rb]);
+            const int32_t k = Aj[pa];
+            const int32_t pb = Bp[k] + (int32_t)(t - wprefix[e]);
+            const int32_t j = Bj[pb];
+            uint8_t *flag = flag_all + (int64_t)rb * ncols;
+            Z *val = val_all + (int64_t)rb * ncols;
+            const uint8_t f = flag[j];
+            if (has_mask) {
+                if (!mask_comp && f == 0) continue;
+                if (mask_comp && f == 2) continue;
             }
+            Z a = Z(), b = Z();
+            if (SR::needs_a) a = ld_val<Z>(Ax, pa, a_iso);
+            if (SR::needs_b) b = ld_val<Z>(Bx, pb, b_iso);
+            const Z tv = SR::F::f(a, b, i, k, j);
+            if constexpr (idem) {
+                if (f == 3) {
+                    if (SR::any_const) continue;
+                    const Z cur = val[j];
+                    if (SR::M::any ? !(tv > cur) : (SR::M::update(cur, tv) == cur)) continue;
+                }
+            }
+            AtomicUpd<SR::add_op, Z>::run(&val[j], tv);
+            if (f != 3) flag[j] = 3;
         }
-        AtomicUpd<SR::add_op, Z>::run(&val[j], tv);
-        if (f != 3) flag[j] = 3;
     }
 }
 
