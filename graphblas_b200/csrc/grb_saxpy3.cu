@@ -69,13 +69,11 @@ k_flops_flat(const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
     const int lane = threadIdx.x & 31;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     // each warp owns spans of `span` consecutive entries (a multiple of 32):
-    // one binary search per span, then the row carries over from one 32-entry
-    // step to the next
+    // one warp-cooperative search per span, then the row carries over from
+    // one 32-entry step to the next
     for (int64_t s0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * span;
          s0 < nnz; s0 += nw * span) {
-        int32_t r0 = 0;
-        if (lane == 0) r0 = upper_bound(Ap, 0, (int32_t)nrows + 1, (int32_t)s0) - 1;
-        r0 = __shfl_sync(0xffffffffu, r0, 0);
+        int32_t r0 = warp_last_le<int32_t, int32_t>(Ap, (int32_t)nrows, (int32_t)s0, lane);
         const int64_t s1 = s0 + span < nnz ? s0 + span : nnz;
         for (int64_t base = s0; base < s1; base += 32) {
             const int64_t e = base + lane;
@@ -1023,16 +1021,7 @@ k_pack(int64_t nrows, int span, const int64_t *__restrict__ slot_off,
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t s0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * span;
          s0 < nnz; s0 += nw * span) {
-        int64_t r0 = 0;
-        if (lane == 0) {
-            int64_t lo = 0, hi = nrows + 1;          // first r with Cp64[r] > s0
-            while (lo < hi) {
-                const int64_t mid = (lo + hi) >> 1;
-                if (Cp64[mid] <= s0) lo = mid + 1; else hi = mid;
-            }
-            r0 = lo - 1;
-        }
-        r0 = __shfl_sync(0xffffffffu, r0, 0);
+        int64_t r0 = warp_last_le<int64_t, int64_t>(Cp64, nrows, s0, lane);
         const int64_t s1 = s0 + span < nnz ? s0 + span : nnz;
         for (int64_t base = s0; base < s1; base += 32) {
             const int64_t e = base + lane;
