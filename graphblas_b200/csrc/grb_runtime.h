@@ -138,7 +138,7 @@ int scan_exclusive_i32_to_i64(const int32_t *in, int64_t *out, int64_t n,
                               cudaStream_t s);
 // allocation-free variant: ws holds scan_ws_elems(n) int64 values
 size_t scan_ws_elems(int64_t n);
-static constexpr int64_t SCAN_SINGLE_MAX = 32768;
+static constexpr int64_t SCAN_SINGLE_MAX = 8192;
 // Arrays of at most SCAN_SINGLE_MAX elements are scanned by one launch of one
 // block.  total (device, may be null) receives the sum of all n inputs;
 // out32 (may be null) receives the offsets narrowed to int32 as well.
