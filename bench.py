@@ -115,9 +115,9 @@ class ClockSampler:
 # workloads
 # ---------------------------------------------------------------------------
 
-def scan_launches(n, tile=4096, single=32768):
+def scan_launches(n, tile=4096, single=8192):
     """Kernel launches of the library's device scan of n values: one block
-    scans up to 32768 values in one launch; longer arrays take a tile-sum
+    scans up to 8192 values in one launch; longer arrays take a tile-sum
     launch and a tile-scan launch around the scan of the tile sums."""
     if n <= single:
         return 1
@@ -280,9 +280,9 @@ class Saxpy:
         return self.flops / 1e9
 
     def launches_per_step(self):
-        # flop counts, bins, slot scan, bin fill, numeric, row counts, row
-        # scan, pack: 8 (counted on this workload's launch list)
-        return 8
+        # flop counts, bins, bin fill, numeric, row counts, pack, and the scans
+        # of the slot and row offsets (n + 1 values each)
+        return 6 + 2 * scan_launches(self.n + 1)
 
     def cpu_baseline(self, R, ncores):
         t = 0.0

@@ -265,10 +265,12 @@ class BenchServe:
         return st["completed"]
 
     def launches_per_step(self):
-        # about 18 per request: a saxpy3 product or vxm step ~16-20 (symbolic
-        # phase, numeric, compaction, pack), a triangle count 5 (small graphs)
-        # to 25 (bitmap path), plus the device checksum reduction
-        return 18 * self.nreq
+        # about 14 per request (a launch list of the first 300 requests of
+        # this trace counts 4268): a saxpy3 product ~8 and an SSSP vxm step
+        # ~14 (symbolic phase, heavy-row path, compaction, pack), a triangle
+        # count 4 (small graphs) to 14 (bitmap path), plus the two-launch
+        # device checksum reduction
+        return 14 * self.nreq
 
     # the reference replays a bounded sample of the trace: its first requests,
     # with the same arrival times, through 8 host workers
