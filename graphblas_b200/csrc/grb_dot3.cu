@@ -933,8 +933,7 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
         prof_end(ps, s);
     }
     unsigned long long hz = 0;
-    cudaMemcpyAsync(&hz, zc, 8, cudaMemcpyDeviceToHost, s);
-    cudaError_t e = cudaStreamSynchronize(s);
+    cudaError_t e = readback(&hz, zc, 8, s);
     if (e != cudaSuccess) { dev_free(C, s); return cuda_to_info(e); }
     C.nzombies = (int64_t)hz;
     return SUCCESS;

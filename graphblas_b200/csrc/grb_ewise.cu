@@ -190,8 +190,7 @@ static int accum_mask_t(DevCSR &C, const DevCSR &T, const DevCSR *M, bool comp,
     scan_exclusive_i64_ws(keepT, keepT, nT + 1, ws, s, tot_d);
     scan_exclusive_i64_ws(keepC, keepC, nC + 1, ws, s, tot_d + 1);
     int64_t tot[2] = {0, 0};
-    cudaMemcpyAsync(tot, tot_d, 16, cudaMemcpyDeviceToHost, s);
-    cudaError_t e = cudaStreamSynchronize(s);
+    cudaError_t e = readback(tot, tot_d, 16, s);
     if (e != cudaSuccess) return cuda_to_info(e);
     const int64_t nR = tot[0] + tot[1];
     if (nR >= INT32_MAX) return OUT_OF_MEMORY;

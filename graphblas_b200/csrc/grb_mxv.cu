@@ -137,8 +137,7 @@ static int mxv_t(DevCSR &w, const DevCSR *mask, bool comp, const DevCSR &A,
     int info = scan_exclusive_i32_to_i64(wflag, pos, m + 1, s);
     if (info != SUCCESS) return info;
     int64_t nw = 0;
-    cudaMemcpyAsync(&nw, pos + m, 8, cudaMemcpyDeviceToHost, s);
-    cudaError_t e = cudaStreamSynchronize(s);
+    cudaError_t e = readback(&nw, pos + m, 8, s);
     if (e != cudaSuccess) return cuda_to_info(e);
     w = DevCSR();
     w.nrows = 1; w.ncols = m; w.nnz = nw; w.iso = false;

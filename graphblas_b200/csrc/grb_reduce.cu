@@ -83,8 +83,7 @@ static int reduce_t(void *out, const DevCSR &A, cudaStream_t s)
         cudaMemsetAsync(ph, 0, sizeof(int) * blocks, s);
         k_reduce_final<ADD, Z><<<1, 32, 0, s>>>(pv, ph, blocks, pv + blocks);
     }
-    cudaMemcpyAsync(out, pv + blocks, sizeof(Z), cudaMemcpyDeviceToHost, s);
-    cudaError_t e = cudaStreamSynchronize(s);
+    cudaError_t e = readback(out, pv + blocks, sizeof(Z), s);
     dfree(pv, s); dfree(ph, s);
     return cuda_to_info(e);
 }

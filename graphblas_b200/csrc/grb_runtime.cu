@@ -163,6 +163,28 @@ void dfree(void *p, cudaStream_t s)
     if (p) cudaFreeAsync(p, s);
 }
 
+// the few bytes a call reads back (bin counts, totals, zombie counts) go
+// through a page-locked buffer of the calling host thread: the copy is a
+// direct DMA instead of a staged one
+static constexpr size_t READBACK_MAX = 4096;
+
+cudaError_t readback(void *dst, const void *src, size_t bytes, cudaStream_t s)
+{
+    thread_local void *buf = nullptr;
+    if (!buf && bytes <= READBACK_MAX && cudaMallocHost(&buf, READBACK_MAX) != cudaSuccess) {
+        cudaGetLastError();
+        buf = nullptr;
+    }
+    if (!buf || bytes > READBACK_MAX) {
+        cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+        return cudaStreamSynchronize(s);
+    }
+    cudaMemcpyAsync(buf, src, bytes, cudaMemcpyDeviceToHost, s);
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) memcpy(dst, buf, bytes);
+    return e;
+}
+
 void dev_free(DevCSR &A, cudaStream_t s)
 {
     dfree(A.p, s); dfree(A.j, s); dfree(A.x, s);

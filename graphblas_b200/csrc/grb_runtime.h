@@ -50,6 +50,10 @@ bool prof_read(const char *name, double *ms, int64_t *count);
 void *dalloc(size_t bytes, cudaStream_t s);
 void dfree(void *p, cudaStream_t s);
 
+// copy `bytes` (at most a few KB) from the device after the stream's work,
+// synchronising the stream; returns its error
+cudaError_t readback(void *dst, const void *src, size_t bytes, cudaStream_t s);
+
 // host-side allocation fault injection (the reference's malloc_debug
 // counter, Source/global/GB_Global.c:83-93): when armed with n > 0, the n-th
 // following device allocation fails.  0 disarms.

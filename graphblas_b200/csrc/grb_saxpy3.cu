@@ -1206,8 +1206,7 @@ static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A
                           (int64_t *)(P->bins + 50));
     const int nb = P->cfg.nb;
     int hb[52];
-    cudaMemcpyAsync(hb, P->bins, sizeof(hb), cudaMemcpyDeviceToHost, s);
-    cudaError_t e = cudaStreamSynchronize(s);
+    cudaError_t e = readback(hb, P->bins, sizeof(hb), s);
     if (e != cudaSuccess) return cuda_to_info(e);
     for (int b = 0; b < nb + 2; b++) P->h_bins[b] = hb[b];
     int64_t total_cap = 0;
@@ -1467,8 +1466,7 @@ int saxpy3(DevCSR &C, const DevCSR *M, bool mask_comp, bool mask_struct,
     }
     info = saxpy_plan_exec(P, M, A, B, T.p, T.j, T.x, nnz_d, s);
     int64_t nnz = 0;
-    cudaMemcpyAsync(&nnz, nnz_d, 8, cudaMemcpyDeviceToHost, s);
-    cudaError_t e = cudaStreamSynchronize(s);
+    cudaError_t e = readback(&nnz, nnz_d, 8, s);
     saxpy_plan_free(P, s);
     if (info == SUCCESS && e != cudaSuccess) info = cuda_to_info(e);
     if (info != SUCCESS) { dev_free(T, s); return info; }
