@@ -77,14 +77,14 @@ __global__ void k_am_tside(int64_t m, const int32_t *__restrict__ Tp,
                            const int32_t *__restrict__ Cp, const int32_t *__restrict__ Cj,
                            const Z *__restrict__ Cx, bool c_iso,
                            const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
-                           bool comp, int accum, int64_t *__restrict__ keepT,
+                           bool comp, bool m_is_t, int accum, int64_t *__restrict__ keepT,
                            Z *__restrict__ valT)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) keepT[nT] = 0;       // the scan's last input
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nT;
          e += (int64_t)gridDim.x * blockDim.x) {
         const int32_t i = row_of(Tp, m, e), j = Tj[e];
-        const bool ok = mask_allows(Mp, Mj, comp, i, j);
+        const bool ok = m_is_t || mask_allows(Mp, Mj, comp, i, j);
         Z t = Tx[t_iso ? 0 : e];
         if (ok && accum) {
             const int32_t q = lower_bound(Cj, Cp[i], Cp[i + 1], j);
@@ -100,16 +100,20 @@ __global__ void k_am_cside(int64_t m, const int32_t *__restrict__ Cp,
                            const int32_t *__restrict__ Cj, int64_t nC,
                            const int32_t *__restrict__ Tp, const int32_t *__restrict__ Tj,
                            const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
-                           bool comp, bool replace, int accum,
+                           bool comp, bool m_is_t, bool replace, int accum,
                            int64_t *__restrict__ keepC)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) keepC[nC] = 0;       // the scan's last input
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nC;
          e += (int64_t)gridDim.x * blockDim.x) {
         const int32_t i = row_of(Cp, m, e), j = Cj[e];
-        const bool ok = mask_allows(Mp, Mj, comp, i, j);
         bool keep;
-        if (ok) {
+        if (m_is_t) {
+            // the mask is T's own pattern: one search answers both questions
+            const int32_t q = lower_bound(Tj, Tp[i], Tp[i + 1], j);
+            const bool in_t = q < Tp[i + 1] && Tj[q] == j;
+            keep = !in_t && !replace;
+        } else if (mask_allows(Mp, Mj, comp, i, j)) {
             const int32_t q = lower_bound(Tj, Tp[i], Tp[i + 1], j);
             const bool in_t = q < Tp[i + 1] && Tj[q] == j;
             keep = !in_t && accum != 0;       // Z(i,j) = C(i,j) when only C has it
@@ -183,10 +187,14 @@ static int accum_mask_t(DevCSR &C, const DevCSR &T, const DevCSR *M, bool comp,
     layout();
     struct Release { Carve &c; ~Release() { dfree(c.base, c.s); } } release{cv};
     const int32_t *Mp = M ? M->p : nullptr, *Mj = M ? M->j : nullptr;
+    // C<T> = T (a structural mask that is T itself, as in w<q> = q): every
+    // entry of T is allowed, and an entry of C is under the mask exactly
+    // when T holds it
+    const bool m_is_t = M && !comp && M->p == T.p && M->j == T.j;
     k_am_tside<Z><<<grid_n(nT), 256, 0, s>>>(m, T.p, T.j, (const Z *)T.x, T.iso, nT,
-        C.p, C.j, (const Z *)C.x, C.iso, Mp, Mj, comp, accum, keepT, valT);
+        C.p, C.j, (const Z *)C.x, C.iso, Mp, Mj, comp, m_is_t, accum, keepT, valT);
     k_am_cside<Z><<<grid_n(nC), 256, 0, s>>>(m, C.p, C.j, nC, T.p, T.j, Mp, Mj,
-        comp, replace, accum, keepC);
+        comp, m_is_t, replace, accum, keepC);
     scan_exclusive_i64_ws(keepT, keepT, nT + 1, ws, s, tot_d);
     scan_exclusive_i64_ws(keepC, keepC, nC + 1, ws, s, tot_d + 1);
     int64_t tot[2] = {0, 0};

@@ -286,3 +286,32 @@ def test_vector_extract_from_device(api):
     for v in (q, w):
         api.vfree(v)
     api.free(A)
+
+
+@pytest.mark.parametrize("accum", [None, "GrB_PLUS_INT64", "GrB_MIN_INT64"])
+@pytest.mark.parametrize("desc", [None, "GrB_DESC_S", "GrB_DESC_RS", "GrB_DESC_SC",
+                                  "GrB_DESC_RSC"])
+def test_assign_with_its_own_pattern_as_mask(api, oracle, accum, desc):
+    """w<u> = accum(w, u) with u as both mask and source (the BFS parent
+    update), against the oracle's accumulate / mask step.  Without GrB_STRUCTURE
+    the mask is u's values (about 1% of them are zero)."""
+    n = 5000
+    rng = np.random.default_rng(11)
+    wi = np.sort(rng.choice(n, 1200, replace=False)).astype(np.int64)
+    ui = np.sort(rng.choice(n, 900, replace=False)).astype(np.int64)
+    wx = rng.integers(-50, 50, len(wi)).astype(np.int64)
+    ux = rng.integers(-50, 50, len(ui)).astype(np.int64)
+    w = api.vector_from(wi, wx, 8, n)
+    u = api.vector_from(ui, ux, 8, n)
+    api.assign_all(w, u, accum, u, n, desc)
+    gi, gx = api.vector_to(w, 8)
+    replace, comp, strct = DESC_FLAGS[desc]
+    acc = {None: None, "GrB_PLUS_INT64": "PLUS", "GrB_MIN_INT64": "MIN"}[accum]
+    p1 = lambda k: np.array([0, k], np.int64)
+    want = oracle.accum_mask(1, n, (p1(len(wi)), wi, wx), (p1(len(ui)), ui, ux), 8,
+                             M=(p1(len(ui)), ui, ux, 8), mask_struct=strct,
+                             mask_comp=comp, replace=replace, accum=acc)
+    assert np.array_equal(gi, want[1]), "pattern, accum=%s desc=%s" % (accum, desc)
+    assert np.array_equal(gx, want[2]), "values, accum=%s desc=%s" % (accum, desc)
+    for v in (w, u):
+        api.vfree(v)
