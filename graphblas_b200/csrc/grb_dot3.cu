@@ -125,10 +125,22 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
                 const int32_t blo = Bj[pb0], bhi = Bj[pb1 - 1];
                 a0 = lower_bound(Aj, pa0, pa1, blo);
                 a1 = upper_bound(Aj, a0, pa1, bhi);
+                // when B's whole row will be the bitmap / hash key (it is
+                // the longer list, its span fits the bitmap and the entry is
+                // not merged here), its trimmed range is never used, so the
+                // two searches in the long row are skipped
+                const bool bkey = bm_bits && (pb1 - pb0) >= (a1 - a0) &&
+                                  (uint32_t)(bhi - blo) < bm_bits &&
+                                  (a1 - a0) + (pb1 - pb0) > D3_SMALL;
                 if (a1 > a0) {
                     const int32_t alo = Aj[a0], ahi = Aj[a1 - 1];
-                    b0 = lower_bound(Bj, pb0, pb1, alo);
-                    b1 = upper_bound(Bj, b0, pb1, ahi);
+                    if (bkey) {
+                        b0 = pb0;
+                        b1 = pb1;
+                    } else {
+                        b0 = lower_bound(Bj, pb0, pb1, alo);
+                        b1 = upper_bound(Bj, b0, pb1, ahi);
+                    }
                     if (b1 > b0) {
                         if ((a1 - a0) + (b1 - b0) <= D3_SMALL) {
                             int32_t a = a0, b = b0;
@@ -147,6 +159,9 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
                                     a++; b++;
                                 }
                             }
+                        } else if (bkey) {
+                            coop = true;
+                            if ((a1 - a0) <= (1 << 20)) key = (int32_t)nrows + j;
                         } else {
                             coop = true;
                             if (bm_bits && min(a1 - a0, b1 - b0) <= (1 << 20)) {
