@@ -123,13 +123,23 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
             const int32_t pb0 = Bp[j], pb1 = Bp[j + 1];
             if (mval && pa1 > pa0 && pb1 > pb0) {
                 const int32_t blo = Bj[pb0], bhi = Bj[pb1 - 1];
-                a0 = lower_bound(Aj, pa0, pa1, blo);
-                a1 = upper_bound(Aj, a0, pa1, bhi);
-                // when B's whole row will be the bitmap / hash key (it is
-                // the longer list, its span fits the bitmap and the entry is
-                // not merged here), its trimmed range is never used, so the
-                // two searches in the long row are skipped
-                const bool bkey = bm_bits && (pb1 - pb0) >= (a1 - a0) &&
+                // A row that will be the bitmap / hash key whole (the longer
+                // list, its column span fits the bitmap, and the entry is not
+                // merged here) needs no trimmed range: its two searches in
+                // the long row are skipped, and only the other list is
+                // trimmed, to the key row's first and last columns.  A's row
+                // is tested on the untrimmed lengths, B's after A's trim.
+                const bool akey = bm_bits && (pa1 - pa0) > (pb1 - pb0) &&
+                                  (pa1 - pa0) + (pb1 - pb0) > D3_SMALL &&
+                                  (uint32_t)(Aj[pa1 - 1] - Aj[pa0]) < bm_bits;
+                if (akey) {
+                    a0 = pa0;
+                    a1 = pa1;
+                } else {
+                    a0 = lower_bound(Aj, pa0, pa1, blo);
+                    a1 = upper_bound(Aj, a0, pa1, bhi);
+                }
+                const bool bkey = !akey && bm_bits && (pb1 - pb0) >= (a1 - a0) &&
                                   (uint32_t)(bhi - blo) < bm_bits &&
                                   (a1 - a0) + (pb1 - pb0) > D3_SMALL;
                 if (a1 > a0) {
@@ -162,6 +172,9 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
                         } else if (bkey) {
                             coop = true;
                             if ((a1 - a0) <= (1 << 20)) key = (int32_t)nrows + j;
+                        } else if (akey) {
+                            coop = true;
+                            if ((b1 - b0) <= (1 << 20)) key = i;
                         } else {
                             coop = true;
                             if (bm_bits && min(a1 - a0, b1 - b0) <= (1 << 20)) {
