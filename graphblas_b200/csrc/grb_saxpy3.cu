@@ -885,7 +885,12 @@ k_dense_atomic_flat(const int32_t *__restrict__ rows, int nr,
     int64_t span = (total + 2 * nw - 1) / (2 * nw);
     span = (span + 31) & ~(int64_t)31;
     span = span < 32 ? 32 : (span > 1024 ? 1024 : span);
-    for (int64_t s0 = wid * span; s0 < total; s0 += nw * span) {
+    const int64_t nspan = (total + span - 1) / span;
+    for (int64_t si = wid; si < nspan; si += nw) {
+        // spans are taken from the last one down: the first blocks to run
+        // carry the largest k, so an idempotent monoid (a max-k ANY) skips
+        // most later atomics; the result does not depend on the order
+        const int64_t s0 = (nspan - 1 - si) * span;
         const int64_t s1 = s0 + span < total ? s0 + span : total;
         int64_t e0 = warp_last_le<int64_t, int64_t>(wprefix, ne, s0, lane);
         for (int64_t base = s0; base < s1; base += 32) {
