@@ -168,9 +168,17 @@ void dfree(void *p, cudaStream_t s)
 // direct DMA instead of a staged one
 static constexpr size_t READBACK_MAX = 4096;
 
+// owned by its thread and released when the thread exits (worker threads of
+// a server come and go)
+struct ReadbackBuffer {
+    void *p = nullptr;
+    ~ReadbackBuffer() { if (p) cudaFreeHost(p); }
+};
+
 cudaError_t readback(void *dst, const void *src, size_t bytes, cudaStream_t s)
 {
-    thread_local void *buf = nullptr;
+    thread_local ReadbackBuffer rb;
+    void *&buf = rb.p;
     if (!buf && bytes <= READBACK_MAX && cudaMallocHost(&buf, READBACK_MAX) != cudaSuccess) {
         cudaGetLastError();
         buf = nullptr;
