@@ -305,6 +305,38 @@ int grb_b200_server_add_graph(grb_b200_server S, int kind, int64_t n, const int6
     return SUCCESS;
 }
 
+// A graph given as a serialized blob (GxB_Matrix_serialize's format, any
+// compression): decoded on the host, then uploaded as add_graph does
+int grb_b200_server_add_graph_blob(grb_b200_server S, int kind, const void *blob,
+                                   size_t blob_size, int *graph_id)
+{
+    if (!S || !blob || !graph_id) return NULL_POINTER;
+    if (kind < K_TRICOUNT || kind > K_MXM) return INVALID_VALUE;
+    const int want = kind == K_SSSP ? T_FP32 : (kind == K_MXM ? T_FP64 : 0);
+    int64_t nrows = 0, ncols = 0, *p = nullptr, *i = nullptr;
+    void *x = nullptr;
+    int type = 0;
+    bool iso = false;
+    int info = grb_b200_blob_decode(blob, blob_size, want, &nrows, &ncols, &type, &p, &i, &x,
+                                    &iso);
+    if (info != SUCCESS) return info;
+    if (nrows != ncols) info = DIMENSION_MISMATCH;
+    void *xs = x;
+    if (info == SUCCESS && want != 0 && iso) {
+        // the server's graphs hold one value per entry
+        const size_t ts = type_size(type);
+        const int64_t nnz = p[nrows];
+        xs = malloc((size_t)(nnz ? nnz : 1) * ts);
+        if (!xs) info = OUT_OF_MEMORY;
+        else for (int64_t q = 0; q < nnz; q++) memcpy((char *)xs + q * ts, x, ts);
+    }
+    if (info == SUCCESS)
+        info = grb_b200_server_add_graph(S, kind, nrows, p, i, want ? xs : nullptr, graph_id);
+    if (xs != x) free(xs);
+    free(p); free(i); free(x);
+    return info;
+}
+
 // Replay an open-loop trace: request k (kind[k] on graph[k]) arrives at
 // t_arrival[k] seconds after the call; SSSP requests take their frontier from
 // (fp[k]..fp[k+1]) of fi/fx.  Returns when every request finished.

@@ -38,7 +38,10 @@ def _bind(L):
                                         ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_double)]
     L.grb_b200_server_free.argtypes = [ctypes.POINTER(vp)]
-    for n in ("create", "add_graph", "replay", "request", "result", "stats", "free"):
+    L.grb_b200_server_add_graph_blob.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t,
+                                                  ctypes.POINTER(ctypes.c_int)]
+    for n in ("create", "add_graph", "add_graph_blob", "replay", "request", "result",
+              "stats", "free"):
         getattr(L, "grb_b200_server_" + n).restype = ctypes.c_int
     L._serve_bound = True
     return L
@@ -66,6 +69,17 @@ class Server:
                                                i.ctypes.data,
                                                None if x is None else x.ctypes.data,
                                                ctypes.byref(gid)), "server_add_graph")
+        self.kinds.append(kind)
+        return gid.value
+
+    def add_graph_blob(self, kind, blob):
+        """A resident graph from a serialized blob (GxB_Matrix_serialize's
+        format, any compression)."""
+        gid = ctypes.c_int()
+        buf = ctypes.create_string_buffer(bytes(blob), max(len(blob), 1))
+        check(self.L.grb_b200_server_add_graph_blob(self.h, kind, buf, len(blob),
+                                                    ctypes.byref(gid)),
+              "server_add_graph_blob")
         self.kinds.append(kind)
         return gid.value
 

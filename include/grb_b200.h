@@ -318,6 +318,13 @@ int grb_b200_server_add_graph(grb_b200_server S, int kind, int64_t n,
                               const int64_t *p, const int64_t *i, const void *x,
                               int *graph_id);
 
+/* The same from a serialized blob (GxB_Matrix_serialize's format: any
+ * sparsity form, raw, LZ4, LZ4HC or ZSTD; grb_b200_blob_decode reads it): a
+ * square matrix, fp32 for kind 2 and fp64 for kind 3 (GrB_DOMAIN_MISMATCH
+ * otherwise), any built-in type for kind 1 (only its pattern is used). */
+int grb_b200_server_add_graph_blob(grb_b200_server S, int kind, const void *blob,
+                                   size_t blob_size, int *graph_id);
+
 /* Open-loop replay: request k of kind[k] on graph[k] arrives t_arrival[k]
  * seconds after the call; SSSP frontiers are fi/fx[fp[k] .. fp[k+1]). */
 int grb_b200_server_replay(grb_b200_server S, int64_t nreq, const int *kind,

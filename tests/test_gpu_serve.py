@@ -110,3 +110,40 @@ def test_injected_allocation_failure_is_isolated(gpu):
     statuses = [S.request(k)["status"] for k in range(40)]
     assert statuses.count(-102) == 1
     S.free()
+
+
+def test_graphs_loaded_from_serialized_blobs(gpu):
+    """Graphs registered from serialized blobs (the library's own writer, and
+    the reference's ZSTD / LZ4 blobs where the reference is built here) serve
+    the same results as the same graphs registered from CSR arrays."""
+    from graphblas_b200 import grb
+    from graphblas_b200.serve import Server, make_trace, K_SSSP, K_MXM
+    from oracle import Reference, reference_available
+    graphs = _graphs()
+    trace = make_trace(graphs, nreq=60, rate=50000.0, seed=9)
+    R = Reference(nthreads=2) if reference_available() else None
+    csr, blob = Server(nslots=4, budget_bytes=8 << 30), Server(nslots=4, budget_bytes=8 << 30)
+    for n, (kind, g) in enumerate(graphs):
+        csr.add_graph(kind, g)
+        t = {K_SSSP: 10, K_MXM: 11}.get(kind, 1)
+        x = (np.ones(g.nnz, np.bool_) if t == 1 else
+             np.ascontiguousarray(g.x, np.float32 if t == 10 else np.float64))
+        if R is not None and n % 2 == 1:
+            b = R.serialize(t, g.nrows, g.ncols, g.p, g.i, x, 2, n % 4 == 1,
+                            1000 if n % 3 == 0 else 0)
+        else:
+            b = grb.blob_encode(g.nrows, g.ncols, t, g.p, g.i, x)
+        blob.add_graph_blob(kind, b)
+    for S in (csr, blob):
+        S.replay(trace)
+        assert S.stats()["completed"] == 60
+    for k in range(60):
+        a, b = csr.request(k), blob.request(k)
+        assert a["status"] == 0 and b["status"] == 0
+        assert a["count"] == b["count"] and a["checksum"] == b["checksum"]
+    with pytest.raises(RuntimeError):
+        g = graphs[0][1]
+        wrong = grb.blob_encode(g.nrows, g.ncols, 8, g.p, g.i, np.ones(g.nnz, np.int64))
+        blob.add_graph_blob(K_MXM, wrong)              # an int64 blob for an fp64 kind
+    for S in (csr, blob):
+        S.free()
