@@ -465,6 +465,21 @@ def run_reference(args, cfg):
     return 0
 
 
+def pin_rank_gpu():
+    """One GPU per rank: under torchrun (WORLD_SIZE > 1) each process sees
+    only its own GPU, chosen before CUDA starts, so torch and the library
+    (which carries its own CUDA runtime) agree on device 0.  Returns the CUDA
+    device index to use and the GPU's index for nvidia-smi."""
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    ids = [v.strip() for v in vis.split(",") if v.strip()] if vis else None
+    physical = ids[local] if ids and local < len(ids) else str(local)
+    if int(os.environ.get("WORLD_SIZE", "1")) <= 1:
+        return local, physical
+    os.environ["CUDA_VISIBLE_DEVICES"] = physical
+    return 0, physical
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -483,13 +498,13 @@ def main():
     if args.impl == "reference":
         return run_reference(args, cfg)
 
+    device, smi_index = pin_rank_gpu()
     import torch
     import graphblas_b200 as gb
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
+    torch.cuda.set_device(device)
     dist = None
     if world > 1:
         import datetime
@@ -530,7 +545,7 @@ def main():
         for _ in range(args.warmup):
             work.step_dev()
     barrier()
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(smi_index)
     sampler.start()
     units, dev_ms = timed(work.step_dev, args.steps, profile_kernel=work.kernel)
     clocks = sampler.stop()
