@@ -529,10 +529,13 @@ __global__ void k_d3_item_fill(const int64_t *__restrict__ ioff, int64_t nkeys,
         const int32_t lo = by_row ? Aj[rp0] : Bj[rp0];
         const int32_t hi = by_row ? Aj[rp1 - 1] : Bj[rp1 - 1];
         const int64_t g0 = goff[t], gn = goff[t + 1] - g0;
-        // lanes per entry: a power of two near half the mean list length
+        // lanes per entry: a power of two near an eighth of the mean list
+        // length, so a lane's D3_PROBE_UNROLL loads are mostly in use and
+        // short lists of a skewed group leave few lanes idle (half and a
+        // quarter of the mean, and a sixteenth, measured slower)
         const unsigned long long mean = gwork[t] / (unsigned long long)gn;
         int lg = 0;
-        while (lg < 5 && (2ull << lg) < mean) lg++;
+        while (lg < 5 && (8ull << lg) < mean) lg++;
         for (int64_t q = 0; q < n; q++)
             items[o + q] = D3Item{(int32_t)t, (int32_t)q, (int32_t)n,
                                   (int32_t)((gn - q + n - 1) / n), rp0, rp1, lo, lg, g0,
