@@ -51,7 +51,7 @@
 
 namespace grb {
 
-static constexpr int D3_SMALL = 32;        // per-lane merge threshold (nA+nB)
+static constexpr int D3_SMALL = 64;        // per-lane merge threshold (nA+nB)
 static constexpr int D3_BATCH = 8;         // queue entries taken per grab
 
 __device__ __forceinline__ bool mask_value_true(const void *Mx, int mtype,
@@ -385,14 +385,14 @@ k_dot3_intersect(const D3Work *__restrict__ queue, const int32_t *__restrict__ s
 // on the merge path.
 // ---------------------------------------------------------------------------
 
-static constexpr int D3_GMIN = 16;             // smallest group worth a bitmap
+static constexpr int D3_GMIN = 8;              // smallest group worth a bitmap
 static constexpr int64_t D3_WCHUNK = 1 << 20;  // probes per bitmap work item
 static constexpr int D3_HKEY = 256;             // key rows up to this long: warp hash
 static constexpr int D3_HSLOTS = 512;           // slots of a warp's hash table
 static constexpr int64_t D3_HCHUNK = 1 << 16;   // probes per warp-hash work item
 static constexpr int D3_HWARPS = 8;             // warps (tables) per hash block
 static constexpr int D3_BM_THREADS = 1024;
-static constexpr int D3_LONG = 2048;          // longer lists go to the shared table
+static constexpr int D3_LONG = 4096;          // longer lists go to the shared table
 static constexpr int D3_PROBE_UNROLL = 4;     // probe loads in flight per lane
 static constexpr int D3_SEG = 512;            // probes per shared long-list segment
 static constexpr int D3_TABLE = 1024;         // long lists registered per item
