@@ -96,27 +96,31 @@ def test_dot3_long_rows(gpu, oracle):
     assert_exact(got, want, "dot3 long rows")
 
 
-@pytest.mark.parametrize("tname,np_t", [("int64", np.int64), ("int32", np.int32)])
-def test_dot3_count_bitmap_and_merge_mix(gpu, oracle, tname, np_t):
+@pytest.mark.parametrize("tname,np_t,alen,blen", [
+    ("int64", np.int64, 400, 400), ("int32", np.int32, 400, 400),
+    ("int64", np.int64, 3000, 80),        # A's rows the longer list: kept whole as keys
+    ("int64", np.int64, 80, 3000)])       # B's rows the longer list
+def test_dot3_count_bitmap_and_merge_mix(gpu, oracle, tname, np_t, alen, blen):
     """PLUS_PAIR on a mask large enough for the bitmap path, with rows whose
     column span fits the shared-memory bitmap (grouped) and rows spanning
-    4M columns (left on the merge path), long and short lists, empty rows."""
+    4M columns (left on the merge path), long and short lists, empty rows;
+    list lengths up to alen (A) and blen (B)."""
     gb = gpu
     m, n, k = 3000, 2500, 4_000_000
 
-    def rows(nr, seed):
+    def rows(nr, seed, maxlen):
         r = np.random.default_rng(seed)
         p = [0]
         idx = []
         for q in range(nr):
-            ln = int(r.integers(0, 400)) if q % 11 else 0
+            ln = int(r.integers(0, maxlen)) if q % 11 else 0
             hi = k if q % 2 else 60_000          # wide or narrow column span
             c = np.unique(r.integers(0, hi, ln))
             idx.append(c)
             p.append(p[-1] + len(c))
         return W.Csr(nr, k, np.array(p, np.int64), np.concatenate(idx).astype(np.int64),
                      np.ones(p[-1], np_t))
-    A, B = rows(m, 1), rows(n, 2)
+    A, B = rows(m, 1, alen), rows(n, 2, blen)
     M = random_csr(m, n, 0.03, 3, np.bool_)
     M.x = None
     assert M.nnz >= 1 << 16
