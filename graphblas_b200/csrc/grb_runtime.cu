@@ -168,20 +168,38 @@ void dfree(void *p, cudaStream_t s)
 // direct DMA instead of a staged one
 static constexpr size_t READBACK_MAX = 4096;
 
-// owned by its thread and released when the thread exits (worker threads of
-// a server come and go)
+// A thread takes a buffer from a shared pool on first use and puts it back
+// when it exits, so the worker threads a server starts for each replay reuse
+// the same few buffers (page-locking memory, and unlocking it, is slow).
+static std::mutex g_rb_mu;
+static std::vector<void *> g_rb_pool;
+
 struct ReadbackBuffer {
     void *p = nullptr;
-    ~ReadbackBuffer() { if (p) cudaFreeHost(p); }
+    ~ReadbackBuffer() {
+        if (p) {
+            std::lock_guard<std::mutex> lk(g_rb_mu);
+            g_rb_pool.push_back(p);
+        }
+    }
 };
 
 cudaError_t readback(void *dst, const void *src, size_t bytes, cudaStream_t s)
 {
     thread_local ReadbackBuffer rb;
     void *&buf = rb.p;
-    if (!buf && bytes <= READBACK_MAX && cudaMallocHost(&buf, READBACK_MAX) != cudaSuccess) {
-        cudaGetLastError();
-        buf = nullptr;
+    if (!buf && bytes <= READBACK_MAX) {
+        {
+            std::lock_guard<std::mutex> lk(g_rb_mu);
+            if (!g_rb_pool.empty()) {
+                buf = g_rb_pool.back();
+                g_rb_pool.pop_back();
+            }
+        }
+        if (!buf && cudaMallocHost(&buf, READBACK_MAX) != cudaSuccess) {
+            cudaGetLastError();
+            buf = nullptr;
+        }
     }
     if (!buf || bytes > READBACK_MAX) {
         cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
