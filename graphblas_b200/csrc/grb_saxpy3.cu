@@ -879,10 +879,10 @@ k_dense_atomic_flat(const int32_t *__restrict__ rows, int nr,
     const int64_t total = wprefix[ne];
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    // each warp takes spans of consecutive products (about two per warp,
+    // each warp takes spans of consecutive products (about four per warp,
     // 32 to 1024 long): the A entry of a span's first product is searched
     // once, and every later step of 32 starts from the previous step's last
-    int64_t span = (total + 2 * nw - 1) / (2 * nw);
+    int64_t span = (total + 4 * nw - 1) / (4 * nw);
     span = (span + 31) & ~(int64_t)31;
     span = span < 32 ? 32 : (span > 1024 ? 1024 : span);
     const int64_t nspan = (total + span - 1) / span;
@@ -1370,7 +1370,7 @@ static int exec_t(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &
                 k_heavy_blen<<<nblocks(P->heavy_alen, 256, 8), 256, 0, s>>>(hrows + c0, nr,
                     P->hoff, A.p, A.j, B.p, P->wlen);
                 scan_exclusive_i64_ws(P->wlen, P->wprefix, P->heavy_alen + 1, P->hw_ws, s);
-                k_dense_atomic_flat<SR><<<runtime().num_sms * 16, 256, 0, s>>>(hrows + c0, nr,
+                k_dense_atomic_flat<SR><<<runtime().num_sms * 32, 256, 0, s>>>(hrows + c0, nr,
                     P->hoff, P->wprefix, A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
                     M != nullptr, P->mask_comp, ncols, flag8, val);
                 const int cblocks = (int)((ncols + DG_CHUNK - 1) / DG_CHUNK);
