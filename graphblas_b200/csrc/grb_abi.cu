@@ -25,7 +25,10 @@ using namespace grb;
 static grb_b200_malloc_fn g_malloc = malloc;
 static grb_b200_free_fn g_free = free;
 
-struct grb_b200_dmatrix_s { DevCSR A; };
+// A device matrix.  sum_ok: `sum` is the PLUS reduction of its live entries,
+// computed by the kernels that produced it (the counting dot3 path); every
+// entry point that changes the matrix in place clears it.
+struct grb_b200_dmatrix_s { DevCSR A; bool sum_ok = false; int64_t sum = 0; };
 
 namespace {
 
@@ -374,8 +377,15 @@ int grb_b200_dmxm_dot3(grb_b200_dmatrix *C, grb_b200_dmatrix M, bool mask_struct
     StreamGuard g;
     grb_b200_dmatrix h = new grb_b200_dmatrix_s();
     SemiringCode sc{sr->add_opcode, sr->mult_opcode, sr->type};
-    int info = dot3(h->A, M->A, mask_struct, A->A, B->A, sc, g.s);
+    int64_t live = 0;
+    int info = dot3(h->A, M->A, mask_struct, A->A, B->A, sc, g.s, &live);
     if (info != SUCCESS) { delete h; return info; }
+    // the counting semirings (PLUS_PAIR on integers) bring C's sum along
+    const bool counting = sr->add_opcode == OP_PLUS && sr->mult_opcode == OP_PAIR &&
+        (sr->type == T_INT32 || sr->type == T_UINT32 || sr->type == T_INT64 ||
+         sr->type == T_UINT64);
+    h->sum_ok = counting;
+    h->sum = live;
     *C = h;
     return SUCCESS;
 }
@@ -398,6 +408,19 @@ int grb_b200_dmxm_saxpy3(grb_b200_dmatrix *C, grb_b200_dmatrix M, bool mask_comp
 int grb_b200_dreduce(void *out, grb_b200_dmatrix D, int monoid_opcode)
 {
     if (!out || !D) return NULL_POINTER;
+    if (D->sum_ok && monoid_opcode == OP_PLUS) {
+        // the sum the producing kernels accumulated, wrapped to the type as
+        // the reduction's own integer adds would wrap
+        switch (D->A.type) {
+            case T_INT64: case T_UINT64: memcpy(out, &D->sum, 8); return SUCCESS;
+            case T_INT32: case T_UINT32: {
+                const uint32_t v = (uint32_t)(uint64_t)D->sum;
+                memcpy(out, &v, 4);
+                return SUCCESS;
+            }
+            default: break;
+        }
+    }
     StreamGuard g;
     return reduce_scalar(out, D->A, monoid_opcode, g.s);
 }
@@ -452,6 +475,7 @@ int grb_b200_daccum_mask(grb_b200_dmatrix C, grb_b200_dmatrix T, grb_b200_dmatri
 {
     if (!C || !T) return NULL_POINTER;
     StreamGuard g;
+    C->sum_ok = false;
     int info = accum_mask(C->A, T->A, M ? &M->A : nullptr, mask_comp, mask_struct,
                           replace, accum_opcode, g.s);
     cudaError_t e = cudaStreamSynchronize(g.s);

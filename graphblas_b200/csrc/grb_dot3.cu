@@ -78,6 +78,13 @@ combine(Part<typename SR::z_t> a, Part<typename SR::z_t> b)
     return {SR::M::add(a.v, b.v), true};
 }
 
+// counting semirings: PLUS_PAIR on integers (C(i,j) = |A(i,:) and B(j,:)|)
+template <class SR> struct IsCount {
+    static constexpr bool value = SR::add_op == OP_PLUS && SR::mult_op == OP_PAIR &&
+        std::is_integral<typename SR::z_t>::value &&
+        !std::is_same<typename SR::z_t, bool>::value;
+};
+
 // queued entry: mask position, row, column, trimmed ranges (absolute)
 struct __align__(32) D3Work { int32_t pm, i, j, a0, a1, b0, b1, pad; };
 
@@ -97,13 +104,13 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
                 int32_t *__restrict__ Cj, typename SR::z_t *__restrict__ Cx,
                 D3Work *__restrict__ queue, int *__restrict__ qlen,
                 unsigned long long *__restrict__ nzombies,
-                int32_t *__restrict__ gcnt, uint32_t bm_bits)
+                unsigned long long *__restrict__ out_sum)
 {
     using Z = typename SR::z_t;
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    unsigned long long zcount = 0;
+    unsigned long long zcount = 0, lsum = 0;
     for (int64_t base = warp * 32; base < mnz; base += nwarps * 32) {
         const int64_t pm = base + lane;
         const bool valid = pm < mnz;
@@ -113,7 +120,7 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
                                                           lane);
         int32_t i = r0;
         if (valid) while (Mp[i + 1] <= pm) i++;
-        int32_t j = 0, a0 = 0, a1 = 0, b0 = 0, b1 = 0, key = -1;
+        int32_t j = 0, a0 = 0, a1 = 0, b0 = 0, b1 = 0;
         bool coop = false, exists = false;
         Z cij = Z();
         if (valid) {
@@ -123,34 +130,12 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
             const int32_t pb0 = Bp[j], pb1 = Bp[j + 1];
             if (mval && pa1 > pa0 && pb1 > pb0) {
                 const int32_t blo = Bj[pb0], bhi = Bj[pb1 - 1];
-                // A row that will be the bitmap / hash key whole (the longer
-                // list, its column span fits the bitmap, and the entry is not
-                // merged here) needs no trimmed range: its two searches in
-                // the long row are skipped, and only the other list is
-                // trimmed, to the key row's first and last columns.  A's row
-                // is tested on the untrimmed lengths, B's after A's trim.
-                const bool akey = bm_bits && (pa1 - pa0) > (pb1 - pb0) &&
-                                  (pa1 - pa0) + (pb1 - pb0) > D3_SMALL &&
-                                  (uint32_t)(Aj[pa1 - 1] - Aj[pa0]) < bm_bits;
-                if (akey) {
-                    a0 = pa0;
-                    a1 = pa1;
-                } else {
-                    a0 = lower_bound(Aj, pa0, pa1, blo);
-                    a1 = upper_bound(Aj, a0, pa1, bhi);
-                }
-                const bool bkey = !akey && bm_bits && (pb1 - pb0) >= (a1 - a0) &&
-                                  (uint32_t)(bhi - blo) < bm_bits &&
-                                  (a1 - a0) + (pb1 - pb0) > D3_SMALL;
+                a0 = lower_bound(Aj, pa0, pa1, blo);
+                a1 = upper_bound(Aj, a0, pa1, bhi);
                 if (a1 > a0) {
                     const int32_t alo = Aj[a0], ahi = Aj[a1 - 1];
-                    if (bkey) {
-                        b0 = pb0;
-                        b1 = pb1;
-                    } else {
-                        b0 = lower_bound(Bj, pb0, pb1, alo);
-                        b1 = upper_bound(Bj, b0, pb1, ahi);
-                    }
+                    b0 = lower_bound(Bj, pb0, pb1, alo);
+                    b1 = upper_bound(Bj, b0, pb1, ahi);
                     if (b1 > b0) {
                         if ((a1 - a0) + (b1 - b0) <= D3_SMALL) {
                             int32_t a = a0, b = b0;
@@ -169,32 +154,19 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
                                     a++; b++;
                                 }
                             }
-                        } else if (bkey) {
-                            coop = true;
-                            if ((a1 - a0) <= (1 << 20)) key = (int32_t)nrows + j;
-                        } else if (akey) {
-                            coop = true;
-                            if ((b1 - b0) <= (1 << 20)) key = i;
                         } else {
                             coop = true;
-                            if (bm_bits && min(a1 - a0, b1 - b0) <= (1 << 20)) {
-                                // bitmap of the longer list's whole row, if
-                                // its column span fits the bitmap (probed
-                                // lists of at most 2^20 keep the bitmap
-                                // kernel's per-round probe sums in int32)
-                                if ((a1 - a0) > (b1 - b0)) {
-                                    if ((uint32_t)(Aj[pa1 - 1] - Aj[pa0]) < bm_bits) key = i;
-                                } else if ((uint32_t)(bhi - blo) < bm_bits) {
-                                    key = (int32_t)nrows + j;
-                                }
-                            }
                         }
                     }
                 }
             }
             if (!coop) {
-                if (exists) { Cj[pm] = j; Cx[pm] = cij; }
-                else { Cj[pm] = flip(j); zcount++; }
+                if (exists) {
+                    Cj[pm] = j; Cx[pm] = cij;
+                    if constexpr (IsCount<SR>::value) lsum += (unsigned long long)cij;
+                } else {
+                    Cj[pm] = flip(j); zcount++;
+                }
             }
         }
         // warp-aggregated append of the long entries
@@ -205,21 +177,16 @@ k_dot3_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
             qbase = __shfl_sync(0xffffffffu, qbase, 0);
             if (coop) {
                 const int slot = qbase + __popc(q & ((1u << lane) - 1));
-                queue[slot] = D3Work{(int32_t)pm, i, j, a0, a1, b0, b1, key};
-            }
-        }
-        if (bm_bits) {
-            // group sizes, one atomic per distinct key in the warp
-            const bool grouped = coop && key >= 0;
-            const unsigned gm = __ballot_sync(0xffffffffu, grouped);
-            if (grouped) {
-                const unsigned same = __match_any_sync(gm, key);
-                if ((int)(__ffs(same) - 1) == lane) atomicAdd(&gcnt[key], __popc(same));
+                queue[slot] = D3Work{(int32_t)pm, i, j, a0, a1, b0, b1, 0};
             }
         }
     }
-    for (int o = 16; o > 0; o >>= 1) zcount += __shfl_down_sync(0xffffffffu, zcount, o);
+    for (int o = 16; o > 0; o >>= 1) {
+        zcount += __shfl_down_sync(0xffffffffu, zcount, o);
+        lsum += __shfl_down_sync(0xffffffffu, lsum, o);
+    }
     if (lane == 0 && zcount) atomicAdd(nzombies, zcount);
+    if (lane == 0 && lsum && out_sum) atomicAdd(out_sum, lsum);
 }
 
 // ---------------------------------------------------------------------------
@@ -255,12 +222,13 @@ k_dot3_intersect(const D3Work *__restrict__ queue, const int32_t *__restrict__ s
                  const int32_t *__restrict__ Aj, const void *__restrict__ Ax, bool a_iso,
                  const int32_t *__restrict__ Bj, const void *__restrict__ Bx, bool b_iso,
                  int32_t *__restrict__ Cj, typename SR::z_t *__restrict__ Cx,
-                 unsigned long long *__restrict__ nzombies)
+                 unsigned long long *__restrict__ nzombies,
+                 unsigned long long *__restrict__ out_sum)
 {
     using Z = typename SR::z_t;
     const int lane = threadIdx.x & 31;
     const int qlen = *qlen_p;
-    unsigned long long zcount = 0;
+    unsigned long long zcount = 0, lsum = 0;
     while (true) {
         int w0 = 0;
         if (lane == 0) w0 = atomicAdd(qnext, D3_BATCH);
@@ -363,481 +331,649 @@ k_dot3_intersect(const D3Work *__restrict__ queue, const int32_t *__restrict__ s
                 acc_has = part.has;
             }
             if (lane == 0) {
-                if (acc_has) { Cj[e.pm] = e.j; Cx[e.pm] = acc; }
-                else { Cj[e.pm] = flip(e.j); zcount++; }
+                if (acc_has) {
+                    Cj[e.pm] = e.j; Cx[e.pm] = acc;
+                    if constexpr (IsCount<SR>::value) lsum += (unsigned long long)acc;
+                } else {
+                    Cj[e.pm] = flip(e.j); zcount++;
+                }
             }
         }
     }
     if (lane == 0 && zcount) atomicAdd(nzombies, zcount);
+    if (lane == 0 && lsum && out_sum) atomicAdd(out_sum, lsum);
 }
 
 // ---------------------------------------------------------------------------
-// bitmap path for counting semirings (PLUS_PAIR on integers: triangle and
-// support counts)
+// counting path: PLUS_PAIR on integers (triangle and support counts)
 //
-// A long entry is intersected by probing the elements of its shorter list in
-// a shared-memory bitmap of its longer list's whole row, so the longer list
-// is read once per group of entries sharing it instead of once per entry:
-// entries whose A(i,:) is longer are grouped by i, those whose B(j,:) is
-// longer by j (key nrows + j).  The result of PLUS_PAIR is the number of
-// matches, which needs neither values nor an order.  Groups with fewer than
-// D3_GMIN entries, and rows whose column span does not fit the bitmap, stay
-// on the merge path.
+// C(i,j) is the number of columns A(i,:) and B(j,:) share.  Every live entry
+// is intersected by probing the elements of one of its two lists in a
+// shared-memory structure built from the other, its "key" row, and the
+// entries sharing a key row form a group that builds the structure once:
+//
+//   classify  one lane per mask entry: empty lists make a zombie at once;
+//             otherwise the longer of A(i,:) and B(j,:) (by row length, no
+//             search) becomes the key - row i of A (key i) or row j of B (key
+//             nrows + j) - and the entry takes a rank in its group (one
+//             warp-aggregated atomic per key).  queue[pm] holds the key, the
+//             rank and the probed row's offsets.
+//   plan      one single-pass scan (decoupled look-back) over the keys: work
+//             items of at most CT_ITEM_* entries for every non-empty group,
+//             key rows longer than CT_BM_KEY for the block-bitmap kernel and
+//             the others for the warp-hash kernel; offsets of the B-keyed
+//             groups' buckets.
+//   route     B-keyed entries scattered to their buckets (A-keyed groups are
+//             a subset of a mask row and are read in place); entries whose
+//             key row spans more columns than the bitmap holds go to the
+//             merge kernel above.
+//   hash      one warp per item: the key row in an open-addressing table of
+//             the warp's own shared memory.
+//   bitmap    one 1024-thread block per SM: the key row as a shared-memory
+//             bitmap over its column span.
+//
+// Inside an item a warp takes 32 entries at a time; an entry's list is
+// probed by the whole warp (lists over 128), by 8 lanes (over 16) or by 2
+// lanes, four elements per lane per step with 16-byte loads.  A list is
+// trimmed to the key row's first column by a search of its group's lanes,
+// and its probing stops at the first step past the key row's last column.
+// The hit count is C(i,j); its sum over the live entries and the zombie count
+// come back with the call, so a following sum reduction of C needs no pass.
 // ---------------------------------------------------------------------------
 
-static constexpr int D3_GMIN = 8;              // smallest group worth a bitmap
-static constexpr int64_t D3_WCHUNK = 1 << 20;  // probes per bitmap work item
-static constexpr int D3_HKEY = 256;             // key rows up to this long: warp hash
-static constexpr int D3_HSLOTS = 512;           // slots of a warp's hash table
-static constexpr int64_t D3_HCHUNK = 1 << 16;   // probes per warp-hash work item
-static constexpr int D3_HWARPS = 8;             // warps (tables) per hash block
-static constexpr int D3_BM_THREADS = 1024;
-static constexpr int D3_LONG = 4096;          // longer lists go to the shared table
-static constexpr int D3_PROBE_UNROLL = 4;     // probe loads in flight per lane
-static constexpr int D3_SEG = 512;            // probes per shared long-list segment
-static constexpr int D3_TABLE = 1024;         // long lists registered per item
+static constexpr int CT_BM_KEY = 1024;       // longer key rows: block bitmap
+static constexpr int CT_H_SLOTS = 2048;      // slots of a warp's hash table
+static constexpr int CT_H_WARPS = 8;         // warps (tables) per hash block
+static constexpr int CT_BM_THREADS = 1024;
+static constexpr int CT_ITEM_BM = 2048;      // entries per bitmap item, at most
+static constexpr int CT_ITEM_H = 1024;       // entries per hash item, at most
+static constexpr int CT_TILE_T = 256;        // plan: threads per tile
+static constexpr int CT_TILE_K = 8;          // plan: keys per thread
+static constexpr int CT_TILE = CT_TILE_T * CT_TILE_K;
+static constexpr int CT_MERGE = -2;          // queue key of an entry for the merge kernel
+static constexpr int CT_LONG = 128;          // lists above: the whole warp
+static constexpr int CT_MID = 16;            // lists above (up to CT_LONG): 8 lanes
+static constexpr int64_t CT_MIN_ENTRIES = 1024;
 
-// a grouped entry as the bitmap kernel reads it: its probed list and where
-// its result goes
-struct __align__(16) D3Rec { int32_t s0, len, pm, j; };
+// per mask entry: group key (-1: done, CT_MERGE: merge kernel), rank in the
+// group, the probed row's first offset and length
+struct __align__(16) CtQ { int32_t key, rank, s0, len; };
+// a B-keyed entry in its group's bucket
+struct __align__(16) CtRec { int32_t s0, len, pm, pad; };
+// a work item: entries [e0, e1) of key's group (mask positions of row key
+// for A-keys, bucket positions for B-keys); the key row's offsets and its
+// first and last column
+struct __align__(16) CtItem { int32_t key, e0, e1, rp0, rp1, klo, khi, pad; };
 
-// a work item: every nit-th entry of key's group, from the t-th; its key row
-// (offsets rp0..rp1, first column lo) and lanes per entry 2^lg
-struct __align__(16) D3Item { int32_t key, t, nit, m_item, rp0, rp1, lo, lg; int64_t g0;
-                               int32_t hi, pad; };
+// totals[] written by the plan kernel and read by the count kernels
+enum { CT_N_BM = 0, CT_N_H = 1, CT_N_BUCKET = 2, CT_ERR = 3 };
 
-template <class SR> struct IsCount {
-    static constexpr bool value = SR::add_op == OP_PLUS && SR::mult_op == OP_PAIR &&
-        std::is_integral<typename SR::z_t>::value &&
-        !std::is_same<typename SR::z_t, bool>::value;
-};
-
-// group size kept (0 below D3_GMIN), as int64 for the offsets scan
-__global__ void k_d3_gsize(const int32_t *__restrict__ gcnt, int64_t nkeys,
-                           int64_t *__restrict__ gsz)
-{
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (; t < nkeys; t += stride) {
-        const int32_t c = gcnt[t];
-        gsz[t] = c >= D3_GMIN ? c : 0;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) gsz[nkeys] = 0;    // the scan's last input
-}
-
-// route every queued entry to its group's bucket or to the merge list
+template <class SR>
 __global__ void __launch_bounds__(256)
-k_d3_route(const D3Work *__restrict__ queue, const int *__restrict__ qlen_p,
-           const int64_t *__restrict__ gsz, const int64_t *__restrict__ goff,
-           int32_t *__restrict__ gfill, unsigned long long *__restrict__ gwork,
-           D3Rec *__restrict__ bucket, int32_t nrows, int32_t *__restrict__ merge_sel,
-           int *__restrict__ merge_len)
+k_ct_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
+              const void *__restrict__ Mx, int mtype, bool mask_struct,
+              int64_t mnz, int64_t nrows,
+              const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+              const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
+              uint32_t bm_bits, bool spans_fit,
+              int32_t *__restrict__ Cj, CtQ *__restrict__ queue,
+              int32_t *__restrict__ gcnt, unsigned long long *__restrict__ nzombies)
 {
     const int lane = threadIdx.x & 31;
-    const int qlen = *qlen_p;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32;
-         base < qlen; base += nw * 32) {
-        const int w = (int)(base + lane);
-        bool grouped = false, merge = false;
-        int32_t key = -1;
-        unsigned long long work = 0;
-        D3Rec rec{0, 0, 0, 0};
-        if (w < qlen) {
-            const D3Work e = queue[w];
-            key = e.pad;
-            grouped = key >= 0 && gsz[key] > 0;
-            merge = !grouped;
-            // probes: the other list's elements (the shorter one)
-            const bool by_row = key < nrows;
-            rec = by_row ? D3Rec{e.b0, e.b1 - e.b0, e.pm, e.j}
-                         : D3Rec{e.a0, e.a1 - e.a0, e.pm, e.j};
-            work = (unsigned long long)rec.len;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long zcount = 0;
+    for (int64_t base = warp * 32; base < mnz; base += nwarps * 32) {
+        const int64_t pm = base + lane;
+        const bool valid = pm < mnz;
+        const int32_t r0 = warp_last_le<int32_t, int32_t>(Mp, (int32_t)nrows, (int32_t)base,
+                                                          lane);
+        int32_t i = r0;
+        if (valid) while (Mp[i + 1] <= pm) i++;
+        int32_t key = -1, s0 = 0, len = 0;
+        if (valid) {
+            const int32_t j = Mj[pm];
+            const bool mval = mask_struct || Mx == nullptr || mask_value_true(Mx, mtype, pm);
+            const int32_t pa0 = Ap[i], pa1 = Ap[i + 1];
+            const int32_t pb0 = Bp[j], pb1 = Bp[j + 1];
+            if (mval && pa1 > pa0 && pb1 > pb0) {
+                const int32_t dA = pa1 - pa0, dB = pb1 - pb0;
+                const bool akey = dA > dB;
+                key = akey ? i : (int32_t)nrows + j;
+                s0 = akey ? pb0 : pa0;
+                len = akey ? dB : dA;
+                if (!spans_fit && (akey ? dA : dB) > CT_BM_KEY) {
+                    const int32_t span = akey ? Aj[pa1 - 1] - Aj[pa0] : Bj[pb1 - 1] - Bj[pb0];
+                    if ((uint32_t)span >= bm_bits) key = CT_MERGE;
+                }
+            } else {
+                Cj[pm] = flip(j);
+                zcount++;
+            }
         }
+        // rank in the group: one atomic per distinct key of the warp
+        int32_t rank = 0;
+        const bool grouped = key >= 0;
         const unsigned gm = __ballot_sync(0xffffffffu, grouped);
         if (grouped) {
             const unsigned same = __match_any_sync(gm, key);
             const int leader = __ffs(same) - 1;
-            // the leader reserves slots and adds the work of its lanes (the
-            // work only balances items: each lane's share is capped at 2^26)
-            const unsigned wsum = __reduce_add_sync(same, (unsigned)min(work, 1ull << 26));
-            int slot0 = 0;
-            if (lane == leader) {
-                slot0 = atomicAdd(&gfill[key], __popc(same));
-                atomicAdd(&gwork[key], (unsigned long long)wsum);
-            }
-            slot0 = __shfl_sync(same, slot0, leader);
-            bucket[goff[key] + slot0 + __popc(same & ((1u << lane) - 1))] = rec;
+            int32_t b = 0;
+            if (lane == leader) b = atomicAdd(&gcnt[key], __popc(same));
+            b = __shfl_sync(same, b, leader);
+            rank = b + __popc(same & ((1u << lane) - 1));
         }
-        const unsigned mm = __ballot_sync(0xffffffffu, merge);
-        if (mm) {
-            int mbase = 0;
-            if (lane == 0) mbase = atomicAdd(merge_len, __popc(mm));
-            mbase = __shfl_sync(0xffffffffu, mbase, 0);
-            if (merge) merge_sel[mbase + __popc(mm & ((1u << lane) - 1))] = w;
-        }
+        if (valid) queue[pm] = CtQ{key, rank, s0, len};
     }
+    for (int o = 16; o > 0; o >>= 1) zcount += __shfl_down_sync(0xffffffffu, zcount, o);
+    if (lane == 0 && zcount) atomicAdd(nzombies, zcount);
 }
 
-// work items per group.  A group whose key row has at most D3_HKEY entries
-// goes to the warp-hash kernel (items of about D3_HCHUNK probes), a longer
-// key row to the block-bitmap kernel (items of about D3_WCHUNK probes); at
-// most one item per 32 entries, so items never outnumber nkeys + entries/32.
-__global__ void k_d3_item_count(const int64_t *__restrict__ gsz,
-                                const unsigned long long *__restrict__ gwork,
-                                int64_t nkeys, int32_t nrows,
-                                const int32_t *__restrict__ Ap,
-                                const int32_t *__restrict__ Bp,
-                                int64_t *__restrict__ nit_big, int64_t *__restrict__ nit_small)
+// ---- plan: single-pass scan over the keys -------------------------------
+
+// A tile publishes its three sums (item counts for the two kernels, bucket
+// entries) as 64-bit words (flag << 62 | value): flag 1 = the tile's own
+// sum, 2 = the sum of every tile up to and including it.  A tile waits for
+// its predecessors' words with a bounded number of polls; if the bound is
+// reached the error flag is set and the call fails.
+static constexpr unsigned long long CT_FLAG_AGG = 1ull << 62, CT_FLAG_INC = 2ull << 62;
+static constexpr unsigned long long CT_VAL = (1ull << 62) - 1;
+static constexpr int CT_SPIN_LIMIT = 1 << 22;
+
+__device__ __forceinline__ void ct_key_plan(const int32_t *__restrict__ gcnt, int64_t t,
+                                            int64_t nkeys, int32_t nrows,
+                                            const int32_t *__restrict__ Ap,
+                                            const int32_t *__restrict__ Bp,
+                                            int32_t &c, int32_t &nb, int32_t &nh, int32_t &bc)
 {
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    if (t == 0) { nit_big[nkeys] = 0; nit_small[nkeys] = 0; }    // the scans' last inputs
-    for (; t < nkeys; t += stride) {
-        const int64_t g = gsz[t];
-        int64_t nb = 0, ns = 0;
-        if (g > 0) {
+    c = 0; nb = 0; nh = 0; bc = 0;
+    if (t >= nkeys) return;
+    c = gcnt[t];
+    if (c <= 0) return;
+    const bool by_row = t < nrows;
+    const int32_t r = by_row ? (int32_t)t : (int32_t)(t - nrows);
+    const int32_t klen = by_row ? Ap[r + 1] - Ap[r] : Bp[r + 1] - Bp[r];
+    if (klen > CT_BM_KEY) nb = (c + CT_ITEM_BM - 1) / CT_ITEM_BM;
+    else nh = (c + CT_ITEM_H - 1) / CT_ITEM_H;
+    if (!by_row) bc = c;
+}
+
+// inclusive scan of three ints across the block (256 threads)
+__device__ __forceinline__ void ct_block_scan3(int &a, int &b, int &c, int &ta, int &tb,
+                                               int &tc, int (*s_w)[CT_TILE_T / 32])
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    #pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int xa = __shfl_up_sync(0xffffffffu, a, o);
+        const int xb = __shfl_up_sync(0xffffffffu, b, o);
+        const int xc = __shfl_up_sync(0xffffffffu, c, o);
+        if (lane >= o) { a += xa; b += xb; c += xc; }
+    }
+    if (lane == 31) { s_w[0][w] = a; s_w[1][w] = b; s_w[2][w] = c; }
+    __syncthreads();
+    int pa = 0, pb = 0, pc = 0;
+    ta = 0; tb = 0; tc = 0;
+    #pragma unroll
+    for (int k = 0; k < CT_TILE_T / 32; k++) {
+        if (k < w) { pa += s_w[0][k]; pb += s_w[1][k]; pc += s_w[2][k]; }
+        ta += s_w[0][k]; tb += s_w[1][k]; tc += s_w[2][k];
+    }
+    a += pa; b += pb; c += pc;
+}
+
+__global__ void __launch_bounds__(CT_TILE_T)
+k_ct_plan(const int32_t *__restrict__ gcnt, int64_t nkeys, int32_t nrows,
+          const int32_t *__restrict__ Mp,
+          const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+          const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
+          unsigned long long *__restrict__ status, int *__restrict__ tile_ctr,
+          int32_t *__restrict__ boff, CtItem *__restrict__ items_bm,
+          CtItem *__restrict__ items_h, int32_t *__restrict__ totals)
+{
+    __shared__ int s_tile;
+    __shared__ int s_w[3][CT_TILE_T / 32];
+    __shared__ long long s_ex[3];
+    const int tid = threadIdx.x;
+    if (tid == 0) s_tile = atomicAdd(tile_ctr, 1);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    const int64_t ntiles = (nkeys + CT_TILE - 1) / CT_TILE;
+    const int64_t t0 = tile * CT_TILE + (int64_t)tid * CT_TILE_K;
+    // this thread's keys: sums
+    int sb = 0, sh = 0, sc = 0;
+    #pragma unroll
+    for (int k = 0; k < CT_TILE_K; k++) {
+        int32_t c, nb, nh, bc;
+        ct_key_plan(gcnt, t0 + k, nkeys, nrows, Ap, Bp, c, nb, nh, bc);
+        sb += nb; sh += nh; sc += bc;
+    }
+    int ib = sb, ih = sh, ic = sc, tb, th, tc;
+    ct_block_scan3(ib, ih, ic, tb, th, tc, s_w);
+    // look back over the predecessors
+    if (tid == 0) {
+        unsigned long long *my = status + tile * 3;
+        const unsigned long long agg[3] = {(unsigned long long)tb, (unsigned long long)th,
+                                           (unsigned long long)tc};
+        if (tile == 0) {
+            for (int v = 0; v < 3; v++) atomicExch(&my[v], CT_FLAG_INC | agg[v]);
+            s_ex[0] = s_ex[1] = s_ex[2] = 0;
+        } else {
+            for (int v = 0; v < 3; v++) atomicExch(&my[v], CT_FLAG_AGG | agg[v]);
+            long long ex[3] = {0, 0, 0};
+            for (int v = 0; v < 3; v++) {
+                int64_t p = tile - 1;
+                int spins = 0;
+                while (p >= 0) {
+                    const unsigned long long w =
+                        *reinterpret_cast<volatile unsigned long long *>(&status[p * 3 + v]);
+                    const unsigned long long f = w & ~CT_VAL;
+                    if (f == 0) {
+                        if (++spins > CT_SPIN_LIMIT) { atomicExch(&totals[CT_ERR], 1); break; }
+                        __nanosleep(64);
+                        continue;
+                    }
+                    ex[v] += (long long)(w & CT_VAL);
+                    if (f == CT_FLAG_INC) break;
+                    p--;
+                }
+            }
+            for (int v = 0; v < 3; v++)
+                atomicExch(&my[v], CT_FLAG_INC | ((unsigned long long)(ex[v] + (long long)agg[v]) & CT_VAL));
+            s_ex[0] = ex[0]; s_ex[1] = ex[1]; s_ex[2] = ex[2];
+        }
+        if (tile == ntiles - 1) {
+            totals[CT_N_BM] = (int32_t)(s_ex[0] + tb);
+            totals[CT_N_H] = (int32_t)(s_ex[1] + th);
+            totals[CT_N_BUCKET] = (int32_t)(s_ex[2] + tc);
+        }
+    }
+    __syncthreads();
+    // exclusive offsets of this thread's first key
+    long long ob = s_ex[0] + ib - sb, oh = s_ex[1] + ih - sh, oc = s_ex[2] + ic - sc;
+    #pragma unroll 1
+    for (int k = 0; k < CT_TILE_K; k++) {
+        const int64_t t = t0 + k;
+        int32_t c, nb, nh, bc;
+        ct_key_plan(gcnt, t, nkeys, nrows, Ap, Bp, c, nb, nh, bc);
+        if (t < nkeys && t >= nrows) boff[t - nrows] = (int32_t)oc;
+        const int32_t n = nb + nh;
+        if (n > 0) {
             const bool by_row = t < nrows;
             const int32_t r = by_row ? (int32_t)t : (int32_t)(t - nrows);
-            const int32_t klen = by_row ? Ap[r + 1] - Ap[r] : Bp[r + 1] - Bp[r];
-            const bool small = klen <= D3_HKEY;
-            int64_t n = 1 + (int64_t)(gwork[t] / (small ? D3_HCHUNK : D3_WCHUNK));
-            const int64_t mx = g / 32 > 1 ? g / 32 : 1;
-            if (n > mx) n = mx;
-            if (small) ns = n; else nb = n;
+            const int32_t *P = by_row ? Ap : Bp;
+            const int32_t *J = by_row ? Aj : Bj;
+            const int32_t rp0 = P[r], rp1 = P[r + 1];
+            const int32_t klo = J[rp0], khi = J[rp1 - 1];
+            // A-keyed: the mask row's positions; B-keyed: the bucket
+            const int64_t e_lo = by_row ? Mp[r] : oc;
+            const int64_t e_n = by_row ? (int64_t)(Mp[r + 1] - Mp[r]) : (int64_t)c;
+            CtItem *out = nb ? items_bm + ob : items_h + oh;
+            for (int32_t q = 0; q < n; q++)
+                out[q] = CtItem{(int32_t)t, (int32_t)(e_lo + e_n * q / n),
+                                (int32_t)(e_lo + e_n * (q + 1) / n), rp0, rp1, klo, khi, 0};
         }
-        nit_big[t] = nb;
-        nit_small[t] = ns;
+        ob += nb; oh += nh; oc += bc;
     }
 }
 
-__global__ void k_d3_item_fill(const int64_t *__restrict__ ioff, int64_t nkeys,
-                               const int64_t *__restrict__ goff,
-                               const unsigned long long *__restrict__ gwork, int32_t nrows,
-                               const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
-                               const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
-                               D3Item *__restrict__ items)
+// B-keyed entries to their buckets; entries for the merge kernel to its queue
+__global__ void __launch_bounds__(256)
+k_ct_route(const CtQ *__restrict__ queue, int64_t mnz, int32_t nrows,
+           const int32_t *__restrict__ boff, CtRec *__restrict__ bucket,
+           const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
+           const int32_t *__restrict__ Ap, const int32_t *__restrict__ Bp,
+           D3Work *__restrict__ mq, int *__restrict__ mq_len)
 {
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (; t < nkeys; t += stride) {
-        const int64_t o = ioff[t], n = ioff[t + 1] - o;
-        if (n == 0) continue;
-        const bool by_row = t < nrows;
-        const int32_t r = by_row ? (int32_t)t : (int32_t)(t - nrows);
-        const int32_t rp0 = by_row ? Ap[r] : Bp[r], rp1 = by_row ? Ap[r + 1] : Bp[r + 1];
-        const int32_t lo = by_row ? Aj[rp0] : Bj[rp0];
-        const int32_t hi = by_row ? Aj[rp1 - 1] : Bj[rp1 - 1];
-        const int64_t g0 = goff[t], gn = goff[t + 1] - g0;
-        // lanes per entry: a power of two near an eighth of the mean list
-        // length, so a lane's D3_PROBE_UNROLL loads are mostly in use and
-        // short lists of a skewed group leave few lanes idle (half and a
-        // quarter of the mean, and a sixteenth, measured slower)
-        const unsigned long long mean = gwork[t] / (unsigned long long)gn;
-        int lg = 0;
-        while (lg < 5 && (8ull << lg) < mean) lg++;
-        for (int64_t q = 0; q < n; q++)
-            items[o + q] = D3Item{(int32_t)t, (int32_t)q, (int32_t)n,
-                                  (int32_t)((gn - q + n - 1) / n), rp0, rp1, lo, lg, g0,
-                                  hi, 0};
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * 32; base < mnz; base += nwarps * 32) {
+        const int64_t pm = base + lane;
+        CtQ q{-1, 0, 0, 0};
+        if (pm < mnz) q = queue[pm];
+        if (q.key >= nrows)
+            bucket[boff[q.key - nrows] + q.rank] = CtRec{q.s0, q.len, (int32_t)pm, 0};
+        const unsigned mm = __ballot_sync(0xffffffffu, q.key == CT_MERGE);
+        if (mm) {
+            const int32_t r0 = warp_last_le<int32_t, int32_t>(Mp, nrows, (int32_t)base, lane);
+            int32_t mb = 0;
+            if (lane == 0) mb = atomicAdd(mq_len, __popc(mm));
+            mb = __shfl_sync(0xffffffffu, mb, 0);
+            if (q.key == CT_MERGE) {
+                int32_t i = r0;
+                while (Mp[i + 1] <= pm) i++;
+                const int32_t j = Mj[pm];
+                mq[mb + __popc(mm & ((1u << lane) - 1))] =
+                    D3Work{(int32_t)pm, i, j, Ap[i], Ap[i + 1], Bp[j], Bp[j + 1], 0};
+            }
+        }
     }
 }
 
-// One block per SM, persistent: take an item, set the bits of its key row
-// (A(i,:) or B(j,:), relative to the row's first column) in shared memory,
-// then count, for every entry of the item, the elements of its other
-// (trimmed) list that hit the bitmap, in two phases:
-//   A. each warp splits into groups of G lanes (G a power of two near half
-//      the group's mean probes per entry, so short lists do not waste
-//      lanes); groups take the item's entries one at a time from a shared
-//      counter and stride over their list; a list longer than D3_LONG is
-//      instead registered in a shared table (up to D3_TABLE entries) as
-//      segments of D3_SEG probes;
-//   B. all warps take the segments from a shared counter, 32 probes per step,
-//      and add their hits to the entry's shared count; then the table's
-//      entries are written.
-// If the table is full, the group that owns the entry finishes it itself.
-// The bits are cleared again from the row before the next item.
+// ---- probing ------------------------------------------------------------
+
+// The G lanes of a group (lane gl of G; gmask = the group's lanes) count the
+// elements of S[p0, p1) for which hit() is 1.  Elements below klo are
+// skipped by a G-ary search (when the first one is below); probing stops at
+// the first step that passes khi.  Steps take 4 elements per lane: 16-byte
+// loads when `vec` (S 16-byte aligned) and the step lies inside the range,
+// else predicated scalar loads (a skipped slot reads klo - 1, never a hit).
+template <int G, class Hit>
+__device__ __forceinline__ int ct_count(const int32_t *__restrict__ S, int32_t p0, int32_t p1,
+                                        int32_t klo, int32_t khi, int gl, unsigned gmask,
+                                        bool vec, const Hit &hit)
+{
+    int32_t q0 = p0;
+    if (S[p0] < klo) {
+        int32_t lo = p0, hi = p1;          // the first element >= klo is in [lo, hi]
+        while (hi - lo > G) {
+            const int32_t step = (hi - lo + G - 1) / G;
+            const int32_t idx = lo + (gl + 1) * step - 1;
+            const bool less = idx < hi && S[idx] < klo;
+            const int32_t nlo = lo + __popc(__ballot_sync(gmask, less)) * step;
+            hi = min(hi, nlo + step);
+            lo = nlo;
+        }
+        const bool less = lo + gl < hi && S[lo + gl] < klo;
+        q0 = lo + __popc(__ballot_sync(gmask, less));
+    }
+    int cnt = 0;
+    for (int32_t base = q0 & ~3; base < p1; base += 4 * G) {
+        const int32_t e = base + 4 * gl;
+        int32_t x0, x1, x2, x3;
+        if (vec && base >= q0 && base + 4 * G <= p1) {
+            const int4 v = __ldg(reinterpret_cast<const int4 *>(S + e));
+            x0 = v.x; x1 = v.y; x2 = v.z; x3 = v.w;
+        } else {
+            const int32_t none = klo - 1;
+            x0 = (e >= q0 && e < p1) ? S[e] : none;
+            x1 = (e + 1 >= q0 && e + 1 < p1) ? S[e + 1] : none;
+            x2 = (e + 2 >= q0 && e + 2 < p1) ? S[e + 2] : none;
+            x3 = (e + 3 >= q0 && e + 3 < p1) ? S[e + 3] : none;
+        }
+        cnt += hit(x0) + hit(x1) + hit(x2) + hit(x3);
+        const int32_t mx = max(max(x0, x1), max(x2, x3));
+        if (__any_sync(gmask, mx > khi)) break;
+    }
+    return cnt;
+}
+
+// write one counted entry: C(i,j) = c, or a zombie when c is 0
+template <typename Z>
+__device__ __forceinline__ void ct_write(int32_t pm, int32_t j, int c, int32_t *__restrict__ Cj,
+                                         Z *__restrict__ Cx, unsigned long long &sum,
+                                         unsigned long long &zc)
+{
+    if (c) { Cj[pm] = j; Cx[pm] = (Z)c; sum += (unsigned long long)c; }
+    else { Cj[pm] = flip(j); zc++; }
+}
+
+// one batch of up to 32 entries, one per lane (valid, probed row s0/len,
+// output position pm and column j): long lists by the whole warp one after
+// another, mid-length lists by groups of 8 lanes, short ones by groups of 2
+template <typename Z, class Hit>
+__device__ __forceinline__ void ct_batch(bool valid, int32_t s0, int32_t len, int32_t pm,
+                                         int32_t j, const int32_t *__restrict__ S,
+                                         int32_t klo, int32_t khi, bool vec, const Hit &hit,
+                                         int32_t *__restrict__ Cj, Z *__restrict__ Cx,
+                                         unsigned long long &sum, unsigned long long &zc)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned vL = __ballot_sync(0xffffffffu, valid && len > CT_LONG);
+    const unsigned vM = __ballot_sync(0xffffffffu, valid && len > CT_MID && len <= CT_LONG);
+    const unsigned vS = __ballot_sync(0xffffffffu, valid && len <= CT_MID);
+    for (unsigned m = vL; m; m &= m - 1) {
+        const int src = __ffs(m) - 1;
+        const int32_t es0 = __shfl_sync(0xffffffffu, s0, src);
+        const int32_t elen = __shfl_sync(0xffffffffu, len, src);
+        int c = ct_count<32>(S, es0, es0 + elen, klo, khi, lane, 0xffffffffu, vec, hit);
+        c = (int)__reduce_add_sync(0xffffffffu, (unsigned)c);
+        if (lane == src) ct_write<Z>(pm, j, c, Cj, Cx, sum, zc);
+    }
+    {
+        const int gi = lane >> 3, gl = lane & 7;
+        const unsigned gmask = 0xffu << (gi * 8);
+        const int n = __popc(vM);
+        for (int r = 0; r < n; r += 4) {
+            const bool act = r + gi < n;
+            const int src = act ? (int)__fns(vM, 0, r + gi + 1) : 0;
+            const int32_t es0 = __shfl_sync(0xffffffffu, s0, src);
+            const int32_t elen = __shfl_sync(0xffffffffu, len, src);
+            const int32_t epm = __shfl_sync(0xffffffffu, pm, src);
+            const int32_t ej = __shfl_sync(0xffffffffu, j, src);
+            if (act) {
+                int c = ct_count<8>(S, es0, es0 + elen, klo, khi, gl, gmask, vec, hit);
+                c = (int)__reduce_add_sync(gmask, (unsigned)c);
+                if (gl == 0) ct_write<Z>(epm, ej, c, Cj, Cx, sum, zc);
+            }
+        }
+    }
+    {
+        const int gi = lane >> 1, gl = lane & 1;
+        const unsigned gmask = 0x3u << (gi * 2);
+        const int n = __popc(vS);
+        for (int r = 0; r < n; r += 16) {
+            const bool act = r + gi < n;
+            const int src = act ? (int)__fns(vS, 0, r + gi + 1) : 0;
+            const int32_t es0 = __shfl_sync(0xffffffffu, s0, src);
+            const int32_t elen = __shfl_sync(0xffffffffu, len, src);
+            const int32_t epm = __shfl_sync(0xffffffffu, pm, src);
+            const int32_t ej = __shfl_sync(0xffffffffu, j, src);
+            if (act) {
+                int c = ct_count<2>(S, es0, es0 + elen, klo, khi, gl, gmask, vec, hit);
+                c = (int)__reduce_add_sync(gmask, (unsigned)c);
+                if (gl == 0) ct_write<Z>(epm, ej, c, Cj, Cx, sum, zc);
+            }
+        }
+    }
+}
+
+// the entries [e, e + 32) of an item as lane-per-entry records
+__device__ __forceinline__ void ct_load_entry(const CtItem &I, int32_t e, int32_t nrows,
+                                              const CtQ *__restrict__ queue,
+                                              const CtRec *__restrict__ bucket,
+                                              const int32_t *__restrict__ Mj, bool &valid,
+                                              int32_t &s0, int32_t &len, int32_t &pm,
+                                              int32_t &j)
+{
+    valid = false; s0 = 0; len = 0; pm = 0; j = 0;
+    if (e >= I.e1) return;
+    if (I.key < nrows) {
+        const CtQ q = queue[e];
+        if (q.key == I.key) { valid = true; s0 = q.s0; len = q.len; pm = e; j = Mj[e]; }
+    } else {
+        const CtRec r = bucket[e];
+        valid = true; s0 = r.s0; len = r.len; pm = r.pm; j = I.key - nrows;
+    }
+}
+
+__device__ __forceinline__ uint32_t ct_hash(int32_t k, int bits)
+{
+    return ((uint32_t)k * 0x9E3779B1u) >> (32 - bits);
+}
+
+// one warp per item whose key row has at most CT_BM_KEY entries: the key
+// row goes into the warp's open-addressing table (a power of two of slots,
+// at least twice the row), then its entries are counted against it
 template <class SR>
-__global__ void __launch_bounds__(D3_BM_THREADS, 1)
-k_dot3_bitmap_count(const D3Item *__restrict__ items, const int64_t *__restrict__ nitems_p,
-                    int *__restrict__ inext, const D3Rec *__restrict__ bucket,
-                    int32_t nrows, const int32_t *__restrict__ Aj,
-                    const int32_t *__restrict__ Bj,
-                    uint32_t bm_words, int32_t *__restrict__ Cj,
-                    typename SR::z_t *__restrict__ Cx,
-                    unsigned long long *__restrict__ nzombies)
+__global__ void __launch_bounds__(CT_H_WARPS * 32)
+k_ct_hash(const CtItem *__restrict__ items, const int32_t *__restrict__ totals,
+          int *__restrict__ inext, int32_t nrows, const CtQ *__restrict__ queue,
+          const CtRec *__restrict__ bucket, const int32_t *__restrict__ Mj,
+          const int32_t *__restrict__ Aj, const int32_t *__restrict__ Bj, bool vec,
+          int32_t *__restrict__ Cj, typename SR::z_t *__restrict__ Cx,
+          unsigned long long *__restrict__ out_sum, unsigned long long *__restrict__ nzombies)
+{
+    using Z = typename SR::z_t;
+    extern __shared__ __align__(16) int32_t ct_tabs[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int32_t *tab = ct_tabs + w * CT_H_SLOTS;
+    for (int q = lane; q < CT_H_SLOTS; q += 32) tab[q] = -1;
+    __syncwarp();
+    const int nitems = totals[CT_N_H];
+    unsigned long long sum = 0, zc = 0;
+    while (true) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(inext, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= nitems) break;
+        const CtItem I = items[it];
+        const bool by_row = I.key < nrows;
+        const int32_t *J = by_row ? Aj : Bj;
+        const int32_t *S = by_row ? Bj : Aj;
+        const int32_t klen = I.rp1 - I.rp0;
+        int bits = 6;
+        while ((1 << bits) < 2 * klen) bits++;
+        const uint32_t tmask = (1u << bits) - 1;
+        for (int32_t q = I.rp0 + lane; q < I.rp1; q += 32) {
+            const int32_t k = J[q];
+            uint32_t h = ct_hash(k, bits);
+            while (atomicCAS(&tab[h], -1, k) != -1) h = (h + 1) & tmask;
+        }
+        __syncwarp();
+        const int32_t klo = I.klo, khi = I.khi;
+        auto hit = [&](int32_t x) -> int {
+            if (x < klo || x > khi) return 0;
+            uint32_t h = ct_hash(x, bits);
+            while (true) {
+                const int32_t v = tab[h];
+                if (v == x) return 1;
+                if (v < 0) return 0;
+                h = (h + 1) & tmask;
+            }
+        };
+        for (int32_t e = I.e0; e < I.e1; e += 32) {
+            bool valid;
+            int32_t s0, len, pm, j;
+            ct_load_entry(I, e + lane, nrows, queue, bucket, Mj, valid, s0, len, pm, j);
+            ct_batch<Z>(valid, s0, len, pm, j, S, klo, khi, vec, hit, Cj, Cx, sum, zc);
+        }
+        __syncwarp();
+        for (int q = lane; q <= (int)tmask; q += 32) tab[q] = -1;
+        __syncwarp();
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sum += __shfl_down_sync(0xffffffffu, sum, o);
+        zc += __shfl_down_sync(0xffffffffu, zc, o);
+    }
+    if (lane == 0) {
+        if (sum) atomicAdd(out_sum, sum);
+        if (zc) atomicAdd(nzombies, zc);
+    }
+}
+
+// One block per SM, persistent over the items whose key row is longer than
+// CT_BM_KEY: the key row's columns (relative to its first) are set as bits
+// of a shared-memory bitmap, the warps take the item's entries 32 at a time
+// from a shared counter and count them, and the bits are cleared again.
+// bm_words words hold the bits; the word after them stays zero and absorbs
+// every probe outside the row's span.
+template <class SR>
+__global__ void __launch_bounds__(CT_BM_THREADS, 1)
+k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals,
+            int *__restrict__ inext, int32_t nrows, const CtQ *__restrict__ queue,
+            const CtRec *__restrict__ bucket, const int32_t *__restrict__ Mj,
+            const int32_t *__restrict__ Aj, const int32_t *__restrict__ Bj, bool vec,
+            uint32_t bm_words, int32_t *__restrict__ Cj, typename SR::z_t *__restrict__ Cx,
+            unsigned long long *__restrict__ out_sum, unsigned long long *__restrict__ nzombies)
 {
     using Z = typename SR::z_t;
     extern __shared__ __align__(16) uint32_t bm[];
-    __shared__ int s_item, s_next, s_gnext;
-    __shared__ D3Item s_I;                        // the next item, fetched ahead
-    __shared__ unsigned long long s_tbl;          // (segments << 32) | entries
-    __shared__ int32_t t_start[D3_TABLE], t_rem[D3_TABLE], t_seg0[D3_TABLE];
-    __shared__ int32_t t_cnt[D3_TABLE], t_pm[D3_TABLE], t_j[D3_TABLE];
+    __shared__ int s_item, s_next;
+    __shared__ CtItem s_I;
     const int tid = threadIdx.x, lane = tid & 31;
-    const uint32_t nbits = bm_words * 32u;
-    for (uint32_t q = tid; q < bm_words; q += blockDim.x) bm[q] = 0;
-    const int64_t nitems = *nitems_p;
-    unsigned long long zc = 0;
-    // hits among S[b0 + t] for t = first, first + step, ... < n
-    // (D3_PROBE_UNROLL predicated loads issued together per step, the tail included;
-    // a skipped slot reads as lo - 1, which is never a bit of the row)
-    auto probes = [&](const int32_t *S, int32_t b0, int32_t first, int32_t step, int32_t n,
-                      int32_t lo) -> int {
-        int c = 0;
-        for (int32_t t = first; t < n; t += D3_PROBE_UNROLL * step) {
-            int32_t x[D3_PROBE_UNROLL];
-            #pragma unroll
-            for (int u = 0; u < D3_PROBE_UNROLL; u++) {
-                const int32_t q = t + u * step;
-                x[u] = q < n ? S[b0 + q] : lo - 1;
-            }
-            #pragma unroll
-            for (int u = 0; u < D3_PROBE_UNROLL; u++) {
-                const uint32_t k = (uint32_t)(x[u] - lo);
-                c += (k < nbits) ? (int)((bm[k >> 5] >> (k & 31)) & 1u) : 0;
-            }
-        }
-        return c;
-    };
+    for (uint32_t q = tid; q <= bm_words; q += blockDim.x) bm[q] = 0;
+    const uint32_t nbits = bm_words * 32u;        // the guard bit
+    const int nitems = totals[CT_N_BM];
+    unsigned long long sum = 0, zc = 0;
     if (tid == 0) {
         s_item = atomicAdd(inext, 1);
         if (s_item < nitems) s_I = items[s_item];
     }
     while (true) {
         __syncthreads();
-        const int it = s_item;
-        if (it >= nitems) break;
-        const D3Item I = s_I;
+        if (s_item >= nitems) break;
+        const CtItem I = s_I;
         __syncthreads();
-        if (tid == 0) { s_next = 0; s_gnext = 0; s_tbl = 0; }
+        if (tid == 0) s_next = 0;
         const bool by_row = I.key < nrows;
         const int32_t *J = by_row ? Aj : Bj;
-        const int32_t *S = by_row ? Bj : Aj;     // the probed lists
-        const int32_t rp0 = I.rp0, rp1 = I.rp1, lo = I.lo;
-        // set the key row's bits: four loads in flight per thread
+        const int32_t *S = by_row ? Bj : Aj;
+        const int32_t klo = I.klo, khi = I.khi;
         {
             const int32_t nt = (int32_t)blockDim.x;
-            int32_t q = rp0 + tid;
-            for (; q + 3 * nt < rp1; q += 4 * nt) {
-                const uint32_t k0 = (uint32_t)(J[q] - lo), k1 = (uint32_t)(J[q + nt] - lo);
-                const uint32_t k2 = (uint32_t)(J[q + 2 * nt] - lo);
-                const uint32_t k3 = (uint32_t)(J[q + 3 * nt] - lo);
+            int32_t q = I.rp0 + tid;
+            for (; q + 3 * nt < I.rp1; q += 4 * nt) {
+                const uint32_t k0 = (uint32_t)(J[q] - klo), k1 = (uint32_t)(J[q + nt] - klo);
+                const uint32_t k2 = (uint32_t)(J[q + 2 * nt] - klo);
+                const uint32_t k3 = (uint32_t)(J[q + 3 * nt] - klo);
                 atomicOr(&bm[k0 >> 5], 1u << (k0 & 31));
                 atomicOr(&bm[k1 >> 5], 1u << (k1 & 31));
                 atomicOr(&bm[k2 >> 5], 1u << (k2 & 31));
                 atomicOr(&bm[k3 >> 5], 1u << (k3 & 31));
             }
-            for (; q < rp1; q += nt) {
-                const uint32_t k = (uint32_t)(J[q] - lo);
+            for (; q < I.rp1; q += nt) {
+                const uint32_t k = (uint32_t)(J[q] - klo);
                 atomicOr(&bm[k >> 5], 1u << (k & 31));
             }
         }
-        const int64_t g0 = I.g0;
-        const int32_t m_item = I.m_item;
-        const int lg = I.lg;
-        const int G = 1 << lg, gi = lane >> lg, gl = lane & (G - 1);
-        const int groups = 32 >> lg;
         __syncthreads();
-        // fetch the next item while this one runs
+        // the next item is fetched while this one runs
         if (tid == 0) {
             s_item = atomicAdd(inext, 1);
             if (s_item < nitems) s_I = items[s_item];
         }
-        // phase A: the next chunk's records are fetched while this chunk
-        // probes, so their load latency overlaps the probes'
-        int c_next = 0;
-        if (lane == 0) c_next = atomicAdd(&s_next, groups);
-        c_next = __shfl_sync(0xffffffffu, c_next, 0);
-        D3Rec e_next{0, 0, 0, 0};
-        if (c_next + gi < m_item) e_next = bucket[g0 + I.t + (int64_t)I.nit * (c_next + gi)];
+        auto hit = [&](int32_t x) -> int {
+            const uint32_t k = min((uint32_t)(x - klo), nbits);
+            return (int)((bm[k >> 5] >> (k & 31)) & 1u);
+        };
         while (true) {
-            const int c0 = c_next;
-            if (c0 >= m_item) break;
-            const int32_t rr = c0 + gi;
-            const int32_t s0 = e_next.s0, len = rr < m_item ? e_next.len : 0;
-            const int32_t pm = e_next.pm, j = e_next.j;
-            if (lane == 0) c_next = atomicAdd(&s_next, groups);
-            c_next = __shfl_sync(0xffffffffu, c_next, 0);
-            if (c_next + gi < m_item) e_next = bucket[g0 + I.t + (int64_t)I.nit * (c_next + gi)];
-            // a long list goes to the table (its group's first lane registers
-            // it); the group keeps it only if the table is full
-            unsigned slot = 0xffffffffu;
-            if (len > D3_LONG && gl == 0) {
-                const unsigned long long nseg =
-                    (unsigned long long)((len + D3_SEG - 1) / D3_SEG);
-                const unsigned long long old = atomicAdd(&s_tbl, (nseg << 32) | 1ull);
-                slot = (unsigned)(old & 0xffffffffull);
-                if (slot < (unsigned)D3_TABLE) {
-                    t_start[slot] = s0;
-                    t_rem[slot] = len;
-                    t_seg0[slot] = (int32_t)(old >> 32);
-                    t_cnt[slot] = 0;
-                    t_pm[slot] = pm;
-                    t_j[slot] = j;
-                }
-            }
-            slot = __shfl_sync(0xffffffffu, slot, gi << lg);
-            const bool own = rr < m_item && slot >= (unsigned)D3_TABLE;
-            int cnt = own ? probes(S, s0, gl, G, len, lo) : 0;
-            for (int o = G >> 1; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o, G);
-            if (own && gl == 0) {
-                if (cnt) { Cj[pm] = j; Cx[pm] = (Z)cnt; }
-                else { Cj[pm] = flip(j); zc++; }
-            }
+            int e = 0;
+            if (lane == 0) e = atomicAdd(&s_next, 32);
+            e = __shfl_sync(0xffffffffu, e, 0) + I.e0;
+            if (e >= I.e1) break;
+            bool valid;
+            int32_t s0, len, pm, j;
+            ct_load_entry(I, e + lane, nrows, queue, bucket, Mj, valid, s0, len, pm, j);
+            ct_batch<Z>(valid, s0, len, pm, j, S, klo, khi, vec, hit, Cj, Cx, sum, zc);
         }
         __syncthreads();
-        // phase B
-        const unsigned long long tb = s_tbl;
-        const int ntab = (int)min((unsigned long long)D3_TABLE, tb & 0xffffffffull);
-        if (ntab > 0) {
-            const int total = t_seg0[ntab - 1] + (t_rem[ntab - 1] + D3_SEG - 1) / D3_SEG;
-            while (true) {
-                int g = 0;
-                if (lane == 0) g = atomicAdd(&s_gnext, 1);
-                g = __shfl_sync(0xffffffffu, g, 0);
-                if (g >= total) break;
-                // table entry holding segment g: last with t_seg0 <= g
-                int a = 0, b = ntab;
-                while (b - a > 1) {
-                    const int mid = (a + b) >> 1;
-                    if (t_seg0[mid] <= g) a = mid; else b = mid;
-                }
-                const int32_t off = (g - t_seg0[a]) * D3_SEG;
-                const int32_t n = min(D3_SEG, t_rem[a] - off);
-                const int c = (int)__reduce_add_sync(
-                    0xffffffffu, (unsigned)probes(S, t_start[a] + off, lane, 32, n, lo));
-                if (lane == 0 && c) atomicAdd(&t_cnt[a], c);
-            }
-        }
-        __syncthreads();
-        for (int q = tid; q < ntab; q += blockDim.x) {
-            const int c = t_cnt[q];
-            const int32_t pm = t_pm[q], j = t_j[q];
-            if (c) { Cj[pm] = j; Cx[pm] = (Z)c; }
-            else { Cj[pm] = flip(j); zc++; }
-        }
-        __syncthreads();
-        // clear: zero the row's word range with 16-byte stores when that is
+        // clear: zero the span's words with 16-byte stores when that is
         // cheaper than revisiting the row's entries
-        const uint32_t span_words = (uint32_t)(I.hi - lo) / 32u + 1u;
-        if (span_words <= 4u * (uint32_t)(rp1 - rp0)) {
+        const uint32_t span_words = (uint32_t)(khi - klo) / 32u + 1u;
+        if (span_words <= 4u * (uint32_t)(I.rp1 - I.rp0)) {
             uint4 *b4 = reinterpret_cast<uint4 *>(bm);
             const uint32_t n4 = (span_words + 3u) / 4u;
             for (uint32_t q = tid; q < n4; q += blockDim.x) b4[q] = make_uint4(0, 0, 0, 0);
         } else {
-            for (int32_t q = rp0 + tid; q < rp1; q += blockDim.x) {
-                const uint32_t k = (uint32_t)(J[q] - lo);
+            for (int32_t q = I.rp0 + tid; q < I.rp1; q += blockDim.x) {
+                const uint32_t k = (uint32_t)(J[q] - klo);
                 bm[k >> 5] = 0;
             }
         }
     }
-    for (int o = 16; o > 0; o >>= 1) zc += __shfl_down_sync(0xffffffffu, zc, o);
-    if (lane == 0 && zc) atomicAdd(nzombies, zc);
-}
-
-// One warp per work item whose key row is short (at most D3_HKEY entries):
-// the key row's columns go into the warp's own shared-memory hash table
-// (D3_HSLOTS slots, open addressing, at most half full), then the warp's
-// lanes, in groups of 2^lg per entry, probe the item's entries' other lists
-// against it.  No block-wide barrier: the many small groups of a skewed
-// graph run side by side, 8 tables (16 KB) per block.
-__device__ __forceinline__ uint32_t d3_hash(int32_t k)
-{
-    return ((uint32_t)k * 0x9E3779B1u) >> (32 - 9);       // 2^9 = D3_HSLOTS
-}
-
-template <class SR>
-__global__ void __launch_bounds__(D3_HWARPS * 32)
-k_dot3_hash_count(const D3Item *__restrict__ items, const int64_t *__restrict__ nitems_p,
-                  int *__restrict__ inext, const D3Rec *__restrict__ bucket,
-                  int32_t nrows, const int32_t *__restrict__ Aj,
-                  const int32_t *__restrict__ Bj, int32_t *__restrict__ Cj,
-                  typename SR::z_t *__restrict__ Cx,
-                  unsigned long long *__restrict__ nzombies)
-{
-    using Z = typename SR::z_t;
-    __shared__ int32_t tab_all[D3_HWARPS][D3_HSLOTS];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int32_t *tab = tab_all[w];
-    for (int q = lane; q < D3_HSLOTS; q += 32) tab[q] = -1;
-    __syncwarp();
-    const int64_t nitems = *nitems_p;
-    unsigned long long zc = 0;
-    auto has = [&](int32_t k) -> int {
-        uint32_t h = d3_hash(k);
-        while (true) {
-            const int32_t v = tab[h];
-            if (v == k) return 1;
-            if (v < 0) return 0;
-            h = (h + 1) & (D3_HSLOTS - 1);
-        }
-    };
-    while (true) {
-        int it = 0;
-        if (lane == 0) it = atomicAdd(inext, 1);
-        it = __shfl_sync(0xffffffffu, it, 0);
-        if (it >= nitems) break;
-        const D3Item I = items[it];
-        const bool by_row = I.key < nrows;
-        const int32_t *J = by_row ? Aj : Bj;
-        const int32_t *S = by_row ? Bj : Aj;
-        for (int32_t q = I.rp0 + lane; q < I.rp1; q += 32) {
-            const int32_t k = J[q];
-            uint32_t h = d3_hash(k);
-            while (atomicCAS(&tab[h], -1, k) != -1) h = (h + 1) & (D3_HSLOTS - 1);
-        }
-        __syncwarp();
-        const int lg = I.lg, G = 1 << lg, gi = lane >> lg, gl = lane & (G - 1);
-        const int groups = 32 >> lg;
-        // the next chunk's records load while this chunk probes; four
-        // predicated loads per step (a skipped slot looks up -2, never a key)
-        D3Rec e_next{0, 0, 0, 0};
-        if (gi < I.m_item) e_next = bucket[I.g0 + I.t + (int64_t)I.nit * gi];
-        for (int32_t c0 = 0; c0 < I.m_item; c0 += groups) {
-            const int32_t rr = c0 + gi;
-            const int32_t s0 = e_next.s0, len = rr < I.m_item ? e_next.len : 0;
-            const int32_t pm = e_next.pm, j = e_next.j;
-            if (rr + groups < I.m_item)
-                e_next = bucket[I.g0 + I.t + (int64_t)I.nit * (rr + groups)];
-            int cnt = 0;
-            for (int32_t t = gl; t < len; t += 4 * G) {
-                int32_t x[4];
-                #pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const int32_t q = t + u * G;
-                    x[u] = q < len ? S[s0 + q] : -2;
-                }
-                #pragma unroll
-                for (int u = 0; u < 4; u++) cnt += x[u] >= 0 ? has(x[u]) : 0;
-            }
-            for (int o = G >> 1; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o, G);
-            if (rr < I.m_item && gl == 0) {
-                if (cnt) { Cj[pm] = j; Cx[pm] = (Z)cnt; }
-                else { Cj[pm] = flip(j); zc++; }
-            }
-        }
-        __syncwarp();
-        for (int q = lane; q < D3_HSLOTS; q += 32) tab[q] = -1;
-        __syncwarp();
+    for (int o = 16; o > 0; o >>= 1) {
+        sum += __shfl_down_sync(0xffffffffu, sum, o);
+        zc += __shfl_down_sync(0xffffffffu, zc, o);
     }
-    for (int o = 16; o > 0; o >>= 1) zc += __shfl_down_sync(0xffffffffu, zc, o);
-    if (lane == 0 && zc) atomicAdd(nzombies, zc);
+    if (lane == 0) {
+        if (sum) atomicAdd(out_sum, sum);
+        if (zc) atomicAdd(nzombies, zc);
+    }
 }
 
-static constexpr int64_t D3_BM_MIN_ENTRIES = 1 << 16;   // mask entries
-
-// Words of the shared-memory bitmap: enough for every column index (plus one
-// word of slack) when that fits beside the kernel's static shared memory,
-// else the most that fits (rows spanning more columns stay on the merge
-// path).  0 disables the bitmap path.
+// Words of the bitmap: enough for every column index when that fits beside
+// the kernel's static shared memory (plus the zero guard word, the total a
+// multiple of 4 words for the 16-byte clears), else the most that fits (key
+// rows spanning more columns go to the merge kernel).  0 disables the
+// bitmap (every key row then needs the hash or merge kernel).
 template <class SR>
-static uint32_t bitmap_words(int64_t ncols)
+static uint32_t ct_bitmap_words(int64_t ncols)
 {
     static int64_t avail = -1;
     if (avail < 0) {
-        const void *fn = (const void *)k_dot3_bitmap_count<SR>;
+        const void *fn = (const void *)k_ct_bitmap<SR>;
         cudaFuncAttributes fa;
         int64_t a = 0;
         if (cudaFuncGetAttributes(&fa, fn) == cudaSuccess) {
@@ -850,63 +986,131 @@ static uint32_t bitmap_words(int64_t ncols)
         cudaGetLastError();
         avail = a / 4;
     }
-    // a multiple of 4 words: the clear writes 16-byte blocks
+    // words for the bits, rounded so that bits + guard is a multiple of 4
     const int64_t need = ((ncols + 31) / 32 + 1 + 3) & ~(int64_t)3;
     const int64_t cap = avail & ~(int64_t)3;
     const int64_t w = need < cap ? need : cap;
-    return w >= 1024 || w == need ? (uint32_t)w : 0;
+    return w >= 1024 ? (uint32_t)(w - 1) : 0;
+}
+
+template <class SR>
+static bool ct_hash_smem_ok()
+{
+    static int ok = -1;
+    if (ok < 0) {
+        ok = cudaFuncSetAttribute((const void *)k_ct_hash<SR>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  CT_H_WARPS * CT_H_SLOTS * 4) == cudaSuccess;
+        cudaGetLastError();
+    }
+    return ok == 1;
+}
+
+template <class SR>
+static int dot3_count_launch(DevCSR &C, const DevCSR &M, bool mask_struct, const DevCSR &A,
+                             const DevCSR &B, cudaStream_t s, int64_t *live_sum)
+{
+    using Z = typename SR::z_t;
+    const int64_t mnz = M.nnz;
+    const int64_t nkeys = M.nrows + B.nrows;
+    const int64_t ntiles = (nkeys + CT_TILE - 1) / CT_TILE;
+    const uint32_t bm_words = ct_bitmap_words<SR>(A.ncols);
+    const bool spans_fit = bm_words > 0 && (int64_t)bm_words * 32 >= A.ncols;
+    if (bm_words == 0 || !ct_hash_smem_ok<SR>()) return NO_VALUE;
+    const int nsm = runtime().num_sms;
+    C.p = (int32_t *)dalloc((size_t)(M.nrows + 1) * 4, s);
+    C.j = (int32_t *)dalloc((size_t)mnz * 4, s);
+    C.x = dalloc((size_t)mnz * sizeof(Z), s);
+    const int64_t nitems_max = std::min<int64_t>(nkeys, mnz) + mnz / CT_ITEM_H + 1;
+    // counters, group counts and tile words first and adjacent: one memset
+    int *counter = nullptr;
+    int32_t *gcnt = nullptr, *boff = nullptr;
+    unsigned long long *status = nullptr;
+    CtQ *queue = nullptr;
+    CtRec *bucket = nullptr;
+    CtItem *items_bm = nullptr, *items_h = nullptr;
+    D3Work *mq = nullptr;
+    Carve cv(s);
+    auto layout = [&]() {
+        counter = cv.take<int>(32);
+        status = cv.take<unsigned long long>((size_t)ntiles * 3);
+        gcnt = cv.take<int32_t>(nkeys);
+        queue = cv.take<CtQ>(mnz);
+        boff = cv.take<int32_t>(B.nrows);
+        bucket = cv.take<CtRec>(mnz);
+        items_bm = cv.take<CtItem>(nitems_max);
+        items_h = cv.take<CtItem>(nitems_max);
+        mq = cv.take<D3Work>(spans_fit ? 1 : mnz);
+    };
+    layout();
+    const bool got = cv.alloc();
+    layout();
+    struct Release { Carve &c; ~Release() { dfree(c.base, c.s); } } release{cv};
+    if (!C.p || !C.j || !C.x || !got) { dev_free(C, s); return OUT_OF_MEMORY; }
+    cudaMemcpyAsync(C.p, M.p, (size_t)(M.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
+    cudaMemsetAsync(counter, 0, (size_t)((const char *)(gcnt + nkeys) - (const char *)counter), s);
+    // counter layout: [0..3] totals, [4] tile ticket, [5] hash items, [6] bitmap
+    // items, [7] merge items, [8] merge taken; zombies at byte 64, sum at 72
+    int32_t *totals = counter;
+    int *tile_ctr = counter + 4, *inext_h = counter + 5, *inext_bm = counter + 6;
+    int *mq_len = counter + 7, *mq_next = counter + 8;
+    unsigned long long *zc = (unsigned long long *)((char *)counter + 64);
+    unsigned long long *sum = zc + 1;
+    const bool vec = ((((uintptr_t)A.j) | ((uintptr_t)B.j)) & 15) == 0;
+    int64_t blocks = ((mnz + 31) / 32 + 7) / 8;
+    if (blocks > (int64_t)nsm * 16) blocks = (int64_t)nsm * 16;
+    const int ps = prof_begin("dot3", s);
+    k_ct_classify<SR><<<(unsigned)blocks, 256, 0, s>>>(
+        M.p, M.j, mask_struct ? nullptr : M.x, M.type, mask_struct, mnz, M.nrows,
+        A.p, A.j, B.p, B.j, bm_words * 32u, spans_fit, C.j, queue, gcnt, zc);
+    k_ct_plan<<<(unsigned)ntiles, CT_TILE_T, 0, s>>>(
+        gcnt, nkeys, (int32_t)M.nrows, M.p, A.p, A.j, B.p, B.j, status, tile_ctr, boff,
+        items_bm, items_h, totals);
+    k_ct_route<<<(unsigned)blocks, 256, 0, s>>>(queue, mnz, (int32_t)M.nrows, boff, bucket,
+                                                 M.p, M.j, A.p, B.p, mq, mq_len);
+    k_ct_hash<SR><<<nsm * 3, CT_H_WARPS * 32, CT_H_WARPS * CT_H_SLOTS * 4, s>>>(
+        items_h, totals, inext_h, (int32_t)M.nrows, queue, bucket, M.j, A.j, B.j, vec,
+        C.j, (Z *)C.x, sum, zc);
+    k_ct_bitmap<SR><<<nsm, CT_BM_THREADS, (size_t)(bm_words + 1) * 4, s>>>(
+        items_bm, totals, inext_bm, (int32_t)M.nrows, queue, bucket, M.j, A.j, B.j, vec,
+        bm_words, C.j, (Z *)C.x, sum, zc);
+    k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
+        mq, nullptr, mq_len, mq_next, A.j, A.x, A.iso, B.j, B.x, B.iso, C.j, (Z *)C.x, zc,
+        sum);
+    prof_end(ps, s);
+    // the totals, the zombie count and the live sum in one read
+    unsigned long long hv[10];
+    cudaError_t e = readback(hv, counter, 80, s);
+    if (e != cudaSuccess) { dev_free(C, s); return cuda_to_info(e); }
+    if (((const int32_t *)hv)[CT_ERR]) { dev_free(C, s); return PANIC; }
+    C.nzombies = (int64_t)hv[8];
+    if (live_sum) *live_sum = (int64_t)hv[9];
+    return SUCCESS;
 }
 
 template <class SR>
 static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
-                       const DevCSR &A, const DevCSR &B, cudaStream_t s)
+                       const DevCSR &A, const DevCSR &B, cudaStream_t s, int64_t *live_sum)
 {
     using Z = typename SR::z_t;
     const int64_t mnz = M.nnz;
     C.nrows = M.nrows; C.ncols = M.ncols; C.nnz = mnz; C.type = 0; C.iso = false;
+    if constexpr (IsCount<SR>::value) {
+        if (mnz >= CT_MIN_ENTRIES && M.nrows + B.nrows < INT32_MAX) {
+            const int info = dot3_count_launch<SR>(C, M, mask_struct, A, B, s, live_sum);
+            if (info != NO_VALUE) return info;
+        }
+    }
     C.p = (int32_t *)dalloc((size_t)(M.nrows + 1) * 4, s);
     C.j = (int32_t *)dalloc((size_t)(mnz ? mnz : 1) * 4, s);
     C.x = dalloc((size_t)(mnz ? mnz : 1) * sizeof(Z), s);
-    // the bitmap path: counting semirings on masks large enough to pay for it
-    const int64_t nkeys = M.nrows + B.nrows;
-    uint32_t bm_words = 0;
-    if constexpr (IsCount<SR>::value) {
-        if (mnz >= D3_BM_MIN_ENTRIES && nkeys < INT32_MAX) bm_words = bitmap_words<SR>(A.ncols);
-    }
-    // the work queue, the counters and the bitmap path's arrays in one
-    // allocation; the counters, group sizes, fill cursors and work sums come
-    // first and adjacent, so that one memset clears them
+    // the work queue and its counters in one allocation
     int *counter = nullptr;
     D3Work *queue = nullptr;
-    int32_t *gcnt = nullptr, *gfill = nullptr, *merge_sel = nullptr;
-    D3Rec *bucket = nullptr;
-    int64_t *gsz = nullptr, *goff = nullptr, *nit = nullptr, *ioff = nullptr, *ws = nullptr;
-    int64_t *nit_s = nullptr, *ioff_s = nullptr;
-    D3Item *items_s = nullptr;
-    unsigned long long *gwork = nullptr;
-    D3Item *items = nullptr;
     Carve cv(s);
     auto layout = [&]() {
         counter = cv.take<int>(16);
-        if (bm_words) {
-            gcnt = cv.take<int32_t>(nkeys);
-            gfill = cv.take<int32_t>(nkeys);
-            gwork = cv.take<unsigned long long>(nkeys);
-        }
         queue = cv.take<D3Work>(mnz ? mnz : 1);
-        if (bm_words) {
-            gsz = cv.take<int64_t>(nkeys + 1);
-            goff = cv.take<int64_t>(nkeys + 1);
-            nit = cv.take<int64_t>(nkeys + 1);
-            ioff = cv.take<int64_t>(nkeys + 1);
-            nit_s = cv.take<int64_t>(nkeys + 1);
-            ioff_s = cv.take<int64_t>(nkeys + 1);
-            items_s = cv.take<D3Item>(nkeys + mnz / 32 + 1);
-            items = cv.take<D3Item>(nkeys + mnz / 32 + 1);
-            bucket = cv.take<D3Rec>(mnz);
-            merge_sel = cv.take<int32_t>(mnz);
-            ws = cv.take<int64_t>((int64_t)scan_ws_elems(nkeys + 1));
-        }
     };
     layout();
     const bool got = cv.alloc();
@@ -916,10 +1120,10 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
         dev_free(C, s); return OUT_OF_MEMORY;
     }
     cudaMemcpyAsync(C.p, M.p, (size_t)(M.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
-    const char *zero_end = bm_words ? (const char *)(gwork + nkeys) : (const char *)(counter + 16);
-    cudaMemsetAsync(counter, 0, (size_t)(zero_end - (const char *)counter), s);
-    int *qlen = counter, *qnext = counter + 1, *merge_len = counter + 2, *inext = counter + 3;
+    cudaMemsetAsync(counter, 0, 16 * sizeof(int), s);
+    int *qlen = counter, *qnext = counter + 1;
     unsigned long long *zc = (unsigned long long *)((char *)counter + 32);
+    unsigned long long *sum = zc + 1;
     if (mnz > 0 && M.nrows > 0) {
         const int nsm = runtime().num_sms;
         int64_t warps_needed = (mnz + 31) / 32;
@@ -929,44 +1133,17 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
         k_dot3_classify<SR><<<(unsigned)blocks, 256, 0, s>>>(
             M.p, M.j, mask_struct ? nullptr : M.x, M.type, mask_struct, mnz, M.nrows,
             A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso, C.j, (Z *)C.x,
-            queue, qlen, zc, gcnt, bm_words * 32u);
-        if (bm_words) {
-            const int kb = (int)std::min<int64_t>((nkeys + 255) / 256, (int64_t)nsm * 8);
-            k_d3_gsize<<<kb, 256, 0, s>>>(gcnt, nkeys, gsz);
-            scan_exclusive_i64_ws(gsz, goff, nkeys + 1, ws, s);
-            k_d3_route<<<(unsigned)blocks, 256, 0, s>>>(queue, qlen, gsz, goff, gfill, gwork,
-                                                       bucket, (int32_t)M.nrows, merge_sel,
-                                                       merge_len);
-            k_d3_item_count<<<kb, 256, 0, s>>>(gsz, gwork, nkeys, (int32_t)M.nrows, A.p, B.p,
-                                               nit, nit_s);
-            scan_exclusive_i64_ws(nit, ioff, nkeys + 1, ws, s);
-            k_d3_item_fill<<<kb, 256, 0, s>>>(ioff, nkeys, goff, gwork, (int32_t)M.nrows,
-                                              A.p, A.j, B.p, B.j, items);
-            scan_exclusive_i64_ws(nit_s, ioff_s, nkeys + 1, ws, s);
-            k_d3_item_fill<<<kb, 256, 0, s>>>(ioff_s, nkeys, goff, gwork, (int32_t)M.nrows,
-                                              A.p, A.j, B.p, B.j, items_s);
-            if constexpr (IsCount<SR>::value)
-                k_dot3_hash_count<SR><<<nsm * 8, D3_HWARPS * 32, 0, s>>>(
-                    items_s, ioff_s + nkeys, inext + 1, bucket, (int32_t)M.nrows, A.j, B.j,
-                    C.j, (Z *)C.x, zc);
-            if constexpr (IsCount<SR>::value)
-                k_dot3_bitmap_count<SR><<<nsm, D3_BM_THREADS, (size_t)bm_words * 4, s>>>(
-                    items, ioff + nkeys, inext, bucket, (int32_t)M.nrows, A.j, B.j,
-                    bm_words, C.j, (Z *)C.x, zc);
-            k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
-                queue, merge_sel, merge_len, qnext, A.j, A.x, A.iso, B.j, B.x, B.iso,
-                C.j, (Z *)C.x, zc);
-        } else {
-            k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
-                queue, nullptr, qlen, qnext, A.j, A.x, A.iso, B.j, B.x, B.iso, C.j,
-                (Z *)C.x, zc);
-        }
+            queue, qlen, zc, sum);
+        k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
+            queue, nullptr, qlen, qnext, A.j, A.x, A.iso, B.j, B.x, B.iso, C.j,
+            (Z *)C.x, zc, sum);
         prof_end(ps, s);
     }
-    unsigned long long hz = 0;
-    cudaError_t e = readback(&hz, zc, 8, s);
+    unsigned long long hv[2] = {0, 0};
+    cudaError_t e = readback(hv, zc, 16, s);
     if (e != cudaSuccess) { dev_free(C, s); return cuda_to_info(e); }
-    C.nzombies = (int64_t)hz;
+    C.nzombies = (int64_t)hv[0];
+    if (live_sum && IsCount<SR>::value) *live_sum = (int64_t)hv[1];
     return SUCCESS;
 }
 
@@ -996,8 +1173,9 @@ static int dot3_all_zombies(DevCSR &C, const DevCSR &M, SemiringCode sr,
 }
 
 int dot3(DevCSR &C, const DevCSR &M, bool mask_struct, const DevCSR &A,
-         const DevCSR &B, SemiringCode sr, cudaStream_t s)
+         const DevCSR &B, SemiringCode sr, cudaStream_t s, int64_t *live_sum)
 {
+    if (live_sum) *live_sum = 0;
     if (A.ncols != B.ncols || M.nrows != A.nrows || M.ncols != B.nrows)
         return DIMENSION_MISMATCH;
     if (M.nzombies > 0) return NO_VALUE;   // the mask must be free of zombies
@@ -1018,7 +1196,8 @@ int dot3(DevCSR &C, const DevCSR &M, bool mask_struct, const DevCSR &A,
     if (all_false) return dot3_all_zombies(C, M, sr, s);
 #define GRB_DOT3_CASE(ADD, MULT, TC, CT)                                       \
     if (sr.add == ADD && sr.mult == MULT && sr.type == TC) {                   \
-        int info = dot3_launch<Semiring<ADD, MULT, CT>>(C, M, mask_struct, A, B, s); \
+        int info = dot3_launch<Semiring<ADD, MULT, CT>>(C, M, mask_struct, A, B, s, \
+                                                        live_sum);                 \
         if (info == SUCCESS) C.type = TC;                                      \
         return info;                                                           \
     }
@@ -1058,6 +1237,9 @@ static constexpr size_t NOALLOC_BYTES = (size_t)32 << 20;
 static constexpr size_t NOALLOC_HEAD = 256;        // counters, then the queue
 static constexpr int64_t NOALLOC_MAX_ENTRIES =
     (int64_t)((NOALLOC_BYTES - NOALLOC_HEAD) / sizeof(D3Work));
+// the limit the header publishes is the one enforced here
+static_assert(NOALLOC_MAX_ENTRIES == GRB_B200_DOT3_NOALLOC_MAX_ENTRIES,
+              "GRB_B200_DOT3_NOALLOC_MAX_ENTRIES must match the scratch array's capacity");
 
 static __device__ __align__(256) unsigned char g_dot3_scratch[NOALLOC_BYTES];
 
@@ -1095,20 +1277,23 @@ static int dot3_noalloc_launch(int64_t nrows, int64_t mnz, const int32_t *Mp,
     void *scratch = nullptr;
     int info = noalloc_scratch(&scratch);
     if (info != SUCCESS) return info;
+    int nsm = 0;
+    info = device_sm_count(&nsm);
+    if (info != SUCCESS) return info;
     int *qlen = (int *)scratch, *qnext = qlen + 1;
     unsigned long long *zc = (unsigned long long *)((char *)scratch + 32);
     D3Work *queue = (D3Work *)((char *)scratch + NOALLOC_HEAD);
     cudaError_t e = cudaMemsetAsync(scratch, 0, NOALLOC_HEAD, s);
     if (e != cudaSuccess) return cuda_to_info(e);
     if (mnz > 0 && nrows > 0) {
-        const int nsm = runtime().num_sms;
         int64_t blocks = ((mnz + 31) / 32 + 7) / 8;
         if (blocks > (int64_t)nsm * 16) blocks = (int64_t)nsm * 16;
         k_dot3_classify<SR><<<(unsigned)blocks, 256, 0, s>>>(
             Mp, Mj, nullptr, T_BOOL, true, mnz, nrows, Ap, Aj, Ax, a_iso,
-            Bp, Bj, Bx, b_iso, Cj, (Z *)Cx, queue, qlen, zc, nullptr, 0u);
+            Bp, Bj, Bx, b_iso, Cj, (Z *)Cx, queue, qlen, zc, nullptr);
         k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
-            queue, nullptr, qlen, qnext, Aj, Ax, a_iso, Bj, Bx, b_iso, Cj, (Z *)Cx, zc);
+            queue, nullptr, qlen, qnext, Aj, Ax, a_iso, Bj, Bx, b_iso, Cj, (Z *)Cx, zc,
+            nullptr);
     }
     unsigned long long hz = 0;
     e = cudaMemcpyAsync(&hz, zc, sizeof(hz), cudaMemcpyDeviceToHost, s);
@@ -1132,14 +1317,19 @@ extern "C" int grb_b200_dot3_noalloc(
     if (!Mp || !Mj || !Ap || !Aj || !Bp || !Bj || !Cj || !Cx || !semiring)
         return NULL_POINTER;
     if (nrows < 0 || ncols < 0 || mnz < 0) return INVALID_VALUE;
-    if (mnz > NOALLOC_MAX_ENTRIES || nrows >= INT32_MAX || ncols >= INT32_MAX) {
+    if (mnz > NOALLOC_MAX_ENTRIES) {
         fprintf(stderr, "grb_b200_dot3_noalloc: %lld mask entries exceed the fixed "
                 "scratch capacity of %lld entries\n", (long long)mnz,
                 (long long)NOALLOC_MAX_ENTRIES);
         return INVALID_VALUE;
     }
-    int info = init_device();
-    if (info != SUCCESS) return info;
+    if (nrows >= INT32_MAX || ncols >= INT32_MAX) {
+        fprintf(stderr, "grb_b200_dot3_noalloc: dimensions %lld x %lld do not fit the "
+                "int32 indices of the device arrays\n", (long long)nrows, (long long)ncols);
+        return INVALID_VALUE;
+    }
+    // no init_device() here: it changes the default memory pool's release
+    // threshold, and this entry point leaves the caller's allocator alone
     cudaStream_t s = (cudaStream_t)stream;
     SemiringCode sr{semiring->add_opcode, semiring->mult_opcode, semiring->type};
 #define GRB_NOALLOC_CASE(ADD, MULT, TC, CT)                                      \

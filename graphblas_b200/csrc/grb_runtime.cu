@@ -24,6 +24,25 @@ int cuda_to_info(cudaError_t e)
     return PANIC;
 }
 
+// The device's SM count, read once per process, without the pool setting
+// that init_device makes: callers that must leave the device's memory state
+// alone (the allocation-free entry point) use this instead.
+int device_sm_count(int *nsm)
+{
+    static std::atomic<int> cached[128];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 128) { cudaGetLastError(); return PANIC; }
+    int v = cached[dev].load();
+    if (v <= 0) {
+        e = cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess || v <= 0) { cudaGetLastError(); return PANIC; }
+        cached[dev].store(v);
+    }
+    *nsm = v;
+    return SUCCESS;
+}
+
 int init_device()
 {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -201,11 +220,15 @@ cudaError_t readback(void *dst, const void *src, size_t bytes, cudaStream_t s)
             buf = nullptr;
         }
     }
+    // a copy refused at submission leaves nothing for the synchronise to
+    // report, so its own status is checked first (the bytes are not read)
     if (!buf || bytes > READBACK_MAX) {
-        cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+        const cudaError_t c = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+        if (c != cudaSuccess) return c;
         return cudaStreamSynchronize(s);
     }
-    cudaMemcpyAsync(buf, src, bytes, cudaMemcpyDeviceToHost, s);
+    const cudaError_t c = cudaMemcpyAsync(buf, src, bytes, cudaMemcpyDeviceToHost, s);
+    if (c != cudaSuccess) return c;
     const cudaError_t e = cudaStreamSynchronize(s);
     if (e == cudaSuccess) memcpy(dst, buf, bytes);
     return e;

@@ -24,8 +24,12 @@ struct Runtime {
 
 Runtime &runtime();
 
-// initialise the device (idempotent); returns an Info code
+// initialise the device (idempotent); returns an Info code.  Sets the
+// release threshold of the device's default memory pool to "never".
 int init_device();
+
+// the current device's SM count (cached), touching no other device state
+int device_sm_count(int *nsm);
 
 // stream pool: acquire/release a non-blocking stream
 cudaStream_t stream_acquire();
@@ -155,9 +159,11 @@ void scan_exclusive_i64_ws(const int64_t *in, int64_t *out, int64_t n, int64_t *
 struct SemiringCode { int add, mult, type; };
 
 // C<M> = A*B' by dot products over M's pattern (Source/mxm/GB_AxB_dot3.c:37).
-// C gets M's pattern with zombies for empty dot products.
+// C gets M's pattern with zombies for empty dot products.  live_sum (may be
+// null) receives the sum of C's live entries for the counting semirings
+// (PLUS_PAIR on integers; wrapping int64 adds), 0 for the others.
 int dot3(DevCSR &C, const DevCSR &M, bool mask_struct, const DevCSR &A,
-         const DevCSR &B, SemiringCode sr, cudaStream_t s);
+         const DevCSR &B, SemiringCode sr, cudaStream_t s, int64_t *live_sum = nullptr);
 
 // C<M> = A*B row by row (Source/mxm/GB_AxB_saxpy3.c:119); M may be null.
 // Output rows are sorted, no zombies.

@@ -24,9 +24,13 @@ _lib = None
 
 
 def _gen():
+    """The generator library: lib/libgrb_b200_gen.so, or the library named by
+    $GRB_B200_GEN_LIB holding the same gen.c (bench.py's reference arm uses
+    the reference runner's copy so that it loads nothing of this package)."""
     global _lib
     if _lib is None:
-        path = os.path.join(_HERE, "lib", "libgrb_b200_gen.so")
+        path = os.environ.get("GRB_B200_GEN_LIB") or os.path.join(_HERE, "lib",
+                                                                  "libgrb_b200_gen.so")
         L = ctypes.CDLL(path)
         i32, i64, f64, f32 = (_P(np.int32), _P(np.int64), _P(np.float64),
                               _P(np.float32))

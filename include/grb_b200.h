@@ -375,7 +375,12 @@ int grb_b200_server_free(grb_b200_server *S);
  * The work queue and counters live in a fixed 32 MiB device array inside the
  * library (held by every GPU that loads it until the process exits), so masks
  * above GRB_B200_DOT3_NOALLOC_MAX_ENTRIES entries are rejected with
- * GrB_INVALID_VALUE.  The first call on each device looks up that array's
+ * GrB_INVALID_VALUE, as are dimensions of 2^31-1 or more.  Every entry takes
+ * the merge / binary-search route (the shared-memory bitmap and hash routes
+ * of the allocating entry point need per-call arrays), so counting semirings
+ * on skewed graphs run slower here than through grb_b200_dmxm_dot3.  The call
+ * changes no device-wide state: the default memory pool's settings are left
+ * as the caller has them.  The first call on each device looks up that array's
  * device address, so make it before any stream capture.  Calls share the
  * array: calls that overlap on the same GPU (concurrent streams or threads)
  * race and must be serialised by the caller.  Runs on `stream` (a

@@ -178,7 +178,7 @@ class Reference:
         L.ref_serve_replay.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64] + [vp] * 10 \
             + [vp]
         L.ref_batch_square.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, vp,
-                                       ctypes.c_int, ctypes.c_int, vp, vp]
+                                       ctypes.c_int, ctypes.c_int, vp, vp, vp]
         L.ref_serialize.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, vp, vp,
                                     vp, ctypes.c_int, ctypes.c_bool, ctypes.c_int,
                                     ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_uint64)]
@@ -294,17 +294,23 @@ class Reference:
             raise RuntimeError("reference bfs failed: %d" % info)
         return parent, float(secs[0]), int(nlev[0])
 
-    def batch_square(self, nsz, poff, ioff, Ap, Ai, Ax, add="MIN", mult="PLUS"):
+    def batch_square(self, nsz, poff, ioff, Ap, Ai, Ax, add="MIN", mult="PLUS",
+                     digests=False):
+        """A loop of GrB_mxm calls C_i = A_i*A_i (fp32); returns nnz(C_i), the
+        loop's seconds and, with `digests`, csr_digest of every C_i."""
         count = len(nsz)
         keep = [_i64(nsz), _i64(poff), _i64(ioff), _i64(Ap), _i64(Ai)]
         Ax = np.ascontiguousarray(Ax, dtype=np.float32)
         nnz_out = np.zeros(count, np.int64)
         secs = np.zeros(1, np.float64)
+        dig = np.zeros(count, np.uint64) if digests else None
         info = self.lib.ref_batch_square(count, *[_ptr(k) for k in keep],
                                          _ptr(Ax), OPS[add], OPS[mult],
-                                         _ptr(nnz_out), _ptr(secs))
+                                         _ptr(nnz_out), _ptr(secs), _ptr(dig))
         if info != 0:
             raise RuntimeError("reference batch failed: %d" % info)
+        if digests:
+            return nnz_out, float(secs[0]), dig
         return nnz_out, float(secs[0])
 
 
@@ -343,6 +349,34 @@ class Reference:
                            _ptr(count), _ptr(checksum), _ptr(latency), _ptr(makespan))
         L.ref_serve_clear()
         return status, count, checksum, latency, float(makespan[0])
+
+
+_DK1, _DK2 = np.uint64(0x9E3779B97F4A7C15), np.uint64(0xC2B2AE3D27D4EB4F)
+_DK3, _DK4 = np.uint64(0x165667B19E3779F9), np.uint64(0x27D4EB2F165667C5)
+
+
+def csr_digest(p, i, x):
+    """Position-weighted 64-bit digest of a CSR matrix: every entry's row,
+    column and value bits, weighted by its position, summed mod 2^64 (the
+    reference runner's csr_digest computes the same).  Equal digests mean the
+    same sorted pattern and bit-identical values, short of a collision."""
+    p = np.asarray(p, np.int64)
+    n = len(p) - 1
+    nnz = int(p[-1]) if n >= 0 else 0
+    i = np.asarray(i[:nnz], np.int64).view(np.uint64)
+    x = np.ascontiguousarray(x[:nnz])
+    if x.dtype.itemsize == 4:
+        bits = x.view(np.uint32).astype(np.uint64)
+    elif x.dtype.itemsize == 8:
+        bits = x.view(np.uint64)
+    else:
+        bits = x.view(np.uint8).astype(np.uint64)
+    rows = np.repeat(np.arange(n, dtype=np.uint64), np.diff(p))
+    t = np.arange(nnz, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        h = np.uint64(n) * _DK1 + np.uint64(nnz)
+        terms = ((rows * _DK1 + i) * _DK2 + bits + np.uint64(1)) * (t * _DK3 + _DK4)
+        return int(h + np.sum(terms, dtype=np.uint64))
 
 
 def reference_available():

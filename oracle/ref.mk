@@ -8,12 +8,12 @@
 # disabled JIT reads, and the no-JIT JITpackage/GB_JITpackage.c) are generated
 # from their templates into oracle/_ref/gen when the tree does not hold them.
 #
-#   make -f oracle/ref.mk REF=/root/reference -j8
+#   make -f oracle/ref.mk -j8        (REF defaults to BASELINE.json's reference_path)
 #
 # The library is test infrastructure: the parity tests and the CPU-baseline
 # leg of bench.py load it as the checker; no product code links it.
 
-REF    ?= /root/reference
+REF    ?= $(shell sed -n 's/.*"reference_path": *"\([^"]*\)".*/\1/p' BASELINE.json)
 OUT    := oracle/_ref
 OBJ    := $(OUT)/obj
 GEN    := $(OUT)/gen

@@ -358,10 +358,31 @@ done:
 // uses rows [off[i], off[i+1]) of the concatenated row pointer arrays:
 // Ap + poff[i] (n_i + 1 entries) indexes Ai + ioff[i] / Ax + ioff[i].
 // nnz_out[i] gets nnz(C_i); returns GrB_Info, *seconds the loop time.
+// Position-weighted digest of a CSR matrix (row, column and value bits of
+// every entry, in storage order); the same function is oracle.csr_digest in
+// Python, so results can be compared without moving them.
+static uint64_t csr_digest(int64_t nrows, const GrB_Index *p, const GrB_Index *i,
+                           const void *x, size_t ts)
+{
+    const uint64_t K1 = 0x9E3779B97F4A7C15ull, K2 = 0xC2B2AE3D27D4EB4Full;
+    const uint64_t K3 = 0x165667B19E3779F9ull, K4 = 0x27D4EB2F165667C5ull;
+    uint64_t h = (uint64_t)nrows * K1 + (uint64_t)p[nrows];
+    for (int64_t r = 0; r < nrows; r++)
+        for (GrB_Index t = p[r]; t < p[r + 1]; t++)
+        {
+            uint64_t bits = 0;
+            memcpy(&bits, (const char *)x + t * ts, ts);
+            h += (((uint64_t)r * K1 + (uint64_t)i[t]) * K2 + bits + 1) * ((uint64_t)t * K3 + K4);
+        }
+    return h;
+}
+
+// digest_out (optional, one per instance): csr_digest of each C_i after the
+// timed loop
 int ref_batch_square(int count, const int64_t *nsz, const int64_t *poff,
                      const int64_t *ioff, const int64_t *Ap, const int64_t *Ai,
                      const float *Ax, int add, int mult, int64_t *nnz_out,
-                     double *seconds)
+                     double *seconds, uint64_t *digest_out)
 {
     GrB_Info info = GrB_SUCCESS;
     GrB_Semiring S = NULL;
@@ -392,6 +413,24 @@ int ref_batch_square(int count, const int64_t *nsz, const int64_t *poff,
         GrB_Index nv = 0;
         GrB_Matrix_nvals(&nv, Cs[b]);
         nnz_out[b] = (int64_t)nv;
+        if (digest_out)
+        {
+            GrB_Index *p = NULL, *i = NULL, psz, isz, xsz;
+            void *x = NULL;
+            bool iso = false;
+            TRY(GxB_Matrix_unpack_CSR(Cs[b], &p, &i, &x, &psz, &isz, &xsz, &iso, NULL,
+                                      NULL));
+            if (iso && p[nsz[b]] > 0)
+            {
+                // expand an iso result to one value per entry
+                float v = *(float *)x;
+                free(x);
+                x = malloc(p[nsz[b]] * sizeof(float));
+                for (GrB_Index t = 0; t < p[nsz[b]]; t++) ((float *)x)[t] = v;
+            }
+            digest_out[b] = csr_digest(nsz[b], p, i, x, sizeof(float));
+            free(p); free(i); free(x);
+        }
     }
 done:
     for (int b = 0; b < count; b++)

@@ -170,3 +170,37 @@ def test_dot3_edge_cases(gpu, oracle):
     want = oracle.dot3(1, 1, (A1.p, A1.i, A1.x, 8), (B1.p, B1.i, B1.x, 8),
                        (M1.p, M1.i, None, 1), "PLUS", "TIMES", 8)
     assert_exact(got, want, "1x1")
+
+
+@pytest.mark.parametrize("tname,np_t", [("int64", np.int64), ("int32", np.int32)])
+@pytest.mark.parametrize("mask_struct", [True, False])
+def test_dot3_count_groups_valued_mask_and_sum(gpu, oracle, tname, np_t, mask_struct):
+    """The counting path (PLUS_PAIR on integers) on skewed operands: key rows
+    of every size (warp hash tables up to 1024 entries, block bitmaps above),
+    groups keyed by A's rows and by B's rows, lists long enough for every
+    lane class, empty rows, and a valued mask a third of whose entries are
+    false.  C must equal the oracle's, and the sum that comes back with C
+    (used by the following reduction) must equal the sum of its values."""
+    gb = gpu
+    S = W.rmat(12, 24, seed=17)
+    n = S.nrows
+    A = W.Csr(n, n, S.p, S.i, np.ones(S.nnz, np_t))
+    T = W.rmat(12, 24, seed=18)
+    B = W.Csr(n, n, T.p, T.i, np.ones(T.nnz, np_t))
+    M = random_csr(n, n, 0.004, 19, np.float64, empty_rows=0.2)
+    M.x = (np.arange(M.nnz) % 3).astype(np.float64)
+    tc = gb.TYPES[tname]
+    sr = gb.semiring("PLUS", "PAIR", tname)
+    dM = gb.DMatrix.upload(M)
+    dA = gb.DMatrix.upload(A)
+    dB = gb.DMatrix.upload(B)
+    C = gb.dot3(dM, dA, dB, sr, mask_struct=mask_struct)
+    total = int(gb.reduce(C, "PLUS", np_t))
+    got = C.download(prune=True)
+    want = oracle.dot3(n, n, (A.p, A.i, A.x, tc), (B.p, B.i, B.x, tc),
+                       (M.p, M.i, None if mask_struct else M.x, 1 if mask_struct else 11),
+                       "PLUS", "PAIR", tc, mask_struct=mask_struct)
+    assert_exact(got, want, "plus_pair groups")
+    assert total == int(np.sum(want[2].astype(np.int64)).astype(np_t))
+    for d in (dM, dA, dB, C):
+        d.free()

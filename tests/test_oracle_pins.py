@@ -22,8 +22,9 @@ from graphblas_b200 import workloads as W
 from tests.helpers import assert_exact, random_csr
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# blobs.npz: test_serialize.py; fullsize.npz: test_oracle_fullsize.py
 GOLD = sorted(g for g in glob.glob(os.path.join(HERE, "golden", "*.npz"))
-              if not g.endswith("blobs.npz"))          # blobs.npz: test_serialize.py
+              if not g.endswith(("blobs.npz", "fullsize.npz")))
 
 
 @pytest.fixture(scope="module")

@@ -37,8 +37,26 @@ def _dev(torch, a, dtype):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).cuda()
 
 
-def _noalloc(gb, torch, M, A, B, sr, np_t):
-    """Run the no-alloc entry point on device copies of M, A, B."""
+def _pool_used():
+    """Bytes in use in the device's default memory pool (the pool the
+    allocating entry points draw from) and the device's free memory."""
+    import torch
+    from cuda.bindings import driver as cu
+    cu.cuInit(0)
+    err, dev = cu.cuDeviceGet(torch.cuda.current_device())
+    assert err == cu.CUresult.CUDA_SUCCESS
+    err, pool = cu.cuDeviceGetDefaultMemPool(dev)
+    assert err == cu.CUresult.CUDA_SUCCESS
+    err, used = cu.cuMemPoolGetAttribute(
+        pool, cu.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_CURRENT)
+    assert err == cu.CUresult.CUDA_SUCCESS
+    return int(used), torch.cuda.mem_get_info()[0]
+
+
+def _noalloc(gb, torch, M, A, B, sr, np_t, watch=False):
+    """Run the no-alloc entry point on device copies of M, A, B.  With
+    `watch`, the call itself is checked to leave the default memory pool's
+    usage and the device's free memory as they were."""
     f = _bind(gb.lib())
     d = {k: _dev(torch, v, np.int32) for k, v in
          (("Mp", M.p), ("Mj", M.i), ("Ap", A.p), ("Aj", A.i), ("Bp", B.p), ("Bj", B.i))}
@@ -51,6 +69,7 @@ def _noalloc(gb, torch, M, A, B, sr, np_t):
     nz = ctypes.c_int64(-1)
     stream = torch.cuda.current_stream().cuda_stream
     torch.cuda.synchronize()
+    before = _pool_used() if watch else None
     info = f(M.nrows, M.ncols, mnz, d["Mp"].data_ptr(), d["Mj"].data_ptr(),
              d["Ap"].data_ptr(), d["Aj"].data_ptr(),
              Ax.data_ptr() if Ax is not None else None, False,
@@ -59,6 +78,8 @@ def _noalloc(gb, torch, M, A, B, sr, np_t):
              ctypes.byref(sr), Cj.data_ptr(), Cx.data_ptr(), ctypes.byref(nz),
              stream)
     assert info == 0, "grb_b200_dot3_noalloc returned %d" % info
+    if watch:
+        assert _pool_used() == before, "the no-alloc call allocated device memory"
     return Cj[:mnz].cpu().numpy(), Cx[:mnz].cpu().numpy(), nz.value
 
 
@@ -104,6 +125,10 @@ def test_noalloc_matches_allocating_dot3_twice(gpu):
     got2 = _noalloc(gb, torch, M, A, B, sr2, np.float64)
     want2 = _allocating(gb, M, A, B, sr2, "fp64")
     _check(got2, want2, M)
+    # the same call once more, now that the library's module is loaded: it
+    # draws nothing from the default pool and takes no device memory
+    got3 = _noalloc(gb, torch, M, A, B, sr2, np.float64, watch=True)
+    _check(got3, want2, M)
 
 
 def test_noalloc_rejects_oversize_mask(gpu):
