@@ -2,17 +2,16 @@
 """Benchmark of the B200 semiring SpGEMM path (SuiteSparse:GraphBLAS GrB_mxm).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config tc|saxpy|bfs|batch|serve]
+                    [--config all|tc|saxpy|bfs|batch|serve]
 
 Workloads (seeded synthetic inputs of the graph500 / Erdos-Renyi shapes the
 reference is measured on; no dataset is read):
 
-  tc     (default, the headline) masked dot3 triangle counting,
-         C<L> = L*U' with plus_pair int64 then a sum reduction, on a
-         symmetrised R-MAT graph of scale 20, edge factor 16,
-         (a,b,c,d) = (0.57,0.19,0.19,0.05), self-loops and duplicates removed.
-         One step = GrB_mxm + GrB_reduce over the whole graph; metric
-         triangles/s.
+  tc     (the headline) masked dot3 triangle counting, C<L> = L*U' with
+         plus_pair int64 then a sum reduction, on a symmetrised R-MAT graph of
+         scale 20, edge factor 16, (a,b,c,d) = (0.57,0.19,0.19,0.05),
+         self-loops and duplicates removed.  One step = GrB_mxm + GrB_reduce
+         over the whole graph; metric triangles/s.
   saxpy  C = A*B, plus_times fp64, A and B 16384x16384 Erdos-Renyi with 8
          uniform columns per row, values U[-1,1]; metric GFLOP/s (2 flops per
          product).
@@ -21,15 +20,23 @@ reference is measured on; no dataset is read):
          scale 22, edge factor 16; metric TEPS (undirected edges / s).
   batch  4096 independent C_k = A_k*A_k, min_plus fp32, n_k log-uniform in
          [64, 8192], Poisson(6) entries per row; metric GFLOP/s.
+  serve  an open-loop Poisson stream (2000 req/s) of mixed requests on
+         device-resident graphs; metric req/s with p50/p99 latency.
+
+The default (--config all) prints one line: the tc workload's figures at the
+top level and the other four under "configs", each with its own value, e2e,
+roofline, cpu_baseline and parity.
 
 * value: device time with the inputs resident in HBM, CUDA events on the
   launching stream, L2 flushed (a 256 MB write) between steps, max over ranks.
 * e2e: the same step through the public API from pinned host buffers, the
   host->device copies and the result read-back inside the timed region.
-* roofline: the dominant kernel's algorithmic bytes per launch over its
-  event-timed duration, against the measured HBM copy bandwidth.
+* roofline: bytes per launch of the dominant kernel (or kernel phase) over
+  its event-timed duration, against the measured HBM copy bandwidth; the
+  byte basis of each workload is named in the line ("basis").
 * cpu_baseline: the reference library (oracle/_ref, SuiteSparse:GraphBLAS
-  built from its own sources) on this host's cores, same inputs.
+  built from its own sources) on this host's cores, same inputs, with the
+  parity of the device's result against the reference's ("parity").
 
 --impl reference times the reference's CPU path alone and prints its line.
 Multi-GPU (torchrun): every rank runs an independent replica (the path has no
@@ -133,15 +140,22 @@ class TriCount:
         S = W.rmat(self.scale, 16, seed=args.seed)
         self.S = S
         self.L, self.U = W.tril_triu(S)
+        n, nnz = S.nrows, self.L.nnz
+        # compulsory bytes of one call (int32 offsets and indices in HBM):
+        # L, U and the mask (L again, read by its own pass) once each, C
+        # written once (offsets, indices, int64 counts)
+        self.alg_bytes = 3.0 * (4.0 * (n + 1) + 4.0 * nnz) + 4.0 * (n + 1) + 12.0 * nnz
+        self.basis = ("compulsory: L, U and the mask read once, C written once "
+                      "(4-byte offsets and indices, 8-byte counts)")
         dL = np.diff(self.L.p).astype(np.float64)
         dU = np.diff(self.U.p).astype(np.float64)
-        # merge reads of every (i,j) in L plus mask read and C write
-        self.alg_bytes = 4.0 * (np.sum(dL * dL) + np.sum(dU * dU)) + 16.0 * self.L.nnz
+        # the merge-equivalent figure: every mask entry merging its two rows
+        self.merge_equiv_bytes = 4.0 * (np.sum(dL * dL) + np.sum(dU * dU)) + 16.0 * nnz
         self.workload = "tricount_rmat%d_ef16_dot3_plus_pair" % self.scale
-        # DRAM bytes of one dot3 call (dram__bytes_read.sum + dram__bytes_write.sum
-        # over its kernels, ncu on R-MAT scale 18: 431.6 MB for 3,805,187 mask
-        # entries), scaled by mask entries
-        self.traffic_per_launch = 431.6e6 / 3805187 * self.L.nnz
+        # DRAM bytes of one dot3 call at scale 20 (dram__bytes_read.sum +
+        # dram__bytes_write.sum over its kernels, one ncu capture of this
+        # workload at this size)
+        self.traffic_per_launch = TC_TRAFFIC_RMAT20 if self.scale == 20 else None
 
     def config(self):
         return {"n": int(self.S.nrows), "nnz_L": int(self.L.nnz),
@@ -185,18 +199,22 @@ class TriCount:
         return n
 
     def launches_per_step(self):
-        # classify, intersect, reduce partial + final; with the bitmap path
-        # (masks of 65536+ entries) also group sizes, route, item count, two
-        # item fills, the bitmap and warp-hash kernels, and three scans over
-        # the group keys
-        if self.L.nnz < (1 << 16):
+        # the counting path (masks of 1024+ entries): classify, plan, route,
+        # the warp-hash and block-bitmap count kernels and the merge kernel;
+        # the sum of C comes back with the call, so the reduction launches
+        # nothing.  Smaller masks: classify and intersect, then the two
+        # reduction launches.
+        if self.L.nnz < 1024:
             return 4
-        return 4 + 7 + 3 * scan_launches(self.S.nrows + self.U.nrows + 1)
+        return 6
 
     def cpu_baseline(self, R, ncores):
-        ntri, times = R.tricount(self.S.nrows, self.L.p, self.L.i, self.U.p, self.U.i, reps=1)
-        assert ntri == self.ntri, "CPU and GPU triangle counts differ"
-        return ntri / float(times[0]), "whole graph, one GrB_mxm + GrB_reduce (%.2f s)" % times[0]
+        ntri, times = R.tricount(self.S.nrows, self.L.p, self.L.i, self.U.p, self.U.i, reps=5)
+        t = float(np.median(times))
+        parity = ("exact: %d triangles, the reference's count" % ntri if ntri == self.ntri
+                  else "MISMATCH: reference %d, device %d" % (ntri, self.ntri))
+        return (ntri / t, "whole graph, GrB_mxm + GrB_reduce, median of 5 (%.2f s)" % t,
+                parity)
 
     def reference_steps(self, R, steps, warmup):
         for _ in range(warmup):
@@ -244,6 +262,8 @@ class Saxpy:
         # algorithmic bytes (4 B index, 8 B value): A once, B rows per product, C once
         self.alg_bytes = (4.0 * (self.n + 1) + 12.0 * self.A.nnz + 12.0 * self.products +
                           12.0 * self.nnz_c + 4.0 * (self.n + 1))
+        self.basis = ("A once, the B row of every product, C once (4-byte indices, "
+                      "8-byte values); the 27 MB problem fits in L2")
 
     def step_dev(self):
         self.api.mxm(self.Cg, None, None, "GrB_PLUS_TIMES_SEMIRING_FP64", self.Ag, self.Bg)
@@ -285,18 +305,24 @@ class Saxpy:
         return 6 + 2 * scan_launches(self.n + 1)
 
     def cpu_baseline(self, R, ncores):
-        t = 0.0
+        from oracle import csr_digest
         reps = 5
+        args = (self.n, self.n, self.n, (self.A.p, self.A.i, self.A.x, 11),
+                (self.B.p, self.B.i, self.B.x, 11), "PLUS", "TIMES", 11)
+        ref = R.mxm(*args)
+        times = []
         for _ in range(reps):
-            _, _, _ = R.mxm(self.n, self.n, self.n, (self.A.p, self.A.i, self.A.x, 11),
-                            (self.B.p, self.B.i, self.B.x, 11), "PLUS", "TIMES", 11)
-        # the runner times GrB_mxm + wait itself; re-run for the timing
-        t0 = time.perf_counter()
-        for _ in range(reps):
-            R.mxm(self.n, self.n, self.n, (self.A.p, self.A.i, self.A.x, 11),
-                  (self.B.p, self.B.i, self.B.x, 11), "PLUS", "TIMES", 11)
-        t = (time.perf_counter() - t0) / reps
-        return self.flops / 1e9 / t, "whole product, %d reps incl. CSR pack/unpack (%.1f ms)" % (reps, 1e3 * t)
+            t0 = time.perf_counter()
+            R.mxm(*args)
+            times.append(time.perf_counter() - t0)
+        t = float(np.median(times))
+        got = self.api.matrix_to_csr(self.Cg, 11, self.n)
+        same = csr_digest(*got) == csr_digest(*ref)
+        parity = ("exact: C bit-identical to the reference's (%d entries)" % len(ref[1])
+                  if same else "MISMATCH: C differs from the reference's")
+        return (self.flops / 1e9 / t,
+                "whole product, median of %d incl. CSR pack/unpack (%.1f ms)" % (reps, 1e3 * t),
+                parity)
 
     def reference_steps(self, R, steps, warmup):
         for _ in range(warmup):
@@ -338,9 +364,11 @@ class Bfs:
         self.gb = gb
         self.api = API()
         self.Sg = self.api.matrix_from_csr(self.S, 1)
-        # algorithmic bytes of the whole traversal: every reached vertex's row
-        # (8 B row pointer + 4 B per index) once, plus 8 B parent writes
+        # bytes of the whole traversal: every row once (8 B of row offsets and
+        # 4 B per index, as if every vertex were reached) plus 8 B parent
+        # writes
         self.alg_bytes = 8.0 * self.n + 4.0 * self.S.nnz + 8.0 * self.n
+        self.basis = "S read once (offsets and indices), the parent vector written once"
 
     def bfs(self, Sg):
         api = self.api
@@ -363,6 +391,16 @@ class Bfs:
         self.api.vfree(q)
         self.api.vfree(p)
         return self.edges
+
+    def parents(self):
+        """The parent vector of one more traversal (untimed), dense."""
+        q, p = self.bfs(self.Sg)
+        idx, par = self.api.vector_to(p, 8)
+        self.api.vfree(q)
+        self.api.vfree(p)
+        out = np.full(self.n, -1, np.int64)
+        out[idx] = par
+        return out
 
     def e2e_setup(self, torch):
         # S arrives from page-locked host memory through GrB_Matrix_import
@@ -397,8 +435,24 @@ class Bfs:
         return 26 * max(getattr(self, "levels", 1), 1)
 
     def cpu_baseline(self, R, ncores):
-        parent, secs, nlev = R.bfs(self.n, self.S.p, self.S.i, self.src)
-        return self.edges / secs, "whole traversal, vxm + assign per level (%.2f s)" % secs
+        """The reference's traversal on all cores, timed (median of 3), and
+        parity against the single-threaded reference (the max-parent rule of
+        its ANY monoid is exact there)."""
+        times = []
+        for _ in range(3):
+            _, secs, nlev = R.bfs(self.n, self.S.p, self.S.i, self.src)
+            times.append(secs)
+        t = float(np.median(times))
+        nt = R.nthreads
+        R.set_nthreads(1)
+        ref, _, _ = R.bfs(self.n, self.S.p, self.S.i, self.src)
+        R.set_nthreads(nt)
+        got = self.parents()
+        bad = int(np.sum(got != ref))
+        parity = ("exact: all %d parents equal the single-threaded reference's" % self.n
+                  if bad == 0 else "MISMATCH: %d parents differ" % bad)
+        return (self.edges / t, "whole traversal, vxm + assign per level, median of 3 "
+                "(%.3f s)" % t, parity)
 
     def reference_steps(self, R, steps, warmup):
         for _ in range(warmup):
@@ -415,6 +469,11 @@ class Bfs:
 
 
 CONFIGS = {"tc": TriCount, "saxpy": Saxpy, "bfs": Bfs}
+SUB_CONFIGS = ("saxpy", "bfs", "batch", "serve")
+
+# DRAM bytes (read + write) of one triangle-count dot3 call at R-MAT scale 20,
+# summed over its kernels from one ncu capture of this workload
+TC_TRAFFIC_RMAT20 = None
 
 
 def make_batch(args):
@@ -427,40 +486,58 @@ def make_serve(args):
     return S.BenchServe(args)
 
 
+def workload_class(name):
+    return CONFIGS.get(name) or {"batch": make_batch, "serve": make_serve}.get(name)
+
+
 # ---------------------------------------------------------------------------
 # harness
 # ---------------------------------------------------------------------------
 
-def run_reference(args, cfg):
+def reference_line(args, name, steps, warmup, R, ncores):
+    """One workload on the reference's CPU path: its figures as a dict."""
+    work = workload_class(name)(args)
+    try:
+        units, secs, sample = work.reference_steps(R, steps, warmup)
+    except NotImplementedError:
+        return {"unavailable": "the reference has no path for this workload"}
+    val = units / secs
+    return {"metric": work.metric, "value": val, "unit": work.unit,
+            "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * secs / steps,
+            "higher_is_better": True, "dtype": work.dtype,
+            "config": dict(workload=work.workload, threads=ncores, **work.config()),
+            "cpu_baseline": {"value": val, "unit": work.unit, "cores": ncores,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": val, "unit": work.unit, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def run_reference(args):
     """The reference's own CPU path (oracle/_ref) on this host's cores."""
-    from oracle import Reference, reference_available
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    # the reference arm builds its inputs with the generators compiled into
+    # the reference runner, so it loads no library of graphblas_b200
+    os.environ["GRB_B200_GEN_LIB"] = os.path.join(ROOT, "oracle", "_ref", "libref_runner.so")
+    from oracle import Reference, reference_available
     if not reference_available():
         print(json.dumps({"impl": "reference",
                           "unavailable": "reference library oracle/_ref not built"}))
         return 0
     ncores = os.cpu_count()
     R = Reference(nthreads=ncores)
-    work = cfg(args)
-    try:
-        units, secs, sample = work.reference_steps(R, args.steps, args.warmup)
-    except NotImplementedError:
-        print(json.dumps({"impl": "reference", "unavailable":
-                          "the reference has no request server for this workload"}))
-        return 0
-    val = units / secs
-    line = {"metric": work.metric, "value": val, "unit": work.unit,
-            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": work.dtype, "data": "synthetic",
-            "config": dict(workload=work.workload, threads=ncores, **work.config()),
-            "cpu_baseline": {"value": val, "unit": work.unit, "cores": ncores,
-                             "kind": "reference", "sample": sample},
-            "e2e": {"value": val, "unit": work.unit, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+    head = "tc" if args.config == "all" else args.config
+    line = reference_line(args, head, args.steps, args.warmup, R, ncores)
+    line.update({"impl": "reference", "n_gpus": args.gpus, "scaling": "weak",
+                 "vs_baseline": None, "data": "synthetic"})
+    if args.config == "all":
+        # the other workloads, each a bounded sample: a few steps
+        subs = {}
+        for name in SUB_CONFIGS:
+            k = 1 if name in ("batch", "serve") else min(args.steps, 5)
+            subs[name] = reference_line(args, name, k, 1, R, ncores)
+        line["configs"] = subs
     print(json.dumps(line))
     return 0
 
@@ -480,23 +557,123 @@ def pin_rank_gpu():
     return 0, physical
 
 
+class Harness:
+    """Timing shared by every workload: warm-up, K timed steps between CUDA
+    events on the library's stream with an L2 flush before each, clocks
+    sampled meanwhile, max over ranks; then the same through the public API
+    from pinned host buffers (e2e); then the reference on the host."""
+
+    def __init__(self, args, gb, torch, dist, smi_index):
+        self.args, self.gb, self.torch, self.dist = args, gb, torch, dist
+        self.smi_index = smi_index
+        self.L = gb.lib()
+        self.stream = torch.cuda.Stream()
+        self.L.grb_b200_set_stream(ctypes.c_void_p(self.stream.cuda_stream))
+        self.flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+
+    def barrier(self):
+        self.torch.cuda.synchronize()
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def timed(self, fn, k_steps, profile_kernel=None):
+        torch, stream, L_ = self.torch, self.stream, self.L
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k_steps)]
+        units = 0.0
+        if profile_kernel:
+            L_.grb_b200_profile_reset()
+            L_.grb_b200_profile_enable(True)
+        with torch.cuda.stream(stream):
+            for k in range(k_steps):
+                self.flush.fill_(k & 0xff)
+                ev[k][0].record(stream)
+                units += fn()
+                ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        if profile_kernel:
+            L_.grb_b200_profile_enable(False)
+        return units, sum(a.elapsed_time(b) for a, b in ev)
+
+    def measure(self, work, steps, warmup, cpu=True):
+        torch, gb = self.torch, self.gb
+        work.dev_setup(gb)
+        with torch.cuda.stream(self.stream):
+            for _ in range(warmup):
+                work.step_dev()
+        self.barrier()
+        sampler = ClockSampler(self.smi_index)
+        sampler.start()
+        units, dev_ms = self.timed(work.step_dev, steps, profile_kernel=work.kernel)
+        clocks = sampler.stop()
+        kms, kcount = profile(self.L, work.kernel)
+        self.barrier()
+        t_max = allreduce_max(self.dist, dev_ms)
+        units_all = allreduce_sum(self.dist, units)
+        h2d, d2h = work.e2e_setup(torch)
+        with torch.cuda.stream(self.stream):
+            for _ in range(warmup):
+                work.step_e2e()
+        self.barrier()
+        units2, e2e_ms = self.timed(work.step_e2e, steps)
+        e2e_max = allreduce_max(self.dist, e2e_ms)
+        units2_all = allreduce_sum(self.dist, units2)
+        if hasattr(work, "finish"):
+            work.finish(t_max / steps)
+        hbm_peak, peak_kind = peaks()
+        kernel_ms = kms / max(kcount, 1)
+        launches_per_step = max(kcount // max(steps, 1), 1)
+        if getattr(work, "kernel_ms_override", None):
+            # numeric phase replayed as a CUDA graph: timed in a separate eager run
+            kernel_ms, launches_per_step = work.kernel_ms_override, 1
+        alg_per_launch = work.alg_bytes / launches_per_step
+        achieved = alg_per_launch / (kernel_ms * 1e-3) / 1e9 if kernel_ms > 0 else None
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": (achieved / hbm_peak) if achieved else None,
+                "peak_kind": peak_kind, "basis": getattr(work, "basis", None),
+                "traffic": getattr(work, "traffic_per_launch", None),
+                "kernel": work.kernel, "kernel_ms_per_launch": kernel_ms,
+                "algorithmic_bytes_per_launch": alg_per_launch}
+        if getattr(work, "merge_equiv_bytes", None):
+            roof["merge_equiv_bytes"] = work.merge_equiv_bytes / launches_per_step
+        line = {
+            "metric": work.metric, "value": units_all / (t_max * 1e-3), "unit": work.unit,
+            "ms_per_step": t_max / steps, "steps": steps, "warmup": warmup,
+            "higher_is_better": True, "dtype": work.dtype,
+            "config": dict(workload=work.workload,
+                           parallelism="replicas" if self.world > 1 else "single",
+                           l2="flushed (256 MB write) between steps", **work.config()),
+            "e2e": {"value": units2_all / (e2e_max * 1e-3), "unit": work.unit,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_max / steps},
+            "gpu_launches": work.launches_per_step() * steps,
+            "roofline": roof, "clocks": clocks,
+        }
+        if self.rank == 0 and cpu:
+            line["cpu_baseline"] = cpu_baseline(work)
+            line["parity"] = line["cpu_baseline"].pop("parity", None)
+        work.free()
+        return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="tc")
+    ap.add_argument("--config", default="all")
     ap.add_argument("--scale", type=int, default=0)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    cfg = CONFIGS.get(args.config) or {"batch": make_batch, "serve": make_serve}.get(args.config)
-    if cfg is None:
+    if args.config != "all" and workload_class(args.config) is None:
         raise SystemExit("unknown --config %s" % args.config)
     if args.impl == "reference":
-        return run_reference(args, cfg)
+        return run_reference(args)
 
     device, smi_index = pin_rank_gpu()
     import torch
@@ -511,106 +688,34 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     gb.init()
-    L_ = gb.lib()
-    stream = torch.cuda.Stream()
-    L_.grb_b200_set_stream(ctypes.c_void_p(stream.cuda_stream))
-    work = cfg(args)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-
-    def timed(fn, k_steps, profile_kernel=None):
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(k_steps)]
-        units = 0.0
-        if profile_kernel:
-            L_.grb_b200_profile_reset()
-            L_.grb_b200_profile_enable(True)
-        with torch.cuda.stream(stream):
-            for k in range(k_steps):
-                flush.fill_(k & 0xff)
-                ev[k][0].record(stream)
-                units += fn()
-                ev[k][1].record(stream)
-        torch.cuda.synchronize()
-        if profile_kernel:
-            L_.grb_b200_profile_enable(False)
-        return units, sum(a.elapsed_time(b) for a, b in ev)
-
-    work.dev_setup(gb)
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            work.step_dev()
-    barrier()
-    sampler = ClockSampler(smi_index)
-    sampler.start()
-    units, dev_ms = timed(work.step_dev, args.steps, profile_kernel=work.kernel)
-    clocks = sampler.stop()
-    kms, kcount = profile(L_, work.kernel)
-    barrier()
-    t_max = allreduce_max(dist, dev_ms)
-    units_all = allreduce_sum(dist, units)
-
-    h2d, d2h = work.e2e_setup(torch)
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            work.step_e2e()
-    barrier()
-    units2, e2e_ms = timed(work.step_e2e, args.steps)
-    e2e_max = allreduce_max(dist, e2e_ms)
-    units2_all = allreduce_sum(dist, units2)
-
-    if hasattr(work, "finish"):
-        work.finish(t_max / args.steps)
-    hbm_peak, peak_kind = peaks()
-    kernel_ms = kms / max(kcount, 1)
-    launches_per_step = max(kcount // max(args.steps, 1), 1)
-    if getattr(work, "kernel_ms_override", None):
-        # numeric phase replayed as a CUDA graph: timed in a separate eager run
-        kernel_ms, launches_per_step = work.kernel_ms_override, 1
-    alg_per_launch = work.alg_bytes / launches_per_step
-    achieved = alg_per_launch / (kernel_ms * 1e-3) / 1e9 if kernel_ms > 0 else None
+    H = Harness(args, gb, torch, dist, smi_index)
+    cpu = not args.no_cpu_baseline
+    head = "tc" if args.config == "all" else args.config
+    line = H.measure(workload_class(head)(args), args.steps, args.warmup, cpu)
+    line.update({"n_gpus": world, "scaling": "weak", "vs_baseline": None,
+                 "data": "synthetic"})
+    mismatch = line.get("parity") and "MISMATCH" in line["parity"]
+    if args.config == "all":
+        subs = {}
+        for name in SUB_CONFIGS:
+            # the serving replay is seconds long: two timed replays
+            k = 2 if name == "serve" else args.steps
+            w = 1 if name == "serve" else args.warmup
+            subs[name] = H.measure(workload_class(name)(args), k, w, cpu)
+            p = subs[name].get("parity")
+            mismatch = mismatch or bool(p and "MISMATCH" in p)
+        line["configs"] = subs
     if rank == 0:
-        cpu = None
-        if not args.no_cpu_baseline:
-            cpu = cpu_baseline(work)
-        line = {
-            "metric": work.metric, "value": units_all / (t_max * 1e-3), "unit": work.unit,
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": work.dtype,
-            "data": "synthetic",
-            "config": dict(workload=work.workload,
-                           parallelism="replicas" if world > 1 else "single",
-                           l2="flushed (256 MB write) between steps", **work.config()),
-            "e2e": {"value": units2_all / (e2e_max * 1e-3), "unit": work.unit,
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": e2e_max / args.steps},
-            "gpu_launches": work.launches_per_step() * args.steps,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                         "unit": "GB/s",
-                         "frac": (achieved / hbm_peak) if achieved else None,
-                         "peak_kind": peak_kind,
-                         "traffic": getattr(work, "traffic_per_launch", None),
-                         "kernel": work.kernel, "kernel_ms_per_launch": kernel_ms,
-                         "algorithmic_bytes_per_launch": alg_per_launch},
-            "clocks": clocks,
-        }
-        if cpu is not None:
-            line["cpu_baseline"] = cpu
         print(json.dumps(line))
-    work.free()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
-    return 0
+    return 1 if mismatch else 0
 
 
 def cpu_baseline(work):
-    """The reference library on this host's cores, checked against the GPU."""
+    """The reference library on this host's cores, and the parity of the
+    device's result against the reference's."""
     try:
         from oracle import Reference, reference_available
         if not reference_available():
@@ -618,9 +723,11 @@ def cpu_baseline(work):
                     "sample": "unavailable: oracle/_ref not built"}
         ncores = os.cpu_count()
         R = Reference(nthreads=ncores)
-        val, sample = work.cpu_baseline(R, ncores)
+        out = work.cpu_baseline(R, ncores)
+        val, sample = out[0], out[1]
+        parity = out[2] if len(out) > 2 else None
         return {"value": val, "unit": work.unit, "cores": ncores, "kind": "reference",
-                "sample": sample}
+                "sample": sample, "parity": parity}
     except Exception as e:   # the baseline is reported, never required
         return {"value": None, "unit": work.unit, "cores": 0, "kind": "reference",
                 "sample": "failed: %s" % e}

@@ -209,15 +209,16 @@ class BenchBatch:
         self.per_call_ms = self.time_per_call()
         self.speedup = None
 
-    def time_per_call(self, limit=256):
+    def time_per_call(self):
         """The plain path: one GrB_mxm per instance through the GraphBLAS API
-        (device-resident inputs), on the first `limit` instances, scaled."""
+        (device-resident inputs), over all instances of the batch; host
+        clock around the loop (each call returns when its product is done),
+        device synchronised on both sides."""
         from .grb import API
         import torch
         api = API()
-        mats = self.mats[:limit]
-        As = [api.matrix_from_csr(a) for a in mats]
-        Cs = [api.matrix_new(10, a.nrows, a.ncols) for a in mats]
+        As = [api.matrix_from_csr(a) for a in self.mats]
+        Cs = [api.matrix_new(10, a.nrows, a.ncols) for a in self.mats]
         for A, C in zip(As, Cs):            # warm (uploads the inputs)
             api.mxm(C, None, None, "GrB_MIN_PLUS_SEMIRING_FP32", A, A)
         torch.cuda.synchronize()
@@ -228,8 +229,13 @@ class BenchBatch:
         dt = time.perf_counter() - t0
         for X in As + Cs:
             api.free(X)
-        frac = sum(int(a.nrows) for a in mats) / float(self.sizes.sum())
-        return 1e3 * dt / frac
+        return 1e3 * dt
+
+    def digests(self):
+        """oracle.csr_digest of every instance's result (the batch's last
+        run), for the comparison with the reference's own results."""
+        from oracle import csr_digest
+        return np.array([csr_digest(*r) for r in self.B.result()], np.uint64)
 
     def step_dev(self):
         self.B.run(use_graph=True)
@@ -274,9 +280,17 @@ class BenchBatch:
         return rows, poff, ioff, P, J, X
 
     def cpu_baseline(self, R, ncores):
+        """The reference's loop of GrB_mxm calls over all instances, and the
+        parity of every instance: the digests of the reference's results
+        against those of the batch's."""
         rows, poff, ioff, P, J, X = self._ref_inputs()
-        nnz, secs = R.batch_square(rows, poff, ioff, P, J, X)
-        return self.flops / 1e9 / secs, "all 4096 instances, one GrB_mxm each (%.2f s)" % secs
+        nnz, secs, ref = R.batch_square(rows, poff, ioff, P, J, X, digests=True)
+        got = self.digests()
+        bad = int(np.sum(got != ref))
+        parity = ("exact: all %d instances bit-identical to the reference" % self.count
+                  if bad == 0 else "MISMATCH: %d of %d instances differ" % (bad, self.count))
+        return (self.flops / 1e9 / secs,
+                "all 4096 instances, one GrB_mxm each (%.2f s)" % secs, parity)
 
     def reference_steps(self, R, steps, warmup):
         rows, poff, ioff, P, J, X = self._ref_inputs()

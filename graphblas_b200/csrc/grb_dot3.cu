@@ -352,57 +352,60 @@ k_dot3_intersect(const D3Work *__restrict__ queue, const int32_t *__restrict__ s
 // shared-memory structure built from the other, its "key" row, and the
 // entries sharing a key row form a group that builds the structure once:
 //
-//   classify  one lane per mask entry: empty lists make a zombie at once;
-//             otherwise the longer of A(i,:) and B(j,:) (by row length, no
-//             search) becomes the key - row i of A (key i) or row j of B (key
-//             nrows + j) - and the entry takes a rank in its group (one
-//             warp-aggregated atomic per key).  queue[pm] holds the key, the
-//             rank and the probed row's offsets.
-//   plan      one single-pass scan (decoupled look-back) over the keys: work
-//             items of at most CT_ITEM_* entries for every non-empty group,
-//             key rows longer than CT_BM_KEY for the block-bitmap kernel and
-//             the others for the warp-hash kernel; offsets of the B-keyed
-//             groups' buckets.
-//   route     B-keyed entries scattered to their buckets (A-keyed groups are
-//             a subset of a mask row and are read in place); entries whose
-//             key row spans more columns than the bitmap holds go to the
-//             merge kernel above.
-//   hash      one warp per item: the key row in an open-addressing table of
-//             the warp's own shared memory.
+//   classify  one lane per mask entry: the longer of A(i,:) and B(j,:) (by
+//             row length) becomes the key - row i of A (key i) or row j of B
+//             (key nrows + j) - and the other list is trimmed to the key
+//             row's first and last columns by binary searches; an empty list
+//             or an empty trimmed remainder is a zombie at once.  The entry
+//             takes a rank in its group, counted apart for long lists
+//             (CT_LONG elements or more) and short ones, and queue[pm] holds
+//             the key, the rank and the trimmed range.
+//   plan      one single-pass scan (decoupled look-back) over the keys: bucket
+//             offsets of every group, and work items of about CT_WORK_*
+//             probes for every non-empty group - key rows longer than
+//             CT_BM_KEY for the block-bitmap kernel, the others for the
+//             warp-hash kernel.
+//   route     every grouped entry to its bucket, long lists at the front and
+//             short ones at the back, so that an item ends on short lists;
+//             entries whose key row spans more columns than the bitmap holds
+//             go to the merge kernel above.
+//   hash      one warp per item: the key row in the warp's table of 4-slot
+//             buckets in shared memory.
 //   bitmap    one 1024-thread block per SM: the key row as a shared-memory
 //             bitmap over its column span.
 //
-// Inside an item a warp takes 32 entries at a time; an entry's list is
-// probed by the whole warp (lists over 128), by 8 lanes (over 16) or by 2
-// lanes, four elements per lane per step with 16-byte loads.  A list is
-// trimmed to the key row's first column by a search of its group's lanes,
-// and its probing stops at the first step past the key row's last column.
-// The hit count is C(i,j); its sum over the live entries and the zombie count
-// come back with the call, so a following sum reduction of C needs no pass.
+// Inside an item a warp takes 32 entries at a time and gives each a group of
+// lanes sized to its list (about CT_PER_LANE elements per lane, 1 to 32
+// lanes), packed into the warp's lanes round by round; a group probes four
+// elements per lane per step with 16-byte loads.  The hit count is C(i,j);
+// its sum over the live entries and the zombie count come back with the
+// call, so a following sum reduction of C needs no pass.
 // ---------------------------------------------------------------------------
 
-static constexpr int CT_BM_KEY = 1024;       // longer key rows: block bitmap
-static constexpr int CT_H_SLOTS = 2048;      // slots of a warp's hash table
+static constexpr int CT_BM_KEY = 512;        // longer key rows: block bitmap
+static constexpr int CT_H_BUCKETS = 256;     // 4-slot buckets of a warp's hash table
 static constexpr int CT_H_WARPS = 8;         // warps (tables) per hash block
 static constexpr int CT_BM_THREADS = 1024;
 static constexpr int CT_ITEM_BM = 2048;      // entries per bitmap item, at most
 static constexpr int CT_ITEM_H = 1024;       // entries per hash item, at most
+static constexpr int64_t CT_WORK_BM = 1 << 20;   // probes per bitmap item, about
+static constexpr int64_t CT_WORK_H = 1 << 14;    // probes per hash item, about
+static constexpr int CT_PER_LANE = 16;       // list elements per lane of an entry's group
+static constexpr int CT_LONG = 256;          // lists this long go to the front of a bucket
 static constexpr int CT_TILE_T = 256;        // plan: threads per tile
 static constexpr int CT_TILE_K = 8;          // plan: keys per thread
 static constexpr int CT_TILE = CT_TILE_T * CT_TILE_K;
 static constexpr int CT_MERGE = -2;          // queue key of an entry for the merge kernel
-static constexpr int CT_LONG = 128;          // lists above: the whole warp
-static constexpr int CT_MID = 16;            // lists above (up to CT_LONG): 8 lanes
 static constexpr int64_t CT_MIN_ENTRIES = 1024;
 
-// per mask entry: group key (-1: done, CT_MERGE: merge kernel), rank in the
-// group, the probed row's first offset and length
-struct __align__(16) CtQ { int32_t key, rank, s0, len; };
-// a B-keyed entry in its group's bucket
-struct __align__(16) CtRec { int32_t s0, len, pm, pad; };
-// a work item: entries [e0, e1) of key's group (mask positions of row key
-// for A-keys, bucket positions for B-keys); the key row's offsets and its
-// first and last column
+// per mask entry: group key (-1: done, CT_MERGE: merge kernel), rank among
+// the group's long (rank >= 0) or short (rank < 0: -rank-1) lists, and the
+// trimmed probed range [q0, q0 + len)
+struct __align__(16) CtQ { int32_t key, rank, q0, len; };
+// a grouped entry in its group's bucket
+struct __align__(16) CtRec { int32_t q0, len, pm, j; };
+// a work item: bucket entries [e0, e1) of key's group; the key row's offsets
+// and its first and last column
 struct __align__(16) CtItem { int32_t key, e0, e1, rp0, rp1, klo, khi, pad; };
 
 // totals[] written by the plan kernel and read by the count kernels
@@ -417,7 +420,8 @@ k_ct_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
               const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
               uint32_t bm_bits, bool spans_fit,
               int32_t *__restrict__ Cj, CtQ *__restrict__ queue,
-              int32_t *__restrict__ gcnt, unsigned long long *__restrict__ nzombies)
+              int32_t *__restrict__ gcnt, unsigned long long *__restrict__ gwork,
+              unsigned long long *__restrict__ nzombies)
 {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -430,40 +434,57 @@ k_ct_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
                                                           lane);
         int32_t i = r0;
         if (valid) while (Mp[i + 1] <= pm) i++;
-        int32_t key = -1, s0 = 0, len = 0;
+        int32_t key = -1, q0 = 0, q1 = 0;
         if (valid) {
             const int32_t j = Mj[pm];
             const bool mval = mask_struct || Mx == nullptr || mask_value_true(Mx, mtype, pm);
             const int32_t pa0 = Ap[i], pa1 = Ap[i + 1];
             const int32_t pb0 = Bp[j], pb1 = Bp[j + 1];
             if (mval && pa1 > pa0 && pb1 > pb0) {
-                const int32_t dA = pa1 - pa0, dB = pb1 - pb0;
-                const bool akey = dA > dB;
-                key = akey ? i : (int32_t)nrows + j;
-                s0 = akey ? pb0 : pa0;
-                len = akey ? dB : dA;
-                if (!spans_fit && (akey ? dA : dB) > CT_BM_KEY) {
-                    const int32_t span = akey ? Aj[pa1 - 1] - Aj[pa0] : Bj[pb1 - 1] - Bj[pb0];
-                    if ((uint32_t)span >= bm_bits) key = CT_MERGE;
+                const bool akey = pa1 - pa0 > pb1 - pb0;
+                const int32_t *K = akey ? Aj : Bj;
+                const int32_t *S = akey ? Bj : Aj;
+                const int32_t k0 = akey ? pa0 : pb0, k1 = akey ? pa1 : pb1;
+                q0 = akey ? pb0 : pa0;
+                q1 = akey ? pb1 : pa1;
+                const int32_t klo = K[k0], khi = K[k1 - 1];
+                const int32_t first = S[q0], last = S[q1 - 1];
+                if (first < klo) q0 = lower_bound(S, q0 + 1, q1, klo);
+                if (last > khi && q0 < q1) q1 = upper_bound(S, q0, q1 - 1, khi);
+                if (q1 > q0) {
+                    key = akey ? i : (int32_t)nrows + j;
+                    if (!spans_fit && k1 - k0 > CT_BM_KEY && (uint32_t)(khi - klo) >= bm_bits)
+                        key = CT_MERGE;
                 }
-            } else {
+            }
+            if (key == -1) {
                 Cj[pm] = flip(j);
                 zcount++;
             }
         }
-        // rank in the group: one atomic per distinct key of the warp
+        // rank among the group's long or short lists, and the group's probe
+        // work (to size its items): one atomic each per distinct key and
+        // kind of the warp
         int32_t rank = 0;
         const bool grouped = key >= 0;
+        const int len = q1 - q0;
+        const bool lng = len >= CT_LONG;
+        const int slot = grouped ? 2 * key + (lng ? 0 : 1) : 0;
         const unsigned gm = __ballot_sync(0xffffffffu, grouped);
         if (grouped) {
-            const unsigned same = __match_any_sync(gm, key);
+            const unsigned same = __match_any_sync(gm, slot);
             const int leader = __ffs(same) - 1;
+            const unsigned w = __reduce_add_sync(same, (unsigned)min(len, 1 << 20));
             int32_t b = 0;
-            if (lane == leader) b = atomicAdd(&gcnt[key], __popc(same));
+            if (lane == leader) {
+                b = atomicAdd(&gcnt[slot], __popc(same));
+                atomicAdd(&gwork[key], (unsigned long long)w);
+            }
             b = __shfl_sync(same, b, leader);
             rank = b + __popc(same & ((1u << lane) - 1));
+            if (!lng) rank = -rank - 1;
         }
-        if (valid) queue[pm] = CtQ{key, rank, s0, len};
+        if (valid) queue[pm] = CtQ{key, rank, q0, len};
     }
     for (int o = 16; o > 0; o >>= 1) zcount += __shfl_down_sync(0xffffffffu, zcount, o);
     if (lane == 0 && zcount) atomicAdd(nzombies, zcount);
@@ -480,22 +501,30 @@ static constexpr unsigned long long CT_FLAG_AGG = 1ull << 62, CT_FLAG_INC = 2ull
 static constexpr unsigned long long CT_VAL = (1ull << 62) - 1;
 static constexpr int CT_SPIN_LIMIT = 1 << 22;
 
-__device__ __forceinline__ void ct_key_plan(const int32_t *__restrict__ gcnt, int64_t t,
-                                            int64_t nkeys, int32_t nrows,
+// A group's entries c (long and short), its bucket share and its items:
+// about CT_WORK_* probes each, at most CT_ITEM_* entries each, at least 16
+// entries each.
+__device__ __forceinline__ void ct_key_plan(const int32_t *__restrict__ gcnt,
+                                            const unsigned long long *__restrict__ gwork,
+                                            int64_t t, int64_t nkeys, int32_t nrows,
                                             const int32_t *__restrict__ Ap,
                                             const int32_t *__restrict__ Bp,
-                                            int32_t &c, int32_t &nb, int32_t &nh, int32_t &bc)
+                                            int32_t &c, int32_t &nb, int32_t &nh)
 {
-    c = 0; nb = 0; nh = 0; bc = 0;
+    c = 0; nb = 0; nh = 0;
     if (t >= nkeys) return;
-    c = gcnt[t];
+    c = gcnt[2 * t] + gcnt[2 * t + 1];
     if (c <= 0) return;
     const bool by_row = t < nrows;
     const int32_t r = by_row ? (int32_t)t : (int32_t)(t - nrows);
     const int32_t klen = by_row ? Ap[r + 1] - Ap[r] : Bp[r + 1] - Bp[r];
-    if (klen > CT_BM_KEY) nb = (c + CT_ITEM_BM - 1) / CT_ITEM_BM;
-    else nh = (c + CT_ITEM_H - 1) / CT_ITEM_H;
-    if (!by_row) bc = c;
+    const bool big = klen > CT_BM_KEY;
+    const int64_t chunk = big ? CT_WORK_BM : CT_WORK_H;
+    const int32_t emax = big ? CT_ITEM_BM : CT_ITEM_H;
+    int64_t n = ((int64_t)gwork[t] + chunk - 1) / chunk;
+    const int64_t nmin = (c + emax - 1) / emax, nmax = c / 16 > nmin ? c / 16 : nmin;
+    n = n < nmin ? nmin : (n > nmax ? nmax : n);
+    if (big) nb = (int32_t)n; else nh = (int32_t)n;
 }
 
 // inclusive scan of three ints across the block (256 threads)
@@ -523,8 +552,8 @@ __device__ __forceinline__ void ct_block_scan3(int &a, int &b, int &c, int &ta, 
 }
 
 __global__ void __launch_bounds__(CT_TILE_T)
-k_ct_plan(const int32_t *__restrict__ gcnt, int64_t nkeys, int32_t nrows,
-          const int32_t *__restrict__ Mp,
+k_ct_plan(const int32_t *__restrict__ gcnt, const unsigned long long *__restrict__ gwork,
+          int64_t nkeys, int32_t nrows,
           const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
           const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
           unsigned long long *__restrict__ status, int *__restrict__ tile_ctr,
@@ -540,17 +569,15 @@ k_ct_plan(const int32_t *__restrict__ gcnt, int64_t nkeys, int32_t nrows,
     const int64_t tile = s_tile;
     const int64_t ntiles = (nkeys + CT_TILE - 1) / CT_TILE;
     const int64_t t0 = tile * CT_TILE + (int64_t)tid * CT_TILE_K;
-    // this thread's keys: sums
     int sb = 0, sh = 0, sc = 0;
     #pragma unroll
     for (int k = 0; k < CT_TILE_K; k++) {
-        int32_t c, nb, nh, bc;
-        ct_key_plan(gcnt, t0 + k, nkeys, nrows, Ap, Bp, c, nb, nh, bc);
-        sb += nb; sh += nh; sc += bc;
+        int32_t c, nb, nh;
+        ct_key_plan(gcnt, gwork, t0 + k, nkeys, nrows, Ap, Bp, c, nb, nh);
+        sb += nb; sh += nh; sc += c;
     }
     int ib = sb, ih = sh, ic = sc, tb, th, tc;
     ct_block_scan3(ib, ih, ic, tb, th, tc, s_w);
-    // look back over the predecessors
     if (tid == 0) {
         unsigned long long *my = status + tile * 3;
         const unsigned long long agg[3] = {(unsigned long long)tb, (unsigned long long)th,
@@ -579,7 +606,8 @@ k_ct_plan(const int32_t *__restrict__ gcnt, int64_t nkeys, int32_t nrows,
                 }
             }
             for (int v = 0; v < 3; v++)
-                atomicExch(&my[v], CT_FLAG_INC | ((unsigned long long)(ex[v] + (long long)agg[v]) & CT_VAL));
+                atomicExch(&my[v], CT_FLAG_INC |
+                                   ((unsigned long long)(ex[v] + (long long)agg[v]) & CT_VAL));
             s_ex[0] = ex[0]; s_ex[1] = ex[1]; s_ex[2] = ex[2];
         }
         if (tile == ntiles - 1) {
@@ -589,14 +617,13 @@ k_ct_plan(const int32_t *__restrict__ gcnt, int64_t nkeys, int32_t nrows,
         }
     }
     __syncthreads();
-    // exclusive offsets of this thread's first key
     long long ob = s_ex[0] + ib - sb, oh = s_ex[1] + ih - sh, oc = s_ex[2] + ic - sc;
     #pragma unroll 1
     for (int k = 0; k < CT_TILE_K; k++) {
         const int64_t t = t0 + k;
-        int32_t c, nb, nh, bc;
-        ct_key_plan(gcnt, t, nkeys, nrows, Ap, Bp, c, nb, nh, bc);
-        if (t < nkeys && t >= nrows) boff[t - nrows] = (int32_t)oc;
+        int32_t c, nb, nh;
+        ct_key_plan(gcnt, gwork, t, nkeys, nrows, Ap, Bp, c, nb, nh);
+        if (t < nkeys) boff[t] = (int32_t)oc;
         const int32_t n = nb + nh;
         if (n > 0) {
             const bool by_row = t < nrows;
@@ -605,25 +632,23 @@ k_ct_plan(const int32_t *__restrict__ gcnt, int64_t nkeys, int32_t nrows,
             const int32_t *J = by_row ? Aj : Bj;
             const int32_t rp0 = P[r], rp1 = P[r + 1];
             const int32_t klo = J[rp0], khi = J[rp1 - 1];
-            // A-keyed: the mask row's positions; B-keyed: the bucket
-            const int64_t e_lo = by_row ? Mp[r] : oc;
-            const int64_t e_n = by_row ? (int64_t)(Mp[r + 1] - Mp[r]) : (int64_t)c;
             CtItem *out = nb ? items_bm + ob : items_h + oh;
             for (int32_t q = 0; q < n; q++)
-                out[q] = CtItem{(int32_t)t, (int32_t)(e_lo + e_n * q / n),
-                                (int32_t)(e_lo + e_n * (q + 1) / n), rp0, rp1, klo, khi, 0};
+                out[q] = CtItem{(int32_t)t, (int32_t)(oc + (int64_t)c * q / n),
+                                (int32_t)(oc + (int64_t)c * (q + 1) / n), rp0, rp1, klo, khi, 0};
         }
-        ob += nb; oh += nh; oc += bc;
+        ob += nb; oh += nh; oc += c;
     }
 }
 
-// B-keyed entries to their buckets; entries for the merge kernel to its queue
+// grouped entries to their buckets (long lists from the front, short ones
+// from the back); entries for the merge kernel to its queue
 __global__ void __launch_bounds__(256)
 k_ct_route(const CtQ *__restrict__ queue, int64_t mnz, int32_t nrows,
-           const int32_t *__restrict__ boff, CtRec *__restrict__ bucket,
-           const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
-           const int32_t *__restrict__ Ap, const int32_t *__restrict__ Bp,
-           D3Work *__restrict__ mq, int *__restrict__ mq_len)
+           const int32_t *__restrict__ gcnt, const int32_t *__restrict__ boff,
+           CtRec *__restrict__ bucket, const int32_t *__restrict__ Mp,
+           const int32_t *__restrict__ Mj, const int32_t *__restrict__ Ap,
+           const int32_t *__restrict__ Bp, D3Work *__restrict__ mq, int *__restrict__ mq_len)
 {
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -632,8 +657,12 @@ k_ct_route(const CtQ *__restrict__ queue, int64_t mnz, int32_t nrows,
         const int64_t pm = base + lane;
         CtQ q{-1, 0, 0, 0};
         if (pm < mnz) q = queue[pm];
-        if (q.key >= nrows)
-            bucket[boff[q.key - nrows] + q.rank] = CtRec{q.s0, q.len, (int32_t)pm, 0};
+        if (q.key >= 0) {
+            const int32_t b0 = boff[q.key];
+            const int32_t pos = q.rank >= 0 ? b0 + q.rank
+                : b0 + gcnt[2 * q.key] + gcnt[2 * q.key + 1] + q.rank;   // rank = -r-1
+            bucket[pos] = CtRec{q.q0, q.len, (int32_t)pm, Mj[pm]};
+        }
         const unsigned mm = __ballot_sync(0xffffffffu, q.key == CT_MERGE);
         if (mm) {
             const int32_t r0 = warp_last_le<int32_t, int32_t>(Mp, nrows, (int32_t)base, lane);
@@ -653,48 +682,25 @@ k_ct_route(const CtQ *__restrict__ queue, int64_t mnz, int32_t nrows,
 
 // ---- probing ------------------------------------------------------------
 
-// The G lanes of a group (lane gl of G; gmask = the group's lanes) count the
-// elements of S[p0, p1) for which hit() is 1.  Elements below klo are
-// skipped by a G-ary search (when the first one is below); probing stops at
-// the first step that passes khi.  Steps take 4 elements per lane: 16-byte
+// The G lanes of a group (lane gl of G, a power of two) count the elements
+// of S[q0, q1) for which hit() is 1, 4 elements per lane per step: 16-byte
 // loads when `vec` (S 16-byte aligned) and the step lies inside the range,
-// else predicated scalar loads (a skipped slot reads klo - 1, never a hit).
-template <int G, class Hit>
-__device__ __forceinline__ int ct_count(const int32_t *__restrict__ S, int32_t p0, int32_t p1,
-                                        int32_t klo, int32_t khi, int gl, unsigned gmask,
-                                        bool vec, const Hit &hit)
+// else predicated scalar loads.
+template <class Hit>
+__device__ __forceinline__ int ct_count(const int32_t *__restrict__ S, int32_t q0, int32_t q1,
+                                        int G, int gl, bool vec, const Hit &hit)
 {
-    int32_t q0 = p0;
-    if (S[p0] < klo) {
-        int32_t lo = p0, hi = p1;          // the first element >= klo is in [lo, hi]
-        while (hi - lo > G) {
-            const int32_t step = (hi - lo + G - 1) / G;
-            const int32_t idx = lo + (gl + 1) * step - 1;
-            const bool less = idx < hi && S[idx] < klo;
-            const int32_t nlo = lo + __popc(__ballot_sync(gmask, less)) * step;
-            hi = min(hi, nlo + step);
-            lo = nlo;
-        }
-        const bool less = lo + gl < hi && S[lo + gl] < klo;
-        q0 = lo + __popc(__ballot_sync(gmask, less));
-    }
     int cnt = 0;
-    for (int32_t base = q0 & ~3; base < p1; base += 4 * G) {
+    for (int32_t base = q0 & ~3; base < q1; base += 4 * G) {
         const int32_t e = base + 4 * gl;
-        int32_t x0, x1, x2, x3;
-        if (vec && base >= q0 && base + 4 * G <= p1) {
+        if (vec && base >= q0 && base + 4 * G <= q1) {
             const int4 v = __ldg(reinterpret_cast<const int4 *>(S + e));
-            x0 = v.x; x1 = v.y; x2 = v.z; x3 = v.w;
+            cnt += hit(v.x) + hit(v.y) + hit(v.z) + hit(v.w);
         } else {
-            const int32_t none = klo - 1;
-            x0 = (e >= q0 && e < p1) ? S[e] : none;
-            x1 = (e + 1 >= q0 && e + 1 < p1) ? S[e + 1] : none;
-            x2 = (e + 2 >= q0 && e + 2 < p1) ? S[e + 2] : none;
-            x3 = (e + 3 >= q0 && e + 3 < p1) ? S[e + 3] : none;
+            #pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (e + u >= q0 && e + u < q1) cnt += hit(S[e + u]);
         }
-        cnt += hit(x0) + hit(x1) + hit(x2) + hit(x3);
-        const int32_t mx = max(max(x0, x1), max(x2, x3));
-        if (__any_sync(gmask, mx > khi)) break;
     }
     return cnt;
 }
@@ -709,83 +715,81 @@ __device__ __forceinline__ void ct_write(int32_t pm, int32_t j, int c, int32_t *
     else { Cj[pm] = flip(j); zc++; }
 }
 
-// one batch of up to 32 entries, one per lane (valid, probed row s0/len,
-// output position pm and column j): long lists by the whole warp one after
-// another, mid-length lists by groups of 8 lanes, short ones by groups of 2
+// One batch of up to 32 bucket entries, one per lane (valid, trimmed list
+// [q0, q0 + len), output position pm and column j).  Every entry gets a
+// group of 2^lg lanes, about CT_PER_LANE elements of its list per lane (1 to
+// 32 lanes).  The groups are packed into lane slots - larger groups first,
+// lane order within a size - so that every group starts on a multiple of its
+// size, and the warp runs the slots 32 at a time: in each round every lane
+// finds its group (the last group start at or below it, from the starts the
+// entries' lanes write into the warp's `owner` row) and the groups probe
+// side by side.  `owner` holds 32 ints, all -1 between calls.
 template <typename Z, class Hit>
-__device__ __forceinline__ void ct_batch(bool valid, int32_t s0, int32_t len, int32_t pm,
-                                         int32_t j, const int32_t *__restrict__ S,
-                                         int32_t klo, int32_t khi, bool vec, const Hit &hit,
-                                         int32_t *__restrict__ Cj, Z *__restrict__ Cx,
-                                         unsigned long long &sum, unsigned long long &zc)
+__device__ __forceinline__ void ct_batch(bool valid, int32_t q0, int32_t len, int32_t pm,
+                                         int32_t j, const int32_t *__restrict__ S, bool vec,
+                                         const Hit &hit, int32_t *__restrict__ Cj,
+                                         Z *__restrict__ Cx, unsigned long long &sum,
+                                         unsigned long long &zc, int *owner)
 {
     const int lane = threadIdx.x & 31;
-    const unsigned vL = __ballot_sync(0xffffffffu, valid && len > CT_LONG);
-    const unsigned vM = __ballot_sync(0xffffffffu, valid && len > CT_MID && len <= CT_LONG);
-    const unsigned vS = __ballot_sync(0xffffffffu, valid && len <= CT_MID);
-    for (unsigned m = vL; m; m &= m - 1) {
-        const int src = __ffs(m) - 1;
-        const int32_t es0 = __shfl_sync(0xffffffffu, s0, src);
+    const unsigned below = (1u << lane) - 1;
+    int lg = -1;
+    if (valid) {
+        const int32_t w = len / CT_PER_LANE;
+        lg = w >= 32 ? 5 : (w > 1 ? 31 - __clz(w) : 0);
+    }
+    int32_t start = 0, total = 0;
+    #pragma unroll
+    for (int c = 5; c >= 0; c--) {
+        const unsigned m = __ballot_sync(0xffffffffu, lg == c);
+        if (lg == c) start = total + (int32_t)(__popc(m & below) << c);
+        total += (int32_t)(__popc(m) << c);
+    }
+    for (int32_t r0 = 0; r0 < total; r0 += 32) {
+        if (lg >= 0 && start >= r0 && start < r0 + 32) owner[start - r0] = lane;
+        __syncwarp();
+        const int o = owner[lane];
+        int v = o >= 0 ? ((lane << 5) | o) : -1;
+        #pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, d);
+            if (lane >= d) v = max(v, u);
+        }
+        __syncwarp();
+        if (o >= 0) owner[lane] = -1;
+        // every reset lands before any lane writes the next round's starts
+        __syncwarp();
+        const int src = v & 31, gs = v >> 5;
+        const int elg = __shfl_sync(0xffffffffu, lg, src);
+        const int32_t eq0 = __shfl_sync(0xffffffffu, q0, src);
         const int32_t elen = __shfl_sync(0xffffffffu, len, src);
-        int c = ct_count<32>(S, es0, es0 + elen, klo, khi, lane, 0xffffffffu, vec, hit);
-        c = (int)__reduce_add_sync(0xffffffffu, (unsigned)c);
-        if (lane == src) ct_write<Z>(pm, j, c, Cj, Cx, sum, zc);
-    }
-    {
-        const int gi = lane >> 3, gl = lane & 7;
-        const unsigned gmask = 0xffu << (gi * 8);
-        const int n = __popc(vM);
-        for (int r = 0; r < n; r += 4) {
-            const bool act = r + gi < n;
-            const int src = act ? (int)__fns(vM, 0, r + gi + 1) : 0;
-            const int32_t es0 = __shfl_sync(0xffffffffu, s0, src);
-            const int32_t elen = __shfl_sync(0xffffffffu, len, src);
-            const int32_t epm = __shfl_sync(0xffffffffu, pm, src);
-            const int32_t ej = __shfl_sync(0xffffffffu, j, src);
-            if (act) {
-                int c = ct_count<8>(S, es0, es0 + elen, klo, khi, gl, gmask, vec, hit);
-                c = (int)__reduce_add_sync(gmask, (unsigned)c);
-                if (gl == 0) ct_write<Z>(epm, ej, c, Cj, Cx, sum, zc);
-            }
+        const int32_t epm = __shfl_sync(0xffffffffu, pm, src);
+        const int32_t ej = __shfl_sync(0xffffffffu, j, src);
+        // lanes past the last group probe an empty range, so every lane
+        // takes part in the group sums (xor shuffles stay inside an aligned
+        // group of G lanes)
+        const bool act = r0 + lane < total;
+        const int G = 1 << elg, gl = lane - gs;
+        int c = act ? ct_count(S, eq0, eq0 + elen, G, gl, vec, hit) : 0;
+        #pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_xor_sync(0xffffffffu, c, d);
+            if (d < G) c += u;
         }
-    }
-    {
-        const int gi = lane >> 1, gl = lane & 1;
-        const unsigned gmask = 0x3u << (gi * 2);
-        const int n = __popc(vS);
-        for (int r = 0; r < n; r += 16) {
-            const bool act = r + gi < n;
-            const int src = act ? (int)__fns(vS, 0, r + gi + 1) : 0;
-            const int32_t es0 = __shfl_sync(0xffffffffu, s0, src);
-            const int32_t elen = __shfl_sync(0xffffffffu, len, src);
-            const int32_t epm = __shfl_sync(0xffffffffu, pm, src);
-            const int32_t ej = __shfl_sync(0xffffffffu, j, src);
-            if (act) {
-                int c = ct_count<2>(S, es0, es0 + elen, klo, khi, gl, gmask, vec, hit);
-                c = (int)__reduce_add_sync(gmask, (unsigned)c);
-                if (gl == 0) ct_write<Z>(epm, ej, c, Cj, Cx, sum, zc);
-            }
-        }
+        if (act && gl == 0) ct_write<Z>(epm, ej, c, Cj, Cx, sum, zc);
+        __syncwarp();
     }
 }
 
-// the entries [e, e + 32) of an item as lane-per-entry records
-__device__ __forceinline__ void ct_load_entry(const CtItem &I, int32_t e, int32_t nrows,
-                                              const CtQ *__restrict__ queue,
-                                              const CtRec *__restrict__ bucket,
-                                              const int32_t *__restrict__ Mj, bool &valid,
-                                              int32_t &s0, int32_t &len, int32_t &pm,
+__device__ __forceinline__ void ct_load_entry(const CtItem &I, int32_t e,
+                                              const CtRec *__restrict__ bucket, bool &valid,
+                                              int32_t &q0, int32_t &len, int32_t &pm,
                                               int32_t &j)
 {
-    valid = false; s0 = 0; len = 0; pm = 0; j = 0;
-    if (e >= I.e1) return;
-    if (I.key < nrows) {
-        const CtQ q = queue[e];
-        if (q.key == I.key) { valid = true; s0 = q.s0; len = q.len; pm = e; j = Mj[e]; }
-    } else {
-        const CtRec r = bucket[e];
-        valid = true; s0 = r.s0; len = r.len; pm = r.pm; j = I.key - nrows;
-    }
+    valid = e < I.e1;
+    CtRec r{0, 0, 0, 0};
+    if (valid) r = bucket[e];
+    q0 = r.q0; len = r.len; pm = r.pm; j = r.j;
 }
 
 __device__ __forceinline__ uint32_t ct_hash(int32_t k, int bits)
@@ -793,23 +797,28 @@ __device__ __forceinline__ uint32_t ct_hash(int32_t k, int bits)
     return ((uint32_t)k * 0x9E3779B1u) >> (32 - bits);
 }
 
-// one warp per item whose key row has at most CT_BM_KEY entries: the key
-// row goes into the warp's open-addressing table (a power of two of slots,
-// at least twice the row), then its entries are counted against it
+// One warp per item whose key row has at most CT_BM_KEY entries.  The key
+// row goes into the warp's hash table of 4-slot buckets (a power of two of
+// buckets, at least half as many as the row's entries; a bucket's slots fill
+// in order, and a full bucket overflows into the next), so most probes read
+// one 16-byte bucket: the element is in the row if a slot holds it, absent
+// if the bucket still has an empty slot.
 template <class SR>
 __global__ void __launch_bounds__(CT_H_WARPS * 32)
 k_ct_hash(const CtItem *__restrict__ items, const int32_t *__restrict__ totals,
-          int *__restrict__ inext, int32_t nrows, const CtQ *__restrict__ queue,
-          const CtRec *__restrict__ bucket, const int32_t *__restrict__ Mj,
+          int *__restrict__ inext, int32_t nrows, const CtRec *__restrict__ bucket,
           const int32_t *__restrict__ Aj, const int32_t *__restrict__ Bj, bool vec,
           int32_t *__restrict__ Cj, typename SR::z_t *__restrict__ Cx,
           unsigned long long *__restrict__ out_sum, unsigned long long *__restrict__ nzombies)
 {
     using Z = typename SR::z_t;
-    extern __shared__ __align__(16) int32_t ct_tabs[];
+    __shared__ int4 s_tab[CT_H_WARPS][CT_H_BUCKETS];
+    __shared__ int s_owner[CT_H_WARPS][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int32_t *tab = ct_tabs + w * CT_H_SLOTS;
-    for (int q = lane; q < CT_H_SLOTS; q += 32) tab[q] = -1;
+    int4 *tab = s_tab[w];
+    int32_t *slots = reinterpret_cast<int32_t *>(tab);
+    for (int q = lane; q < CT_H_BUCKETS; q += 32) tab[q] = make_int4(-1, -1, -1, -1);
+    s_owner[w][lane] = -1;
     __syncwarp();
     const int nitems = totals[CT_N_H];
     unsigned long long sum = 0, zc = 0;
@@ -823,34 +832,40 @@ k_ct_hash(const CtItem *__restrict__ items, const int32_t *__restrict__ totals,
         const int32_t *J = by_row ? Aj : Bj;
         const int32_t *S = by_row ? Bj : Aj;
         const int32_t klen = I.rp1 - I.rp0;
-        int bits = 6;
-        while ((1 << bits) < 2 * klen) bits++;
-        const uint32_t tmask = (1u << bits) - 1;
+        int bits = 3;
+        while ((1 << bits) * 2 < klen) bits++;
+        const uint32_t bmask = (1u << bits) - 1;
+        // the first batch's entries load while the table fills
+        bool valid;
+        int32_t q0, len, pm, j;
+        ct_load_entry(I, I.e0 + lane, bucket, valid, q0, len, pm, j);
         for (int32_t q = I.rp0 + lane; q < I.rp1; q += 32) {
             const int32_t k = J[q];
-            uint32_t h = ct_hash(k, bits);
-            while (atomicCAS(&tab[h], -1, k) != -1) h = (h + 1) & tmask;
+            uint32_t b = ct_hash(k, bits);
+            for (int t = 0;; t++) {
+                if (atomicCAS(&slots[b * 4 + (t & 3)], -1, k) == -1) break;
+                if ((t & 3) == 3) b = (b + 1) & bmask;
+            }
         }
         __syncwarp();
-        const int32_t klo = I.klo, khi = I.khi;
         auto hit = [&](int32_t x) -> int {
-            if (x < klo || x > khi) return 0;
-            uint32_t h = ct_hash(x, bits);
+            uint32_t b = ct_hash(x, bits);
             while (true) {
-                const int32_t v = tab[h];
-                if (v == x) return 1;
-                if (v < 0) return 0;
-                h = (h + 1) & tmask;
+                const int4 v = tab[b];
+                if (v.x == x || v.y == x || v.z == x || v.w == x) return 1;
+                if (v.w < 0) return 0;
+                b = (b + 1) & bmask;
             }
         };
         for (int32_t e = I.e0; e < I.e1; e += 32) {
-            bool valid;
-            int32_t s0, len, pm, j;
-            ct_load_entry(I, e + lane, nrows, queue, bucket, Mj, valid, s0, len, pm, j);
-            ct_batch<Z>(valid, s0, len, pm, j, S, klo, khi, vec, hit, Cj, Cx, sum, zc);
+            bool nvalid;
+            int32_t nq0, nlen, npm, nj;
+            ct_load_entry(I, e + 32 + lane, bucket, nvalid, nq0, nlen, npm, nj);
+            ct_batch<Z>(valid, q0, len, pm, j, S, vec, hit, Cj, Cx, sum, zc, s_owner[w]);
+            valid = nvalid; q0 = nq0; len = nlen; pm = npm; j = nj;
         }
         __syncwarp();
-        for (int q = lane; q <= (int)tmask; q += 32) tab[q] = -1;
+        for (int q = lane; q <= (int)bmask; q += 32) tab[q] = make_int4(-1, -1, -1, -1);
         __syncwarp();
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -872,29 +887,38 @@ k_ct_hash(const CtItem *__restrict__ items, const int32_t *__restrict__ totals,
 template <class SR>
 __global__ void __launch_bounds__(CT_BM_THREADS, 1)
 k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals,
-            int *__restrict__ inext, int32_t nrows, const CtQ *__restrict__ queue,
-            const CtRec *__restrict__ bucket, const int32_t *__restrict__ Mj,
+            int *__restrict__ inext, int32_t nrows, const CtRec *__restrict__ bucket,
             const int32_t *__restrict__ Aj, const int32_t *__restrict__ Bj, bool vec,
             uint32_t bm_words, int32_t *__restrict__ Cj, typename SR::z_t *__restrict__ Cx,
             unsigned long long *__restrict__ out_sum, unsigned long long *__restrict__ nzombies)
 {
     using Z = typename SR::z_t;
     extern __shared__ __align__(16) uint32_t bm[];
-    __shared__ int s_item, s_next;
-    __shared__ CtItem s_I;
+    // the item being processed and the one fetched ahead alternate between
+    // two slots, so the fetch never writes the slot the block is reading
+    __shared__ int s_item[2], s_next;
+    __shared__ CtItem s_I[2];
+    __shared__ int s_owner[CT_BM_THREADS / 32][32];
     const int tid = threadIdx.x, lane = tid & 31;
     for (uint32_t q = tid; q <= bm_words; q += blockDim.x) bm[q] = 0;
+    s_owner[tid >> 5][lane] = -1;
     const uint32_t nbits = bm_words * 32u;        // the guard bit
     const int nitems = totals[CT_N_BM];
     unsigned long long sum = 0, zc = 0;
+    int cur = 0;
     if (tid == 0) {
-        s_item = atomicAdd(inext, 1);
-        if (s_item < nitems) s_I = items[s_item];
+        s_item[0] = atomicAdd(inext, 1);
+        if (s_item[0] < nitems) s_I[0] = items[s_item[0]];
     }
+    // every block barrier below follows code in which a warp's lanes may
+    // diverge (the lane groups, the strided set and clear loops): each warp
+    // reconverges first, as a block barrier must be reached by whole warps
     while (true) {
+        __syncwarp();
         __syncthreads();
-        if (s_item >= nitems) break;
-        const CtItem I = s_I;
+        if (s_item[cur] >= nitems) break;
+        const CtItem I = s_I[cur];
+        __syncwarp();
         __syncthreads();
         if (tid == 0) s_next = 0;
         const bool by_row = I.key < nrows;
@@ -918,11 +942,13 @@ k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals
                 atomicOr(&bm[k >> 5], 1u << (k & 31));
             }
         }
+        __syncwarp();
         __syncthreads();
         // the next item is fetched while this one runs
         if (tid == 0) {
-            s_item = atomicAdd(inext, 1);
-            if (s_item < nitems) s_I = items[s_item];
+            const int nx = atomicAdd(inext, 1);
+            s_item[cur ^ 1] = nx;
+            if (nx < nitems) s_I[cur ^ 1] = items[nx];
         }
         auto hit = [&](int32_t x) -> int {
             const uint32_t k = min((uint32_t)(x - klo), nbits);
@@ -934,10 +960,12 @@ k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals
             e = __shfl_sync(0xffffffffu, e, 0) + I.e0;
             if (e >= I.e1) break;
             bool valid;
-            int32_t s0, len, pm, j;
-            ct_load_entry(I, e + lane, nrows, queue, bucket, Mj, valid, s0, len, pm, j);
-            ct_batch<Z>(valid, s0, len, pm, j, S, klo, khi, vec, hit, Cj, Cx, sum, zc);
+            int32_t q0, len, pm, j;
+            ct_load_entry(I, e + lane, bucket, valid, q0, len, pm, j);
+            ct_batch<Z>(valid, q0, len, pm, j, S, vec, hit, Cj, Cx, sum, zc,
+                        s_owner[tid >> 5]);
         }
+        __syncwarp();
         __syncthreads();
         // clear: zero the span's words with 16-byte stores when that is
         // cheaper than revisiting the row's entries
@@ -952,6 +980,7 @@ k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals
                 bm[k >> 5] = 0;
             }
         }
+        cur ^= 1;
     }
     for (int o = 16; o > 0; o >>= 1) {
         sum += __shfl_down_sync(0xffffffffu, sum, o);
@@ -967,7 +996,7 @@ k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals
 // the kernel's static shared memory (plus the zero guard word, the total a
 // multiple of 4 words for the 16-byte clears), else the most that fits (key
 // rows spanning more columns go to the merge kernel).  0 disables the
-// bitmap (every key row then needs the hash or merge kernel).
+// bitmap (the counting path is then not taken).
 template <class SR>
 static uint32_t ct_bitmap_words(int64_t ncols)
 {
@@ -994,19 +1023,6 @@ static uint32_t ct_bitmap_words(int64_t ncols)
 }
 
 template <class SR>
-static bool ct_hash_smem_ok()
-{
-    static int ok = -1;
-    if (ok < 0) {
-        ok = cudaFuncSetAttribute((const void *)k_ct_hash<SR>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  CT_H_WARPS * CT_H_SLOTS * 4) == cudaSuccess;
-        cudaGetLastError();
-    }
-    return ok == 1;
-}
-
-template <class SR>
 static int dot3_count_launch(DevCSR &C, const DevCSR &M, bool mask_struct, const DevCSR &A,
                              const DevCSR &B, cudaStream_t s, int64_t *live_sum)
 {
@@ -1016,16 +1032,17 @@ static int dot3_count_launch(DevCSR &C, const DevCSR &M, bool mask_struct, const
     const int64_t ntiles = (nkeys + CT_TILE - 1) / CT_TILE;
     const uint32_t bm_words = ct_bitmap_words<SR>(A.ncols);
     const bool spans_fit = bm_words > 0 && (int64_t)bm_words * 32 >= A.ncols;
-    if (bm_words == 0 || !ct_hash_smem_ok<SR>()) return NO_VALUE;
+    if (bm_words == 0) return NO_VALUE;
     const int nsm = runtime().num_sms;
     C.p = (int32_t *)dalloc((size_t)(M.nrows + 1) * 4, s);
     C.j = (int32_t *)dalloc((size_t)mnz * 4, s);
     C.x = dalloc((size_t)mnz * sizeof(Z), s);
-    const int64_t nitems_max = std::min<int64_t>(nkeys, mnz) + mnz / CT_ITEM_H + 1;
-    // counters, group counts and tile words first and adjacent: one memset
+    const int64_t nitems_max = std::min<int64_t>(nkeys, mnz) + mnz / 16 + 1;
+    // counters, tile words, group work and group counts first and adjacent:
+    // one memset
     int *counter = nullptr;
     int32_t *gcnt = nullptr, *boff = nullptr;
-    unsigned long long *status = nullptr;
+    unsigned long long *status = nullptr, *gwork = nullptr;
     CtQ *queue = nullptr;
     CtRec *bucket = nullptr;
     CtItem *items_bm = nullptr, *items_h = nullptr;
@@ -1034,9 +1051,10 @@ static int dot3_count_launch(DevCSR &C, const DevCSR &M, bool mask_struct, const
     auto layout = [&]() {
         counter = cv.take<int>(32);
         status = cv.take<unsigned long long>((size_t)ntiles * 3);
-        gcnt = cv.take<int32_t>(nkeys);
+        gwork = cv.take<unsigned long long>(nkeys);
+        gcnt = cv.take<int32_t>(2 * nkeys);
         queue = cv.take<CtQ>(mnz);
-        boff = cv.take<int32_t>(B.nrows);
+        boff = cv.take<int32_t>(nkeys);
         bucket = cv.take<CtRec>(mnz);
         items_bm = cv.take<CtItem>(nitems_max);
         items_h = cv.take<CtItem>(nitems_max);
@@ -1048,7 +1066,8 @@ static int dot3_count_launch(DevCSR &C, const DevCSR &M, bool mask_struct, const
     struct Release { Carve &c; ~Release() { dfree(c.base, c.s); } } release{cv};
     if (!C.p || !C.j || !C.x || !got) { dev_free(C, s); return OUT_OF_MEMORY; }
     cudaMemcpyAsync(C.p, M.p, (size_t)(M.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
-    cudaMemsetAsync(counter, 0, (size_t)((const char *)(gcnt + nkeys) - (const char *)counter), s);
+    cudaMemsetAsync(counter, 0, (size_t)((const char *)(gcnt + 2 * nkeys) - (const char *)counter),
+                    s);
     // counter layout: [0..3] totals, [4] tile ticket, [5] hash items, [6] bitmap
     // items, [7] merge items, [8] merge taken; zombies at byte 64, sum at 72
     int32_t *totals = counter;
@@ -1062,17 +1081,17 @@ static int dot3_count_launch(DevCSR &C, const DevCSR &M, bool mask_struct, const
     const int ps = prof_begin("dot3", s);
     k_ct_classify<SR><<<(unsigned)blocks, 256, 0, s>>>(
         M.p, M.j, mask_struct ? nullptr : M.x, M.type, mask_struct, mnz, M.nrows,
-        A.p, A.j, B.p, B.j, bm_words * 32u, spans_fit, C.j, queue, gcnt, zc);
+        A.p, A.j, B.p, B.j, bm_words * 32u, spans_fit, C.j, queue, gcnt, gwork, zc);
     k_ct_plan<<<(unsigned)ntiles, CT_TILE_T, 0, s>>>(
-        gcnt, nkeys, (int32_t)M.nrows, M.p, A.p, A.j, B.p, B.j, status, tile_ctr, boff,
+        gcnt, gwork, nkeys, (int32_t)M.nrows, A.p, A.j, B.p, B.j, status, tile_ctr, boff,
         items_bm, items_h, totals);
-    k_ct_route<<<(unsigned)blocks, 256, 0, s>>>(queue, mnz, (int32_t)M.nrows, boff, bucket,
-                                                 M.p, M.j, A.p, B.p, mq, mq_len);
-    k_ct_hash<SR><<<nsm * 3, CT_H_WARPS * 32, CT_H_WARPS * CT_H_SLOTS * 4, s>>>(
-        items_h, totals, inext_h, (int32_t)M.nrows, queue, bucket, M.j, A.j, B.j, vec,
+    k_ct_route<<<(unsigned)blocks, 256, 0, s>>>(queue, mnz, (int32_t)M.nrows, gcnt, boff,
+                                                 bucket, M.p, M.j, A.p, B.p, mq, mq_len);
+    k_ct_hash<SR><<<nsm * 4, CT_H_WARPS * 32, 0, s>>>(
+        items_h, totals, inext_h, (int32_t)M.nrows, bucket, A.j, B.j, vec,
         C.j, (Z *)C.x, sum, zc);
     k_ct_bitmap<SR><<<nsm, CT_BM_THREADS, (size_t)(bm_words + 1) * 4, s>>>(
-        items_bm, totals, inext_bm, (int32_t)M.nrows, queue, bucket, M.j, A.j, B.j, vec,
+        items_bm, totals, inext_bm, (int32_t)M.nrows, bucket, A.j, B.j, vec,
         bm_words, C.j, (Z *)C.x, sum, zc);
     k_dot3_intersect<SR><<<nsm * 8, 256, 0, s>>>(
         mq, nullptr, mq_len, mq_next, A.j, A.x, A.iso, B.j, B.x, B.iso, C.j, (Z *)C.x, zc,

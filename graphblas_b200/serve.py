@@ -296,7 +296,7 @@ class BenchServe:
         return {"t": t["t"][:k], "kind": t["kind"][:k], "graph": t["graph"][:k],
                 "fp": t["fp"][:k + 1], "fi": t["fi"], "fx": t["fx"]}
 
-    def _ref_run(self, R, ncores):
+    def _ref_run(self, R, ncores, results=False):
         tr = self._ref_trace()
         per = max(1, ncores // 8)
         status, count, cs, lat, mk = R.serve(self.graphs, tr, 8, per)
@@ -305,11 +305,27 @@ class BenchServe:
                 "threads, p50 %.2f ms, p99 %.2f ms" %
                 (self.REF_SAMPLE, per, 1e3 * np.percentile(lat, 50),
                  1e3 * np.percentile(lat, 99)))
+        if results:
+            return done, mk, desc, status, count, cs
         return done, mk, desc
 
     def cpu_baseline(self, R, ncores):
-        done, mk, desc = self._ref_run(R, ncores)
-        return done / mk, desc
+        """The reference replaying the trace's first requests, and the parity
+        of those requests' results: counts (triangles, result entries) equal,
+        checksums (sums of the result values, summed in different orders)
+        within 1e-9 relative."""
+        done, mk, desc, status, count, cs = self._ref_run(R, ncores, results=True)
+        bad = 0
+        for k in range(self.REF_SAMPLE):
+            a = self.S.request(k)
+            if status[k] != 0 or a["status"] != 0 or a["count"] != int(count[k]):
+                bad += 1
+            elif abs(a["checksum"] - cs[k]) > 1e-9 * max(1.0, abs(cs[k])):
+                bad += 1
+        parity = ("exact counts, checksums within 1e-9 on the %d replayed requests"
+                  % self.REF_SAMPLE if bad == 0 else
+                  "MISMATCH: %d of %d requests differ" % (bad, self.REF_SAMPLE))
+        return done / mk, desc, parity
 
     def reference_steps(self, R, steps, warmup):
         ncores = os.cpu_count() or 1
