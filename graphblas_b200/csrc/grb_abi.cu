@@ -167,10 +167,10 @@ bool grb_b200_AxB_dot3_branch(const grb_b200_matrix *M, const grb_b200_matrix *A
     return true;
 }
 
-int grb_b200_AxB_dot3(grb_b200_matrix *C, const grb_b200_matrix *M,
-                      bool Mask_struct, const grb_b200_matrix *A,
-                      const grb_b200_matrix *B,
-                      const grb_b200_semiring *semiring, bool flipxy)
+int grb_b200_AxB_dot3_device(grb_b200_dmatrix *C, const grb_b200_matrix *M,
+                             bool Mask_struct, const grb_b200_matrix *A,
+                             const grb_b200_matrix *B,
+                             const grb_b200_semiring *semiring, bool flipxy)
 {
     if (!C || !M || !A || !B || !semiring) return NULL_POINTER;
     int info = init_device();
@@ -183,7 +183,8 @@ int grb_b200_AxB_dot3(grb_b200_matrix *C, const grb_b200_matrix *M,
                     swap_mult(semiring->mult_opcode, flipxy, &ok), semiring->type};
     StreamGuard g;
     cudaStream_t s = g.s;
-    DevCSR dM, dA, dB, dC;
+    DevCSR dM, dA, dB;
+    grb_b200_dmatrix h = new grb_b200_dmatrix_s();
     // kernel rows: mask row j, kernel A := reference B, kernel B := reference A
     grb_b200_matrix Mu = *M;
     Mu.jumbled = false;                 // the dot3 kernel reads M in any order
@@ -193,16 +194,39 @@ int grb_b200_AxB_dot3(grb_b200_matrix *C, const grb_b200_matrix *M,
         (info = ensure_values(dA, s)) == SUCCESS &&
         (info = ensure_values(dB, s)) == SUCCESS) {
         bool mstruct = Mask_struct || M->x == nullptr;
-        info = dot3(dC, dM, mstruct, dA, dB, sc, s);
+        info = dot3(h->A, dM, mstruct, dA, dB, sc, s);
     }
     dev_free(dM, s); dev_free(dA, s); dev_free(dB, s);
-    if (info != SUCCESS) { dev_free(dC, s); cudaStreamSynchronize(s); return info; }
-    int64_t *p = nullptr, *i = nullptr;
-    void *x = nullptr;
-    info = dev_download(dC, &p, &i, &x, true, g_malloc, s);
-    int64_t nz = dC.nzombies;
-    dev_free(dC, s);
     cudaStreamSynchronize(s);
+    if (info != SUCCESS) { delete h; return info; }
+    *C = h;
+    return SUCCESS;
+}
+
+int grb_b200_dmatrix_copy_out(grb_b200_dmatrix D, int64_t *p, int64_t *i, void *x)
+{
+    if (!D || !p || !i) return NULL_POINTER;
+    StreamGuard g;
+    return dev_copy_out(D->A, p, i, x, g.s);
+}
+
+int grb_b200_AxB_dot3(grb_b200_matrix *C, const grb_b200_matrix *M,
+                      bool Mask_struct, const grb_b200_matrix *A,
+                      const grb_b200_matrix *B,
+                      const grb_b200_semiring *semiring, bool flipxy)
+{
+    if (!C) return NULL_POINTER;
+    grb_b200_dmatrix D = nullptr;
+    int info = grb_b200_AxB_dot3_device(&D, M, Mask_struct, A, B, semiring, flipxy);
+    if (info != SUCCESS) return info;
+    const int64_t n = D->A.nrows, nnz = D->A.nnz;
+    const size_t ts = type_size(D->A.type);
+    int64_t *p = (int64_t *)g_malloc((size_t)(n + 1) * 8);
+    int64_t *i = (int64_t *)g_malloc((size_t)(nnz ? nnz : 1) * 8);
+    void *x = g_malloc((size_t)(nnz ? nnz : 1) * ts);
+    info = (p && i && x) ? grb_b200_dmatrix_copy_out(D, p, i, x) : OUT_OF_MEMORY;
+    const int64_t nz = D->A.nzombies;
+    grb_b200_dmatrix_free(&D);
     if (info != SUCCESS) {
         if (p) g_free(p);
         if (i) g_free(i);
@@ -217,13 +241,12 @@ int grb_b200_AxB_dot3(grb_b200_matrix *C, const grb_b200_matrix *M,
     return SUCCESS;
 }
 
-int grb_b200_AxB_saxpy3(grb_b200_matrix *C, const grb_b200_matrix *M,
-                        bool Mask_comp, bool Mask_struct,
-                        const grb_b200_matrix *A, const grb_b200_matrix *B,
-                        const grb_b200_semiring *semiring, bool flipxy,
-                        bool *mask_applied, int do_sort)
+int grb_b200_AxB_saxpy3_device(grb_b200_dmatrix *C, const grb_b200_matrix *M,
+                               bool Mask_comp, bool Mask_struct,
+                               const grb_b200_matrix *A, const grb_b200_matrix *B,
+                               const grb_b200_semiring *semiring, bool flipxy,
+                               bool *mask_applied)
 {
-    (void)do_sort;
     if (!C || !A || !B || !semiring) return NULL_POINTER;
     int info = init_device();
     if (info != SUCCESS) return info;
@@ -238,7 +261,8 @@ int grb_b200_AxB_saxpy3(grb_b200_matrix *C, const grb_b200_matrix *M,
     if (M && (M->vlen != A->vlen || M->vdim != B->vdim)) return DIMENSION_MISMATCH;
     StreamGuard g;
     cudaStream_t s = g.s;
-    DevCSR dM, dA, dB, dC;
+    DevCSR dM, dA, dB;
+    grb_b200_dmatrix h = new grb_b200_dmatrix_s();
     info = upload(dA, B, s);                       // kernel rows: vectors of B
     if (info == SUCCESS) info = upload(dB, A, s);  // gathered rows: vectors of A
     if (info == SUCCESS && M) {
@@ -250,15 +274,35 @@ int grb_b200_AxB_saxpy3(grb_b200_matrix *C, const grb_b200_matrix *M,
     if (info == SUCCESS) info = ensure_values(dB, s);
     if (info == SUCCESS) {
         bool mstruct = Mask_struct || (M && M->x == nullptr);
-        info = saxpy3(dC, M ? &dM : nullptr, Mask_comp, mstruct, dA, dB, sc, s);
+        info = saxpy3(h->A, M ? &dM : nullptr, Mask_comp, mstruct, dA, dB, sc, s);
     }
     dev_free(dM, s); dev_free(dA, s); dev_free(dB, s);
-    if (info != SUCCESS) { dev_free(dC, s); cudaStreamSynchronize(s); return info; }
-    int64_t *p = nullptr, *i = nullptr;
-    void *x = nullptr;
-    info = dev_download(dC, &p, &i, &x, false, g_malloc, s);
-    dev_free(dC, s);
     cudaStreamSynchronize(s);
+    if (info != SUCCESS) { dev_free(h->A, s); delete h; return info; }
+    if (mask_applied) *mask_applied = (M != nullptr);
+    *C = h;
+    return SUCCESS;
+}
+
+int grb_b200_AxB_saxpy3(grb_b200_matrix *C, const grb_b200_matrix *M,
+                        bool Mask_comp, bool Mask_struct,
+                        const grb_b200_matrix *A, const grb_b200_matrix *B,
+                        const grb_b200_semiring *semiring, bool flipxy,
+                        bool *mask_applied, int do_sort)
+{
+    (void)do_sort;
+    if (!C) return NULL_POINTER;
+    grb_b200_dmatrix D = nullptr;
+    int info = grb_b200_AxB_saxpy3_device(&D, M, Mask_comp, Mask_struct, A, B, semiring,
+                                          flipxy, mask_applied);
+    if (info != SUCCESS) return info;
+    const int64_t n = D->A.nrows, nnz = D->A.nnz;
+    const size_t ts = type_size(D->A.type);
+    int64_t *p = (int64_t *)g_malloc((size_t)(n + 1) * 8);
+    int64_t *i = (int64_t *)g_malloc((size_t)(nnz ? nnz : 1) * 8);
+    void *x = g_malloc((size_t)(nnz ? nnz : 1) * ts);
+    info = (p && i && x) ? grb_b200_dmatrix_copy_out(D, p, i, x) : OUT_OF_MEMORY;
+    grb_b200_dmatrix_free(&D);
     if (info != SUCCESS) {
         if (p) g_free(p);
         if (i) g_free(i);
@@ -269,7 +313,6 @@ int grb_b200_AxB_saxpy3(grb_b200_matrix *C, const grb_b200_matrix *M,
     C->p = p; C->i = i; C->x = x;
     C->type = semiring->type; C->iso = false; C->jumbled = false;
     C->nzombies = 0;
-    if (mask_applied) *mask_applied = (M != nullptr);
     return SUCCESS;
 }
 

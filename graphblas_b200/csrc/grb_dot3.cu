@@ -683,24 +683,35 @@ k_ct_route(const CtQ *__restrict__ queue, int64_t mnz, int32_t nrows,
 // ---- probing ------------------------------------------------------------
 
 // The G lanes of a group (lane gl of G, a power of two) count the elements
-// of S[q0, q1) for which hit() is 1, 4 elements per lane per step: 16-byte
-// loads when `vec` (S 16-byte aligned) and the step lies inside the range,
-// else predicated scalar loads.
+// of S[q0, q1) for which hit() is 1.  A step covers 16 elements per lane:
+// four 16-byte vectors (lane gl takes vectors gl, G + gl, 2G + gl, 3G + gl
+// of the step, so each of the four loads is coalesced across the group),
+// all loaded before any is probed so that their latencies overlap.  A vector
+// that lies inside the range is one 16-byte load when `vec` (S 16-byte
+// aligned); a vector at either end is read element by element, and its
+// slots outside the range read `none`, a value hit() always misses.
 template <class Hit>
 __device__ __forceinline__ int ct_count(const int32_t *__restrict__ S, int32_t q0, int32_t q1,
-                                        int G, int gl, bool vec, const Hit &hit)
+                                        int G, int gl, bool vec, int32_t none, const Hit &hit)
 {
     int cnt = 0;
-    for (int32_t base = q0 & ~3; base < q1; base += 4 * G) {
-        const int32_t e = base + 4 * gl;
-        if (vec && base >= q0 && base + 4 * G <= q1) {
-            const int4 v = __ldg(reinterpret_cast<const int4 *>(S + e));
-            cnt += hit(v.x) + hit(v.y) + hit(v.z) + hit(v.w);
-        } else {
-            #pragma unroll
-            for (int u = 0; u < 4; u++)
-                if (e + u >= q0 && e + u < q1) cnt += hit(S[e + u]);
+    for (int32_t base = q0 & ~3; base < q1; base += 16 * G) {
+        int4 v[4];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int32_t b = base + 4 * (u * G + gl);
+            if (vec && b >= q0 && b + 4 <= q1) {
+                v[u] = __ldg(reinterpret_cast<const int4 *>(S + b));
+            } else {
+                v[u].x = (b >= q0 && b < q1) ? S[b] : none;
+                v[u].y = (b + 1 >= q0 && b + 1 < q1) ? S[b + 1] : none;
+                v[u].z = (b + 2 >= q0 && b + 2 < q1) ? S[b + 2] : none;
+                v[u].w = (b + 3 >= q0 && b + 3 < q1) ? S[b + 3] : none;
+            }
         }
+        #pragma unroll
+        for (int u = 0; u < 4; u++)
+            cnt += hit(v[u].x) + hit(v[u].y) + hit(v[u].z) + hit(v[u].w);
     }
     return cnt;
 }
@@ -727,7 +738,7 @@ __device__ __forceinline__ void ct_write(int32_t pm, int32_t j, int c, int32_t *
 template <typename Z, class Hit>
 __device__ __forceinline__ void ct_batch(bool valid, int32_t q0, int32_t len, int32_t pm,
                                          int32_t j, const int32_t *__restrict__ S, bool vec,
-                                         const Hit &hit, int32_t *__restrict__ Cj,
+                                         int32_t none, const Hit &hit, int32_t *__restrict__ Cj,
                                          Z *__restrict__ Cx, unsigned long long &sum,
                                          unsigned long long &zc, int *owner)
 {
@@ -770,7 +781,7 @@ __device__ __forceinline__ void ct_batch(bool valid, int32_t q0, int32_t len, in
         // group of G lanes)
         const bool act = r0 + lane < total;
         const int G = 1 << elg, gl = lane - gs;
-        int c = act ? ct_count(S, eq0, eq0 + elen, G, gl, vec, hit) : 0;
+        int c = act ? ct_count(S, eq0, eq0 + elen, G, gl, vec, none, hit) : 0;
         #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
             const int u = __shfl_xor_sync(0xffffffffu, c, d);
@@ -861,7 +872,9 @@ k_ct_hash(const CtItem *__restrict__ items, const int32_t *__restrict__ totals,
             bool nvalid;
             int32_t nq0, nlen, npm, nj;
             ct_load_entry(I, e + 32 + lane, bucket, nvalid, nq0, nlen, npm, nj);
-            ct_batch<Z>(valid, q0, len, pm, j, S, vec, hit, Cj, Cx, sum, zc, s_owner[w]);
+            // `none` is INT32_MIN: never a column, and not the empty-slot mark
+            ct_batch<Z>(valid, q0, len, pm, j, S, vec, INT32_MIN, hit, Cj, Cx, sum, zc,
+                        s_owner[w]);
             valid = nvalid; q0 = nq0; len = nlen; pm = npm; j = nj;
         }
         __syncwarp();
@@ -950,10 +963,12 @@ k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals
             s_item[cur ^ 1] = nx;
             if (nx < nitems) s_I[cur ^ 1] = items[nx];
         }
+        // probed ranges lie inside [klo, khi]; `none` maps to the guard bit
         auto hit = [&](int32_t x) -> int {
-            const uint32_t k = min((uint32_t)(x - klo), nbits);
+            const uint32_t k = (uint32_t)(x - klo);
             return (int)((bm[k >> 5] >> (k & 31)) & 1u);
         };
+        const int32_t none = klo + (int32_t)nbits;
         while (true) {
             int e = 0;
             if (lane == 0) e = atomicAdd(&s_next, 32);
@@ -962,23 +977,18 @@ k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals
             bool valid;
             int32_t q0, len, pm, j;
             ct_load_entry(I, e + lane, bucket, valid, q0, len, pm, j);
-            ct_batch<Z>(valid, q0, len, pm, j, S, vec, hit, Cj, Cx, sum, zc,
+            ct_batch<Z>(valid, q0, len, pm, j, S, vec, none, hit, Cj, Cx, sum, zc,
                         s_owner[tid >> 5]);
         }
         __syncwarp();
         __syncthreads();
-        // clear: zero the span's words with 16-byte stores when that is
-        // cheaper than revisiting the row's entries
-        const uint32_t span_words = (uint32_t)(khi - klo) / 32u + 1u;
-        if (span_words <= 4u * (uint32_t)(I.rp1 - I.rp0)) {
+        // clear: zero the span's words with 16-byte stores (at most a few
+        // per thread, and no global loads)
+        {
+            const uint32_t span_words = (uint32_t)(khi - klo) / 32u + 1u;
             uint4 *b4 = reinterpret_cast<uint4 *>(bm);
             const uint32_t n4 = (span_words + 3u) / 4u;
             for (uint32_t q = tid; q < n4; q += blockDim.x) b4[q] = make_uint4(0, 0, 0, 0);
-        } else {
-            for (int32_t q = I.rp0 + tid; q < I.rp1; q += blockDim.x) {
-                const uint32_t k = (uint32_t)(J[q] - klo);
-                bm[k >> 5] = 0;
-            }
         }
         cur ^= 1;
     }

@@ -425,7 +425,10 @@ __global__ void k_fill_value(T *__restrict__ out, const T *__restrict__ v, int64
         out[t] = x;
 }
 
-static int download_to_t(const DevCSR &A, int64_t *p, int64_t *i, void *x, cudaStream_t s)
+// every entry of A as it is (zombies keep their flipped indices) into the
+// caller's arrays: nrows+1 offsets, nnz indices and, when x is given, nnz
+// values (iso values expanded); synchronises s
+int dev_copy_out(const DevCSR &A, int64_t *p, int64_t *i, void *x, cudaStream_t s)
 {
     Scratch ws(s);
     const size_t ts = type_size(A.type);
@@ -460,7 +463,7 @@ static int download_to_t(const DevCSR &A, int64_t *p, int64_t *i, void *x, cudaS
 
 int dev_download_to(const DevCSR &A0, int64_t *p, int64_t *i, void *x, cudaStream_t s)
 {
-    if (A0.nzombies == 0) return download_to_t(A0, p, i, x, s);
+    if (A0.nzombies == 0) return dev_copy_out(A0, p, i, x, s);
     // prune a private copy so the caller's matrix is untouched
     DevCSR B = A0;
     const size_t ts = type_size(A0.type);
@@ -474,7 +477,7 @@ int dev_download_to(const DevCSR &A0, int64_t *p, int64_t *i, void *x, cudaStrea
     if (A0.x) cudaMemcpyAsync(B.x, A0.x, A0.iso ? ts : (size_t)A0.nnz * ts,
                               cudaMemcpyDeviceToDevice, s);
     int info = dev_prune_zombies(B, s);
-    if (info == SUCCESS) info = download_to_t(B, p, i, x, s);
+    if (info == SUCCESS) info = dev_copy_out(B, p, i, x, s);
     dev_free(B, s);
     cudaStreamSynchronize(s);
     return info;

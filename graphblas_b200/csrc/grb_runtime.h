@@ -137,6 +137,11 @@ int dev_import(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
 // live indices and values; iso values expanded); synchronises s
 int dev_download_to(const DevCSR &A, int64_t *p, int64_t *i, void *x, cudaStream_t s);
 
+// copy every entry (zombies kept as flipped indices) into the caller's
+// arrays (nrows+1 offsets, nnz indices, and nnz values unless x is null;
+// iso values expanded); synchronises s
+int dev_copy_out(const DevCSR &A, int64_t *p, int64_t *i, void *x, cudaStream_t s);
+
 // ---- scans ----
 // exclusive scan of n int64 values in place; out[n] receives the total when
 // `with_total`.  `in` and `out` may alias.

@@ -9,13 +9,18 @@
 // same two functions can instead be called from the existing
 // `#if GRAPHBLAS_HAS_CUDA` branch of GB_AxB_dot.c:189-197 and a new branch in
 // GB_AxB_saxpy.c.  Anything the GPU does not take (hypersparse, bitmap or
-// full operands, iso outputs, user types, semirings outside the compiled
-// list) is declined with GrB_NO_VALUE and runs on the CPU as before.
+// full operands, user types, semirings outside the compiled list) is
+// declined with GrB_NO_VALUE and runs on the CPU as before.
 //
-// The GPU result is copied into a C built exactly as the CPU kernels build
-// it (GB_new_bix with the same sizes, GB_AxB_dot3.c:172-176 and
-// GB_AxB_saxpy3.c:242-244), so every later step of the library (GB_wait's
-// zombie removal, GB_accum_mask, reductions) sees the same object.
+// The product stays on the device until C has been built exactly as the CPU
+// kernels build it (GB_new_bix with the same sizes, GB_AxB_dot3.c:172-176
+// and GB_AxB_saxpy3.c:242-244); the device result is then copied straight
+// into C's arrays, which belong to the library's allocator from the start,
+// so every later step of the library (GB_wait's zombie removal,
+// GB_accum_mask, reductions, GrB_free) sees its own kind of object.  An iso
+// result (GB_AxB_iso.c:79: every entry the same value, cscalar) is computed
+// as a pattern with the ANY_PAIR semiring - the pattern of a product does
+// not depend on values - and C gets the one value.
 
 #include "GB.h"
 #include "mxm/GB_mxm.h"
@@ -81,27 +86,48 @@ static bool gb_b200_semiring (grb_b200_semiring *s, const GrB_Semiring S)
 
 // build C like the CPU kernel does and copy the device result into it
 static GrB_Info gb_b200_adopt (GrB_Matrix C, GrB_Type ctype, int64_t vlen,
-    int64_t vdim, const GrB_Matrix like, grb_b200_matrix *R)
+    int64_t vdim, const GrB_Matrix like, grb_b200_dmatrix *R, bool C_iso,
+    const GB_void *cscalar)
 {
     GrB_Info info ;
-    int64_t cnz = R->p [vdim] ;
+    int64_t cnz = 0, nzombies = 0 ;
+    grb_b200_dmatrix_info (*R, NULL, NULL, &cnz, &nzombies, NULL, NULL) ;
     info = GB_new_bix (&C, ctype, vlen, vdim, GB_Ap_malloc, like->is_csc,
         GxB_SPARSE, true, like->hyper_switch, vdim, GB_IMAX (cnz, 1), true,
-        false) ;
+        C_iso) ;
     if (info == GrB_SUCCESS)
     {
-        memcpy (C->p, R->p, (vdim + 1) * sizeof (int64_t)) ;
-        memcpy (C->i, R->i, cnz * sizeof (int64_t)) ;
-        memcpy (C->x, R->x, cnz * ctype->size) ;
-        C->nvec = vdim ;
-        C->nvec_nonempty = -1 ;
-        C->nvals = cnz ;
-        C->nzombies = R->nzombies ;
-        C->jumbled = R->jumbled ;
-        C->magic = GB_MAGIC ;
+        int gi = grb_b200_dmatrix_copy_out (*R, C->p, C->i, C_iso ? NULL : C->x) ;
+        if (gi != 0)
+        {
+            GB_phybix_free (C) ;
+            info = (GrB_Info) gi ;
+        }
+        else
+        {
+            if (C_iso) memcpy (C->x, cscalar, ctype->size) ;
+            C->nvec = vdim ;
+            C->nvec_nonempty = -1 ;
+            C->nvals = cnz ;
+            C->nzombies = nzombies ;
+            C->iso = C_iso ;
+            C->magic = GB_MAGIC ;
+        }
     }
-    free (R->p) ; free (R->i) ; free (R->x) ;
+    grb_b200_dmatrix_free (R) ;
     return info ;
+}
+
+// the semiring the device runs: the caller's, or ANY_PAIR (bool) for an iso
+// result, whose pattern is all the device needs to find
+static bool gb_b200_device_semiring (grb_b200_semiring *s,
+    const GrB_Semiring S, bool C_iso)
+{
+    if (!C_iso) return gb_b200_semiring (s, S) ;
+    s->add_opcode = (int) GB_ANY_binop_code ;
+    s->mult_opcode = (int) GB_PAIR_binop_code ;
+    s->type = (int) GB_BOOL_code ;
+    return true ;
 }
 
 GrB_Info __wrap_GB_AxB_dot3 (GrB_Matrix C, const bool C_iso,
@@ -109,20 +135,27 @@ GrB_Info __wrap_GB_AxB_dot3 (GrB_Matrix C, const bool C_iso,
     const GrB_Matrix A, const GrB_Matrix B, const GrB_Semiring semiring,
     const bool flipxy, GB_Werk Werk)
 {
-    grb_b200_matrix m, a, b, r ;
+    grb_b200_matrix m, a, b ;
     grb_b200_semiring s ;
-    memset (&r, 0, sizeof (r)) ;
-    if (gb_b200_enabled ( ) && !C_iso && gb_b200_view (&m, M)
+    if (gb_b200_enabled ( ) && gb_b200_view (&m, M)
         && gb_b200_view (&a, A) && gb_b200_view (&b, B)
-        && M->nzombies == 0 && gb_b200_semiring (&s, semiring)
+        && M->nzombies == 0 && gb_b200_device_semiring (&s, semiring, C_iso)
         && grb_b200_AxB_dot3_branch (&m, &a, &b, &s, flipxy))
     {
-        int info = grb_b200_AxB_dot3 (&r, &m, Mask_struct, &a, &b, &s, flipxy) ;
+        grb_b200_dmatrix R = NULL ;
+        int info = grb_b200_AxB_dot3_device (&R, &m, Mask_struct, &a, &b, &s,
+            flipxy) ;
         if (info == 0)
         {
-            gb_b200_gateway_taken++ ;
-            return gb_b200_adopt (C, semiring->add->op->ztype, M->vlen, M->vdim,
-                M, &r) ;
+            // C keeps M's vector pointers, its zombies and M's order
+            info = gb_b200_adopt (C, semiring->add->op->ztype, M->vlen,
+                M->vdim, M, &R, C_iso, cscalar) ;
+            if (info == GrB_SUCCESS)
+            {
+                C->jumbled = M->jumbled ;
+                gb_b200_gateway_taken++ ;
+            }
+            return (GrB_Info) info ;
         }
         if (info != GrB_NO_VALUE) return (GrB_Info) info ;
     }
@@ -138,20 +171,27 @@ GrB_Info __wrap_GB_AxB_saxpy3 (GrB_Matrix C, const bool C_iso,
     bool *mask_applied, const GrB_Desc_Value AxB_method, const int do_sort,
     GB_Werk Werk)
 {
-    grb_b200_matrix m, a, b, r ;
+    grb_b200_matrix m, a, b ;
     grb_b200_semiring s ;
-    memset (&r, 0, sizeof (r)) ;
-    if (gb_b200_enabled ( ) && !C_iso && C_sparsity == GxB_SPARSE
+    if (gb_b200_enabled ( ) && C_sparsity == GxB_SPARSE
         && gb_b200_view (&m, M) && gb_b200_view (&a, A) && gb_b200_view (&b, B)
-        && (M == NULL || M->nzombies == 0) && gb_b200_semiring (&s, semiring))
+        && (M == NULL || M->nzombies == 0)
+        && gb_b200_device_semiring (&s, semiring, C_iso))
     {
-        int info = grb_b200_AxB_saxpy3 (&r, M ? &m : NULL, Mask_comp, Mask_struct,
-            &a, &b, &s, flipxy, mask_applied, do_sort) ;
+        grb_b200_dmatrix R = NULL ;
+        int info = grb_b200_AxB_saxpy3_device (&R, M ? &m : NULL, Mask_comp,
+            Mask_struct, &a, &b, &s, flipxy, mask_applied) ;
         if (info == 0)
         {
-            gb_b200_gateway_taken++ ;
-            return gb_b200_adopt (C, semiring->add->op->ztype, A->vlen, B->vdim,
-                B, &r) ;
+            // sorted, no zombies
+            info = gb_b200_adopt (C, semiring->add->op->ztype, A->vlen,
+                B->vdim, B, &R, C_iso, cscalar) ;
+            if (info == GrB_SUCCESS)
+            {
+                C->jumbled = false ;
+                gb_b200_gateway_taken++ ;
+            }
+            return (GrB_Info) info ;
         }
         if (info != GrB_NO_VALUE) return (GrB_Info) info ;
     }

@@ -201,6 +201,31 @@ int grb_b200_dmatrix_info(grb_b200_dmatrix D, int64_t *nrows, int64_t *ncols,
                           int64_t *nnz, int64_t *nzombies, int *type,
                           bool *iso);
 
+/* The drop-in calls in two stages, for a caller that builds its own result
+ * object: the product is left on the device as *C (free it with
+ * grb_b200_dmatrix_free), grb_b200_dmatrix_info gives its sizes, and
+ * grb_b200_dmatrix_copy_out copies it into arrays the caller allocated
+ * with those sizes - the shim of the reference copies straight into the
+ * arrays of the GrB_Matrix that GB_new_bix made (GB_AxB_dot3.c:172-176,
+ * GB_AxB_saxpy3.c:242-244).  Same operands, rules and results as
+ * grb_b200_AxB_dot3 / grb_b200_AxB_saxpy3 above (the dot3 result keeps
+ * M's vector pointers and its zombies). */
+int grb_b200_AxB_dot3_device(grb_b200_dmatrix *C, const grb_b200_matrix *M,
+                             bool Mask_struct, const grb_b200_matrix *A,
+                             const grb_b200_matrix *B,
+                             const grb_b200_semiring *semiring, bool flipxy);
+
+int grb_b200_AxB_saxpy3_device(grb_b200_dmatrix *C, const grb_b200_matrix *M,
+                               bool Mask_comp, bool Mask_struct,
+                               const grb_b200_matrix *A, const grb_b200_matrix *B,
+                               const grb_b200_semiring *semiring, bool flipxy,
+                               bool *mask_applied);
+
+/* Every stored entry of D, zombies included (as GB_FLIP(i), the reference's
+ * -(i)-2), into caller-owned arrays: p (vdim+1 offsets), i (nnz indices) and,
+ * unless x is NULL, x (nnz values, iso values expanded).  Synchronous. */
+int grb_b200_dmatrix_copy_out(grb_b200_dmatrix D, int64_t *p, int64_t *i, void *x);
+
 /* C<M> = A*B' over M's pattern (row i of A . row j of B); zombies kept */
 int grb_b200_dmxm_dot3(grb_b200_dmatrix *C, grb_b200_dmatrix M,
                        bool mask_struct, grb_b200_dmatrix A,
