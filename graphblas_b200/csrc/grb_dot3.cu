@@ -374,11 +374,11 @@ k_dot3_intersect(const D3Work *__restrict__ queue, const int32_t *__restrict__ s
 //   bitmap    one 1024-thread block per SM: the key row as a shared-memory
 //             bitmap over its column span.
 //
-// Inside an item a warp takes 32 entries at a time and gives each a group of
-// lanes sized to its list (about CT_PER_LANE elements per lane, 1 to 32
-// lanes), packed into the warp's lanes round by round; a group probes four
-// elements per lane per step with 16-byte loads.  The hit count is C(i,j);
-// its sum over the live entries and the zombie count come back with the
+// Inside an item the warps take the long lists (CT_LONG elements or more)
+// one at a time, each probed by the whole warp, then the short lists 32 at a
+// time, probed flat (their elements end to end, one per lane); a lane keeps
+// four 16-byte or scalar loads in flight.  The hit count is C(i,j); its sum
+// over the live entries and the zombie count come back with the
 // call, so a following sum reduction of C needs no pass.
 // ---------------------------------------------------------------------------
 
@@ -390,7 +390,7 @@ static constexpr int CT_ITEM_BM = 2048;      // entries per bitmap item, at most
 static constexpr int CT_ITEM_H = 1024;       // entries per hash item, at most
 static constexpr int64_t CT_WORK_BM = 1 << 20;   // probes per bitmap item, about
 static constexpr int64_t CT_WORK_H = 1 << 14;    // probes per hash item, about
-static constexpr int CT_PER_LANE = 16;       // list elements per lane of an entry's group
+static constexpr int CT_PER_LANE = 16;       // list elements per lane of a lane group
 static constexpr int CT_LONG = 256;          // lists this long go to the front of a bucket
 static constexpr int CT_TILE_T = 256;        // plan: threads per tile
 static constexpr int CT_TILE_K = 8;          // plan: keys per thread
@@ -404,9 +404,9 @@ static constexpr int64_t CT_MIN_ENTRIES = 1024;
 struct __align__(16) CtQ { int32_t key, rank, q0, len; };
 // a grouped entry in its group's bucket
 struct __align__(16) CtRec { int32_t q0, len, pm, j; };
-// a work item: bucket entries [e0, e1) of key's group; the key row's offsets
-// and its first and last column
-struct __align__(16) CtItem { int32_t key, e0, e1, rp0, rp1, klo, khi, pad; };
+// a work item: bucket entries [e0, e1) of key's group, the long lists first
+// ([e0, el)); the key row's offsets and its first and last column
+struct __align__(16) CtItem { int32_t key, e0, e1, rp0, rp1, klo, khi, el; };
 
 // totals[] written by the plan kernel and read by the count kernels
 enum { CT_N_BM = 0, CT_N_H = 1, CT_N_BUCKET = 2, CT_ERR = 3 };
@@ -633,9 +633,13 @@ k_ct_plan(const int32_t *__restrict__ gcnt, const unsigned long long *__restrict
             const int32_t rp0 = P[r], rp1 = P[r + 1];
             const int32_t klo = J[rp0], khi = J[rp1 - 1];
             CtItem *out = nb ? items_bm + ob : items_h + oh;
-            for (int32_t q = 0; q < n; q++)
-                out[q] = CtItem{(int32_t)t, (int32_t)(oc + (int64_t)c * q / n),
-                                (int32_t)(oc + (int64_t)c * (q + 1) / n), rp0, rp1, klo, khi, 0};
+            const int64_t lend = oc + gcnt[2 * t];          // end of the long lists
+            for (int32_t q = 0; q < n; q++) {
+                const int64_t e0 = oc + (int64_t)c * q / n, e1 = oc + (int64_t)c * (q + 1) / n;
+                const int64_t el = lend < e0 ? e0 : (lend > e1 ? e1 : lend);
+                out[q] = CtItem{(int32_t)t, (int32_t)e0, (int32_t)e1, rp0, rp1, klo, khi,
+                                (int32_t)el};
+            }
         }
         ob += nb; oh += nh; oc += c;
     }
@@ -726,8 +730,10 @@ __device__ __forceinline__ void ct_write(int32_t pm, int32_t j, int c, int32_t *
     else { Cj[pm] = flip(j); zc++; }
 }
 
-// One batch of up to 32 bucket entries, one per lane (valid, trimmed list
-// [q0, q0 + len), output position pm and column j).  Every entry gets a
+// The bitmap kernel's batches of short lists: up to 32 bucket entries, one
+// per lane (valid, trimmed list [q0, q0 + len), output position pm and
+// column j), probed by lane groups (a bitmap probe is cheap enough that the
+// flat batches' per-window bookkeeping would cost more than idle lanes).  Every entry gets a
 // group of 2^lg lanes, about CT_PER_LANE elements of its list per lane (1 to
 // 32 lanes).  The groups are packed into lane slots - larger groups first,
 // lane order within a size - so that every group starts on a multiple of its
@@ -736,7 +742,7 @@ __device__ __forceinline__ void ct_write(int32_t pm, int32_t j, int c, int32_t *
 // entries' lanes write into the warp's `owner` row) and the groups probe
 // side by side.  `owner` holds 32 ints, all -1 between calls.
 template <typename Z, class Hit>
-__device__ __forceinline__ void ct_batch(bool valid, int32_t q0, int32_t len, int32_t pm,
+__device__ __forceinline__ void ct_batch_packed(bool valid, int32_t q0, int32_t len, int32_t pm,
                                          int32_t j, const int32_t *__restrict__ S, bool vec,
                                          int32_t none, const Hit &hit, int32_t *__restrict__ Cj,
                                          Z *__restrict__ Cx, unsigned long long &sum,
@@ -792,6 +798,90 @@ __device__ __forceinline__ void ct_batch(bool valid, int32_t q0, int32_t len, in
     }
 }
 
+// One batch of up to 32 short lists, one entry per lane (valid, trimmed list
+// [q0, q0 + len), output position pm and column j), probed flat: the
+// entries' elements are laid end to end and the warp takes windows of 32
+// consecutive elements, lane d the d-th of each, four windows per step (four
+// loads in flight per lane).  In a window a lane's entry is the window's
+// first entry (the last one starting at or before the window, a ballot) plus
+// the entries starting between the window's start and the lane (a popcount
+// of the OR of their start offsets), so every lane probes in every window
+// but the batch's last.  Hits go to the entry's counter in `cnt` (32 ints,
+// all zero between calls).
+template <typename Z, class Hit>
+__device__ __forceinline__ void ct_batch(bool valid, int32_t q0, int32_t len, int32_t pm,
+                                         int32_t j, const int32_t *__restrict__ S,
+                                         int32_t none, const Hit &hit,
+                                         int32_t *__restrict__ Cj, Z *__restrict__ Cx,
+                                         unsigned long long &sum, unsigned long long &zc,
+                                         int *cnt)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned vm = __ballot_sync(0xffffffffu, valid);
+    const int n = __popc(vm);
+    if (n == 0) return;
+    // the valid entries move to lanes 0 .. n-1, in order
+    const int src = lane < n ? (int)__fns(vm, 0, lane + 1) : 0;
+    const int32_t eq0 = __shfl_sync(0xffffffffu, q0, src);
+    int32_t elen = __shfl_sync(0xffffffffu, len, src);
+    const int32_t epm = __shfl_sync(0xffffffffu, pm, src);
+    const int32_t ej = __shfl_sync(0xffffffffu, j, src);
+    if (lane >= n) elen = 0;
+    int32_t inc = elen;
+    #pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int32_t u = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc += u;
+    }
+    const int32_t start = inc - elen;
+    const int32_t total = __shfl_sync(0xffffffffu, inc, 31);
+    const unsigned upto = lane == 31 ? 0xffffffffu : (2u << lane) - 1u;
+    for (int32_t f0 = 0; f0 < total; f0 += 128) {
+        int32_t x[4];
+        int ent[4];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int32_t w0 = f0 + 32 * u;
+            const unsigned le = __ballot_sync(0xffffffffu, lane < n && start <= w0);
+            const int elo = 31 - __clz(le);
+            const bool inside = lane < n && start > w0 && start < w0 + 32;
+            const unsigned sm = __reduce_or_sync(0xffffffffu,
+                                                 inside ? 1u << (start - w0) : 0u);
+            const int e = elo + __popc(sm & upto);
+            const int32_t se = __shfl_sync(0xffffffffu, start, e);
+            const int32_t qe = __shfl_sync(0xffffffffu, eq0, e);
+            const int32_t f = w0 + lane;
+            x[u] = f < total ? S[qe + (f - se)] : none;
+            ent[u] = e;
+        }
+        #pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (hit(x[u])) atomicAdd(&cnt[ent[u]], 1);
+    }
+    __syncwarp();
+    if (lane < n) {
+        const int c = cnt[lane];
+        cnt[lane] = 0;
+        ct_write<Z>(epm, ej, c, Cj, Cx, sum, zc);
+    }
+    __syncwarp();
+}
+
+// one long list by the whole warp: C(i,j) for the entry in bucket slot e
+template <typename Z, class Hit>
+__device__ __forceinline__ void ct_long(const CtRec *__restrict__ bucket, int32_t e,
+                                        const int32_t *__restrict__ S, bool vec, int32_t none,
+                                        const Hit &hit, int32_t *__restrict__ Cj,
+                                        Z *__restrict__ Cx, unsigned long long &sum,
+                                        unsigned long long &zc)
+{
+    const int lane = threadIdx.x & 31;
+    const CtRec r = bucket[e];
+    int c = ct_count(S, r.q0, r.q0 + r.len, 32, lane, vec, none, hit);
+    c = (int)__reduce_add_sync(0xffffffffu, (unsigned)c);
+    if (lane == 0) ct_write<Z>(r.pm, r.j, c, Cj, Cx, sum, zc);
+}
+
 __device__ __forceinline__ void ct_load_entry(const CtItem &I, int32_t e,
                                               const CtRec *__restrict__ bucket, bool &valid,
                                               int32_t &q0, int32_t &len, int32_t &pm,
@@ -824,12 +914,12 @@ k_ct_hash(const CtItem *__restrict__ items, const int32_t *__restrict__ totals,
 {
     using Z = typename SR::z_t;
     __shared__ int4 s_tab[CT_H_WARPS][CT_H_BUCKETS];
-    __shared__ int s_owner[CT_H_WARPS][32];
+    __shared__ int s_cnt[CT_H_WARPS][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int4 *tab = s_tab[w];
     int32_t *slots = reinterpret_cast<int32_t *>(tab);
     for (int q = lane; q < CT_H_BUCKETS; q += 32) tab[q] = make_int4(-1, -1, -1, -1);
-    s_owner[w][lane] = -1;
+    s_cnt[w][lane] = 0;
     __syncwarp();
     const int nitems = totals[CT_N_H];
     unsigned long long sum = 0, zc = 0;
@@ -846,10 +936,6 @@ k_ct_hash(const CtItem *__restrict__ items, const int32_t *__restrict__ totals,
         int bits = 3;
         while ((1 << bits) * 2 < klen) bits++;
         const uint32_t bmask = (1u << bits) - 1;
-        // the first batch's entries load while the table fills
-        bool valid;
-        int32_t q0, len, pm, j;
-        ct_load_entry(I, I.e0 + lane, bucket, valid, q0, len, pm, j);
         for (int32_t q = I.rp0 + lane; q < I.rp1; q += 32) {
             const int32_t k = J[q];
             uint32_t b = ct_hash(k, bits);
@@ -868,14 +954,15 @@ k_ct_hash(const CtItem *__restrict__ items, const int32_t *__restrict__ totals,
                 b = (b + 1) & bmask;
             }
         };
-        for (int32_t e = I.e0; e < I.e1; e += 32) {
-            bool nvalid;
-            int32_t nq0, nlen, npm, nj;
-            ct_load_entry(I, e + 32 + lane, bucket, nvalid, nq0, nlen, npm, nj);
-            // `none` is INT32_MIN: never a column, and not the empty-slot mark
-            ct_batch<Z>(valid, q0, len, pm, j, S, vec, INT32_MIN, hit, Cj, Cx, sum, zc,
-                        s_owner[w]);
-            valid = nvalid; q0 = nq0; len = nlen; pm = npm; j = nj;
+        // `none` is INT32_MIN: never a column, and not the empty-slot mark
+        for (int32_t e = I.e0; e < I.el; e++)
+            ct_long<Z>(bucket, e, S, vec, INT32_MIN, hit, Cj, Cx, sum, zc);
+        for (int32_t e = I.el; e < I.e1; e += 32) {
+            bool valid;
+            int32_t q0, len, pm, j;
+            ct_load_entry(I, e + lane, bucket, valid, q0, len, pm, j);
+            ct_batch<Z>(valid, q0, len, pm, j, S, INT32_MIN, hit, Cj, Cx, sum, zc,
+                        s_cnt[w]);
         }
         __syncwarp();
         for (int q = lane; q <= (int)bmask; q += 32) tab[q] = make_int4(-1, -1, -1, -1);
@@ -909,12 +996,12 @@ k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals
     extern __shared__ __align__(16) uint32_t bm[];
     // the item being processed and the one fetched ahead alternate between
     // two slots, so the fetch never writes the slot the block is reading
-    __shared__ int s_item[2], s_next;
+    __shared__ int s_item[2], s_next, s_long;
     __shared__ CtItem s_I[2];
-    __shared__ int s_owner[CT_BM_THREADS / 32][32];
+    __shared__ int s_cnt[CT_BM_THREADS / 32][32];
     const int tid = threadIdx.x, lane = tid & 31;
     for (uint32_t q = tid; q <= bm_words; q += blockDim.x) bm[q] = 0;
-    s_owner[tid >> 5][lane] = -1;
+    s_cnt[tid >> 5][lane] = -1;        // the lane groups' owner rows
     const uint32_t nbits = bm_words * 32u;        // the guard bit
     const int nitems = totals[CT_N_BM];
     unsigned long long sum = 0, zc = 0;
@@ -933,7 +1020,7 @@ k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals
         const CtItem I = s_I[cur];
         __syncwarp();
         __syncthreads();
-        if (tid == 0) s_next = 0;
+        if (tid == 0) { s_next = 0; s_long = 0; }
         const bool by_row = I.key < nrows;
         const int32_t *J = by_row ? Aj : Bj;
         const int32_t *S = by_row ? Bj : Aj;
@@ -969,16 +1056,25 @@ k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals
             return (int)((bm[k >> 5] >> (k & 31)) & 1u);
         };
         const int32_t none = klo + (int32_t)nbits;
+        // long lists one at a time, each by the whole warp, so that no warp
+        // holds many of them; then the short ones 32 at a time
+        while (true) {
+            int e = 0;
+            if (lane == 0) e = atomicAdd(&s_long, 1);
+            e = __shfl_sync(0xffffffffu, e, 0) + I.e0;
+            if (e >= I.el) break;
+            ct_long<Z>(bucket, e, S, vec, none, hit, Cj, Cx, sum, zc);
+        }
         while (true) {
             int e = 0;
             if (lane == 0) e = atomicAdd(&s_next, 32);
-            e = __shfl_sync(0xffffffffu, e, 0) + I.e0;
+            e = __shfl_sync(0xffffffffu, e, 0) + I.el;
             if (e >= I.e1) break;
             bool valid;
             int32_t q0, len, pm, j;
             ct_load_entry(I, e + lane, bucket, valid, q0, len, pm, j);
-            ct_batch<Z>(valid, q0, len, pm, j, S, vec, none, hit, Cj, Cx, sum, zc,
-                        s_owner[tid >> 5]);
+            ct_batch_packed<Z>(valid, q0, len, pm, j, S, vec, none, hit, Cj, Cx, sum, zc,
+                               s_cnt[tid >> 5]);
         }
         __syncwarp();
         __syncthreads();
@@ -1097,7 +1193,7 @@ static int dot3_count_launch(DevCSR &C, const DevCSR &M, bool mask_struct, const
         items_bm, items_h, totals);
     k_ct_route<<<(unsigned)blocks, 256, 0, s>>>(queue, mnz, (int32_t)M.nrows, gcnt, boff,
                                                  bucket, M.p, M.j, A.p, B.p, mq, mq_len);
-    k_ct_hash<SR><<<nsm * 4, CT_H_WARPS * 32, 0, s>>>(
+    k_ct_hash<SR><<<nsm * 5, CT_H_WARPS * 32, 0, s>>>(
         items_h, totals, inext_h, (int32_t)M.nrows, bucket, A.j, B.j, vec,
         C.j, (Z *)C.x, sum, zc);
     k_ct_bitmap<SR><<<nsm, CT_BM_THREADS, (size_t)(bm_words + 1) * 4, s>>>(
