@@ -243,8 +243,9 @@ class Saxpy:
         self.flops = 2.0 * self.products
         self.workload = "saxpy3_er16384_d8_plus_times_fp64"
         # DRAM bytes of the numeric kernel per launch (ncu capture of this
-        # workload: the inputs come from L2, the written slots stay there)
-        self.traffic_per_launch = 3.49e6
+        # workload at this size: the inputs come from L2, the written slots
+        # stay there)
+        self.traffic_per_launch = 3.54e6
 
     def config(self):
         return {"n": self.n, "nnz_A": int(self.A.nnz), "products": self.products,
@@ -369,6 +370,11 @@ class Bfs:
         # writes
         self.alg_bytes = 8.0 * self.n + 4.0 * self.S.nnz + 8.0 * self.n
         self.basis = "S read once (offsets and indices), the parent vector written once"
+        # DRAM bytes of the traversal's numeric launches (one per level): the
+        # heavy-row kernel, which runs at the three largest levels, read and
+        # wrote 682 MB over a traversal in one ncu capture at this size; the
+        # other levels' kernels move little.  Per numeric launch:
+        self.traffic_per_launch = 682e6 / 6 if self.scale == 22 else None
 
     def bfs(self, Sg):
         api = self.api
@@ -472,8 +478,9 @@ CONFIGS = {"tc": TriCount, "saxpy": Saxpy, "bfs": Bfs}
 SUB_CONFIGS = ("saxpy", "bfs", "batch", "serve")
 
 # DRAM bytes (read + write) of one triangle-count dot3 call at R-MAT scale 20,
-# summed over its kernels from one ncu capture of this workload
-TC_TRAFFIC_RMAT20 = None
+# summed over its six kernels from one ncu capture of this workload at this
+# size (dram__bytes_read.sum + dram__bytes_write.sum)
+TC_TRAFFIC_RMAT20 = 2.98e9
 
 
 def make_batch(args):
