@@ -688,6 +688,138 @@ void scan_exclusive_i64_ws(const int64_t *in, int64_t *out, int64_t n, int64_t *
     scan_ws_impl<int64_t>(in, out, n, ws, s, total, out32);
 }
 
+// ---------------------------------------------------------------------------
+// single-pass scan (decoupled look-back): one launch for any length
+//
+// Tiles of 2048 values take their index from a ticket, so a tile's
+// predecessors are always running or done.  A tile scans its values, posts
+// its sum (flag 1) - or, for tile 0, its inclusive prefix (flag 2) - in a
+// 64-bit word (flag << 62 | value), walks back over its predecessors' words
+// until one holds an inclusive prefix, and posts its own inclusive prefix.
+// Waits are bounded: a tile that polls CT-style past the limit sets *err and
+// takes the word as zero (the caller fails the call).  The last tile to
+// finish (a completion counter) clears the words and both counters, so the
+// workspace is ready for the next scan without a memset; it must be zero
+// before its first use.
+// ---------------------------------------------------------------------------
+
+static constexpr int LB_THREADS = 256;
+static constexpr int LB_ROWS = 8;
+static constexpr int LB_TILE = LB_THREADS * LB_ROWS;
+static constexpr unsigned long long LB_AGG = 1ull << 62, LB_INC = 2ull << 62;
+static constexpr unsigned long long LB_VAL = (1ull << 62) - 1;
+static constexpr int LB_SPIN_LIMIT = 1 << 22;
+
+size_t scan_lb_ws_elems(int64_t n)
+{
+    return (size_t)((n + LB_TILE - 1) / LB_TILE) + 2;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(LB_THREADS)
+k_scan_lookback(const T *in, int64_t *out, int64_t n, unsigned long long *__restrict__ ws,
+                int64_t *__restrict__ total, int32_t *__restrict__ out32,
+                int *__restrict__ err)
+{
+    __shared__ int s_tile, s_last;
+    __shared__ long long s_ex;
+    __shared__ int64_t warp_sums[LB_THREADS / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned long long *status = ws + 2;
+    if (tid == 0) s_tile = (int)atomicAdd(&ws[0], 1ull);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    const int64_t ntiles = (n + LB_TILE - 1) / LB_TILE;
+    // a warp owns 256 consecutive values as 8 rows of 32 (coalesced)
+    const int64_t base = tile * LB_TILE + (int64_t)warp * (32 * LB_ROWS) + lane;
+    int64_t v[LB_ROWS];
+    #pragma unroll
+    for (int r = 0; r < LB_ROWS; r++) {
+        const int64_t idx = base + r * 32;
+        v[r] = idx < n ? (int64_t)in[idx] : 0;
+    }
+    int64_t run = 0;
+    #pragma unroll
+    for (int r = 0; r < LB_ROWS; r++) {
+        int64_t x = v[r];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        v[r] = run + x - v[r];
+        run += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0) warp_sums[warp] = run;
+    __syncthreads();
+    if (tid == 0) {
+        int64_t agg = 0;
+        for (int w = 0; w < LB_THREADS / 32; w++) {
+            const int64_t t = warp_sums[w];
+            warp_sums[w] = agg;
+            agg += t;
+        }
+        if (tile == 0) {
+            atomicExch(&status[0], LB_INC | ((unsigned long long)agg & LB_VAL));
+            s_ex = 0;
+        } else {
+            atomicExch(&status[tile], LB_AGG | ((unsigned long long)agg & LB_VAL));
+            long long ex = 0;
+            int64_t p = tile - 1;
+            int spins = 0;
+            while (p >= 0) {
+                const unsigned long long w =
+                    *reinterpret_cast<volatile unsigned long long *>(&status[p]);
+                const unsigned long long f = w & ~LB_VAL;
+                if (f == 0) {
+                    if (++spins > LB_SPIN_LIMIT) { if (err) atomicExch(err, 1); break; }
+                    __nanosleep(32);
+                    continue;
+                }
+                ex += (long long)(w & LB_VAL);
+                if (f == LB_INC) break;
+                p--;
+            }
+            atomicExch(&status[tile], LB_INC | ((unsigned long long)(ex + agg) & LB_VAL));
+            s_ex = ex;
+        }
+        if (total && tile == ntiles - 1) *total = s_ex + agg;
+    }
+    __syncthreads();
+    const int64_t wbase = s_ex + warp_sums[warp];
+    #pragma unroll
+    for (int r = 0; r < LB_ROWS; r++) {
+        const int64_t idx = base + r * 32;
+        if (idx < n) {
+            const int64_t o = wbase + v[r];
+            out[idx] = o;
+            if (out32) out32[idx] = (int32_t)o;
+        }
+    }
+    // the last tile to finish its look-back clears the workspace
+    if (tid == 0) {
+        __threadfence();
+        s_last = atomicAdd(&ws[1], 1ull) == (unsigned long long)(ntiles - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        for (int64_t t = tid; t < ntiles; t += LB_THREADS) status[t] = 0;
+        if (tid == 0) { ws[0] = 0; ws[1] = 0; }
+    }
+}
+
+void scan_exclusive_lb(const int64_t *in, int64_t *out, int64_t n, unsigned long long *ws,
+                       cudaStream_t s, int64_t *total, int32_t *out32, int *err)
+{
+    if (n <= 0) return;
+    if (n <= SCAN_SINGLE_MAX) {
+        k_scan_single<int64_t><<<1, SCAN1_THREADS, 0, s>>>(in, out, n, total, out32);
+        return;
+    }
+    const int64_t ntiles = (n + LB_TILE - 1) / LB_TILE;
+    k_scan_lookback<int64_t><<<(unsigned)ntiles, LB_THREADS, 0, s>>>(in, out, n, ws, total,
+                                                                    out32, err);
+}
+
 int scan_exclusive_i32_to_i64(const int32_t *in, int64_t *out, int64_t n,
                               cudaStream_t s)
 {

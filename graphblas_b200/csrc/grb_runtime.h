@@ -159,6 +159,16 @@ void scan_exclusive_i64_ws(const int64_t *in, int64_t *out, int64_t n, int64_t *
                            cudaStream_t s, int64_t *total = nullptr,
                            int32_t *out32 = nullptr);
 
+// The same exclusive scan as one launch for any length (decoupled
+// look-back; up to 8192 values it is the single-block scan).  ws holds
+// scan_lb_ws_elems(n) words that are zero before the first use; every
+// scan leaves them zero again.  *err (may be null) is set if a tile's wait
+// for its predecessors passes its bound.  in may equal out.
+size_t scan_lb_ws_elems(int64_t n);
+void scan_exclusive_lb(const int64_t *in, int64_t *out, int64_t n, unsigned long long *ws,
+                       cudaStream_t s, int64_t *total = nullptr, int32_t *out32 = nullptr,
+                       int *err = nullptr);
+
 // ---- operations (device matrices) ----
 
 struct SemiringCode { int add, mult, type; };

@@ -1117,7 +1117,10 @@ struct SaxpyPlan {
     int h_bins[MAX_SMEM_BINS + 2] = {0};
     int h_start[MAX_SMEM_BINS + 2] = {0};
     // device buffers
-    int64_t *flops = nullptr, *slot_off = nullptr, *Cp64 = nullptr, *scan_ws = nullptr;
+    int64_t *flops = nullptr, *slot_off = nullptr, *Cp64 = nullptr;
+    // single-pass scan workspaces of the slot and row offsets (zeroed with
+    // the bin counters, left zero by every scan)
+    unsigned long long *lb_slot = nullptr, *lb_row = nullptr;
     int8_t *row_bin = nullptr;
     int32_t *bin_rows = nullptr, *row_cnt = nullptr, *Tj = nullptr;
     void *Tx = nullptr;
@@ -1174,19 +1177,21 @@ static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A
     P->m = m; P->ncols = ncols;
     P->has_mask = M != nullptr; P->mask_comp = mask_comp;
     // the symbolic arrays in one allocation: the bin counters (256 bytes),
-    // the flop counts and the slot offsets first and adjacent, so that one
-    // memset clears all three
+    // the scans' workspaces, the output count and its scan's error word, the
+    // flop counts and the slot offsets first and adjacent, so that one memset
+    // clears them all
     Carve cv(s);
     auto layout = [&]() {
         P->bins = cv.take<int>(64);
+        P->lb_slot = cv.take<unsigned long long>(scan_lb_ws_elems(m + 1));
+        P->lb_row = cv.take<unsigned long long>(scan_lb_ws_elems(m + 1));
+        P->nnz_d = cv.take<int64_t>(2);
         P->flops = cv.take<int64_t>(m + 1);
         P->slot_off = cv.take<int64_t>(m + 1);
         P->Cp64 = cv.take<int64_t>(m + 2);
-        P->scan_ws = cv.take<int64_t>(scan_ws_elems(m + 1));
         P->row_bin = cv.take<int8_t>(m + 1);
         P->bin_rows = cv.take<int32_t>(m + 1);
         P->row_cnt = cv.take<int32_t>(m + 1);
-        P->nnz_d = cv.take<int64_t>(1);
     };
     layout();
     if (!cv.alloc()) return OUT_OF_MEMORY;
@@ -1207,12 +1212,14 @@ static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A
         k_bin_rows<<<nblocks(m, 256), 256, 0, s>>>(P->flops, M ? M->p : nullptr,
             M != nullptr, mask_bounds, ncols, m, lim, P->bins, P->row_bin, P->slot_off,
             A.p, (unsigned long long *)(P->bins + 48));
-    scan_exclusive_i64_ws(P->slot_off, P->slot_off, m + 1, P->scan_ws, s,
-                          (int64_t *)(P->bins + 50));
+    // bins[56]: the slot scan's error word
+    scan_exclusive_lb(P->slot_off, P->slot_off, m + 1, P->lb_slot, s,
+                      (int64_t *)(P->bins + 50), nullptr, P->bins + 56);
     const int nb = P->cfg.nb;
-    int hb[52];
+    int hb[57];
     cudaError_t e = readback(hb, P->bins, sizeof(hb), s);
     if (e != cudaSuccess) return cuda_to_info(e);
+    if (hb[56]) return PANIC;
     for (int b = 0; b < nb + 2; b++) P->h_bins[b] = hb[b];
     int64_t total_cap = 0;
     memcpy(&P->heavy_alen, hb + 48, 8);
@@ -1393,7 +1400,9 @@ static int exec_t(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &
     prof_end(ps, s);
     // exact row counts -> C row pointers, then pack the slots
     k_cnt_to_i64<<<nblocks(m + 1, 256), 256, 0, s>>>(P->row_cnt, P->row_bin, m, P->Cp64);
-    scan_exclusive_i64_ws(P->Cp64, P->Cp64, m + 1, P->scan_ws, s, Cnnz64, Cp);
+    // the scan's error word follows the output count
+    scan_exclusive_lb(P->Cp64, P->Cp64, m + 1, P->lb_row, s, Cnnz64, Cp,
+                      (int *)(P->nnz_d + 1));
     if (m > 0 && P->total_cap > 0)
         k_pack<Z><<<nblocks(P->total_cap, 256, 16), 256, 0, s>>>(m, flat_span(P->total_cap),
             P->slot_off, P->Tj,
@@ -1470,10 +1479,12 @@ int saxpy3(DevCSR &C, const DevCSR *M, bool mask_comp, bool mask_struct,
         dev_free(T, s); saxpy_plan_free(P, s); return OUT_OF_MEMORY;
     }
     info = saxpy_plan_exec(P, M, A, B, T.p, T.j, T.x, nnz_d, s);
-    int64_t nnz = 0;
-    cudaError_t e = readback(&nnz, nnz_d, 8, s);
+    int64_t hv[2] = {0, 0};
+    cudaError_t e = readback(hv, nnz_d, 16, s);
+    const int64_t nnz = hv[0];
     saxpy_plan_free(P, s);
     if (info == SUCCESS && e != cudaSuccess) info = cuda_to_info(e);
+    if (info == SUCCESS && hv[1]) info = PANIC;
     if (info != SUCCESS) { dev_free(T, s); return info; }
     if (nnz >= INT32_MAX) { dev_free(T, s); return OUT_OF_MEMORY; }
     T.nnz = nnz;
