@@ -206,6 +206,8 @@ class BenchBatch:
         nnzA = sum(a.nnz for a in self.mats)
         self.alg_bytes = (8.0 * nnzA + 4.0 * (self.sizes.sum() + self.count) +
                           8.0 * self.products + 8.0 * nnz + 4.0 * (self.sizes.sum() + self.count))
+        self.basis = ("every instance's A once and C once (row offsets, 4-byte indices, "
+                      "fp32 values) plus the B row of every product (index and value)")
         self.per_call_ms = self.time_per_call()
         self.speedup = None
 

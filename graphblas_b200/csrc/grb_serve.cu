@@ -15,6 +15,17 @@
 // budget, and one that can never fit is rejected.  Latency = completion time
 // minus arrival time (the open-loop replay submits each request at its
 // arrival time on a steady clock).
+//
+// Requests of the same kind on the same graph that wait together are fused:
+// a worker that takes an SSSP step also takes the other waiting SSSP steps
+// on that graph (up to max_group, as the budget allows) and runs them as one
+// product W = U min.+ S whose rows are their frontiers - row r of W is
+// exactly request r's vxm, because the product is computed row by row - so
+// small requests share one symbolic phase, one set of launches and one host
+// synchronisation.  Each request's checksum is the sum of its own row taken
+// in a fixed order, the same whether it ran alone or fused.  A fused product
+// that fails (a device allocation, say) is retried request by request, so
+// one request's failure never fails the others it was fused with.
 
 #include <atomic>
 #include <chrono>
@@ -74,6 +85,9 @@ struct grb_b200_server_s {
     int64_t in_use = 0, peak_use = 0;
     int64_t admitted = 0, rejected = 0, completed = 0, failed = 0;
     int active = 0, peak_active = 0;
+    int max_group = 64;               // SSSP steps fused into one product, at most
+    int64_t fused_runs = 0, fused_requests = 0;
+    int largest_group = 1;
     Clock::time_point t0;
     bool keep_results = true;
 };
@@ -102,6 +116,90 @@ int64_t footprint(const grb_b200_server_s *S, const Req *r)
     return 1 << 20;
 }
 
+// per-row sums of an fp32 CSR (one warp per row: lane-strided partial sums in
+// index order, then a fixed shuffle tree), so a row's sum depends only on the
+// row; out[r] as double
+__global__ void k_row_sums_fp32(const int32_t *__restrict__ p, const float *__restrict__ x,
+                                int64_t nrows, double *__restrict__ out)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nrows;
+         r += nw) {
+        float acc = 0.0f;
+        for (int32_t q = p[r] + lane; q < p[r + 1]; q += 32) acc = __fadd_rn(acc, x[q]);
+        for (int o = 16; o > 0; o >>= 1) acc = __fadd_rn(acc, __shfl_down_sync(0xffffffffu, acc, o));
+        if (lane == 0) out[r] = (double)acc;
+    }
+}
+
+// SSSP steps on one graph, fused: W = U min.+ S with one row of U per request
+int run_sssp_group(grb_b200_server_s *S, std::vector<Req *> &grp, cudaStream_t s)
+{
+    const Graph &g = S->graphs[grp[0]->graph];
+    const int64_t k = (int64_t)grp.size();
+    std::vector<int64_t> up(k + 1, 0), ui;
+    std::vector<float> ux;
+    for (int64_t q = 0; q < k; q++) {
+        ui.insert(ui.end(), grp[q]->ui.begin(), grp[q]->ui.end());
+        ux.insert(ux.end(), grp[q]->ux.begin(), grp[q]->ux.end());
+        up[q + 1] = (int64_t)ui.size();
+    }
+    DevCSR U, W;
+    int info = dev_upload(U, k, g.S.nrows, up.data(), ui.empty() ? nullptr : ui.data(),
+                          ux.empty() ? nullptr : ux.data(), T_FP32, false, s);
+    if (info == SUCCESS) {
+        SemiringCode sr{OP_MIN, OP_PLUS, T_FP32};
+        info = saxpy3(W, nullptr, false, true, U, g.S, sr, s);
+    }
+    std::vector<int64_t> wp(k + 1, 0);
+    std::vector<double> sums(k, 0.0);
+    if (info == SUCCESS) {
+        double *d_sums = (double *)dalloc((size_t)k * 8, s);
+        if (!d_sums) info = OUT_OF_MEMORY;
+        if (info == SUCCESS) {
+            if (W.nnz > 0)
+                k_row_sums_fp32<<<(unsigned)((k + 7) / 8), 256, 0, s>>>(W.p, (const float *)W.x,
+                                                                      k, d_sums);
+            else
+                cudaMemsetAsync(d_sums, 0, (size_t)k * 8, s);
+            std::vector<int32_t> wp32(k + 1);
+            cudaMemcpyAsync(wp32.data(), W.p, (size_t)(k + 1) * 4, cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(sums.data(), d_sums, (size_t)k * 8, cudaMemcpyDeviceToHost, s);
+            cudaError_t e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) info = cuda_to_info(e);
+            for (int64_t q = 0; q <= k; q++) wp[q] = wp32[q];
+            dfree(d_sums, s);
+        }
+    }
+    if (info == SUCCESS && S->keep_results && W.nnz > 0) {
+        int64_t *p = nullptr, *i = nullptr;
+        void *x = nullptr;
+        info = dev_download(W, &p, &i, &x, false, malloc, s);
+        if (info == SUCCESS) {
+            for (int64_t q = 0; q < k; q++) {
+                Req *r = grp[q];
+                const int64_t lo = p[q], hi = p[q + 1];
+                r->rp = {0, hi - lo};
+                r->ri.assign(i + lo, i + hi);
+                r->rx.assign((uint8_t *)x + lo * 4, (uint8_t *)x + hi * 4);
+            }
+        }
+        free(p); free(i); free(x);
+    } else if (info == SUCCESS && S->keep_results) {
+        for (Req *r : grp) { r->rp = {0, 0}; r->ri.clear(); r->rx.clear(); }
+    }
+    for (int64_t q = 0; q < k; q++) {
+        grp[q]->count = wp[q + 1] - wp[q];
+        grp[q]->checksum = sums[q];
+    }
+    dev_free(U, s);
+    dev_free(W, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (info == SUCCESS && e != cudaSuccess) info = cuda_to_info(e);
+    return info;
+}
+
 int run_request(grb_b200_server_s *S, Req *r, cudaStream_t s)
 {
     const Graph &g = S->graphs[r->graph];
@@ -118,37 +216,9 @@ int run_request(grb_b200_server_s *S, Req *r, cudaStream_t s)
         }
         dev_free(C, s);
     } else if (r->kind == K_SSSP) {
-        // one relaxation step: w = u' min.+ S (fp32), u sparse
-        DevCSR u, w;
-        const int64_t nu = (int64_t)r->ui.size();
-        std::vector<int64_t> up = {0, nu};
-        info = dev_upload(u, 1, g.S.nrows, up.data(), r->ui.data(), r->ux.data(), T_FP32,
-                          false, s);
-        if (info == SUCCESS) {
-            SemiringCode sr{OP_MIN, OP_PLUS, T_FP32};
-            info = saxpy3(w, nullptr, false, true, u, g.S, sr, s);
-        }
-        if (info == SUCCESS) {
-            r->count = w.nnz;
-            float sum = 0;
-            info = reduce_scalar(&sum, w, OP_PLUS, s);
-            r->checksum = sum;
-        }
-        if (info == SUCCESS) {
-            if (S->keep_results) {
-                int64_t *p = nullptr, *i = nullptr;
-                void *x = nullptr;
-                info = dev_download(w, &p, &i, &x, false, malloc, s);
-                if (info == SUCCESS) {
-                    r->rp.assign(p, p + 2);
-                    r->ri.assign(i, i + w.nnz);
-                    r->rx.assign((uint8_t *)x, (uint8_t *)x + w.nnz * 4);
-                }
-                free(p); free(i); free(x);
-            }
-        }
-        dev_free(u, s);
-        dev_free(w, s);
+        // one relaxation step, w = u' min.+ S (fp32, u sparse): a group of one
+        std::vector<Req *> one{r};
+        return run_sssp_group(S, one, s);
     } else {
         DevCSR C;
         SemiringCode sr{OP_PLUS, OP_TIMES, T_FP64};
@@ -184,6 +254,7 @@ void worker_main(grb_b200_server_s *S, int dev)
     cudaSetDevice(dev);
     cudaStream_t s;
     cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    std::vector<Req *> grp;
     while (true) {
         Req *r = nullptr;
         {
@@ -198,39 +269,86 @@ void worker_main(grb_b200_server_s *S, int dev)
             if (S->pending.empty()) break;
             r = S->pending.front();
             S->pending.pop_front();
-            S->in_use += r->footprint;
+            grp.assign(1, r);
+            int64_t fp = r->footprint;
+            if (r->kind == K_SSSP) {
+                // the other waiting SSSP steps on the same graph join it
+                for (auto it = S->pending.begin();
+                     it != S->pending.end() && (int)grp.size() < S->max_group;) {
+                    Req *q = *it;
+                    if (q->kind == K_SSSP && q->graph == r->graph &&
+                        S->in_use + fp + q->footprint <= S->budget) {
+                        grp.push_back(q);
+                        fp += q->footprint;
+                        it = S->pending.erase(it);
+                    } else {
+                        ++it;
+                    }
+                }
+            }
+            S->in_use += fp;
             S->peak_use = std::max(S->peak_use, S->in_use);
-            S->admitted++;
-            S->active++;
+            S->admitted += (int64_t)grp.size();
+            S->active += (int)grp.size();
             S->peak_active = std::max(S->peak_active, S->active);
         }
-        r->t_start = now_s(S);
-        r->status = run_request(S, r, s);
-        r->t_done = now_s(S);
+        const double t_start = now_s(S);
+        for (Req *q : grp) q->t_start = t_start;
+        if (grp.size() > 1) {
+            const int status = run_sssp_group(S, grp, s);
+            const double t_done = now_s(S);
+            for (Req *q : grp) {
+                q->status = status;
+                q->t_done = t_done;
+            }
+            if (status != SUCCESS) {
+                // retried one by one: a member's own failure stays its own
+                for (Req *q : grp) {
+                    q->status = run_request(S, q, s);
+                    q->t_done = now_s(S);
+                }
+            }
+        } else {
+            r->status = run_request(S, r, s);
+            r->t_done = now_s(S);
+        }
         {
             std::lock_guard<std::mutex> lk(S->mu);
-            S->in_use -= r->footprint;
-            S->active--;
-            if (r->status == SUCCESS) S->completed++;
-            else S->failed++;
+            if (grp.size() > 1) {
+                S->fused_runs++;
+                S->fused_requests += (int64_t)grp.size();
+                S->largest_group = std::max(S->largest_group, (int)grp.size());
+            }
+            for (Req *q : grp) {
+                S->in_use -= q->footprint;
+                S->active--;
+                if (q->status == SUCCESS) S->completed++;
+                else S->failed++;
+            }
         }
         S->cv.notify_all();
     }
     cudaStreamDestroy(s);
 }
 
-void submit(grb_b200_server_s *S, Req *r)
+// requests [r0, r1) have arrived: queued together, under one lock
+void submit(grb_b200_server_s *S, Req *const *r0, Req *const *r1)
 {
-    r->footprint = footprint(S, r);
-    std::lock_guard<std::mutex> lk(S->mu);
-    S->all.push_back(r);
-    if (r->footprint > S->budget) {
-        r->status = OUT_OF_MEMORY;          // can never fit: rejected
-        r->t_start = r->t_done = r->t_arrival;
-        S->rejected++;
-        return;
+    for (Req *const *q = r0; q < r1; q++) (*q)->footprint = footprint(S, *q);
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        for (Req *const *q = r0; q < r1; q++) {
+            Req *r = *q;
+            S->all.push_back(r);
+            if (r->footprint > S->budget) {
+                r->status = OUT_OF_MEMORY;          // can never fit: rejected
+                r->t_start = r->t_done = r->t_arrival;
+                S->rejected++;
+                continue;
+            }
+            S->pending.push_back(r);
+        }
     }
-    S->pending.push_back(r);
     S->cv.notify_all();
 }
 
@@ -356,6 +474,8 @@ int grb_b200_server_replay(grb_b200_server S, int64_t nreq, const int *kind,
         S->in_use = S->peak_use = 0;
         S->admitted = S->rejected = S->completed = S->failed = 0;
         S->active = S->peak_active = 0;
+        S->fused_runs = S->fused_requests = 0;
+        S->largest_group = 1;
     }
     for (int64_t k = 0; k < nreq; k++)
         if (graph[k] < 0 || graph[k] >= (int)S->graphs.size() ||
@@ -363,6 +483,7 @@ int grb_b200_server_replay(grb_b200_server S, int64_t nreq, const int *kind,
             return INVALID_VALUE;
     S->t0 = Clock::now();
     for (int w = 0; w < S->nslots; w++) S->workers.emplace_back(worker_main, S, dev);
+    std::vector<Req *> reqs((size_t)nreq);
     for (int64_t k = 0; k < nreq; k++) {
         Req *r = new Req();
         r->id = k;
@@ -373,11 +494,19 @@ int grb_b200_server_replay(grb_b200_server S, int64_t nreq, const int *kind,
             r->ux.assign(fx + fp[k], fx + fp[k + 1]);
         }
         r->t_arrival = t_arrival[k];
-        // open loop: wait for the arrival time, never for the server
+        reqs[k] = r;
+    }
+    for (int64_t k = 0; k < nreq;) {
+        // open loop: wait for the arrival time, never for the server; then
+        // queue every request that has arrived by now (in arrival order)
         const auto due = S->t0 + std::chrono::duration_cast<Clock::duration>(
                                      std::chrono::duration<double>(t_arrival[k]));
         std::this_thread::sleep_until(due);
-        submit(S, r);
+        const double now = now_s(S);
+        int64_t e = k + 1;
+        while (e < nreq && t_arrival[e] <= now) e++;
+        submit(S, reqs.data() + k, reqs.data() + e);
+        k = e;
     }
     {
         std::lock_guard<std::mutex> lk(S->mu);
@@ -443,6 +572,26 @@ int grb_b200_server_stats(grb_b200_server S, int64_t *admitted, int64_t *rejecte
         for (const Req *r : S->all) t = std::max(t, r->t_done);
         *makespan_s = t;
     }
+    return SUCCESS;
+}
+
+int grb_b200_server_set_fusion(grb_b200_server S, int max_group)
+{
+    if (!S) return NULL_POINTER;
+    if (max_group < 1 || max_group > 4096) return INVALID_VALUE;
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->max_group = max_group;
+    return SUCCESS;
+}
+
+int grb_b200_server_fusion_stats(grb_b200_server S, int64_t *fused_runs,
+                                 int64_t *fused_requests, int *largest_group)
+{
+    if (!S) return NULL_POINTER;
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (fused_runs) *fused_runs = S->fused_runs;
+    if (fused_requests) *fused_requests = S->fused_requests;
+    if (largest_group) *largest_group = S->largest_group;
     return SUCCESS;
 }
 

@@ -40,21 +40,29 @@ def _bind(L):
     L.grb_b200_server_free.argtypes = [ctypes.POINTER(vp)]
     L.grb_b200_server_add_graph_blob.argtypes = [vp, ctypes.c_int, vp, ctypes.c_size_t,
                                                   ctypes.POINTER(ctypes.c_int)]
+    L.grb_b200_server_set_fusion.argtypes = [vp, ctypes.c_int]
+    L.grb_b200_server_fusion_stats.argtypes = [vp, i64p, i64p, ctypes.POINTER(ctypes.c_int)]
     for n in ("create", "add_graph", "add_graph_blob", "replay", "request", "result",
-              "stats", "free"):
+              "stats", "free", "set_fusion", "fusion_stats"):
         getattr(L, "grb_b200_server_" + n).restype = ctypes.c_int
     L._serve_bound = True
     return L
 
 
 class Server:
-    def __init__(self, nslots=8, budget_bytes=40 << 30, keep_results=True):
+    """``fuse``: the most SSSP steps on one graph that run as one product when
+    they wait together (1 = each request alone; None = the library's
+    default, 64)."""
+
+    def __init__(self, nslots=8, budget_bytes=40 << 30, keep_results=True, fuse=None):
         self.L = _bind(_lib())
         h = vp()
         check(self.L.grb_b200_server_create(ctypes.byref(h), nslots, budget_bytes,
                                             keep_results), "server_create")
         self.h = h
         self.kinds = []
+        if fuse is not None:
+            check(self.L.grb_b200_server_set_fusion(h, fuse), "server_set_fusion")
 
     def add_graph(self, kind, csr):
         gid = ctypes.c_int()
@@ -122,9 +130,14 @@ class Server:
         mk = ctypes.c_double()
         check(self.L.grb_b200_server_stats(self.h, *[ctypes.byref(a) for a in v],
                                            ctypes.byref(pa), ctypes.byref(mk)))
+        fr, fq = ctypes.c_int64(), ctypes.c_int64()
+        lg = ctypes.c_int()
+        check(self.L.grb_b200_server_fusion_stats(self.h, ctypes.byref(fr), ctypes.byref(fq),
+                                                  ctypes.byref(lg)))
         return dict(admitted=v[0].value, rejected=v[1].value, completed=v[2].value,
                     failed=v[3].value, peak_bytes=v[4].value, peak_active=pa.value,
-                    makespan_s=mk.value)
+                    makespan_s=mk.value, fused_runs=fr.value, fused_requests=fq.value,
+                    largest_group=lg.value)
 
     def free(self):
         if self.h and self.h.value:
@@ -192,6 +205,10 @@ class BenchServe:
         self.trace = make_trace(self.graphs, nreq=self.nreq, rate=2000.0, seed=args.seed + 2)
         self.workload = "serve_poisson2000_tc_rmat10-16_sssp_minplus_fp32_mxm_er_fp64"
         self.alg_bytes = 0.0
+        self.basis = ("per request: a triangle count reads L, U and the mask once and "
+                      "writes C; an SSSP step reads its frontier and the rows of S it "
+                      "touches and writes w; A*A reads A and the B row of every product "
+                      "and writes C; over the replay's makespan, idle gaps included")
 
     def config(self):
         return dict(requests=self.nreq, rate_req_s=2000.0, slots=8,
@@ -215,7 +232,9 @@ class BenchServe:
         self.S.replay(burst)
         st = self.S.stats()
         self.capacity = {"capacity_req_s": st["completed"] / max(st["makespan_s"], 1e-9),
-                         "capacity_peak_concurrent": st["peak_active"]}
+                         "capacity_peak_concurrent": st["peak_active"],
+                         "capacity_fused_requests": st["fused_requests"],
+                         "capacity_largest_group": st["largest_group"]}
         # per-graph sizes for the bytes each request must move (4-byte
         # indices; fp32 / fp64 values): triangle count reads L, U and the
         # mask once and writes C; SSSP reads u and the rows of S it touches
@@ -256,6 +275,7 @@ class BenchServe:
                     "admitted": st["admitted"], "rejected": st["rejected"],
                     "failed": st["failed"], "peak_hbm_gb": st["peak_bytes"] / 2**30,
                     "peak_concurrent": st["peak_active"],
+                    "fused_runs": st["fused_runs"], "fused_requests": st["fused_requests"],
                     "makespan_s": st["makespan_s"]}
         return st
 

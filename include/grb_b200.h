@@ -372,6 +372,18 @@ int grb_b200_server_stats(grb_b200_server S, int64_t *admitted,
                           int64_t *failed, int64_t *peak_bytes,
                           int *peak_active, double *makespan_s);
 
+/* Fusion of SSSP steps that wait together on the same graph: up to max_group
+ * of them run as one product W = U min.+ A, one frontier per row of U (each
+ * request's result and checksum are the same as when it runs alone).  1
+ * turns fusion off; the default is 64.  Applies to the requests admitted
+ * after the call. */
+int grb_b200_server_set_fusion(grb_b200_server S, int max_group);
+
+/* Products that fused more than one request, the requests they held, and the
+ * largest group, over the last replay. */
+int grb_b200_server_fusion_stats(grb_b200_server S, int64_t *fused_runs,
+                                 int64_t *fused_requests, int *largest_group);
+
 int grb_b200_server_free(grb_b200_server *S);
 
 /* ------------------------------------------------------------------------ */

@@ -9,6 +9,9 @@
   holds more than the budget.
 * Failure injection on the host: a device allocation that fails makes its
   request fail cleanly (GrB_OUT_OF_MEMORY) and the server carries on.
+* Fusion: SSSP steps on one graph that wait together run as one product, one
+  frontier per row; each result and checksum equals the request run alone,
+  and a failure of the fused product is retried request by request.
 """
 
 import numpy as np
@@ -36,13 +39,14 @@ def test_mixed_results_equal_alone_and_oracle(gpu, oracle):
     st = mix.stats()
     assert st["completed"] == 180 and st["failed"] == 0 and st["rejected"] == 0
     assert st["peak_active"] > 1                     # requests overlapped
-    alone = Server(nslots=1, budget_bytes=8 << 30)
+    alone = Server(nslots=1, budget_bytes=8 << 30, fuse=1)
     for kind, g in graphs:
         alone.add_graph(kind, g)
     slow = dict(trace)
     slow["t"] = np.arange(len(trace["t"])) * 1e-4    # one at a time, in order
     alone.replay(slow)
     assert alone.stats()["peak_active"] == 1
+    assert alone.stats()["fused_runs"] == 0
     tri_cache = {}
     for k in range(180):
         kind = int(trace["kind"][k])
@@ -98,7 +102,7 @@ def test_injected_allocation_failure_is_isolated(gpu):
     from graphblas_b200.serve import Server, make_trace
     graphs = _graphs()
     trace = make_trace(graphs, nreq=40, rate=2000.0, seed=11)
-    S = Server(nslots=1, budget_bytes=8 << 30)
+    S = Server(nslots=1, budget_bytes=8 << 30, fuse=1)
     for kind, g in graphs:
         S.add_graph(kind, g)
     gpu.lib().grb_b200_debug_fail_alloc(3)            # the 3rd allocation fails
@@ -110,6 +114,83 @@ def test_injected_allocation_failure_is_isolated(gpu):
     statuses = [S.request(k)["status"] for k in range(40)]
     assert statuses.count(-102) == 1
     S.free()
+
+
+def _sssp_burst(graphs, nreq, seed):
+    """nreq SSSP steps on the first SSSP graph, all arriving at once."""
+    from graphblas_b200.serve import make_trace, K_SSSP
+    tr = make_trace(graphs, nreq=4 * nreq, rate=1e6, seed=seed)
+    ks = [k for k in range(len(tr["kind"])) if tr["kind"][k] == K_SSSP][:nreq]
+    gid = int(tr["graph"][ks[0]])
+    ks = [k for k in ks if int(tr["graph"][k]) == gid]
+    fp, fi, fx = [0], [], []
+    for k in ks:
+        lo, hi = tr["fp"][k], tr["fp"][k + 1]
+        fi.append(tr["fi"][lo:hi])
+        fx.append(tr["fx"][lo:hi])
+        fp.append(fp[-1] + hi - lo)
+    m = len(ks)
+    return {"t": np.zeros(m), "kind": np.full(m, K_SSSP, np.int32),
+            "graph": np.full(m, gid, np.int32), "fp": np.array(fp, np.int64),
+            "fi": np.concatenate(fi), "fx": np.concatenate(fx)}, gid
+
+
+def test_fused_sssp_equals_alone_and_oracle(gpu, oracle):
+    from graphblas_b200.serve import Server, K_SSSP
+    graphs = _graphs()
+    burst, gid = _sssp_burst(graphs, 40, seed=13)
+    m = len(burst["t"])
+    assert m >= 8
+    runs = {}
+    for fuse in (1, 64):
+        S = Server(nslots=1, budget_bytes=8 << 30, fuse=fuse)
+        for kind, g in graphs:
+            S.add_graph(kind, g)
+        S.replay(burst)
+        st = S.stats()
+        assert st["completed"] == m and st["failed"] == 0
+        if fuse == 1:
+            assert st["fused_runs"] == 0
+        else:
+            # all arrive together, one worker: the first product takes them all
+            assert st["largest_group"] == m and st["fused_requests"] == m
+        runs[fuse] = ([S.request(k) for k in range(m)], [S.result(k, K_SSSP) for k in range(m)])
+        S.free()
+    g = graphs[gid][1]
+    for k in range(m):
+        a, b = runs[64][0][k], runs[1][0][k]
+        assert a["count"] == b["count"] and a["checksum"] == b["checksum"]
+        assert_exact(runs[64][1][k], runs[1][1][k], "request %d fused vs alone" % k)
+        lo, hi = burst["fp"][k], burst["fp"][k + 1]
+        u = (np.array([0, hi - lo], np.int64), burst["fi"][lo:hi], burst["fx"][lo:hi], 10)
+        want = oracle.saxpy(1, g.ncols, u, (g.p, g.i, g.x, 10), "MIN", "PLUS", 10)
+        assert_exact(runs[64][1][k], want, "request %d fused vs oracle" % k)
+
+
+def test_fused_failure_is_retried_alone(gpu):
+    from graphblas_b200.serve import Server, K_SSSP
+    graphs = _graphs()
+    burst, _ = _sssp_burst(graphs, 24, seed=17)
+    m = len(burst["t"])
+    S = Server(nslots=1, budget_bytes=8 << 30)
+    for kind, g in graphs:
+        S.add_graph(kind, g)
+    gpu.lib().grb_b200_debug_fail_alloc(1)            # the fused product's first allocation
+    S.replay(burst)
+    gpu.lib().grb_b200_debug_fail_alloc(0)
+    st = S.stats()
+    assert st["largest_group"] == m
+    assert st["failed"] == 0 and st["completed"] == m
+    T = Server(nslots=1, budget_bytes=8 << 30, fuse=1)
+    for kind, g in graphs:
+        T.add_graph(kind, g)
+    T.replay(burst)
+    for k in range(m):
+        a, b = S.request(k), T.request(k)
+        assert a["status"] == 0 and a["count"] == b["count"] and a["checksum"] == b["checksum"]
+        assert_exact(S.result(k, K_SSSP), T.result(k, K_SSSP), "request %d" % k)
+    S.free()
+    T.free()
 
 
 def test_graphs_loaded_from_serialized_blobs(gpu):
