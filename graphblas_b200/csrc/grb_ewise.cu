@@ -4,9 +4,11 @@
 //                GB_accum_mask (Source/mask/GB_accum_mask.c:126) for sparse
 //                C, T and M.  Flat over entries (no row is too long): every
 //                entry of T and of C decides, by binary searches in its row of
-//                C/T and M, whether it survives; two scans give each survivor
-//                its rank inside its row (the union of two sorted lists), and
-//                a scatter writes the sorted result.
+//                C/T and M, whether it survives; two single-launch scans give
+//                each survivor its rank inside its row (the union of two
+//                sorted lists), and a scatter writes the sorted result into
+//                arrays sized for every entry of T and C, so the result's
+//                size comes back with the call's one host read.
 //   transpose    B = A' (Source/transpose/GB_transpose_cast.c:18): column
 //                counts, scan, atomic scatter, then each row of B is sorted
 //                by its (unique) indices with a bitonic network.
@@ -169,23 +171,28 @@ static int accum_mask_t(DevCSR &C, const DevCSR &T, const DevCSR *M, bool comp,
                         bool replace, int accum, cudaStream_t s)
 {
     const int64_t m = T.nrows, nT = T.nnz, nC = C.nnz;
-    // the keep flags / offsets of both sides, T's values, the scan workspace
-    // and the two totals in one allocation
+    // the totals and error word, the two scans' workspaces, the keep flags /
+    // offsets of both sides and T's values in one allocation; the first three
+    // are cleared by one memset
     Carve cv(s);
-    int64_t *keepT = nullptr, *keepC = nullptr, *ws = nullptr, *tot_d = nullptr;
+    int64_t *keepT = nullptr, *keepC = nullptr, *tot_d = nullptr;
+    unsigned long long *lbT = nullptr, *lbC = nullptr;
     Z *valT = nullptr;
-    const int64_t nmax = nT > nC ? nT : nC;
     auto layout = [&]() {
-        tot_d = cv.take<int64_t>(2);
+        tot_d = cv.take<int64_t>(4);
+        lbT = cv.take<unsigned long long>(scan_lb_ws_elems(nT + 1));
+        lbC = cv.take<unsigned long long>(scan_lb_ws_elems(nC + 1));
         keepT = cv.take<int64_t>(nT + 1);
         keepC = cv.take<int64_t>(nC + 1);
         valT = cv.take<Z>(nT + 1);
-        ws = cv.take<int64_t>(scan_ws_elems(nmax + 1));
     };
     layout();
     if (!cv.alloc()) return OUT_OF_MEMORY;
     layout();
     struct Release { Carve &c; ~Release() { dfree(c.base, c.s); } } release{cv};
+    cudaMemsetAsync(tot_d, 0, (size_t)((char *)(lbC + scan_lb_ws_elems(nC + 1)) - (char *)tot_d),
+                    s);
+    int *err = (int *)(tot_d + 2);
     const int32_t *Mp = M ? M->p : nullptr, *Mj = M ? M->j : nullptr;
     // C<T> = T (a structural mask that is T itself, as in w<q> = q): every
     // entry of T is allowed, and an entry of C is under the mask exactly
@@ -195,18 +202,18 @@ static int accum_mask_t(DevCSR &C, const DevCSR &T, const DevCSR *M, bool comp,
         C.p, C.j, (const Z *)C.x, C.iso, Mp, Mj, comp, m_is_t, accum, keepT, valT);
     k_am_cside<Z><<<grid_n(nC), 256, 0, s>>>(m, C.p, C.j, nC, T.p, T.j, Mp, Mj,
         comp, m_is_t, replace, accum, keepC);
-    scan_exclusive_i64_ws(keepT, keepT, nT + 1, ws, s, tot_d);
-    scan_exclusive_i64_ws(keepC, keepC, nC + 1, ws, s, tot_d + 1);
-    int64_t tot[2] = {0, 0};
-    cudaError_t e = readback(tot, tot_d, 16, s);
-    if (e != cudaSuccess) return cuda_to_info(e);
-    const int64_t nR = tot[0] + tot[1];
-    if (nR >= INT32_MAX) return OUT_OF_MEMORY;
+    scan_exclusive_lb(keepT, keepT, nT + 1, lbT, s, tot_d, nullptr, err);
+    scan_exclusive_lb(keepC, keepC, nC + 1, lbC, s, tot_d + 1, nullptr, err);
+    // the result is written before its size comes back, into arrays that
+    // hold every entry of T and C; they are trimmed afterwards if the result
+    // is much smaller
+    const int64_t cap = nT + nC;
+    if (cap >= INT32_MAX) return OUT_OF_MEMORY;
     DevCSR R;
-    R.nrows = m; R.ncols = T.ncols; R.nnz = nR; R.type = T.type; R.iso = false;
+    R.nrows = m; R.ncols = T.ncols; R.type = T.type; R.iso = false;
     R.p = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
-    R.j = (int32_t *)dalloc((size_t)(nR ? nR : 1) * 4, s);
-    R.x = dalloc((size_t)(nR ? nR : 1) * sizeof(Z), s);
+    R.j = (int32_t *)dalloc((size_t)(cap ? cap : 1) * 4, s);
+    R.x = dalloc((size_t)(cap ? cap : 1) * sizeof(Z), s);
     if (!R.p || !R.j || !R.x) { dev_free(R, s); return OUT_OF_MEMORY; }
     k_am_rowptr<<<grid_n(m + 1), 256, 0, s>>>(m, C.p, T.p, keepC, keepT, R.p);
     if (nT > 0)
@@ -215,8 +222,25 @@ static int accum_mask_t(DevCSR &C, const DevCSR &T, const DevCSR *M, bool comp,
     if (nC > 0)
         k_am_write<Z><<<grid_n(nC), 256, 0, s>>>(m, C.p, C.j, (const Z *)C.x, C.iso, nC,
             keepC, T.p, T.j, keepT, R.p, R.j, (Z *)R.x);
-    e = cudaGetLastError();
+    int64_t tot[3] = {0, 0, 0};
+    cudaError_t e = readback(tot, tot_d, 24, s);
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) { dev_free(R, s); return cuda_to_info(e); }
+    if ((int)tot[2] != 0) { dev_free(R, s); return PANIC; }
+    const int64_t nR = tot[0] + tot[1];
+    R.nnz = nR;
+    if (cap > 2 * nR + 4096) {
+        int32_t *j2 = (int32_t *)dalloc((size_t)(nR ? nR : 1) * 4, s);
+        void *x2 = dalloc((size_t)(nR ? nR : 1) * sizeof(Z), s);
+        if (j2 && x2) {
+            cudaMemcpyAsync(j2, R.j, (size_t)nR * 4, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(x2, R.x, (size_t)nR * sizeof(Z), cudaMemcpyDeviceToDevice, s);
+            dfree(R.j, s); dfree(R.x, s);
+            R.j = j2; R.x = x2;
+        } else {
+            dfree(j2, s); dfree(x2, s);
+        }
+    }
     dev_free(C, s);
     C = R;
     return SUCCESS;

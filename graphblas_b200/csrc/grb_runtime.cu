@@ -7,6 +7,7 @@
 #include <cstring>
 #include <cstdio>
 #include "grb_runtime.h"
+#include "grb_lookback.cuh"
 
 namespace grb {
 
@@ -80,6 +81,7 @@ cudaStream_t stream_acquire()
     cudaStream_t s = nullptr;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
         return nullptr;
+    stream_scratch_enable(s);      // the pool's streams live as long as the library
     return s;
 }
 
@@ -91,6 +93,68 @@ void stream_release(cudaStream_t s)
 }
 
 void set_alloc_fail_countdown(int64_t n) { g_fail_countdown.store(n); }
+
+// per-stream scratch buffers
+struct StreamScratch { cudaStream_t s; void *p; size_t bytes; };
+static std::mutex g_scratch_mu;
+static std::vector<StreamScratch> g_scratch;
+
+void stream_scratch_enable(cudaStream_t s)
+{
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    for (auto &x : g_scratch)
+        if (x.s == s) return;
+    g_scratch.push_back({s, nullptr, 0});
+}
+
+bool stream_scratch_enabled(cudaStream_t s)
+{
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    for (auto &x : g_scratch)
+        if (x.s == s) return true;
+    return false;
+}
+
+void *stream_scratch(cudaStream_t s, size_t min_bytes, size_t *bytes)
+{
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    StreamScratch *e = nullptr;
+    for (auto &x : g_scratch)
+        if (x.s == s) { e = &x; break; }
+    if (!e) { if (bytes) *bytes = 0; return nullptr; }
+    if (e->bytes < min_bytes || !e->p) {
+        dfree(e->p, s);
+        e->p = nullptr;
+        e->bytes = 0;
+        size_t want = min_bytes < 4096 ? 4096 : min_bytes;
+        void *p = dalloc(want, s);
+        if (!p) { if (bytes) *bytes = 0; return nullptr; }
+        e->p = p;
+        e->bytes = want;
+    }
+    if (bytes) *bytes = e->bytes;
+    return e->p;
+}
+
+size_t stream_scratch_size(cudaStream_t s)
+{
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    for (auto &x : g_scratch)
+        if (x.s == s) return x.p ? x.bytes : 0;
+    return 0;
+}
+
+void stream_scratch_release(cudaStream_t s)
+{
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    for (size_t k = 0; k < g_scratch.size(); k++) {
+        if (g_scratch[k].s != s) continue;
+        dfree(g_scratch[k].p, s);
+        g_scratch[k] = g_scratch.back();
+        g_scratch.pop_back();
+        return;
+    }
+}
 
 static thread_local cudaStream_t t_stream = nullptr;
 void set_thread_stream(cudaStream_t s) { t_stream = s; }
@@ -689,123 +753,28 @@ void scan_exclusive_i64_ws(const int64_t *in, int64_t *out, int64_t n, int64_t *
 }
 
 // ---------------------------------------------------------------------------
-// single-pass scan (decoupled look-back): one launch for any length
-//
-// Tiles of 2048 values take their index from a ticket, so a tile's
-// predecessors are always running or done.  A tile scans its values, posts
-// its sum (flag 1) - or, for tile 0, its inclusive prefix (flag 2) - in a
-// 64-bit word (flag << 62 | value), walks back over its predecessors' words
-// until one holds an inclusive prefix, and posts its own inclusive prefix.
-// Waits are bounded: a tile that polls CT-style past the limit sets *err and
-// takes the word as zero (the caller fails the call).  The last tile to
-// finish (a completion counter) clears the words and both counters, so the
-// workspace is ready for the next scan without a memset; it must be zero
-// before its first use.
+// single-pass scans: the look-back kernel of grb_lookback.cuh
 // ---------------------------------------------------------------------------
 
-static constexpr int LB_THREADS = 256;
-static constexpr int LB_ROWS = 8;
-static constexpr int LB_TILE = LB_THREADS * LB_ROWS;
-static constexpr unsigned long long LB_AGG = 1ull << 62, LB_INC = 2ull << 62;
-static constexpr unsigned long long LB_VAL = (1ull << 62) - 1;
-static constexpr int LB_SPIN_LIMIT = 1 << 22;
+size_t scan_lb_ws_elems(int64_t n) { return lb_ws_elems(n); }
 
-size_t scan_lb_ws_elems(int64_t n)
-{
-    return (size_t)((n + LB_TILE - 1) / LB_TILE) + 2;
-}
+// value i of the scan: an int64 array
+struct LbLoadI64 {
+    const int64_t *in;
+    __device__ int64_t operator()(int64_t i) const { return in[i]; }
+};
 
-template <typename T>
-__global__ void __launch_bounds__(LB_THREADS)
-k_scan_lookback(const T *in, int64_t *out, int64_t n, unsigned long long *__restrict__ ws,
-                int64_t *__restrict__ total, int32_t *__restrict__ out32,
-                int *__restrict__ err)
-{
-    __shared__ int s_tile, s_last;
-    __shared__ long long s_ex;
-    __shared__ int64_t warp_sums[LB_THREADS / 32];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    unsigned long long *status = ws + 2;
-    if (tid == 0) s_tile = (int)atomicAdd(&ws[0], 1ull);
-    __syncthreads();
-    const int64_t tile = s_tile;
-    const int64_t ntiles = (n + LB_TILE - 1) / LB_TILE;
-    // a warp owns 256 consecutive values as 8 rows of 32 (coalesced)
-    const int64_t base = tile * LB_TILE + (int64_t)warp * (32 * LB_ROWS) + lane;
-    int64_t v[LB_ROWS];
-    #pragma unroll
-    for (int r = 0; r < LB_ROWS; r++) {
-        const int64_t idx = base + r * 32;
-        v[r] = idx < n ? (int64_t)in[idx] : 0;
+// value i of the scan: cnt[i] where keep[i] (every i when keep is null), 0
+// elsewhere and at i = n
+struct LbLoadCounts {
+    const int32_t *cnt;
+    const int8_t *keep;
+    int64_t n;
+    __device__ int64_t operator()(int64_t i) const
+    {
+        return (i < n && (!keep || keep[i])) ? (int64_t)cnt[i] : 0;
     }
-    int64_t run = 0;
-    #pragma unroll
-    for (int r = 0; r < LB_ROWS; r++) {
-        int64_t x = v[r];
-        for (int o = 1; o < 32; o <<= 1) {
-            const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        v[r] = run + x - v[r];
-        run += __shfl_sync(0xffffffffu, x, 31);
-    }
-    if (lane == 0) warp_sums[warp] = run;
-    __syncthreads();
-    if (tid == 0) {
-        int64_t agg = 0;
-        for (int w = 0; w < LB_THREADS / 32; w++) {
-            const int64_t t = warp_sums[w];
-            warp_sums[w] = agg;
-            agg += t;
-        }
-        if (tile == 0) {
-            atomicExch(&status[0], LB_INC | ((unsigned long long)agg & LB_VAL));
-            s_ex = 0;
-        } else {
-            atomicExch(&status[tile], LB_AGG | ((unsigned long long)agg & LB_VAL));
-            long long ex = 0;
-            int64_t p = tile - 1;
-            int spins = 0;
-            while (p >= 0) {
-                const unsigned long long w =
-                    *reinterpret_cast<volatile unsigned long long *>(&status[p]);
-                const unsigned long long f = w & ~LB_VAL;
-                if (f == 0) {
-                    if (++spins > LB_SPIN_LIMIT) { if (err) atomicExch(err, 1); break; }
-                    __nanosleep(32);
-                    continue;
-                }
-                ex += (long long)(w & LB_VAL);
-                if (f == LB_INC) break;
-                p--;
-            }
-            atomicExch(&status[tile], LB_INC | ((unsigned long long)(ex + agg) & LB_VAL));
-            s_ex = ex;
-        }
-        if (total && tile == ntiles - 1) *total = s_ex + agg;
-    }
-    __syncthreads();
-    const int64_t wbase = s_ex + warp_sums[warp];
-    #pragma unroll
-    for (int r = 0; r < LB_ROWS; r++) {
-        const int64_t idx = base + r * 32;
-        if (idx < n) {
-            const int64_t o = wbase + v[r];
-            out[idx] = o;
-            if (out32) out32[idx] = (int32_t)o;
-        }
-    }
-    // the last tile to finish its look-back clears the workspace
-    if (tid == 0) {
-        __threadfence();
-        s_last = atomicAdd(&ws[1], 1ull) == (unsigned long long)(ntiles - 1);
-    }
-    __syncthreads();
-    if (s_last) {
-        for (int64_t t = tid; t < ntiles; t += LB_THREADS) status[t] = 0;
-        if (tid == 0) { ws[0] = 0; ws[1] = 0; }
-    }
-}
+};
 
 void scan_exclusive_lb(const int64_t *in, int64_t *out, int64_t n, unsigned long long *ws,
                        cudaStream_t s, int64_t *total, int32_t *out32, int *err)
@@ -816,8 +785,17 @@ void scan_exclusive_lb(const int64_t *in, int64_t *out, int64_t n, unsigned long
         return;
     }
     const int64_t ntiles = (n + LB_TILE - 1) / LB_TILE;
-    k_scan_lookback<int64_t><<<(unsigned)ntiles, LB_THREADS, 0, s>>>(in, out, n, ws, total,
-                                                                    out32, err);
+    k_scan_lookback<LbLoadI64><<<(unsigned)ntiles, LB_THREADS, 0, s>>>(LbLoadI64{in}, out, n,
+                                                                      ws, total, out32, err);
+}
+
+void scan_exclusive_lb_counts(const int32_t *cnt, const int8_t *keep, int64_t n,
+                              int64_t *out, unsigned long long *ws, cudaStream_t s,
+                              int64_t *total, int32_t *out32, int *err)
+{
+    const int64_t ntiles = (n + 1 + LB_TILE - 1) / LB_TILE;
+    k_scan_lookback<LbLoadCounts><<<(unsigned)ntiles, LB_THREADS, 0, s>>>(
+        LbLoadCounts{cnt, keep, n}, out, n + 1, ws, total, out32, err);
 }
 
 int scan_exclusive_i32_to_i64(const int32_t *in, int64_t *out, int64_t n,

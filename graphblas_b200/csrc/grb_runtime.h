@@ -54,6 +54,19 @@ bool prof_read(const char *name, double *ms, int64_t *count);
 void *dalloc(size_t bytes, cudaStream_t s);
 void dfree(void *p, cudaStream_t s);
 
+// A scratch buffer owned by a stream, kept between calls (work on the stream
+// is ordered, so the stream's calls can share it without a synchronisation),
+// for streams the library owns: the pool's, and those a component enables
+// (and releases before destroying the stream).  stream_scratch grows it to
+// at least min_bytes (the old buffer is released in stream order) and gives
+// its size in *bytes; nullptr if the allocation fails or the stream has no
+// scratch (a caller's stream: the caller then allocates for the call).
+void stream_scratch_enable(cudaStream_t s);
+bool stream_scratch_enabled(cudaStream_t s);
+void *stream_scratch(cudaStream_t s, size_t min_bytes, size_t *bytes);
+size_t stream_scratch_size(cudaStream_t s);
+void stream_scratch_release(cudaStream_t s);
+
 // copy `bytes` (at most a few KB) from the device after the stream's work,
 // synchronising the stream; returns its error
 cudaError_t readback(void *dst, const void *src, size_t bytes, cudaStream_t s);
@@ -168,6 +181,13 @@ size_t scan_lb_ws_elems(int64_t n);
 void scan_exclusive_lb(const int64_t *in, int64_t *out, int64_t n, unsigned long long *ws,
                        cudaStream_t s, int64_t *total = nullptr, int32_t *out32 = nullptr,
                        int *err = nullptr);
+// The same over n + 1 values taken from int32 counts: value i is cnt[i]
+// where keep[i] is non-zero (every i when keep is null), else 0, and value n
+// is 0 (row counts to row offsets, rows outside every bin counting 0).
+// Always the look-back kernel.
+void scan_exclusive_lb_counts(const int32_t *cnt, const int8_t *keep, int64_t n,
+                              int64_t *out, unsigned long long *ws, cudaStream_t s,
+                              int64_t *total, int32_t *out32, int *err);
 
 // ---- operations (device matrices) ----
 

@@ -40,10 +40,13 @@
 // mark the dense row's flags.
 
 #include <functional>
+#include <mutex>
+#include <vector>
 #include <cstdio>
 #include <cstring>
 #include "grb_saxpy3.h"
 #include "grb_semirings.h"
+#include "grb_lookback.cuh"
 
 namespace grb {
 
@@ -52,6 +55,28 @@ static constexpr int MAX_SMEM_BINS = 6;
 // slot states
 static constexpr uint8_t S_EMPTY = 0, S_ALLOWED = 1, S_SET = 2, S_FORBID = 3;
 
+// The rows of one shared-memory bin, read on the device: the bins' row lists
+// lie end to end in `list` in bin order, count[b] rows in bin b (count[0],
+// the rows without products, is 0).  When `need` is set the kernel first
+// checks that the slots it writes fit: *need (the slot total) <= avail, else
+// it does nothing and the host, which reads the total, runs it again with
+// more slots.
+struct BinRows {
+    const int32_t *list;
+    const int *count;
+    int b;
+    const int64_t *need;
+    int64_t avail;
+    __device__ int get(const int32_t *&rows) const
+    {
+        if (need && *need > avail) { rows = list; return 0; }
+        int start = 0;
+        for (int q = 0; q < b; q++) start += count[q];
+        rows = list + start;
+        return count[b];
+    }
+};
+
 // ---------------------------------------------------------------------------
 // phase 1: flops and capacity per row
 // ---------------------------------------------------------------------------
@@ -59,8 +84,11 @@ static constexpr uint8_t S_EMPTY = 0, S_ALLOWED = 1, S_SET = 2, S_FORBID = 3;
 // Flat over A's entries, so a row of any length is spread over the whole
 // grid (a one-row A, as in vxm, would otherwise run on one warp): each lane
 // takes one entry A(i,k) and adds nnz(B(k,:)); a segmented scan over the
-// warp's lanes (rows are contiguous in lane order) leaves one atomic per row
-// segment.  flops[] must be zero on entry.
+// warp's lanes (rows are contiguous in lane order) gives each row segment its
+// sum, and the segment that runs on into the next 32 entries is carried
+// instead of added, so a warp adds once per row it touches in its span (a
+// single long row takes one atomic per span, not one per 32 entries).
+// flops[] must be zero on entry.
 __global__ void __launch_bounds__(256)
 k_flops_flat(const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
              const int32_t *__restrict__ Bp, int64_t nrows, int64_t nnz, int span,
@@ -75,6 +103,9 @@ k_flops_flat(const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
          s0 < nnz; s0 += nw * span) {
         int32_t r0 = warp_last_le<int32_t, int32_t>(Ap, (int32_t)nrows, (int32_t)s0, lane);
         const int64_t s1 = s0 + span < nnz ? s0 + span : nnz;
+        // the open segment of the previous step: its row and its sum so far
+        int32_t crow = -1;
+        unsigned long long carry = 0;
         for (int64_t base = s0; base < s1; base += 32) {
             const int64_t e = base + lane;
             int32_t r = -1;
@@ -91,12 +122,21 @@ k_flops_flat(const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
                 const int32_t ry = __shfl_up_sync(0xffffffffu, r, o);
                 if (lane >= o && ry == r) f += y;
             }
+            // rows only grow along the span: only this step's first segment
+            // can continue the open one
+            if (r >= 0 && r == crow) f += carry;
+            const int32_t first = __shfl_sync(0xffffffffu, r, 0);
+            if (crow >= 0 && first != crow && lane == 0) atomicAdd(&flops[crow], carry);
             const int32_t rn = __shfl_down_sync(0xffffffffu, r, 1);
-            if (r >= 0 && (lane == 31 || rn != r)) atomicAdd(&flops[r], f);
+            const bool end = r >= 0 && (lane == 31 || rn != r);
+            if (end && lane != 31) atomicAdd(&flops[r], f);
+            // lane 31's segment stays open (flushed when its row ends)
+            crow = __shfl_sync(0xffffffffu, r, 31);
+            carry = __shfl_sync(0xffffffffu, f, 31);
             // the next step starts in the row of this step's last entry
-            const int32_t rl = __shfl_sync(0xffffffffu, r, 31);
-            r0 = rl >= 0 ? rl : r0;
+            r0 = crow >= 0 ? crow : r0;
         }
+        if (crow >= 0 && lane == 0) atomicAdd(&flops[crow], carry);
     }
 }
 
@@ -218,7 +258,7 @@ template <typename Z> __host__ __device__ inline size_t group_bytes(int cap)
 // 256-thread block when BLOCK) owns one row and one hash table of cap slots.
 template <class SR, bool BLOCK>
 __global__ void __launch_bounds__(BLOCK ? 256 : 128, BLOCK ? 4 : 8)
-k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin, int tpr_log2, int cap,
+k_saxpy_hash(BinRows br, int tpr_log2, int cap,
              const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
              const void *__restrict__ Ax, bool a_iso,
              const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
@@ -245,6 +285,8 @@ k_saxpy_hash(const int32_t *__restrict__ rows, int nrows_bin, int tpr_log2, int 
     Z *vals = (Z *)(base + (size_t)cap * 4);
     uint8_t *state = (uint8_t *)(base + (size_t)cap * (4 + sizeof(Z)));
     const uint32_t hmask = (uint32_t)cap - 1;
+    const int32_t *rows;
+    const int nrows_bin = br.get(rows);
 
     for (int64_t rb = (int64_t)blockIdx.x * G + g; rb < nrows_bin;
          rb += (int64_t)gridDim.x * G) {
@@ -416,7 +458,7 @@ __device__ __forceinline__ void warp_sort_regs(KT *key, int n, int lane)
 // the values stay where the expansion wrote them.
 template <class SR, typename KT>
 __global__ void __launch_bounds__(ESC_WARPS * 32, 6)
-k_saxpy_esc(const int32_t *__restrict__ rows, int nrows_bin, int cap, int posb,
+k_saxpy_esc(BinRows br, int cap, int posb,
             const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
             const void *__restrict__ Ax, bool a_iso,
             const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
@@ -434,6 +476,8 @@ k_saxpy_esc(const int32_t *__restrict__ rows, int nrows_bin, int cap, int posb,
     Z *val = (Z *)((unsigned char *)key + (size_t)cap * sizeof(KT));
     const unsigned below = (1u << lane) - 1u;
     const KT posmask = ((KT)1 << posb) - 1;
+    const int32_t *rows;
+    const int nrows_bin = br.get(rows);
 
     for (int64_t rb = (int64_t)blockIdx.x * ESC_WARPS + w; rb < nrows_bin;
          rb += (int64_t)gridDim.x * ESC_WARPS) {
@@ -842,19 +886,52 @@ __device__ __forceinline__ int64_t upper_bound64(const int64_t *a, int64_t lo, i
     return lo;
 }
 
-__global__ void k_heavy_blen(const int32_t *__restrict__ rows, int nr,
-                             const int64_t *__restrict__ hoff,
-                             const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
-                             const int32_t *__restrict__ Bp, int64_t *__restrict__ wlen)
+
+// heavy rows' offsets into the flat entry index (up to 1024 rows, one block)
+__global__ void __launch_bounds__(1024)
+k_heavy_offsets(const int32_t *__restrict__ rows, int nr, const int32_t *__restrict__ Ap,
+                int64_t *__restrict__ hoff)
 {
-    const int64_t ne = hoff[nr];
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < ne;
-         e += (int64_t)gridDim.x * blockDim.x) {
+    __shared__ int64_t s_w[32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    int64_t x = 0;
+    if (t < nr) { const int32_t i = rows[t]; x = Ap[i + 1] - Ap[i]; }
+    const int64_t own = x;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int64_t v = s_w[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        s_w[lane] = v;
+    }
+    __syncthreads();
+    const int64_t ex = (w > 0 ? s_w[w - 1] : 0) + x - own;
+    if (t < nr) hoff[t] = ex;
+    if (t == nr - 1) hoff[nr] = ex + own;
+}
+
+// value e of the flat product index: nnz(B(k,:)) for the heavy rows' entry e
+// (A(i,k), rows in order), 0 past the chunk's entries
+struct LbLoadBlen {
+    const int32_t *rows;
+    int nr;
+    const int64_t *hoff;
+    const int32_t *Ap, *Aj, *Bp;
+    __device__ int64_t operator()(int64_t e) const
+    {
+        if (e >= hoff[nr]) return 0;
         const int rb = nr == 1 ? 0 : (int)(upper_bound64(hoff, 0, nr + 1, e) - 1);
         const int32_t k = Aj[Ap[rows[rb]] + (e - hoff[rb])];
-        wlen[e] = Bp[k + 1] - Bp[k];
+        return Bp[k + 1] - Bp[k];
     }
-}
+};
 
 // Every product of the chunk's heavy rows, flat over the product index: a
 // warp takes 32 consecutive products (one binary search for the first one's
@@ -929,80 +1006,106 @@ k_dense_atomic_flat(const int32_t *__restrict__ rows, int nr,
     }
 }
 
-// grid-wide ordered compaction of dense heavy rows: blocks own 4096-column
-// chunks of a row (grid.y = row); one pass counts, a scan places the chunks,
-// a second pass writes (so a single long row uses the whole GPU)
+// grid-wide ordered compaction of dense heavy rows, so a single long row
+// uses the whole GPU
 static constexpr int DG_THREADS = 256, DG_ITEMS = 16, DG_CHUNK = DG_THREADS * DG_ITEMS;
 
-__global__ void __launch_bounds__(DG_THREADS)
-k_dense_count(int nrows_bin, int64_t ncols, int cblocks, const uint8_t *__restrict__ flag_all,
-              int64_t *__restrict__ cnt)
-{
-    __shared__ int s_w[DG_THREADS / 32];
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0)
-        cnt[(int64_t)nrows_bin * cblocks] = 0;
-    for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
-        const uint8_t *flag = flag_all + rb * ncols;
-        const int64_t c0 = (int64_t)blockIdx.x * DG_CHUNK;
-        int c = 0;
-        for (int it = 0; it < DG_ITEMS; it++) {
-            const int64_t j = c0 + (int64_t)it * DG_THREADS + threadIdx.x;
-            c += (j < ncols && flag[j] == 3);
-        }
-        for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
-        if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = c;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int t = 0;
-            for (int q = 0; q < DG_THREADS / 32; q++) t += s_w[q];
-            cnt[rb * cblocks + blockIdx.x] = t;
-        }
-        __syncthreads();
-    }
-}
-
+// The same compaction in one launch: tiles of DG_CHUNK columns of one heavy
+// row (tile = row * cblocks + chunk, from a ticket), 16 columns per thread;
+// a tile counts its entries, takes its offset in the row from its
+// predecessors by decoupled look-back (a row's first tile starts at 0), and
+// writes them in column order: the tile's columns are staged in shared
+// memory in order, then written out (and their values gathered) by
+// consecutive threads.  ws: ntiles + 2 zero words, left zero.
 template <class SR>
 __global__ void __launch_bounds__(DG_THREADS)
-k_dense_write(const int32_t *__restrict__ rows, int nrows_bin, int64_t ncols, int cblocks,
-              const uint8_t *__restrict__ flag_all,
-              const typename SR::z_t *__restrict__ val_all,
-              const int64_t *__restrict__ off /* scanned counts */,
-              const int64_t *__restrict__ slot_off, int32_t *__restrict__ Tj,
-              typename SR::z_t *__restrict__ Tx, int32_t *__restrict__ row_cnt)
+k_dense_compact(const int32_t *__restrict__ rows, int cblocks, int64_t ncols,
+                const uint8_t *__restrict__ flag_all,
+                const typename SR::z_t *__restrict__ val_all,
+                const int64_t *__restrict__ slot_off, int32_t *__restrict__ Tj,
+                typename SR::z_t *__restrict__ Tx, int32_t *__restrict__ row_cnt,
+                int64_t ntiles, unsigned long long *__restrict__ ws, int *__restrict__ err)
 {
+    __shared__ int s_tile, s_last, s_agg;
+    __shared__ long long s_ex;
     __shared__ int s_w[DG_THREADS / 32];
-    __shared__ int s_base;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
-        const int32_t i = rows[rb];
-        const uint8_t *flag = flag_all + rb * ncols;
-        const typename SR::z_t *val = val_all + rb * ncols;
-        const int64_t row0 = off[rb * cblocks];
-        int64_t pos = slot_off[i] + (off[rb * cblocks + blockIdx.x] - row0);
-        const int64_t c0 = (int64_t)blockIdx.x * DG_CHUNK;
-        for (int it = 0; it < DG_ITEMS; it++) {
-            const int64_t j = c0 + (int64_t)it * DG_THREADS + threadIdx.x;
-            const bool on = j < ncols && flag[j] == 3;
-            const unsigned m = __ballot_sync(0xffffffffu, on);
-            if (lane == 0) s_w[w] = __popc(m);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                int acc = 0;
-                for (int q = 0; q < DG_THREADS / 32; q++) { int c = s_w[q]; s_w[q] = acc; acc += c; }
-                s_base = acc;
-            }
-            __syncthreads();
-            if (on) {
-                const int64_t q = pos + s_w[w] + __popc(m & ((1u << lane) - 1));
-                Tj[q] = (int32_t)j;
-                Tx[q] = val[j];
-            }
-            pos += s_base;
-            __syncthreads();
+    __shared__ int32_t s_j[DG_CHUNK];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    unsigned long long *status = ws + 2;
+    if (tid == 0) s_tile = (int)atomicAdd(&ws[0], 1ull);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    const int64_t rb = tile / cblocks, cb = tile % cblocks;
+    const int32_t i = rows[rb];
+    const uint8_t *flag = flag_all + rb * ncols;
+    const int64_t c0 = cb * DG_CHUNK + (int64_t)tid * DG_ITEMS;
+    unsigned bits = 0;
+    if (c0 + DG_ITEMS <= ncols && (((uintptr_t)(flag + c0)) & 15) == 0) {
+        const uint4 v = *reinterpret_cast<const uint4 *>(flag + c0);
+        const uint32_t word[4] = {v.x, v.y, v.z, v.w};
+        #pragma unroll
+        for (int q = 0; q < 16; q++)
+            if (((word[q >> 2] >> ((q & 3) * 8)) & 0xff) == 3) bits |= 1u << q;
+    } else {
+        for (int q = 0; q < DG_ITEMS; q++)
+            if (c0 + q < ncols && flag[c0 + q] == 3) bits |= 1u << q;
+    }
+    const int cnt = __popc(bits);
+    int x = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int v = lane < DG_THREADS / 32 ? s_w[lane] : 0;
+        const int ownv = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0)
-            row_cnt[i] = (int32_t)(off[(rb + 1) * cblocks] - row0);
-        __syncthreads();
+        const long long agg = __shfl_sync(0xffffffffu, v, 31);
+        if (lane < DG_THREADS / 32) s_w[lane] = v - ownv;
+        long long ex = 0;
+        if (cb == 0) {
+            if (lane == 0) atomicExch(&status[tile], LB_INC | ((unsigned long long)agg & LB_VAL));
+        } else {
+            if (lane == 0) atomicExch(&status[tile], LB_AGG | ((unsigned long long)agg & LB_VAL));
+            ex = lb_lookback(status, tile, lane, err);
+            if (lane == 0)
+                atomicExch(&status[tile], LB_INC | ((unsigned long long)(ex + agg) & LB_VAL));
+        }
+        if (lane == 0) {
+            s_ex = ex;
+            s_agg = (int)agg;
+            if (cb == cblocks - 1) row_cnt[i] = (int32_t)(ex + agg);
+        }
+    }
+    __syncthreads();
+    int loc = s_w[w] + (x - cnt);
+    while (bits) {
+        const int q = __ffs(bits) - 1;
+        bits &= bits - 1;
+        s_j[loc++] = (int32_t)(c0 + q);
+    }
+    __syncthreads();
+    const int64_t base = slot_off[i] + s_ex;
+    const typename SR::z_t *val = val_all + rb * ncols;
+    for (int k = tid; k < s_agg; k += DG_THREADS) {
+        const int32_t j = s_j[k];
+        Tj[base + k] = j;
+        Tx[base + k] = val[j];
+    }
+    // the last tile to finish clears the workspace
+    if (tid == 0) {
+        __threadfence();
+        s_last = atomicAdd(&ws[1], 1ull) == (unsigned long long)(ntiles - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        for (int64_t t = tid; t < ntiles; t += DG_THREADS) status[t] = 0;
+        if (tid == 0) { ws[0] = 0; ws[1] = 0; }
     }
 }
 
@@ -1042,14 +1145,6 @@ k_pack(int64_t nrows, int span, const int64_t *__restrict__ slot_off,
     }
 }
 
-// out[0..n) the counts of the binned rows (0 for empty ones), out[n] = 0
-__global__ void k_cnt_to_i64(const int32_t *__restrict__ cnt, const int8_t *__restrict__ row_bin,
-                             int64_t n, int64_t *__restrict__ out)
-{
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (; t <= n; t += stride) out[t] = (t < n && row_bin[t]) ? (int64_t)cnt[t] : 0;
-}
 
 
 // ---------------------------------------------------------------------------
@@ -1106,6 +1201,16 @@ bool saxpy_config_valid(const SaxpyConfig &cfg, size_t zsize)
     return cfg.blocks_per_sm >= 1 && cfg.blocks_per_sm <= 64;
 }
 
+// bins[] (ints) of a plan: 0..15 rows per bin, 32..47 fill cursors, 48-49
+// the A entries of heavy rows (u64), 50-51 the slot total (i64), 52-53 the
+// output count (i64), 54 the row-offset scan's error word, 55 the heavy-row
+// scans' error word, 56 the slot-offset scan's error word.  The first
+// BINS_READ ints come back to the host.
+static constexpr int BINS_WORDS = 64;
+static constexpr int BINS_READ = 57;
+static constexpr int BIN_HEAVY_ALEN = 48, BIN_TOTAL_CAP = 50, BIN_NNZ = 52,
+                     BIN_ROW_ERR = 54, BIN_HEAVY_ERR = 55, BIN_SLOT_ERR = 56;
+
 struct SaxpyPlan {
     SemiringCode sr;
     SaxpyConfig cfg;
@@ -1113,7 +1218,9 @@ struct SaxpyPlan {
     bool order_free = false;
     int64_t m = 0, ncols = 0;
     bool has_mask = false, mask_comp = false;
-    int64_t total_cap = 0;
+    int64_t total_cap = 0;      // slots the rows need
+    int64_t slot_avail = 0;     // slots Tj / Tx hold
+    int64_t nnz = 0;            // output entries, once read back
     int h_bins[MAX_SMEM_BINS + 2] = {0};
     int h_start[MAX_SMEM_BINS + 2] = {0};
     // device buffers
@@ -1129,13 +1236,14 @@ struct SaxpyPlan {
     int64_t *flag = nullptr;                       // order-dependent rows: row marks
     uint8_t *flag8 = nullptr;                      // order-free rows: 0/1/2/3 states
     void *val = nullptr;
-    int64_t *dg_cnt = nullptr, *dg_ws = nullptr;   // dense-row compaction
     int64_t heavy_alen = 0;                         // A entries in the heavy rows
     int64_t *hlen = nullptr, *hoff = nullptr;       // flat product index (per chunk)
-    int64_t *wlen = nullptr, *wprefix = nullptr, *hw_ws = nullptr;
-    int64_t *nnz_d = nullptr;                       // one-shot calls: nnz(C)
-    // the three allocations the buffers above are carved from: symbolic
-    // arrays, slots (Tj, Tx), heavy-row accumulators
+    int64_t *wprefix = nullptr, *hw_ws = nullptr;
+    // look-back workspaces of the product-index scan and the compaction
+    unsigned long long *lb_w = nullptr, *lb_c = nullptr;
+    // the allocations the buffers above are carved from: symbolic arrays,
+    // slots (Tj, Tx; null when the slots are the stream's scratch buffer),
+    // heavy-row accumulators
     void *block = nullptr, *tblock = nullptr, *hblock = nullptr;
 };
 
@@ -1166,9 +1274,12 @@ static inline int nblocks(int64_t n, int threads, int per_sm = 8)
     return b < 1 ? 1 : (int)b;
 }
 
+// Symbolic phase, with no host round trip: flop counts, bins and slot
+// capacities, the slot offsets (their total lands in bins[50]) and the
+// bins' row lists.
 template <class SR>
-static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A,
-                  const DevCSR &B, cudaStream_t s)
+static int plan_symbolic(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A,
+                         const DevCSR &B, cudaStream_t s)
 {
     using Z = typename SR::z_t;
     const int64_t m = A.nrows, ncols = B.ncols;
@@ -1176,29 +1287,27 @@ static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A
     P->order_free = SR::order_free;
     P->m = m; P->ncols = ncols;
     P->has_mask = M != nullptr; P->mask_comp = mask_comp;
-    // the symbolic arrays in one allocation: the bin counters (256 bytes),
-    // the scans' workspaces, the output count and its scan's error word, the
-    // flop counts and the slot offsets first and adjacent, so that one memset
-    // clears them all
+    // the symbolic arrays in one allocation: the bin counters, the scans'
+    // workspaces, the flop counts, the slot offsets and the row counts first
+    // and adjacent, so that one memset clears them all
     Carve cv(s);
     auto layout = [&]() {
-        P->bins = cv.take<int>(64);
+        P->bins = cv.take<int>(BINS_WORDS);
         P->lb_slot = cv.take<unsigned long long>(scan_lb_ws_elems(m + 1));
         P->lb_row = cv.take<unsigned long long>(scan_lb_ws_elems(m + 1));
-        P->nnz_d = cv.take<int64_t>(2);
         P->flops = cv.take<int64_t>(m + 1);
         P->slot_off = cv.take<int64_t>(m + 1);
+        P->row_cnt = cv.take<int32_t>(m + 1);
         P->Cp64 = cv.take<int64_t>(m + 2);
         P->row_bin = cv.take<int8_t>(m + 1);
         P->bin_rows = cv.take<int32_t>(m + 1);
-        P->row_cnt = cv.take<int32_t>(m + 1);
     };
     layout();
     if (!cv.alloc()) return OUT_OF_MEMORY;
     layout();
     P->block = cv.base;
     const bool mask_bounds = (M != nullptr) && !mask_comp;
-    cudaMemsetAsync(P->bins, 0, (size_t)((char *)(P->slot_off + m + 1) - (char *)P->bins), s);
+    cudaMemsetAsync(P->bins, 0, (size_t)((char *)(P->row_cnt + m + 1) - (char *)P->bins), s);
     if (m > 0 && A.nnz > 0)
         k_flops_flat<<<nblocks(A.nnz, 256, 16), 256, 0, s>>>(A.p, A.j, B.p, m, A.nnz,
             flat_span(A.nnz),
@@ -1206,90 +1315,171 @@ static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A
     BinLimits lim;
     lim.nb = P->cfg.nb;
     for (int q = 0; q < P->cfg.nb; q++) lim.limit[q] = P->cfg.bin[q].limit;
-    // bins[]: 0..15 row counts per bin, 32..47 fill cursors, 48-49 the A
-    // entries of heavy rows (u64), 50-51 the total slot count (i64)
     if (m > 0)
         k_bin_rows<<<nblocks(m, 256), 256, 0, s>>>(P->flops, M ? M->p : nullptr,
             M != nullptr, mask_bounds, ncols, m, lim, P->bins, P->row_bin, P->slot_off,
-            A.p, (unsigned long long *)(P->bins + 48));
-    // bins[56]: the slot scan's error word
+            A.p, (unsigned long long *)(P->bins + BIN_HEAVY_ALEN));
     scan_exclusive_lb(P->slot_off, P->slot_off, m + 1, P->lb_slot, s,
-                      (int64_t *)(P->bins + 50), nullptr, P->bins + 56);
-    const int nb = P->cfg.nb;
-    int hb[57];
-    cudaError_t e = readback(hb, P->bins, sizeof(hb), s);
-    if (e != cudaSuccess) return cuda_to_info(e);
-    if (hb[56]) return PANIC;
-    for (int b = 0; b < nb + 2; b++) P->h_bins[b] = hb[b];
-    int64_t total_cap = 0;
-    memcpy(&P->heavy_alen, hb + 48, 8);
-    memcpy(&total_cap, hb + 50, 8);
-    P->total_cap = total_cap;
-    P->h_start[0] = 0;
-    for (int b = 1; b < nb + 2; b++) P->h_start[b] = P->h_start[b - 1] + P->h_bins[b - 1];
+                      (int64_t *)(P->bins + BIN_TOTAL_CAP), nullptr, P->bins + BIN_SLOT_ERR);
+    // the row lists: a bin's list starts after those of the bins before it
+    // (the fill kernel adds up the counts itself)
     if (m > 0)
         k_fill_bins<<<nblocks(m, 256), 256, 0, s>>>(P->row_bin, m, P->bins + 32, P->bins,
-                                                   nb + 2, P->bin_rows);
+                                                   P->cfg.nb + 2, P->bin_rows);
+    return cuda_to_info(cudaGetLastError());
+}
+
+// the bin counts, heavy-row size, slot total and output count, to the host
+static int plan_read(SaxpyPlan *P, cudaStream_t s)
+{
+    int hb[BINS_READ];
+    cudaError_t e = readback(hb, P->bins, sizeof(hb), s);
+    if (e != cudaSuccess) return cuda_to_info(e);
+    if (hb[BIN_SLOT_ERR] || hb[BIN_ROW_ERR] || hb[BIN_HEAVY_ERR]) return PANIC;
+    const int nb = P->cfg.nb;
+    for (int b = 0; b < nb + 2; b++) P->h_bins[b] = hb[b];
+    memcpy(&P->heavy_alen, hb + BIN_HEAVY_ALEN, 8);
+    memcpy(&P->total_cap, hb + BIN_TOTAL_CAP, 8);
+    memcpy(&P->nnz, hb + BIN_NNZ, 8);
+    P->h_start[0] = 0;
+    for (int b = 1; b < nb + 2; b++) P->h_start[b] = P->h_start[b - 1] + P->h_bins[b - 1];
+    return SUCCESS;
+}
+
+// Tj / Tx in a block of `bytes` at `base`: as many slots as fit
+static void plan_place_slots(SaxpyPlan *P, void *base, size_t bytes)
+{
+    const int64_t per = 4 + (int64_t)P->zsize;
+    int64_t slots = ((int64_t)bytes - 512) / per;
+    if (slots < 1) slots = 1;
+    P->Tj = (int32_t *)base;
+    P->Tx = (char *)base + (((size_t)slots * 4 + 255) & ~(size_t)255);
+    P->slot_avail = slots - 1;
+}
+
+static size_t slot_bytes(const SaxpyPlan *P, int64_t slots)
+{
+    return (size_t)(slots + 1) * (4 + P->zsize) + 512;
+}
+
+// the heavy rows' accumulators (sizes from plan_read)
+template <class SR>
+static int plan_alloc_heavy(SaxpyPlan *P, cudaStream_t s)
+{
+    using Z = typename SR::z_t;
+    const int nb = P->cfg.nb;
+    const int64_t ncols = P->ncols;
+    const int nheavy = P->h_bins[nb + 1];
+    if (nheavy == 0 || P->hblock) return SUCCESS;
+    Carve hv(s);
+    std::function<void()> hlayout;
+    if (SR::order_free) {
+        int64_t chunk = nheavy;
+        const int64_t per_row = ncols * (1 + (int64_t)sizeof(Z));
+        const int64_t budget = (int64_t)4 << 30;
+        if (chunk * per_row > budget) chunk = budget / per_row > 0 ? budget / per_row : 1;
+        P->heavy_chunk = chunk;
+        const int64_t cblocks = (ncols + DG_CHUNK - 1) / DG_CHUNK;
+        const int64_t ntiles = chunk * cblocks;
+        hlayout = [&, chunk, ntiles]() {
+            P->flag8 = hv.take<uint8_t>(chunk * ncols + 1);
+            P->val = hv.take<Z>(chunk * ncols + 1);
+            P->hlen = hv.take<int64_t>(chunk + 1);
+            P->hoff = hv.take<int64_t>(chunk + 1);
+            P->wprefix = hv.take<int64_t>(P->heavy_alen + 1);
+            P->hw_ws = hv.take<int64_t>(scan_ws_elems(chunk + 1));
+            P->lb_w = hv.take<unsigned long long>(lb_ws_elems(P->heavy_alen + 1));
+            P->lb_c = hv.take<unsigned long long>(ntiles + 2);   // a word per tile
+        };
+    } else {
+        const int nbk = nheavy < runtime().num_sms * 2 ? nheavy : runtime().num_sms * 2;
+        P->heavy_chunk = nbk;
+        hlayout = [&, nbk]() {
+            P->flag = hv.take<int64_t>((int64_t)nbk * ncols + 1);
+            P->val = hv.take<Z>((int64_t)nbk * ncols + 1);
+        };
+    }
+    hlayout();
+    if (!hv.alloc()) return OUT_OF_MEMORY;
+    hlayout();
+    P->hblock = hv.base;
+    if (P->lb_w) {
+        // the two look-back workspaces, adjacent, zero before their first use
+        const int64_t ntiles = P->heavy_chunk * ((ncols + DG_CHUNK - 1) / DG_CHUNK);
+        cudaMemsetAsync(P->lb_w, 0,
+                        (size_t)((char *)(P->lb_c + ntiles + 2) - (char *)P->lb_w), s);
+    }
+    return SUCCESS;
+}
+
+template <class SR>
+static int plan_t(SaxpyPlan *P, const DevCSR *M, bool mask_comp, const DevCSR &A,
+                  const DevCSR &B, cudaStream_t s)
+{
+    using Z = typename SR::z_t;
+    int info = plan_symbolic<SR>(P, M, mask_comp, A, B, s);
+    if (info == SUCCESS) info = plan_read(P, s);
+    if (info != SUCCESS) return info;
     Carve tv(s);
     auto tlayout = [&]() {
-        P->Tj = tv.take<int32_t>(total_cap + 1);
-        P->Tx = tv.take<Z>(total_cap + 1);
+        P->Tj = tv.take<int32_t>(P->total_cap + 1);
+        P->Tx = tv.take<Z>(P->total_cap + 1);
     };
     tlayout();
     if (!tv.alloc()) return OUT_OF_MEMORY;
     tlayout();
     P->tblock = tv.base;
-    const int nheavy = P->h_bins[nb + 1];
-    if (nheavy > 0) {
-        Carve hv(s);
-        std::function<void()> hlayout;
-        if (SR::order_free) {
-            int64_t chunk = nheavy;
-            const int64_t per_row = ncols * (1 + (int64_t)sizeof(Z));
-            const int64_t budget = (int64_t)4 << 30;
-            if (chunk * per_row > budget) chunk = budget / per_row > 0 ? budget / per_row : 1;
-            P->heavy_chunk = chunk;
-            const int64_t cblocks = (ncols + DG_CHUNK - 1) / DG_CHUNK;
-            const int64_t ncnt = chunk * cblocks + 1;
-            const int64_t hmax = (chunk + 1) > (P->heavy_alen + 1) ? chunk + 1 : P->heavy_alen + 1;
-            hlayout = [&, chunk, ncnt, hmax]() {
-                P->flag8 = hv.take<uint8_t>(chunk * ncols + 1);
-                P->val = hv.take<Z>(chunk * ncols + 1);
-                P->dg_cnt = hv.take<int64_t>(ncnt + 1);
-                P->dg_ws = hv.take<int64_t>(scan_ws_elems(ncnt));
-                P->hlen = hv.take<int64_t>(chunk + 1);
-                P->hoff = hv.take<int64_t>(chunk + 1);
-                P->wlen = hv.take<int64_t>(P->heavy_alen + 1);
-                P->wprefix = hv.take<int64_t>(P->heavy_alen + 1);
-                P->hw_ws = hv.take<int64_t>(scan_ws_elems(hmax));
-            };
-        } else {
-            const int nbk = nheavy < runtime().num_sms * 2 ? nheavy : runtime().num_sms * 2;
-            P->heavy_chunk = nbk;
-            hlayout = [&, nbk]() {
-                P->flag = hv.take<int64_t>((int64_t)nbk * ncols + 1);
-                P->val = hv.take<Z>((int64_t)nbk * ncols + 1);
-            };
-        }
-        hlayout();
-        if (!hv.alloc()) return OUT_OF_MEMORY;
-        hlayout();
-        P->hblock = hv.base;
-    }
+    P->slot_avail = P->total_cap;
+    info = plan_alloc_heavy<SR>(P, s);
+    if (info != SUCCESS) return info;
     return cuda_to_info(cudaGetLastError());
 }
 
+// blocks of a kernel that can be resident on the device at once (cached per
+// kernel and shared-memory size)
+static int resident_blocks(const void *fn, int threads, size_t smem)
+{
+    struct Entry { const void *fn; size_t smem; int blocks; };
+    static std::mutex mu;
+    static std::vector<Entry> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    for (const Entry &e : cache)
+        if (e.fn == fn && e.smem == smem) return e.blocks;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    if (per_sm < 1) per_sm = 1;
+    const int blocks = per_sm * runtime().num_sms;
+    cache.push_back({fn, smem, blocks});
+    return blocks;
+}
+
+// Launch shared-memory bin q.  rows_bound: the bin's row count when the host
+// knows it (exact = true: an empty bin launches nothing), else an upper bound
+// (the grid is then at most one resident wave, and the kernel reads the count
+// and, through `need`, whether the slots fit).
 template <class SR>
 static void launch_bin(const SaxpyPlan *P, int q, const DevCSR &A, const DevCSR &B,
-                       const DevCSR *M, cudaStream_t s)
+                       const DevCSR *M, int64_t rows_bound, bool exact, const int64_t *need,
+                       cudaStream_t s)
 {
     using Z = typename SR::z_t;
     const BinSpec &b = P->cfg.bin[q];
-    const int cnt = P->h_bins[q + 1];
-    if (cnt == 0) return;
-    const int32_t *rows = P->bin_rows + P->h_start[q + 1];
+    if (rows_bound <= 0) return;
+    const BinRows br{P->bin_rows, P->bins, q + 1, need, P->slot_avail};
     const size_t smem = bin_smem(b, sizeof(Z));
-    const int cap_blocks = runtime().num_sms * P->cfg.blocks_per_sm;
+    int64_t cap_blocks = (int64_t)runtime().num_sms * P->cfg.blocks_per_sm;
+    auto clamp = [&](int64_t want, const void *fn, int threads, size_t sm) {
+        int64_t c = cap_blocks;
+        if (!exact) {
+            const int64_t wave = resident_blocks(fn, threads, sm);
+            if (wave < c) c = wave;
+        }
+        if (want > c) want = c;
+        return (int)(want < 1 ? 1 : want);
+    };
     if (b.tpr == 1) {
         static bool attr = false;
         if (!attr) {
@@ -1299,17 +1489,20 @@ static void launch_bin(const SaxpyPlan *P, int q, const DevCSR &A, const DevCSR 
         }
         int posb = 0;
         while ((1 << posb) < b.cap) posb++;
-        int blocks = (cnt + ESC_WARPS - 1) / ESC_WARPS;
-        if (blocks > cap_blocks) blocks = cap_blocks;
+        const int64_t want = (rows_bound + ESC_WARPS - 1) / ESC_WARPS;
         // 32-bit keys when every (column << posb) and the padding fit
         if (((uint64_t)B.ncols << posb) < 0xffffffffull) {
             const size_t sm32 = (size_t)ESC_WARPS * b.cap * (4 + sizeof(Z));
-            k_saxpy_esc<SR, uint32_t><<<blocks, ESC_WARPS * 32, sm32, s>>>(rows, cnt, b.cap,
+            const int blocks = clamp(want, (const void *)k_saxpy_esc<SR, uint32_t>,
+                                     ESC_WARPS * 32, sm32);
+            k_saxpy_esc<SR, uint32_t><<<blocks, ESC_WARPS * 32, sm32, s>>>(br, b.cap,
                 posb, A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
                 M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, P->mask_comp,
                 P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
         } else {
-            k_saxpy_esc<SR, uint64_t><<<blocks, ESC_WARPS * 32, smem, s>>>(rows, cnt, b.cap,
+            const int blocks = clamp(want, (const void *)k_saxpy_esc<SR, uint64_t>,
+                                     ESC_WARPS * 32, smem);
+            k_saxpy_esc<SR, uint64_t><<<blocks, ESC_WARPS * 32, smem, s>>>(br, b.cap,
                 posb, A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
                 M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, P->mask_comp,
                 P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
@@ -1320,8 +1513,8 @@ static void launch_bin(const SaxpyPlan *P, int q, const DevCSR &A, const DevCSR 
             allow_dynamic_smem((const void *)k_saxpy_hash<SR, true>);
             attr = true;
         }
-        int blocks = cnt < cap_blocks ? cnt : cap_blocks;
-        k_saxpy_hash<SR, true><<<blocks, 256, smem, s>>>(rows, cnt, 8, b.cap,
+        const int blocks = clamp(rows_bound, (const void *)k_saxpy_hash<SR, true>, 256, smem);
+        k_saxpy_hash<SR, true><<<blocks, 256, smem, s>>>(br, 8, b.cap,
             A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
             M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, P->mask_comp,
             P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
@@ -1333,13 +1526,98 @@ static void launch_bin(const SaxpyPlan *P, int q, const DevCSR &A, const DevCSR 
         }
         const int lg = b.tpr == 4 ? 2 : b.tpr == 8 ? 3 : b.tpr == 16 ? 4 : 5;
         const int groups = 128 / b.tpr;
-        int blocks = (cnt + groups - 1) / groups;
-        if (blocks > cap_blocks) blocks = cap_blocks;
-        k_saxpy_hash<SR, false><<<blocks, 128, smem, s>>>(rows, cnt, lg, b.cap,
+        const int blocks = clamp((rows_bound + groups - 1) / groups,
+                                 (const void *)k_saxpy_hash<SR, false>, 128, smem);
+        k_saxpy_hash<SR, false><<<blocks, 128, smem, s>>>(br, lg, b.cap,
             A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
             M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, P->mask_comp,
             P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
     }
+}
+
+// the shared-memory bins: with exact host counts (after plan_read), or with
+// m as every bin's bound and the fit check on the device
+template <class SR>
+static void exec_light(const SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &B,
+                       bool exact, cudaStream_t s)
+{
+    const int64_t *need = exact ? nullptr : (const int64_t *)(P->bins + BIN_TOTAL_CAP);
+    for (int q = 0; q < P->cfg.nb; q++)
+        launch_bin<SR>(P, q, A, B, M, exact ? P->h_bins[q + 1] : P->m, exact, need, s);
+}
+
+// the heavy rows (counts from plan_read, accumulators from plan_alloc_heavy)
+template <class SR>
+static void exec_heavy(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &B,
+                       cudaStream_t s)
+{
+    using Z = typename SR::z_t;
+    const int64_t ncols = P->ncols;
+    const int nb = P->cfg.nb;
+    const int nheavy = P->h_bins[nb + 1];
+    if (nheavy == 0) return;
+    const int32_t *hrows = P->bin_rows + P->h_start[nb + 1];
+    int64_t *flag = P->flag;
+    uint8_t *flag8 = P->flag8;
+    Z *val = (Z *)P->val;
+    if constexpr (SR::order_free) {
+        const int64_t chunk = P->heavy_chunk;
+        for (int64_t c0 = 0; c0 < nheavy; c0 += chunk) {
+            const int nr = (int)((nheavy - c0 < chunk) ? nheavy - c0 : chunk);
+            dim3 g1(nblocks(ncols, 256, 4), nr > 65535 ? 65535 : nr);
+            k_dense_init<SR><<<g1, 256, 0, s>>>(hrows + c0, nr, ncols, flag8, val);
+            if (M) {
+                dim3 g2(runtime().num_sms * 2 / (nr < 8 ? nr : 8) + 1, nr > 65535 ? 65535 : nr);
+                k_dense_mask<<<g2, 256, 0, s>>>(hrows + c0, nr, M->p, M->j, P->mask_comp,
+                                                ncols, flag8);
+            }
+            // flat product index of the chunk (the rows' offsets into their
+            // entries, then each entry's B-row length scanned), then every
+            // product over the grid
+            if (nr <= 1024) {
+                k_heavy_offsets<<<1, 1024, 0, s>>>(hrows + c0, nr, A.p, P->hoff);
+            } else {
+                k_heavy_alen<<<(nr + 255) / 256, 256, 0, s>>>(hrows + c0, nr, A.p, P->hlen);
+                scan_exclusive_i64_ws(P->hlen, P->hoff, nr + 1, P->hw_ws, s);
+            }
+            lb_scan(LbLoadBlen{hrows + c0, nr, P->hoff, A.p, A.j, B.p}, P->wprefix,
+                    P->heavy_alen + 1, P->lb_w, s, nullptr, nullptr, P->bins + BIN_HEAVY_ERR);
+            k_dense_atomic_flat<SR><<<runtime().num_sms * 32, 256, 0, s>>>(hrows + c0, nr,
+                P->hoff, P->wprefix, A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
+                M != nullptr, P->mask_comp, ncols, flag8, val);
+            // ordered compaction into the rows' slots
+            const int cblocks = (int)((ncols + DG_CHUNK - 1) / DG_CHUNK);
+            const int64_t ntiles = (int64_t)nr * cblocks;
+            k_dense_compact<SR><<<(unsigned)ntiles, DG_THREADS, 0, s>>>(hrows + c0, cblocks,
+                ncols, flag8, val, P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt, ntiles,
+                P->lb_c, P->bins + BIN_HEAVY_ERR);
+        }
+    } else {
+        const int nbk = (int)P->heavy_chunk;
+        cudaMemsetAsync(flag, 0, (size_t)nbk * ncols * 8, s);
+        k_saxpy_dense_seq<SR><<<nbk, 256, 0, s>>>(hrows, nheavy, A.p, A.j, A.x, A.iso,
+            B.p, B.j, B.x, B.iso, M ? M->p : nullptr, M ? M->j : nullptr,
+            M != nullptr, P->mask_comp, ncols, flag, val, P->slot_off, P->Tj,
+            (Z *)P->Tx, P->row_cnt);
+    }
+}
+
+// exact row counts -> C's row offsets (int64 in Cp64, int32 in Cp) and the
+// output count
+static void exec_counts(SaxpyPlan *P, int32_t *Cp, int64_t *Cnnz64, cudaStream_t s)
+{
+    scan_exclusive_lb_counts(P->row_cnt, P->row_bin, P->m, P->Cp64, P->lb_row, s,
+                             Cnnz64 ? Cnnz64 : (int64_t *)(P->bins + BIN_NNZ), Cp,
+                             P->bins + BIN_ROW_ERR);
+}
+
+// the slots, packed into C's exact arrays
+template <typename Z>
+static void exec_pack(const SaxpyPlan *P, int32_t *Cj, Z *Cx, cudaStream_t s)
+{
+    if (P->m > 0 && P->total_cap > 0)
+        k_pack<Z><<<nblocks(P->total_cap, 256, 16), 256, 0, s>>>(P->m,
+            flat_span(P->total_cap), P->slot_off, P->Tj, (const Z *)P->Tx, P->Cp64, Cj, Cx);
 }
 
 template <class SR>
@@ -1347,66 +1625,12 @@ static int exec_t(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR &
                   int32_t *Cp, int32_t *Cj, void *Cx, int64_t *Cnnz64, cudaStream_t s)
 {
     using Z = typename SR::z_t;
-    const int64_t m = P->m, ncols = P->ncols;
-    const int nb = P->cfg.nb;
-    cudaMemsetAsync(P->row_cnt, 0, (size_t)(m + 1) * 4, s);
     const int ps = prof_begin("saxpy3_numeric", s);
-    for (int q = 0; q < nb; q++) launch_bin<SR>(P, q, A, B, M, s);
-    const int nheavy = P->h_bins[nb + 1];
-    if (nheavy > 0) {
-        const int32_t *hrows = P->bin_rows + P->h_start[nb + 1];
-        int64_t *flag = P->flag;
-        uint8_t *flag8 = P->flag8;
-        Z *val = (Z *)P->val;
-        if constexpr (SR::order_free) {
-            const int64_t chunk = P->heavy_chunk;
-            for (int64_t c0 = 0; c0 < nheavy; c0 += chunk) {
-                const int nr = (int)((nheavy - c0 < chunk) ? nheavy - c0 : chunk);
-                dim3 g1(nblocks(ncols, 256, 4), nr > 65535 ? 65535 : nr);
-                k_dense_init<SR><<<g1, 256, 0, s>>>(hrows + c0, nr, ncols, flag8, val);
-                if (M) {
-                    dim3 g2(runtime().num_sms * 2 / (nr < 8 ? nr : 8) + 1, nr > 65535 ? 65535 : nr);
-                    k_dense_mask<<<g2, 256, 0, s>>>(hrows + c0, nr, M->p, M->j, P->mask_comp,
-                                                    ncols, flag8);
-                }
-                // flat product index of the chunk, then every product over the grid
-                k_heavy_alen<<<(nr + 255) / 256, 256, 0, s>>>(hrows + c0, nr, A.p, P->hlen);
-                scan_exclusive_i64_ws(P->hlen, P->hoff, nr + 1, P->hw_ws, s);
-                // entries past this chunk's count stay 0 (wprefix[ne] is the total)
-                cudaMemsetAsync(P->wlen, 0, (size_t)(P->heavy_alen + 1) * 8, s);
-                k_heavy_blen<<<nblocks(P->heavy_alen, 256, 8), 256, 0, s>>>(hrows + c0, nr,
-                    P->hoff, A.p, A.j, B.p, P->wlen);
-                scan_exclusive_i64_ws(P->wlen, P->wprefix, P->heavy_alen + 1, P->hw_ws, s);
-                k_dense_atomic_flat<SR><<<runtime().num_sms * 32, 256, 0, s>>>(hrows + c0, nr,
-                    P->hoff, P->wprefix, A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
-                    M != nullptr, P->mask_comp, ncols, flag8, val);
-                const int cblocks = (int)((ncols + DG_CHUNK - 1) / DG_CHUNK);
-                dim3 g4(cblocks, nr > 65535 ? 65535 : nr);
-                k_dense_count<<<g4, DG_THREADS, 0, s>>>(nr, ncols, cblocks, flag8, P->dg_cnt);
-                const int64_t ncnt = (int64_t)nr * cblocks;
-                scan_exclusive_i64_ws(P->dg_cnt, P->dg_cnt, ncnt + 1, P->dg_ws, s);
-                k_dense_write<SR><<<g4, DG_THREADS, 0, s>>>(hrows + c0, nr, ncols, cblocks,
-                    flag8, val, P->dg_cnt, P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt);
-            }
-        } else {
-            const int nbk = (int)P->heavy_chunk;
-            cudaMemsetAsync(flag, 0, (size_t)nbk * ncols * 8, s);
-            k_saxpy_dense_seq<SR><<<nbk, 256, 0, s>>>(hrows, nheavy, A.p, A.j, A.x, A.iso,
-                B.p, B.j, B.x, B.iso, M ? M->p : nullptr, M ? M->j : nullptr,
-                M != nullptr, P->mask_comp, ncols, flag, val, P->slot_off, P->Tj,
-                (Z *)P->Tx, P->row_cnt);
-        }
-    }
+    exec_light<SR>(P, M, A, B, true, s);
+    exec_heavy<SR>(P, M, A, B, s);
     prof_end(ps, s);
-    // exact row counts -> C row pointers, then pack the slots
-    k_cnt_to_i64<<<nblocks(m + 1, 256), 256, 0, s>>>(P->row_cnt, P->row_bin, m, P->Cp64);
-    // the scan's error word follows the output count
-    scan_exclusive_lb(P->Cp64, P->Cp64, m + 1, P->lb_row, s, Cnnz64, Cp,
-                      (int *)(P->nnz_d + 1));
-    if (m > 0 && P->total_cap > 0)
-        k_pack<Z><<<nblocks(P->total_cap, 256, 16), 256, 0, s>>>(m, flat_span(P->total_cap),
-            P->slot_off, P->Tj,
-            (Z *)P->Tx, P->Cp64, Cj, (Z *)Cx);
+    exec_counts(P, Cp, Cnnz64, s);
+    exec_pack<Z>(P, Cj, (Z *)Cx, s);
     return cuda_to_info(cudaGetLastError());
 }
 
@@ -1444,7 +1668,197 @@ int saxpy_plan_exec(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const DevCSR
     return NO_VALUE;
 }
 
-// one-shot C<M> = A*B: plan, execute, then trim the output to its exact size
+// Where the slots of a one-shot product live: the stream's scratch buffer
+// when the library owns the stream, else a buffer for this call.
+struct SlotSource {
+    cudaStream_t s;
+    bool shared;
+    void *own = nullptr;
+    size_t have = 0;
+    explicit SlotSource(cudaStream_t st) : s(st), shared(stream_scratch_enabled(st))
+    {
+        if (shared) have = stream_scratch_size(st);
+    }
+    ~SlotSource() { dfree(own, s); }
+    void *get(size_t want)
+    {
+        if (shared) return stream_scratch(s, want, &have);
+        dfree(own, s);
+        own = dalloc(want, s);
+        have = own ? want : 0;
+        return own;
+    }
+};
+
+// A one-row product whose row is expected to be heavy (vxm with a large
+// frontier), with an order-free monoid: straight to the dense accumulator,
+// with no symbolic phase and no host round trip before it.  The row's A
+// entries are its whole flat index; its slots hold every column.
+template <class SR>
+static int saxpy3_row_dense(DevCSR &C, const DevCSR *M, bool mask_comp, const DevCSR &A,
+                            const DevCSR &B, SemiringCode sr, cudaStream_t s)
+{
+    using Z = typename SR::z_t;
+    const int64_t ncols = B.ncols;
+    SaxpyPlan *P = new SaxpyPlan();
+    struct PlanGuard { SaxpyPlan *P; cudaStream_t s; ~PlanGuard() { saxpy_plan_free(P, s); } }
+        pg{P, s};
+    P->sr = sr;
+    P->cfg = saxpy_default_config();
+    P->zsize = sizeof(Z);
+    P->order_free = true;
+    P->m = 1; P->ncols = ncols;
+    P->has_mask = M != nullptr; P->mask_comp = mask_comp;
+    const int nb = P->cfg.nb;
+    P->h_bins[nb + 1] = 1;
+    P->h_start[nb + 1] = 0;
+    P->heavy_alen = A.nnz;
+    P->heavy_chunk = 1;
+    P->total_cap = ncols;
+    const int64_t ntiles = (ncols + DG_CHUNK - 1) / DG_CHUNK;
+    // everything in one allocation; the counters, the look-back workspaces,
+    // the slot offset, the row count and the row list (row 0) are zero
+    Carve cv(s);
+    auto layout = [&]() {
+        P->bins = cv.take<int>(BINS_WORDS);
+        P->lb_row = cv.take<unsigned long long>(scan_lb_ws_elems(2));
+        P->slot_off = cv.take<int64_t>(2);
+        P->row_cnt = cv.take<int32_t>(2);
+        P->bin_rows = cv.take<int32_t>(2);
+        P->lb_w = cv.take<unsigned long long>(lb_ws_elems(A.nnz + 1));
+        P->lb_c = cv.take<unsigned long long>(ntiles + 2);
+        P->Cp64 = cv.take<int64_t>(3);
+        P->hoff = cv.take<int64_t>(2);
+        P->hlen = cv.take<int64_t>(2);
+        P->hw_ws = cv.take<int64_t>(scan_ws_elems(2));
+        P->wprefix = cv.take<int64_t>(A.nnz + 1);
+        P->flag8 = cv.take<uint8_t>(ncols + 1);
+        P->val = cv.take<Z>(ncols + 1);
+    };
+    layout();
+    if (!cv.alloc()) return OUT_OF_MEMORY;
+    layout();
+    P->block = cv.base;
+    P->row_bin = nullptr;                 // the one row counts
+    cudaMemsetAsync(P->bins, 0, (size_t)((char *)(P->lb_c + ntiles + 2) - (char *)P->bins), s);
+    DevCSR T;
+    T.nrows = 1; T.ncols = ncols; T.type = sr.type; T.iso = false;
+    T.p = (int32_t *)dalloc(2 * 4, s);
+    if (!T.p) return OUT_OF_MEMORY;
+    SlotSource src(s);
+    void *slots = src.get(src.have >= slot_bytes(P, ncols) ? src.have : slot_bytes(P, ncols));
+    if (!slots) { dev_free(T, s); return OUT_OF_MEMORY; }
+    plan_place_slots(P, slots, src.have);
+    const int ps = prof_begin("saxpy3_numeric", s);
+    exec_heavy<SR>(P, M, A, B, s);
+    prof_end(ps, s);
+    exec_counts(P, T.p, nullptr, s);
+    int hb[BINS_READ];
+    cudaError_t e = readback(hb, P->bins, sizeof(hb), s);
+    if (e != cudaSuccess) { dev_free(T, s); return cuda_to_info(e); }
+    if (hb[BIN_ROW_ERR] || hb[BIN_HEAVY_ERR]) { dev_free(T, s); return PANIC; }
+    int64_t nnz = 0;
+    memcpy(&nnz, hb + BIN_NNZ, 8);
+    T.nnz = nnz;
+    T.j = (int32_t *)dalloc((size_t)(nnz + 1) * 4, s);
+    T.x = dalloc((size_t)(nnz + 1) * sizeof(Z), s);
+    if (!T.j || !T.x) { dev_free(T, s); return OUT_OF_MEMORY; }
+    exec_pack<Z>(P, T.j, (Z *)T.x, s);
+    const int info = cuda_to_info(cudaGetLastError());
+    if (info != SUCCESS) { dev_free(T, s); return info; }
+    C = T;
+    return SUCCESS;
+}
+
+// One-shot C<M> = A*B with one host round trip in the common case.  The
+// symbolic phase, the shared-memory bins and the row offsets are queued
+// together: the bins write their slots into the stream's scratch buffer and
+// read their row counts and the slot total on the device.  One read brings
+// back the counts, the slot total and the output size; only if the slots
+// did not fit (the buffer then grows and the bins run again) or heavy rows
+// need their accumulators sized does a second read follow.  C's arrays are
+// then allocated at their exact size and the slots packed into them.
+template <class SR>
+static int saxpy3_t(DevCSR &C, const DevCSR *M, bool mask_comp, const DevCSR &A,
+                    const DevCSR &B, SemiringCode sr, cudaStream_t s)
+{
+    using Z = typename SR::z_t;
+    const int64_t m = A.nrows;
+    const double mean_b = B.nrows > 0 ? (double)B.nnz / (double)B.nrows : 0.0;
+    if constexpr (SR::order_free) {
+        // a one-row product expected far past the shared-memory bins, whose
+        // dense row fits comfortably: the dense path directly
+        const SaxpyConfig dc = saxpy_default_config();
+        const double est = (double)A.nnz * mean_b;
+        if (m == 1 && A.nnz > 0 && est >= 2.0 * (double)dc.bin[dc.nb - 1].limit &&
+            (double)B.ncols * (1.0 + sizeof(Z)) <= (double)((int64_t)4 << 30))
+            return saxpy3_row_dense<SR>(C, M, mask_comp, A, B, sr, s);
+    }
+    SaxpyPlan *P = new SaxpyPlan();
+    P->sr = sr;
+    P->cfg = saxpy_default_config();
+    struct PlanGuard { SaxpyPlan *P; cudaStream_t s; ~PlanGuard() { saxpy_plan_free(P, s); } }
+        pg{P, s};
+    int info = plan_symbolic<SR>(P, M, mask_comp, A, B, s);
+    if (info != SUCCESS) return info;
+    DevCSR T;
+    T.nrows = m; T.ncols = B.ncols; T.type = sr.type; T.iso = false;
+    T.p = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
+    if (!T.p) return OUT_OF_MEMORY;
+    // the slots: the stream's buffer as it is, or a first one sized from the
+    // mean row length of B (grown below if the rows need more)
+    SlotSource src(s);
+    size_t want = src.have;
+    if (want == 0) {
+        double guess = 2.0 * (double)A.nnz * (mean_b > 1.0 ? mean_b : 1.0) + (double)m + 1024;
+        const double full = (double)m * (double)B.ncols;
+        if (guess > full + 1024) guess = full + 1024;
+        if (guess > (double)(64 << 20)) guess = (double)(64 << 20);
+        want = slot_bytes(P, (int64_t)guess);
+    }
+    void *slots = src.get(want);
+    if (!slots) { dev_free(T, s); return OUT_OF_MEMORY; }
+    plan_place_slots(P, slots, src.have);
+    const int ps = prof_begin("saxpy3_numeric", s);
+    exec_light<SR>(P, M, A, B, false, s);
+    prof_end(ps, s);
+    exec_counts(P, T.p, nullptr, s);
+    info = plan_read(P, s);
+    if (info != SUCCESS) { dev_free(T, s); return info; }
+    bool again = false;
+    if (P->total_cap > P->slot_avail) {
+        // the bins did nothing: more slots, then the bins with exact counts
+        slots = src.get(slot_bytes(P, P->total_cap + P->total_cap / 4));
+        if (!slots) { dev_free(T, s); return OUT_OF_MEMORY; }
+        plan_place_slots(P, slots, src.have);
+        exec_light<SR>(P, M, A, B, true, s);
+        again = true;
+    }
+    if (P->h_bins[P->cfg.nb + 1] > 0) {
+        info = plan_alloc_heavy<SR>(P, s);
+        if (info != SUCCESS) { dev_free(T, s); return info; }
+        exec_heavy<SR>(P, M, A, B, s);
+        again = true;
+    }
+    if (again) {
+        exec_counts(P, T.p, nullptr, s);
+        info = plan_read(P, s);
+        if (info != SUCCESS) { dev_free(T, s); return info; }
+    }
+    const int64_t nnz = P->nnz;
+    if (nnz >= INT32_MAX) { dev_free(T, s); return OUT_OF_MEMORY; }
+    T.nnz = nnz;
+    T.j = (int32_t *)dalloc((size_t)(nnz + 1) * 4, s);
+    T.x = dalloc((size_t)(nnz + 1) * sizeof(Z), s);
+    if (!T.j || !T.x) { dev_free(T, s); return OUT_OF_MEMORY; }
+    exec_pack<Z>(P, T.j, (Z *)T.x, s);
+    info = cuda_to_info(cudaGetLastError());
+    if (info != SUCCESS) { dev_free(T, s); return info; }
+    C = T;
+    return SUCCESS;
+}
+
+// one-shot C<M> = A*B
 int saxpy3(DevCSR &C, const DevCSR *M, bool mask_comp, bool mask_struct,
            const DevCSR &A, const DevCSR &B, SemiringCode sr, cudaStream_t s)
 {
@@ -1464,44 +1878,14 @@ int saxpy3(DevCSR &C, const DevCSR *M, bool mask_comp, bool mask_struct,
     }
     struct Guard { DevCSR *m; bool own; cudaStream_t s;
         ~Guard() { if (own) dev_free(*m, s); } } guard{&Ms, own_mask, s};
-    SaxpyPlan *P = nullptr;
-    int info = saxpy_plan_create(&P, M, mask_comp, A, B, sr, saxpy_default_config(), s);
+    int info = NO_VALUE;
+#define GRB_ONESHOT_CASE(ADD, MULT, TC, CT)                                     \
+    if (sr.add == ADD && sr.mult == MULT && sr.type == TC)                      \
+        info = saxpy3_t<Semiring<ADD, MULT, CT>>(C, M, mask_comp, A, B, sr, s); \
+    else
+    GRB_FOR_EACH_SEMIRING(GRB_ONESHOT_CASE) { info = NO_VALUE; }
+#undef GRB_ONESHOT_CASE
     if (info != SUCCESS) return info;
-    const size_t zs = P->zsize;
-    const int64_t cap = P->total_cap, m = A.nrows;
-    DevCSR T;
-    T.nrows = m; T.ncols = B.ncols; T.type = sr.type; T.iso = false;
-    T.p = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
-    T.j = (int32_t *)dalloc((size_t)(cap + 1) * 4, s);
-    T.x = dalloc((size_t)(cap + 1) * zs, s);
-    int64_t *nnz_d = P->nnz_d;
-    if (!T.p || !T.j || !T.x) {
-        dev_free(T, s); saxpy_plan_free(P, s); return OUT_OF_MEMORY;
-    }
-    info = saxpy_plan_exec(P, M, A, B, T.p, T.j, T.x, nnz_d, s);
-    int64_t hv[2] = {0, 0};
-    cudaError_t e = readback(hv, nnz_d, 16, s);
-    const int64_t nnz = hv[0];
-    saxpy_plan_free(P, s);
-    if (info == SUCCESS && e != cudaSuccess) info = cuda_to_info(e);
-    if (info == SUCCESS && hv[1]) info = PANIC;
-    if (info != SUCCESS) { dev_free(T, s); return info; }
-    if (nnz >= INT32_MAX) { dev_free(T, s); return OUT_OF_MEMORY; }
-    T.nnz = nnz;
-    if (cap > 2 * nnz + 1024) {
-        // the flop bound overestimated the output a lot: keep exact arrays
-        int32_t *j2 = (int32_t *)dalloc((size_t)(nnz + 1) * 4, s);
-        void *x2 = dalloc((size_t)(nnz + 1) * zs, s);
-        if (j2 && x2) {
-            cudaMemcpyAsync(j2, T.j, (size_t)nnz * 4, cudaMemcpyDeviceToDevice, s);
-            cudaMemcpyAsync(x2, T.x, (size_t)nnz * zs, cudaMemcpyDeviceToDevice, s);
-            dfree(T.j, s); dfree(T.x, s);
-            T.j = j2; T.x = x2;
-        } else {
-            dfree(j2, s); dfree(x2, s);
-        }
-    }
-    C = T;
     return cuda_to_info(cudaStreamSynchronize(s));
 }
 

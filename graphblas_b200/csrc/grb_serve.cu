@@ -254,6 +254,7 @@ void worker_main(grb_b200_server_s *S, int dev)
     cudaSetDevice(dev);
     cudaStream_t s;
     cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    stream_scratch_enable(s);
     std::vector<Req *> grp;
     while (true) {
         Req *r = nullptr;
@@ -328,6 +329,8 @@ void worker_main(grb_b200_server_s *S, int dev)
         }
         S->cv.notify_all();
     }
+    cudaStreamSynchronize(s);
+    stream_scratch_release(s);
     cudaStreamDestroy(s);
 }
 
