@@ -23,6 +23,7 @@
 #include <cstring>
 #include <vector>
 #include "grb_runtime.h"
+#include "grb_lookback.cuh"
 
 namespace grb {
 
@@ -166,11 +167,225 @@ static inline int grid_n(int64_t n, int threads = 256)
     return b < 1 ? 1 : (int)b;
 }
 
+// ---------------------------------------------------------------------------
+// one-row union: w<u> = u with u's pattern as the structural mask, no
+// accumulator, no replace (the BFS parent update) on row vectors.  The
+// result is the merge of two sorted index lists in which u's entry wins a
+// tie.  One launch: tiles of UN_TILE merged positions (from a ticket); a
+// tile finds where its positions start in each list (merge path: a
+// warp-cooperative search over the diagonal), stages both ranges in shared
+// memory, each thread merges UN_ITEMS positions, the tile's kept count gets
+// its offset by decoupled look-back, and the tile's output is written from
+// shared memory by consecutive threads.
+// ---------------------------------------------------------------------------
+
+static constexpr int UN_THREADS = 256, UN_ITEMS = 8, UN_TILE = UN_THREADS * UN_ITEMS;
+
+// T before C on equal keys: C[i-1] precedes T[d-i] iff C[i-1] < T[d-i].
+// The number of C entries among the first d merged positions: the largest
+// i in [max(0, d - nT), min(d, nC)] with i == 0, d - i >= nT or
+// C[i-1] < T[d-i]; all lanes of the warp search together, 32 candidates a
+// step.
+__device__ __forceinline__ int64_t union_split(const int32_t *__restrict__ C, int64_t nC,
+                                               const int32_t *__restrict__ T, int64_t nT,
+                                               int64_t d, int lane)
+{
+    int64_t lo = d - nT > 0 ? d - nT : 0;
+    int64_t hi = d < nC ? d : nC;
+    while (lo < hi) {
+        const int64_t step = (hi - lo + 31) / 32;
+        const int64_t c = lo + 1 + (int64_t)lane * step;
+        bool q = false;
+        if (c <= hi) q = (d - c >= nT) || (C[c - 1] < T[d - c]);
+        const unsigned m = __ballot_sync(0xffffffffu, q);
+        if (m == 0) { hi = lo; break; }
+        const int k = 31 - __clz(m);
+        lo = lo + 1 + (int64_t)k * step;
+        const int64_t h2 = lo + step - 1;
+        hi = h2 < hi ? h2 : hi;
+    }
+    return lo;
+}
+
+template <typename Z>
+__global__ void __launch_bounds__(UN_THREADS)
+k_union_row(const int32_t *__restrict__ Cj, const Z *__restrict__ Cx, bool c_iso, int64_t nC,
+            const int32_t *__restrict__ Tj, const Z *__restrict__ Tx, bool t_iso, int64_t nT,
+            int32_t *__restrict__ Rp, int32_t *__restrict__ Rj, Z *__restrict__ Rx,
+            int64_t *__restrict__ total, int64_t ntiles, unsigned long long *__restrict__ ws,
+            int *__restrict__ err)
+{
+    __shared__ int s_tile, s_last, s_agg;
+    __shared__ long long s_ex;
+    __shared__ int64_t s_i0, s_i1;
+    __shared__ int s_w[UN_THREADS / 32];
+    // the staged input ranges, then (after the merge) the staged output: its
+    // values over the inputs' space, its indices after them
+    __shared__ __align__(16) unsigned char s_buf[UN_TILE * (sizeof(Z) > 8 ? sizeof(Z) : 8) +
+                                                 UN_TILE * 4];
+    int32_t *s_c = (int32_t *)s_buf, *s_t = s_c + UN_TILE;
+    Z *s_ox = (Z *)s_buf;
+    int32_t *s_oj = (int32_t *)(s_buf + UN_TILE * (sizeof(Z) > 8 ? sizeof(Z) : 8));
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    unsigned long long *status = ws + 2;
+    if (tid == 0) s_tile = (int)atomicAdd(&ws[0], 1ull);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    const int64_t nd = nC + nT;
+    const int64_t d0 = tile * UN_TILE;
+    const int64_t d1 = d0 + UN_TILE < nd ? d0 + UN_TILE : nd;
+    if (w == 0) {
+        const int64_t a = union_split(Cj, nC, Tj, nT, d0, lane);
+        if (lane == 0) s_i0 = a;
+    } else if (w == 1) {
+        const int64_t b = union_split(Cj, nC, Tj, nT, d1, lane);
+        if (lane == 0) s_i1 = b;
+    }
+    __syncthreads();
+    const int64_t i0 = s_i0, i1 = s_i1, j0 = d0 - i0, j1 = d1 - i1;
+    const int nc = (int)(i1 - i0), nt = (int)(j1 - j0);
+    for (int k = tid; k < nc; k += UN_THREADS) s_c[k] = Cj[i0 + k];
+    for (int k = tid; k < nt; k += UN_THREADS) s_t[k] = Tj[j0 + k];
+    const int32_t tprev = j0 > 0 ? Tj[j0 - 1] : -1;     // the T entry before the tile's
+    __syncthreads();
+    // this thread's positions [dl, dl + UN_ITEMS) of the tile, merged locally
+    const int dl = tid * UN_ITEMS;
+    const int nl = (int)(d1 - d0);
+    int ci = 0, tj = 0;
+    if (dl < nl) {
+        // the split of diagonal dl within the staged ranges
+        int lo = dl - nt > 0 ? dl - nt : 0, hi = dl < nc ? dl : nc;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if ((dl - mid >= nt) || (s_c[mid - 1] < s_t[dl - mid])) lo = mid; else hi = mid - 1;
+        }
+        ci = lo;
+        tj = dl - lo;
+    }
+    int32_t oj[UN_ITEMS];
+    Z ox[UN_ITEMS];
+    int kept = 0;
+    for (int k = 0; k < UN_ITEMS && dl + k < nl; k++) {
+        if (tj < nt && (ci >= nc || s_t[tj] <= s_c[ci])) {
+            oj[kept] = s_t[tj];
+            ox[kept] = Tx[t_iso ? 0 : j0 + tj];
+            kept++;
+            tj++;
+        } else {
+            const int32_t key = s_c[ci];
+            const int32_t before = tj > 0 ? s_t[tj - 1] : tprev;
+            if (before != key) {
+                oj[kept] = key;
+                ox[kept] = Cx[c_iso ? 0 : i0 + ci];
+                kept++;
+            }
+            ci++;
+        }
+    }
+    int x = kept;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int v = lane < UN_THREADS / 32 ? s_w[lane] : 0;
+        const int ownv = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        const long long agg = __shfl_sync(0xffffffffu, v, 31);
+        if (lane < UN_THREADS / 32) s_w[lane] = v - ownv;
+        long long ex = 0;
+        if (tile == 0) {
+            if (lane == 0) atomicExch(&status[0], LB_INC | ((unsigned long long)agg & LB_VAL));
+        } else {
+            if (lane == 0) atomicExch(&status[tile], LB_AGG | ((unsigned long long)agg & LB_VAL));
+            ex = lb_lookback(status, tile, lane, err);
+            if (lane == 0)
+                atomicExch(&status[tile], LB_INC | ((unsigned long long)(ex + agg) & LB_VAL));
+        }
+        if (lane == 0) {
+            s_ex = ex;
+            s_agg = (int)agg;
+            if (tile == 0) Rp[0] = 0;
+            if (tile == ntiles - 1) { Rp[1] = (int32_t)(ex + agg); *total = ex + agg; }
+        }
+    }
+    // (the block barrier above also ends every read of the staged inputs)
+    __syncthreads();
+    int loc = s_w[w] + (x - kept);
+    for (int k = 0; k < kept; k++) { s_oj[loc + k] = oj[k]; s_ox[loc + k] = ox[k]; }
+    __syncthreads();
+    const int64_t base = s_ex;
+    for (int k = tid; k < s_agg; k += UN_THREADS) {
+        Rj[base + k] = s_oj[k];
+        Rx[base + k] = s_ox[k];
+    }
+    // the last tile to finish clears the workspace
+    if (tid == 0) {
+        __threadfence();
+        s_last = atomicAdd(&ws[1], 1ull) == (unsigned long long)(ntiles - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        for (int64_t t = tid; t < ntiles; t += UN_THREADS) status[t] = 0;
+        if (tid == 0) { ws[0] = 0; ws[1] = 0; }
+    }
+}
+
+// C = C union T on one row, T's entries winning ties (w<u> = u)
+template <typename Z>
+static int union_row_t(DevCSR &C, const DevCSR &T, cudaStream_t s)
+{
+    const int64_t nC = C.nnz, nT = T.nnz, nd = nC + nT;
+    if (nd >= INT32_MAX) return OUT_OF_MEMORY;
+    const int64_t ntiles = nd > 0 ? (nd + UN_TILE - 1) / UN_TILE : 0;
+    Carve cv(s);
+    int64_t *tot_d = nullptr;
+    unsigned long long *ws = nullptr;
+    auto layout = [&]() {
+        tot_d = cv.take<int64_t>(2);
+        ws = cv.take<unsigned long long>(ntiles + 2);
+    };
+    layout();
+    if (!cv.alloc()) return OUT_OF_MEMORY;
+    layout();
+    struct Release { Carve &c; ~Release() { dfree(c.base, c.s); } } release{cv};
+    DevCSR R;
+    R.nrows = 1; R.ncols = T.ncols; R.type = T.type; R.iso = false;
+    R.p = (int32_t *)dalloc(2 * 4, s);
+    R.j = (int32_t *)dalloc((size_t)(nd ? nd : 1) * 4, s);
+    R.x = dalloc((size_t)(nd ? nd : 1) * sizeof(Z), s);
+    if (!R.p || !R.j || !R.x) { dev_free(R, s); return OUT_OF_MEMORY; }
+    int64_t tot[2] = {0, 0};
+    if (ntiles > 0) {
+        cudaMemsetAsync(tot_d, 0, (size_t)((char *)(ws + ntiles + 2) - (char *)tot_d), s);
+        k_union_row<Z><<<(unsigned)ntiles, UN_THREADS, 0, s>>>(C.j, (const Z *)C.x, C.iso, nC,
+            T.j, (const Z *)T.x, T.iso, nT, R.p, R.j, (Z *)R.x, tot_d, ntiles, ws,
+            (int *)(tot_d + 1));
+        cudaError_t e = readback(tot, tot_d, 16, s);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e != cudaSuccess) { dev_free(R, s); return cuda_to_info(e); }
+        if ((int)tot[1] != 0) { dev_free(R, s); return PANIC; }
+    } else {
+        cudaMemsetAsync(R.p, 0, 2 * 4, s);
+    }
+    R.nnz = tot[0];
+    dev_free(C, s);
+    C = R;
+    return SUCCESS;
+}
+
 template <typename Z>
 static int accum_mask_t(DevCSR &C, const DevCSR &T, const DevCSR *M, bool comp,
                         bool replace, int accum, cudaStream_t s)
 {
     const int64_t m = T.nrows, nT = T.nnz, nC = C.nnz;
+    if (m == 1 && M && !comp && !replace && !accum && M->p == T.p && M->j == T.j)
+        return union_row_t<Z>(C, T, s);
     // the totals and error word, the two scans' workspaces, the keep flags /
     // offsets of both sides and T's values in one allocation; the first three
     // are cleared by one memset

@@ -830,42 +830,91 @@ template <class SR> __device__ __forceinline__ typename SR::z_t dense_init()
     return SR::M::identity();
 }
 
+// The dense row of a max-k ANY (any_secondi, any_firstj) on integer values:
+// each column is one 64-bit word, state << 32 | k (state 0 empty, 1 allowed
+// by a mask, 2 forbidden by a complemented mask, 3 holding k; every k is a
+// row or column index, below 2^31).  A product reads one word instead of a
+// flag and a value, and atomicMax on the word keeps the largest k, because
+// every word holding a value has the same state bits and is above every
+// word that does not.  The byte flags then only mark, for the compaction,
+// the columns that received a value.
+template <class SR> struct PackedDense {
+    using Z = typename SR::z_t;
+    static constexpr bool on = SR::any_max_k && std::is_integral<Z>::value && sizeof(Z) >= 4;
+};
 template <class SR>
-__global__ void k_dense_init(const int32_t *__restrict__ rows, int nrows_bin,
-                             int64_t ncols, uint8_t *__restrict__ flag_all,
-                             typename SR::z_t *__restrict__ val_all)
+using dense_val_t = typename std::conditional<PackedDense<SR>::on, unsigned long long,
+                                              typename SR::z_t>::type;
+static constexpr unsigned long long PK_SET = 3ull << 32;
+
+// the first p in [lo, hi) with a[p] >= key (hi if none), a nondecreasing,
+// found by the 32 lanes of a warp together (32 probes a step)
+__device__ __forceinline__ int32_t warp_lower_bound(const int32_t *__restrict__ a, int32_t lo,
+                                                    int32_t hi, int32_t key, int lane)
 {
-    // one block-row of workspace per heavy row (rows are few)
+    while (lo < hi) {
+        const int32_t step = (hi - lo + 31) / 32;
+        const int32_t c = lo + lane * step;
+        const bool less = c < hi && a[c] < key;
+        const int k = __popc(__ballot_sync(0xffffffffu, less));
+        if (k == 0) break;                        // a[lo] >= key
+        const int32_t nhi = lo + k * step;
+        lo = lo + (k - 1) * step + 1;
+        hi = nhi < hi ? nhi : hi;
+    }
+    return lo;
+}
+
+// The dense rows of a chunk prepared in one pass: block x of grid row y
+// owns a contiguous range of columns of heavy row y; it clears their flags,
+// sets their values to the monoid's identity, then marks the row's mask
+// entries that fall in its range (found by two warp-cooperative searches in
+// the sorted mask row): 1 = allowed (plain mask), 2 = forbidden (complement).
+// With one heavy row its flat index offsets {0, nnz(A(i,:))} are written too.
+template <class SR>
+__global__ void __launch_bounds__(256)
+k_dense_prep(const int32_t *__restrict__ rows, int nrows_bin, int64_t ncols,
+             uint8_t *__restrict__ flag_all, dense_val_t<SR> *__restrict__ val_all,
+             const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
+             bool has_mask, bool mask_comp, const int32_t *__restrict__ Ap,
+             int64_t *__restrict__ hoff)
+{
+    __shared__ int32_t s_lo, s_hi;
+    const int64_t per = ((ncols + gridDim.x - 1) / gridDim.x + 255) & ~(int64_t)255;
+    const int64_t c0 = (int64_t)blockIdx.x * per;
+    const int64_t c1 = c0 + per < ncols ? c0 + per : ncols;
+    if (nrows_bin == 1 && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+        const int32_t i = rows[0];
+        hoff[0] = 0;
+        hoff[1] = Ap[i + 1] - Ap[i];
+    }
+    constexpr bool packed = PackedDense<SR>::on;
     for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
         uint8_t *flag = flag_all + rb * ncols;
-        typename SR::z_t *val = val_all + rb * ncols;
-        for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < ncols;
-             j += (int64_t)gridDim.x * blockDim.x) {
+        dense_val_t<SR> *val = val_all + rb * ncols;
+        for (int64_t j = c0 + threadIdx.x; j < c1; j += blockDim.x) {
             flag[j] = 0;
-            val[j] = dense_init<SR>();
+            if constexpr (packed) val[j] = 0;
+            else val[j] = dense_init<SR>();
         }
+        if (has_mask && c0 < c1) {
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            if (w < 2) {
+                const int32_t i = rows[rb];
+                const int32_t key = (int32_t)(w == 0 ? c0 : (c1 < INT32_MAX ? c1 : INT32_MAX));
+                const int32_t r = warp_lower_bound(Mj, Mp[i], Mp[i + 1], key, lane);
+                if (lane == 0) { if (w == 0) s_lo = r; else s_hi = r; }
+            }
+            __syncthreads();
+            const uint8_t st = mask_comp ? 2 : 1;
+            for (int32_t pm = s_lo + threadIdx.x; pm < s_hi; pm += blockDim.x) {
+                if constexpr (packed) val[Mj[pm]] = (unsigned long long)st << 32;
+                else flag[Mj[pm]] = st;
+            }
+        }
+        __syncthreads();
     }
 }
-
-// mark mask columns: 1 allowed / 2 forbidden
-__global__ void k_dense_mask(const int32_t *__restrict__ rows, int nrows_bin,
-                             const int32_t *__restrict__ Mp,
-                             const int32_t *__restrict__ Mj, bool mask_comp,
-                             int64_t ncols, uint8_t *__restrict__ flag_all)
-{
-    for (int64_t rb = blockIdx.y; rb < nrows_bin; rb += gridDim.y) {
-        const int32_t i = rows[rb];
-        uint8_t *flag = flag_all + rb * ncols;
-        for (int32_t pm = Mp[i] + blockIdx.x * blockDim.x + threadIdx.x; pm < Mp[i + 1];
-             pm += gridDim.x * blockDim.x)
-            flag[Mj[pm]] = mask_comp ? 2 : 1;
-    }
-}
-
-// Flat product index of a chunk of heavy rows: hlen[rb] = nnz(A(i,:)) for the
-// chunk's rows (scanned into hoff), then wlen[e] = nnz(B(k,:)) for the e-th
-// A entry of the chunk (scanned into wprefix), so product t lies in entry e
-// with wprefix[e] <= t < wprefix[e+1].
 __global__ void k_heavy_alen(const int32_t *__restrict__ rows, int nr,
                              const int32_t *__restrict__ Ap, int64_t *__restrict__ hlen)
 {
@@ -946,7 +995,7 @@ k_dense_atomic_flat(const int32_t *__restrict__ rows, int nr,
                     const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
                     const void *__restrict__ Bx, bool b_iso,
                     bool has_mask, bool mask_comp, int64_t ncols,
-                    uint8_t *__restrict__ flag_all, typename SR::z_t *__restrict__ val_all)
+                    uint8_t *__restrict__ flag_all, dense_val_t<SR> *__restrict__ val_all)
 {
     using Z = typename SR::z_t;
     constexpr bool idem = SR::M::any || SR::add_op == OP_MIN || SR::add_op == OP_MAX ||
@@ -982,8 +1031,26 @@ k_dense_atomic_flat(const int32_t *__restrict__ rows, int nr,
             const int32_t k = Aj[pa];
             const int32_t pb = Bp[k] + (int32_t)(t - wprefix[e]);
             const int32_t j = Bj[pb];
+            if constexpr (PackedDense<SR>::on) {
+                // one word: state and k
+                unsigned long long *word = val_all + (int64_t)rb * ncols + j;
+                const unsigned long long wv = *word;
+                const unsigned st = (unsigned)(wv >> 32);
+                if (has_mask) {
+                    if (!mask_comp && st == 0) continue;
+                    if (mask_comp && st == 2) continue;
+                }
+                Z a = Z(), b = Z();
+                const Z tv = SR::F::f(a, b, i, k, j);
+                const unsigned long long nv = PK_SET | (unsigned long long)(uint32_t)tv;
+                if (wv >= nv) continue;
+                atomicMax(word, nv);
+                // the compaction's mark (the word holds the value)
+                if (st != 3) flag_all[(int64_t)rb * ncols + j] = 3;
+                continue;
+            }
             uint8_t *flag = flag_all + (int64_t)rb * ncols;
-            Z *val = val_all + (int64_t)rb * ncols;
+            Z *val = (Z *)val_all + (int64_t)rb * ncols;
             const uint8_t f = flag[j];
             if (has_mask) {
                 if (!mask_comp && f == 0) continue;
@@ -1009,19 +1076,21 @@ k_dense_atomic_flat(const int32_t *__restrict__ rows, int nr,
 // grid-wide ordered compaction of dense heavy rows, so a single long row
 // uses the whole GPU
 static constexpr int DG_THREADS = 256, DG_ITEMS = 16, DG_CHUNK = DG_THREADS * DG_ITEMS;
+template <class SR> constexpr int dense_tile() { return DG_CHUNK; }
 
-// The same compaction in one launch: tiles of DG_CHUNK columns of one heavy
+// The same compaction in one launch: tiles of dense_tile() columns of one heavy
 // row (tile = row * cblocks + chunk, from a ticket), 16 columns per thread;
 // a tile counts its entries, takes its offset in the row from its
 // predecessors by decoupled look-back (a row's first tile starts at 0), and
 // writes them in column order: the tile's columns are staged in shared
 // memory in order, then written out (and their values gathered) by
-// consecutive threads.  ws: ntiles + 2 zero words, left zero.
+// consecutive threads (a packed row's values from its words).  ws: ntiles +
+// 2 zero words, left zero.
 template <class SR>
 __global__ void __launch_bounds__(DG_THREADS)
 k_dense_compact(const int32_t *__restrict__ rows, int cblocks, int64_t ncols,
                 const uint8_t *__restrict__ flag_all,
-                const typename SR::z_t *__restrict__ val_all,
+                const dense_val_t<SR> *__restrict__ val_all,
                 const int64_t *__restrict__ slot_off, int32_t *__restrict__ Tj,
                 typename SR::z_t *__restrict__ Tx, int32_t *__restrict__ row_cnt,
                 int64_t ntiles, unsigned long long *__restrict__ ws, int *__restrict__ err)
@@ -1029,6 +1098,7 @@ k_dense_compact(const int32_t *__restrict__ rows, int cblocks, int64_t ncols,
     __shared__ int s_tile, s_last, s_agg;
     __shared__ long long s_ex;
     __shared__ int s_w[DG_THREADS / 32];
+    constexpr bool packed = PackedDense<SR>::on;
     __shared__ int32_t s_j[DG_CHUNK];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     unsigned long long *status = ws + 2;
@@ -1037,9 +1107,9 @@ k_dense_compact(const int32_t *__restrict__ rows, int cblocks, int64_t ncols,
     const int64_t tile = s_tile;
     const int64_t rb = tile / cblocks, cb = tile % cblocks;
     const int32_t i = rows[rb];
-    const uint8_t *flag = flag_all + rb * ncols;
     const int64_t c0 = cb * DG_CHUNK + (int64_t)tid * DG_ITEMS;
     unsigned bits = 0;
+    const uint8_t *flag = flag_all + rb * ncols;
     if (c0 + DG_ITEMS <= ncols && (((uintptr_t)(flag + c0)) & 15) == 0) {
         const uint4 v = *reinterpret_cast<const uint4 *>(flag + c0);
         const uint32_t word[4] = {v.x, v.y, v.z, v.w};
@@ -1091,11 +1161,14 @@ k_dense_compact(const int32_t *__restrict__ rows, int cblocks, int64_t ncols,
     }
     __syncthreads();
     const int64_t base = slot_off[i] + s_ex;
-    const typename SR::z_t *val = val_all + rb * ncols;
+    const dense_val_t<SR> *val = val_all + rb * ncols;
     for (int k = tid; k < s_agg; k += DG_THREADS) {
         const int32_t j = s_j[k];
         Tj[base + k] = j;
-        Tx[base + k] = val[j];
+        if constexpr (packed)
+            Tx[base + k] = (typename SR::z_t)(uint32_t)(val[j] & 0xffffffffull);
+        else
+            Tx[base + k] = val[j];
     }
     // the last tile to finish clears the workspace
     if (tid == 0) {
@@ -1379,11 +1452,11 @@ static int plan_alloc_heavy(SaxpyPlan *P, cudaStream_t s)
         const int64_t budget = (int64_t)4 << 30;
         if (chunk * per_row > budget) chunk = budget / per_row > 0 ? budget / per_row : 1;
         P->heavy_chunk = chunk;
-        const int64_t cblocks = (ncols + DG_CHUNK - 1) / DG_CHUNK;
+        const int64_t cblocks = (ncols + dense_tile<SR>() - 1) / dense_tile<SR>();
         const int64_t ntiles = chunk * cblocks;
         hlayout = [&, chunk, ntiles]() {
             P->flag8 = hv.take<uint8_t>(chunk * ncols + 1);
-            P->val = hv.take<Z>(chunk * ncols + 1);
+            P->val = hv.take<dense_val_t<SR>>(chunk * ncols + 1);
             P->hlen = hv.take<int64_t>(chunk + 1);
             P->hoff = hv.take<int64_t>(chunk + 1);
             P->wprefix = hv.take<int64_t>(P->heavy_alen + 1);
@@ -1405,7 +1478,8 @@ static int plan_alloc_heavy(SaxpyPlan *P, cudaStream_t s)
     P->hblock = hv.base;
     if (P->lb_w) {
         // the two look-back workspaces, adjacent, zero before their first use
-        const int64_t ntiles = P->heavy_chunk * ((ncols + DG_CHUNK - 1) / DG_CHUNK);
+        const int64_t ntiles =
+            P->heavy_chunk * ((ncols + dense_tile<SR>() - 1) / dense_tile<SR>());
         cudaMemsetAsync(P->lb_w, 0,
                         (size_t)((char *)(P->lb_c + ntiles + 2) - (char *)P->lb_w), s);
     }
@@ -1560,21 +1634,23 @@ static void exec_heavy(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const Dev
     int64_t *flag = P->flag;
     uint8_t *flag8 = P->flag8;
     Z *val = (Z *)P->val;
+    dense_val_t<SR> *dval = (dense_val_t<SR> *)P->val;
     if constexpr (SR::order_free) {
         const int64_t chunk = P->heavy_chunk;
         for (int64_t c0 = 0; c0 < nheavy; c0 += chunk) {
             const int nr = (int)((nheavy - c0 < chunk) ? nheavy - c0 : chunk);
+            // cleared flags, identity values and mask marks (and, for one
+            // row, its flat index offsets)
             dim3 g1(nblocks(ncols, 256, 4), nr > 65535 ? 65535 : nr);
-            k_dense_init<SR><<<g1, 256, 0, s>>>(hrows + c0, nr, ncols, flag8, val);
-            if (M) {
-                dim3 g2(runtime().num_sms * 2 / (nr < 8 ? nr : 8) + 1, nr > 65535 ? 65535 : nr);
-                k_dense_mask<<<g2, 256, 0, s>>>(hrows + c0, nr, M->p, M->j, P->mask_comp,
-                                                ncols, flag8);
-            }
+            k_dense_prep<SR><<<g1, 256, 0, s>>>(hrows + c0, nr, ncols, flag8, dval,
+                M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, P->mask_comp, A.p,
+                P->hoff);
             // flat product index of the chunk (the rows' offsets into their
             // entries, then each entry's B-row length scanned), then every
             // product over the grid
-            if (nr <= 1024) {
+            if (nr == 1) {
+                // offsets written by the prep kernel
+            } else if (nr <= 1024) {
                 k_heavy_offsets<<<1, 1024, 0, s>>>(hrows + c0, nr, A.p, P->hoff);
             } else {
                 k_heavy_alen<<<(nr + 255) / 256, 256, 0, s>>>(hrows + c0, nr, A.p, P->hlen);
@@ -1584,12 +1660,12 @@ static void exec_heavy(SaxpyPlan *P, const DevCSR *M, const DevCSR &A, const Dev
                     P->heavy_alen + 1, P->lb_w, s, nullptr, nullptr, P->bins + BIN_HEAVY_ERR);
             k_dense_atomic_flat<SR><<<runtime().num_sms * 32, 256, 0, s>>>(hrows + c0, nr,
                 P->hoff, P->wprefix, A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
-                M != nullptr, P->mask_comp, ncols, flag8, val);
+                M != nullptr, P->mask_comp, ncols, flag8, dval);
             // ordered compaction into the rows' slots
-            const int cblocks = (int)((ncols + DG_CHUNK - 1) / DG_CHUNK);
+            const int cblocks = (int)((ncols + dense_tile<SR>() - 1) / dense_tile<SR>());
             const int64_t ntiles = (int64_t)nr * cblocks;
             k_dense_compact<SR><<<(unsigned)ntiles, DG_THREADS, 0, s>>>(hrows + c0, cblocks,
-                ncols, flag8, val, P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt, ntiles,
+                ncols, flag8, dval, P->slot_off, P->Tj, (Z *)P->Tx, P->row_cnt, ntiles,
                 P->lb_c, P->bins + BIN_HEAVY_ERR);
         }
     } else {
@@ -1715,7 +1791,7 @@ static int saxpy3_row_dense(DevCSR &C, const DevCSR *M, bool mask_comp, const De
     P->heavy_alen = A.nnz;
     P->heavy_chunk = 1;
     P->total_cap = ncols;
-    const int64_t ntiles = (ncols + DG_CHUNK - 1) / DG_CHUNK;
+    const int64_t ntiles = (ncols + dense_tile<SR>() - 1) / dense_tile<SR>();
     // everything in one allocation; the counters, the look-back workspaces,
     // the slot offset, the row count and the row list (row 0) are zero
     Carve cv(s);
@@ -1733,7 +1809,7 @@ static int saxpy3_row_dense(DevCSR &C, const DevCSR *M, bool mask_comp, const De
         P->hw_ws = cv.take<int64_t>(scan_ws_elems(2));
         P->wprefix = cv.take<int64_t>(A.nnz + 1);
         P->flag8 = cv.take<uint8_t>(ncols + 1);
-        P->val = cv.take<Z>(ncols + 1);
+        P->val = cv.take<dense_val_t<SR>>(ncols + 1);
     };
     layout();
     if (!cv.alloc()) return OUT_OF_MEMORY;
