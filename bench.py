@@ -301,9 +301,10 @@ class Saxpy:
         return self.flops / 1e9
 
     def launches_per_step(self):
-        # flop counts, bins, bin fill, numeric, row counts, pack, and the scans
-        # of the slot and row offsets (n + 1 values each)
-        return 6 + 2 * scan_launches(self.n + 1)
+        # flop counts, bins, slot-offset scan, bin fill, the three
+        # shared-memory bin kernels (expand-sort-compress, warp hash, block
+        # hash), the row-offset scan and the pack
+        return 9
 
     def cpu_baseline(self, R, ncores):
         from oracle import csr_digest
@@ -371,10 +372,10 @@ class Bfs:
         self.alg_bytes = 8.0 * self.n + 4.0 * self.S.nnz + 8.0 * self.n
         self.basis = "S read once (offsets and indices), the parent vector written once"
         # DRAM bytes of the traversal's numeric launches (one per level): the
-        # heavy-row kernel, which runs at the three largest levels, read and
-        # wrote 682 MB over a traversal in one ncu capture at this size; the
-        # other levels' kernels move little.  Per numeric launch:
-        self.traffic_per_launch = 682e6 / 6 if self.scale == 22 else None
+        # dense-row product kernel read and wrote 744 MB over a traversal in
+        # one ncu capture at this size (the dense row itself stays in L2);
+        # the other kernels of the level move little.  Per numeric launch:
+        self.traffic_per_launch = 744e6 / 6 if self.scale == 22 else None
 
     def bfs(self, Sg):
         api = self.api
@@ -434,11 +435,14 @@ class Bfs:
         return self.edges
 
     def launches_per_step(self):
-        # per level, the vxm (symbolic phase, flat heavy-row product index and
-        # dense row, compaction, pack: 12 kernels plus scans) and the parent
-        # assign (5 kernels plus two scans): 26 on average (this workload's
-        # launch list counts 157 for the 6-level traversal)
-        return 26 * max(getattr(self, "levels", 1), 1)
+        # levels whose frontier makes the row heavy go straight to the dense
+        # row: prep, product-index scan, products, compaction, row-offset
+        # scan, pack (6); the first and last levels (small frontiers) take
+        # the binned path first: flop counts, bins, slot scan, bin fill,
+        # three bin kernels, row-offset scan, then the dense row (14); each
+        # parent assign but the last level's is one union launch
+        lev = max(getattr(self, "levels", 1), 1)
+        return 2 * 14 + 6 * max(lev - 2, 0) + (lev - 1)
 
     def cpu_baseline(self, R, ncores):
         """The reference's traversal on all cores, timed (median of 3), and

@@ -48,6 +48,7 @@
 #include "../../include/grb_b200.h"
 #include "grb_runtime.h"
 #include "grb_semirings.h"
+#include "grb_lookback.cuh"
 
 namespace grb {
 
@@ -578,42 +579,34 @@ k_ct_plan(const int32_t *__restrict__ gcnt, const unsigned long long *__restrict
     }
     int ib = sb, ih = sh, ic = sc, tb, th, tc;
     ct_block_scan3(ib, ih, ic, tb, th, tc, s_w);
-    if (tid == 0) {
+    if (tid < 32) {
+        // warp 0: post the tile's three sums, then look back over 32
+        // predecessors at a time for each of them
+        const int lane = tid;
         unsigned long long *my = status + tile * 3;
         const unsigned long long agg[3] = {(unsigned long long)tb, (unsigned long long)th,
                                            (unsigned long long)tc};
+        long long ex[3] = {0, 0, 0};
         if (tile == 0) {
-            for (int v = 0; v < 3; v++) atomicExch(&my[v], CT_FLAG_INC | agg[v]);
-            s_ex[0] = s_ex[1] = s_ex[2] = 0;
+            if (lane == 0)
+                for (int v = 0; v < 3; v++) atomicExch(&my[v], CT_FLAG_INC | agg[v]);
         } else {
-            for (int v = 0; v < 3; v++) atomicExch(&my[v], CT_FLAG_AGG | agg[v]);
-            long long ex[3] = {0, 0, 0};
-            for (int v = 0; v < 3; v++) {
-                int64_t p = tile - 1;
-                int spins = 0;
-                while (p >= 0) {
-                    const unsigned long long w =
-                        *reinterpret_cast<volatile unsigned long long *>(&status[p * 3 + v]);
-                    const unsigned long long f = w & ~CT_VAL;
-                    if (f == 0) {
-                        if (++spins > CT_SPIN_LIMIT) { atomicExch(&totals[CT_ERR], 1); break; }
-                        __nanosleep(64);
-                        continue;
-                    }
-                    ex[v] += (long long)(w & CT_VAL);
-                    if (f == CT_FLAG_INC) break;
-                    p--;
-                }
-            }
+            if (lane == 0)
+                for (int v = 0; v < 3; v++) atomicExch(&my[v], CT_FLAG_AGG | agg[v]);
             for (int v = 0; v < 3; v++)
-                atomicExch(&my[v], CT_FLAG_INC |
-                                   ((unsigned long long)(ex[v] + (long long)agg[v]) & CT_VAL));
-            s_ex[0] = ex[0]; s_ex[1] = ex[1]; s_ex[2] = ex[2];
+                ex[v] = lb_lookback(status, tile, lane, (int *)&totals[CT_ERR], 3, v);
+            if (lane == 0)
+                for (int v = 0; v < 3; v++)
+                    atomicExch(&my[v], CT_FLAG_INC |
+                                       ((unsigned long long)(ex[v] + (long long)agg[v]) & CT_VAL));
         }
-        if (tile == ntiles - 1) {
-            totals[CT_N_BM] = (int32_t)(s_ex[0] + tb);
-            totals[CT_N_H] = (int32_t)(s_ex[1] + th);
-            totals[CT_N_BUCKET] = (int32_t)(s_ex[2] + tc);
+        if (lane == 0) {
+            s_ex[0] = ex[0]; s_ex[1] = ex[1]; s_ex[2] = ex[2];
+            if (tile == ntiles - 1) {
+                totals[CT_N_BM] = (int32_t)(ex[0] + tb);
+                totals[CT_N_H] = (int32_t)(ex[1] + th);
+                totals[CT_N_BUCKET] = (int32_t)(ex[2] + tc);
+            }
         }
     }
     __syncthreads();

@@ -34,8 +34,10 @@ inline size_t lb_ws_elems(int64_t n) { return (size_t)((n + LB_TILE - 1) / LB_TI
 // 32 predecessors at once, and once the nearest inclusive prefix in the
 // window and every word above it are posted, adds them; otherwise it moves
 // the window 32 tiles down.  Returns the exclusive prefix (lane 0's value).
+// The words may be interleaved: tile t's word is status[t * stride + v].
 static __device__ __forceinline__ long long lb_lookback(unsigned long long *status,
-                                                       int64_t tile, int lane, int *err)
+                                                       int64_t tile, int lane, int *err,
+                                                       int stride = 1, int v = 0)
 {
     long long ex = 0;
     int64_t hi = tile - 1;
@@ -43,7 +45,8 @@ static __device__ __forceinline__ long long lb_lookback(unsigned long long *stat
     while (true) {
         const int64_t idx = hi - (31 - lane);
         unsigned long long w = LB_INC;
-        if (idx >= 0) w = *reinterpret_cast<volatile unsigned long long *>(&status[idx]);
+        if (idx >= 0)
+            w = *reinterpret_cast<volatile unsigned long long *>(&status[idx * stride + v]);
         const unsigned long long f = w & ~LB_VAL;
         const unsigned inc = __ballot_sync(0xffffffffu, f == LB_INC);
         const unsigned pending = __ballot_sync(0xffffffffu, f == 0);

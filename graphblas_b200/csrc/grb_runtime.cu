@@ -772,7 +772,11 @@ struct LbLoadCounts {
     int64_t n;
     __device__ int64_t operator()(int64_t i) const
     {
-        return (i < n && (!keep || keep[i])) ? (int64_t)cnt[i] : 0;
+        if (i >= n) return 0;
+        // both loads issued before either is used
+        const int32_t c = cnt[i];
+        const int8_t k = keep ? keep[i] : (int8_t)1;
+        return k ? (int64_t)c : 0;
     }
 };
 
