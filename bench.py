@@ -2,7 +2,7 @@
 """Benchmark of the B200 semiring SpGEMM path (SuiteSparse:GraphBLAS GrB_mxm).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config all|tc|saxpy|bfs|batch|serve]
+                    [--config all|tc|saxpy|bfs|bfs_pushpull|batch|serve]
 
 Workloads (seeded synthetic inputs of the graph500 / Erdos-Renyi shapes the
 reference is measured on; no dataset is read):
@@ -18,13 +18,16 @@ reference is measured on; no dataset is read):
   bfs    level-synchronous BFS parents (GrB_vxm any_secondi int64 with a
          complemented structural mask and replace, then GrB_assign) on R-MAT
          scale 22, edge factor 16; metric TEPS (undirected edges / s).
+  bfs_pushpull  the same traversal direction-optimising: levels with a large
+         frontier pull (GrB_mxv max_secondi on S, its own transpose), the
+         others push; the parents are the push-only traversal's, bit for bit.
   batch  4096 independent C_k = A_k*A_k, min_plus fp32, n_k log-uniform in
          [64, 8192], Poisson(6) entries per row; metric GFLOP/s.
   serve  an open-loop Poisson stream (2000 req/s) of mixed requests on
          device-resident graphs; metric req/s with p50/p99 latency.
 
 The default (--config all) prints one line: the tc workload's figures at the
-top level and the other four under "configs", each with its own value, e2e,
+top level and the other five under "configs", each with its own value, e2e,
 roofline, cpu_baseline and parity.
 
 * value: device time with the inputs resident in HBM, CUDA events on the
@@ -478,8 +481,55 @@ class Bfs:
             self.api.free(self.Sg)
 
 
-CONFIGS = {"tc": TriCount, "saxpy": Saxpy, "bfs": Bfs}
-SUB_CONFIGS = ("saxpy", "bfs", "batch", "serve")
+class BfsPushPull(Bfs):
+    """The same traversal, direction-optimising: a level whose frontier holds
+    more than n/32 vertices pulls - GrB_mxv(q, p, MAX_SECONDI, S, q, RSC),
+    S being symmetric its own transpose, each unvisited vertex walking its
+    row from the end to its largest frontier neighbour - and the others push
+    as before.  Both directions pick the largest frontier neighbour, so the
+    parents are those of the push-only traversal, bit for bit."""
+
+    def __init__(self, args):
+        super().__init__(args)
+        self.workload = "bfs_rmat%d_ef16_push_pull_max_secondi" % self.scale
+
+    def bfs(self, Sg):
+        api = self.api
+        n, src = self.n, self.src
+        q = api.vector_from([src], [src], 8, n)
+        p = api.vector_from([src], [src], 8, n)
+        lev = pulls = 0
+        while True:
+            lev += 1
+            if api.vnvals(q) > n // 32:
+                api.mxv(q, p, None, "GxB_MAX_SECONDI_INT64", Sg, q, "GrB_DESC_RSC")
+                pulls += 1
+            else:
+                api.vxm(q, p, None, "GxB_ANY_SECONDI_INT64", q, Sg, "GrB_DESC_RSC")
+            if api.vnvals(q) == 0:
+                break
+            api.assign_all(p, q, None, q, n, "GrB_DESC_S")
+        self.levels, self.pull_levels = lev, pulls
+        return q, p
+
+    def config(self):
+        c = super().config()
+        c["pull_levels"] = int(getattr(self, "pull_levels", -1))
+        return c
+
+    def launches_per_step(self):
+        # a pull level: two bitmap scatters, the row kernel, the flag scan
+        # (multi-launch over n + 1 values) and the compaction; push levels
+        # as in the push-only traversal; one union per parent update
+        lev = max(getattr(self, "levels", 1), 1)
+        pulls = max(getattr(self, "pull_levels", 0), 0)
+        push = lev - pulls
+        return (4 + scan_launches(self.n + 1)) * pulls + 14 * min(push, 2) + \
+            6 * max(push - 2, 0) + (lev - 1)
+
+
+CONFIGS = {"tc": TriCount, "saxpy": Saxpy, "bfs": Bfs, "bfs_pushpull": BfsPushPull}
+SUB_CONFIGS = ("saxpy", "bfs", "bfs_pushpull", "batch", "serve")
 
 # DRAM bytes (read + write) of one triangle-count dot3 call at R-MAT scale 20,
 # summed over its six kernels from one ncu capture of this workload at this

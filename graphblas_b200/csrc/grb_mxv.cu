@@ -6,6 +6,11 @@
 // the reference's sequential dot products (GB_AxB_dot_cij.c:516-652).  The
 // mask m on w is scattered the same way; rows the mask rejects are skipped.
 // Results are compacted into a sorted sparse vector (a 1-by-nrows CSR row).
+//
+// MAX with a multiplier whose value is k (SECONDI, FIRSTJ: the parent in a
+// pull BFS step) is the largest k that matches, so such a row is walked from
+// its end and stops at its first match: an unvisited vertex usually finds a
+// frontier neighbour within its last few entries.
 
 #include "grb_runtime.h"
 #include "grb_semirings.h"
@@ -59,6 +64,29 @@ k_mxv_rows(int64_t m, const int32_t *__restrict__ Ap, const int32_t *__restrict_
         Z acc = Z();
         bool has = false;
         const int32_t lo = Ap[i], hi = Ap[i + 1];
+        if constexpr (SR::add_op == OP_MAX && (SR::mult_op == OP_SECONDI ||
+                                                SR::mult_op == OP_FIRSTJ)) {
+            // the largest matching k: 32 entries at a time from the end
+            for (int32_t c1 = hi; c1 > lo; c1 -= 32) {
+                const int32_t p = c1 - 32 + lane;
+                bool match = false;
+                int32_t k = 0;
+                if (p >= lo) {
+                    k = Aj[p];
+                    match = (ubits[k >> 5] >> (k & 31)) & 1u;
+                }
+                const unsigned mm = __ballot_sync(0xffffffffu, match);
+                if (mm) {
+                    const int b = 31 - __clz(mm);
+                    const int32_t kb = __shfl_sync(0xffffffffu, k, b);
+                    acc = (Z)kb;
+                    has = true;
+                    break;
+                }
+            }
+            if (lane == 0) { wflag[i] = has ? 1 : 0; if (has) wd[i] = acc; }
+            continue;
+        }
         for (int32_t c0 = lo; c0 < hi; c0 += 32) {
             const int32_t p = c0 + lane;
             bool match = false;

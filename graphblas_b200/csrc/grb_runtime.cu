@@ -344,15 +344,20 @@ int dev_upload(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
     A.nrows = nrows; A.ncols = ncols; A.nnz = nnz; A.type = type; A.iso = iso;
     A.nzombies = 0;
     size_t ts = type_size(type);
-    // stage int64 arrays through one device buffer, then narrow on the device
+    // stage int64 arrays through one device buffer (the stream's scratch
+    // buffer when the library owns the stream), then narrow on the device
     int64_t stage_n = (nrows + 1 > nnz) ? nrows + 1 : nnz;
-    int64_t *stage = (int64_t *)dalloc((size_t)stage_n * 8, s);
+    const bool shared = stream_scratch_enabled(s);
+    int64_t *stage = shared ? (int64_t *)stream_scratch(s, (size_t)stage_n * 8, nullptr)
+                            : (int64_t *)dalloc((size_t)stage_n * 8, s);
     A.p = (int32_t *)dalloc((size_t)(nrows + 1) * 4, s);
     A.j = (int32_t *)dalloc((size_t)(nnz ? nnz : 1) * 4, s);
     A.x = nullptr;
     if (x) A.x = dalloc(iso ? ts : (size_t)(nnz ? nnz : 1) * ts, s);
     if (!stage || !A.p || !A.j || (x && !A.x)) {
-        dfree(stage, s); dev_free(A, s); return OUT_OF_MEMORY;
+        if (!shared) dfree(stage, s);
+        dev_free(A, s);
+        return OUT_OF_MEMORY;
     }
     cudaMemcpyAsync(stage, p, (size_t)(nrows + 1) * 8, cudaMemcpyHostToDevice, s);
     k_narrow<<<grid_for(nrows + 1, 256), 256, 0, s>>>(stage, A.p, nrows + 1);
@@ -362,7 +367,7 @@ int dev_upload(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
     }
     if (x) cudaMemcpyAsync(A.x, x, iso ? ts : (size_t)nnz * ts,
                            cudaMemcpyHostToDevice, s);
-    dfree(stage, s);
+    if (!shared) dfree(stage, s);
     return cuda_to_info(cudaGetLastError());
 }
 

@@ -315,3 +315,65 @@ def test_assign_with_its_own_pattern_as_mask(api, oracle, accum, desc):
     assert np.array_equal(gx, want[2]), "values, accum=%s desc=%s" % (accum, desc)
     for v in (w, u):
         api.vfree(v)
+
+
+@pytest.mark.parametrize("nw,nu", [(60000, 50000), (0, 3000), (3000, 0), (1, 1)])
+def test_assign_union_many_tiles(api, oracle, nw, nu):
+    """w<u> = u (structural, no accumulator, no replace) on row vectors is
+    one merge-path union launch over tiles of 2048 merged positions: many
+    tiles with ties across tile boundaries, and empty sides."""
+    n = 200000
+    rng = np.random.default_rng(nw + 7 * nu)
+    wi = np.sort(rng.choice(n, nw, replace=False)).astype(np.int64)
+    # u shares about a third of its indices with w
+    share = wi[rng.random(nw) < (nu / max(nw, 1)) / 3] if nw else np.zeros(0, np.int64)
+    rest = np.setdiff1d(rng.choice(n, nu, replace=False), share)[: max(nu - len(share), 0)]
+    ui = np.sort(np.unique(np.concatenate([share, rest]))).astype(np.int64)
+    wx = rng.integers(-50, 50, len(wi)).astype(np.int64)
+    ux = rng.integers(-50, 50, len(ui)).astype(np.int64)
+    w = api.vector_from(wi, wx, 8, n)
+    u = api.vector_from(ui, ux, 8, n)
+    api.assign_all(w, u, None, u, n, "GrB_DESC_S")
+    gi, gx = api.vector_to(w, 8)
+    p1 = lambda k: np.array([0, k], np.int64)
+    want = oracle.accum_mask(1, n, (p1(len(wi)), wi, wx), (p1(len(ui)), ui, ux), 8,
+                             M=(p1(len(ui)), ui, ux, 8), mask_struct=True)
+    assert np.array_equal(gi, want[1])
+    assert np.array_equal(gx, want[2])
+    for v in (w, u):
+        api.vfree(v)
+
+
+def test_bfs_push_pull_parents_exact(api, oracle):
+    """Direction-optimising BFS on R-MAT scale 18: levels with a large
+    frontier pull (GrB_mxv with S as its own transpose, S symmetric: each
+    unvisited vertex walks its row from the end to its largest frontier
+    neighbour), the others push (GrB_vxm).  MAX_SECONDI makes both
+    directions pick the largest frontier neighbour, the single-threaded
+    reference's ANY rule, so every parent is bit-identical to the push-only
+    traversal's."""
+    S = W.rmat(18, 16, seed=2)
+    n = S.nrows
+    src = int(np.argmax(np.diff(S.p) > 0))
+    A = api.matrix_from_csr(S, 1)
+    q = api.vector_from([src], [src], 8, n)
+    p = api.vector_from([src], [src], 8, n)
+    pulls = 0
+    while True:
+        if api.vnvals(q) > n // 32:
+            api.mxv(q, p, None, "GxB_MAX_SECONDI_INT64", A, q, "GrB_DESC_RSC")
+            pulls += 1
+        else:
+            api.vxm(q, p, None, "GxB_MAX_SECONDI_INT64", q, A, "GrB_DESC_RSC")
+        if api.vnvals(q) == 0:
+            break
+        api.assign_all(p, q, None, q, n, "GrB_DESC_S")
+    idx, par = api.vector_to(p, 8)
+    parent = np.full(n, -1, np.int64)
+    parent[idx] = par
+    want, _ = oracle.bfs(n, S.p, S.i, src)
+    assert pulls >= 1
+    assert np.array_equal(parent, want)
+    for v in (q, p):
+        api.vfree(v)
+    api.free(A)

@@ -189,3 +189,112 @@ def test_saxpy_short_rows_wide_columns(gpu, oracle, add, mult, tname, np_t):
     got = _saxpy_dev(gb, A, B, gb.semiring(add, mult, tname))
     want = oracle.saxpy(m, n, (A.p, A.i, A.x, tc), (B.p, B.i, B.x, tc), add, mult, tc)
     assert_exact(got, want, "wide columns %s_%s" % (add, mult))
+
+
+def _frontier_case(seed, n_front=2000, scale=12):
+    """A one-row product with a large frontier over R-MAT (the direct dense
+    row), its B, and masks: the frontier's visited set and a random plain
+    mask."""
+    S = W.rmat(scale, 16, seed=seed)
+    n = S.nrows
+    rng = np.random.default_rng(seed)
+    front = np.sort(rng.choice(n, n_front, replace=False)).astype(np.int64)
+    visited = np.sort(np.unique(np.concatenate([front, rng.choice(n, n // 3, replace=False)])))
+    plain = np.sort(rng.choice(n, n // 2, replace=False)).astype(np.int64)
+    return S, n, front, visited.astype(np.int64), plain
+
+
+@pytest.mark.parametrize("add,mult,tname,mask", [
+    ("ANY", "SECONDI", "int64", "comp"), ("ANY", "SECONDI", "int64", None),
+    ("ANY", "SECONDI", "int32", "plain"), ("ANY", "FIRSTJ", "int64", "comp"),
+    ("MIN", "PLUS", "fp32", "comp"), ("PLUS", "TIMES", "int64", "plain"),
+    ("ANY", "PAIR", "bool", "comp"), ("MAX", "SECONDI", "int64", None)])
+def test_vxm_large_frontier_dense_row(gpu, oracle, add, mult, tname, mask):
+    """u' (x) S with a large frontier goes straight to the dense row (no
+    symbolic phase); packed state|k words for the max-k ANY semirings, byte
+    flags and values for the others; plain and complemented masks."""
+    gb = gpu
+    S, n, front, visited, plain = _frontier_case(21)
+    tc = gb.TYPES[tname]
+    np_t = {"int64": np.int64, "int32": np.int32, "fp32": np.float32, "bool": np.bool_}[tname]
+    rng = np.random.default_rng(5)
+    ux = (1 + rng.integers(0, 50, len(front))).astype(np_t)
+    sx = (1 + rng.integers(0, 9, S.nnz)).astype(np_t)
+    u = W.Csr(1, n, np.array([0, len(front)], np.int64), front, ux)
+    B = W.Csr(n, n, S.p, S.i, sx)
+    M = None
+    if mask == "comp":
+        M = W.Csr(1, n, np.array([0, len(visited)], np.int64), visited)
+    elif mask == "plain":
+        M = W.Csr(1, n, np.array([0, len(plain)], np.int64), plain)
+    got = _saxpy_dev(gb, u, B, gb.semiring(add, mult, tname), M=M,
+                     mask_comp=(mask == "comp"), type_name=tname)
+    want = oracle.saxpy(1, n, (u.p, u.i, u.x, tc), (B.p, B.i, B.x, tc), add, mult, tc,
+                        M=None if M is None else (M.p, M.i, None, 1),
+                        mask_comp=(mask == "comp"))
+    assert_exact(got, want, "dense row %s_%s_%s mask=%s" % (add, mult, tname, mask))
+
+
+def test_saxpy_slots_overflow_on_caller_stream(gpu, oracle):
+    """On a caller's stream the slots are the call's own buffer, first sized
+    from B's mean row length: rows that all hit one long row of B need far
+    more, so the bins run again with the buffer grown, and the result is
+    unchanged."""
+    import torch
+    gb = gpu
+    L = gb.lib()
+    n = 20001
+    rng = np.random.default_rng(4)
+    bp = np.zeros(n + 1, np.int64)
+    bp[1:] = 20000                         # row 0 holds columns 1..20000
+    bi = np.arange(1, 20001, dtype=np.int64)
+    B = W.Csr(n, n, bp, bi, rng.random(20000))
+    m = 200
+    A = W.Csr(m, n, np.arange(m + 1, dtype=np.int64), np.zeros(m, np.int64),
+              1.0 + rng.random(m))
+    st = torch.cuda.Stream()
+    L.grb_b200_set_stream(ctypes_void(st.cuda_stream))
+    try:
+        got = _saxpy_dev(gb, A, B, gb.semiring("PLUS", "TIMES", "fp64"))
+    finally:
+        L.grb_b200_set_stream(None)
+    want = oracle.saxpy(m, n, (A.p, A.i, A.x, 11), (B.p, B.i, B.x, 11), "PLUS", "TIMES", 11)
+    assert_exact(got, want, "slots grown on a caller stream")
+    # the same on the library's own stream, then a small product after it
+    got = _saxpy_dev(gb, A, B, gb.semiring("PLUS", "TIMES", "fp64"))
+    assert_exact(got, want, "slots on the library stream")
+    A2 = random_csr(30, n, 0.001, 9)
+    got = _saxpy_dev(gb, A2, B, gb.semiring("PLUS", "TIMES", "fp64"))
+    want = oracle.saxpy(30, n, (A2.p, A2.i, A2.x, 11), (B.p, B.i, B.x, 11), "PLUS",
+                        "TIMES", 11)
+    assert_exact(got, want, "small product after a large one")
+
+
+def ctypes_void(ptr):
+    import ctypes
+    return ctypes.c_void_p(ptr)
+
+
+@pytest.mark.parametrize("add,mult,tname", [("PLUS", "TIMES", "int64"),
+                                            ("ANY", "SECONDI", "int64")])
+def test_saxpy_many_heavy_rows(gpu, oracle, add, mult, tname):
+    """More than 1024 heavy rows in one product: their offsets into the flat
+    product index take the multi-launch path, and the rows share the
+    grid-wide compaction."""
+    gb = gpu
+    tc = gb.TYPES[tname]
+    m, k, n = 1500, 200, 5000
+    rng = np.random.default_rng(8)
+    A = W.Csr(m, k, np.arange(0, (m + 1) * k, k, dtype=np.int64),
+              np.tile(np.arange(k, dtype=np.int64), m),
+              rng.integers(1, 5, m * k).astype(np.int64))
+    bp, bi = [0], []
+    for _ in range(k):
+        c = np.sort(rng.choice(n, 100, replace=False))
+        bi.append(c)
+        bp.append(bp[-1] + 100)
+    B = W.Csr(k, n, np.array(bp, np.int64), np.concatenate(bi).astype(np.int64),
+              rng.integers(1, 5, 100 * k).astype(np.int64))
+    got = _saxpy_dev(gb, A, B, gb.semiring(add, mult, tname))
+    want = oracle.saxpy(m, n, (A.p, A.i, A.x, tc), (B.p, B.i, B.x, tc), add, mult, tc)
+    assert_exact(got, want, "many heavy rows %s_%s" % (add, mult))
