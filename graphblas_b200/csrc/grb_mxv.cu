@@ -5,39 +5,59 @@
 // present k in ascending k (ballot order), so floating PLUS is bit-exact with
 // the reference's sequential dot products (GB_AxB_dot_cij.c:516-652).  The
 // mask m on w is scattered the same way; rows the mask rejects are skipped.
-// Results are compacted into a sorted sparse vector (a 1-by-nrows CSR row).
+// Results are compacted into a sorted sparse vector (a 1-by-nrows CSR row)
+// with one host read per call.
 //
 // MAX with a multiplier whose value is k (SECONDI, FIRSTJ: the parent in a
 // pull BFS step) is the largest k that matches, so such a row is walked from
 // its end and stops at its first match: an unvisited vertex usually finds a
-// frontier neighbour within its last few entries.
+// frontier neighbour within its last few entries.  Those rows are taken one
+// per lane (most rows of a graph are short), and a row longer than
+// MAXK_SHORT by the whole warp, 32 entries a step.
 
 #include "grb_runtime.h"
 #include "grb_semirings.h"
+#include "grb_lookback.cuh"
 
 namespace grb {
+
+// set bit k of `bits` for the indices of a sorted list (zombies, k < 0,
+// skipped): the lanes of a warp that fall in the same 32-bit word combine
+// their bits first, so a word takes one atomic per warp
+__device__ __forceinline__ void warp_set_bit(uint32_t *__restrict__ bits, int32_t k, bool on)
+{
+    const unsigned act = __ballot_sync(0xffffffffu, on);
+    if (!on) return;
+    const int32_t word = k >> 5;
+    const unsigned same = __match_any_sync(act, word);
+    const unsigned v = __reduce_or_sync(same, 1u << (k & 31));
+    if ((int)(__ffs(same) - 1) == (int)(threadIdx.x & 31)) atomicOr(&bits[word], v);
+}
 
 template <typename Z>
 __global__ void k_scatter_vec(const int32_t *__restrict__ uj, const Z *__restrict__ ux,
                               bool iso, int64_t nu, Z *__restrict__ dense,
                               uint32_t *__restrict__ bits)
 {
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nu;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t k = uj[e];
-        if (k < 0) continue;
-        dense[k] = ux[iso ? 0 : e];
-        atomicOr(&bits[k >> 5], 1u << (k & 31));
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); e0 < nu;
+         e0 += stride) {
+        const int64_t e = e0 + (threadIdx.x & 31);
+        const int32_t k = e < nu ? uj[e] : -1;
+        if (k >= 0) dense[k] = ux[iso ? 0 : e];
+        warp_set_bit(bits, k, k >= 0);
     }
 }
 
 __global__ void k_scatter_bits(const int32_t *__restrict__ mj, int64_t nm,
                                uint32_t *__restrict__ bits)
 {
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nm;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t k = mj[e];
-        if (k >= 0) atomicOr(&bits[k >> 5], 1u << (k & 31));
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); e0 < nm;
+         e0 += stride) {
+        const int64_t e = e0 + (threadIdx.x & 31);
+        const int32_t k = e < nm ? mj[e] : -1;
+        warp_set_bit(bits, k, k >= 0);
     }
 }
 
@@ -64,29 +84,6 @@ k_mxv_rows(int64_t m, const int32_t *__restrict__ Ap, const int32_t *__restrict_
         Z acc = Z();
         bool has = false;
         const int32_t lo = Ap[i], hi = Ap[i + 1];
-        if constexpr (SR::add_op == OP_MAX && (SR::mult_op == OP_SECONDI ||
-                                                SR::mult_op == OP_FIRSTJ)) {
-            // the largest matching k: 32 entries at a time from the end
-            for (int32_t c1 = hi; c1 > lo; c1 -= 32) {
-                const int32_t p = c1 - 32 + lane;
-                bool match = false;
-                int32_t k = 0;
-                if (p >= lo) {
-                    k = Aj[p];
-                    match = (ubits[k >> 5] >> (k & 31)) & 1u;
-                }
-                const unsigned mm = __ballot_sync(0xffffffffu, match);
-                if (mm) {
-                    const int b = 31 - __clz(mm);
-                    const int32_t kb = __shfl_sync(0xffffffffu, k, b);
-                    acc = (Z)kb;
-                    has = true;
-                    break;
-                }
-            }
-            if (lane == 0) { wflag[i] = has ? 1 : 0; if (has) wd[i] = acc; }
-            continue;
-        }
         for (int32_t c0 = lo; c0 < hi; c0 += 32) {
             const int32_t p = c0 + lane;
             bool match = false;
@@ -116,16 +113,104 @@ k_mxv_rows(int64_t m, const int32_t *__restrict__ Ap, const int32_t *__restrict_
     }
 }
 
+static constexpr int MAXK_SHORT = 64;
+
+template <class SR>
+__global__ void __launch_bounds__(256)
+k_mxv_rows_maxk(int64_t m, const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+                const uint32_t *__restrict__ ubits, const uint32_t *__restrict__ mbits,
+                bool has_mask, bool comp, typename SR::z_t *__restrict__ wd,
+                int32_t *__restrict__ wflag)
+{
+    using Z = typename SR::z_t;
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < m;
+         base += nw * 32) {
+        const int64_t i = base + lane;
+        bool ok = i < m;
+        if (ok) {
+            if (has_mask) {
+                const bool present = (mbits[i >> 5] >> (i & 31)) & 1u;
+                ok = comp ? !present : present;
+            } else if (comp) {
+                ok = false;
+            }
+        }
+        int32_t lo = 0, hi = 0;
+        if (ok) { lo = Ap[i]; hi = Ap[i + 1]; }
+        const bool lng = ok && hi - lo > MAXK_SHORT;
+        bool found = false;
+        int32_t kf = 0;
+        if (ok && !lng) {
+            // four entries a step, from the end
+            for (int32_t p = hi; p > lo && !found; p -= 4) {
+                int32_t k[4];
+                bool hit[4];
+                #pragma unroll
+                for (int t = 0; t < 4; t++) {
+                    const int32_t q = p - 1 - t;
+                    k[t] = q >= lo ? Aj[q] : 0;
+                    hit[t] = q >= lo && ((ubits[k[t] >> 5] >> (k[t] & 31)) & 1u);
+                }
+                // the largest match is the one nearest the end (smallest t)
+                #pragma unroll
+                for (int t = 3; t >= 0; t--)
+                    if (hit[t]) { found = true; kf = k[t]; }
+            }
+        }
+        // long rows: the whole warp, one row at a time
+        unsigned lm = __ballot_sync(0xffffffffu, lng);
+        while (lm) {
+            const int b = __ffs(lm) - 1;
+            lm &= lm - 1;
+            const int32_t blo = __shfl_sync(0xffffffffu, lo, b);
+            const int32_t bhi = __shfl_sync(0xffffffffu, hi, b);
+            bool bf = false;
+            int32_t bk = 0;
+            for (int32_t c1 = bhi; c1 > blo; c1 -= 32) {
+                const int32_t q = c1 - 32 + lane;
+                int32_t k = 0;
+                bool match = false;
+                if (q >= blo) {
+                    k = Aj[q];
+                    match = (ubits[k >> 5] >> (k & 31)) & 1u;
+                }
+                const unsigned mm = __ballot_sync(0xffffffffu, match);
+                if (mm) {
+                    bk = __shfl_sync(0xffffffffu, k, 31 - __clz(mm));
+                    bf = true;
+                    break;
+                }
+            }
+            if (lane == b) { found = bf; kf = bk; }
+        }
+        if (i < m) {
+            wflag[i] = found ? 1 : 0;
+            if (found) wd[i] = (Z)kf;
+        }
+    }
+}
+
 template <typename Z>
 __global__ void k_compact_dense(int64_t m, const int32_t *__restrict__ flag,
                                 const int64_t *__restrict__ pos, const Z *__restrict__ wd,
-                                int32_t *__restrict__ wj, Z *__restrict__ wx)
+                                int32_t *__restrict__ wp, int32_t *__restrict__ wj,
+                                Z *__restrict__ wx)
 {
+    if (blockIdx.x == 0 && threadIdx.x == 0) { wp[0] = 0; wp[1] = (int32_t)pos[m]; }
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
          i += (int64_t)gridDim.x * blockDim.x) {
         if (flag[i]) { wj[pos[i]] = (int32_t)i; wx[pos[i]] = wd[i]; }
     }
 }
+
+// value i of the output-position scan: the row's flag (0 or 1)
+struct MxvLoadFlag {
+    const int32_t *flag;
+    int64_t m;
+    __device__ int64_t operator()(int64_t i) const { return i < m ? flag[i] : 0; }
+};
 
 static inline int grid_v(int64_t n, int threads = 256)
 {
@@ -135,47 +220,75 @@ static inline int grid_v(int64_t n, int threads = 256)
     return b < 1 ? 1 : (int)b;
 }
 
+// One host read per call: the scratch in one block (the stream's scratch
+// buffer when the library owns the stream; the totals, the two bitmaps and
+// the scan's workspace adjacent, cleared by one memset), the output
+// positions by a single-launch scan, then the result at its exact size.
 template <class SR>
 static int mxv_t(DevCSR &w, const DevCSR *mask, bool comp, const DevCSR &A,
                  const DevCSR &u, cudaStream_t s)
 {
     using Z = typename SR::z_t;
     const int64_t m = A.nrows, n = A.ncols;
-    Scratch ws(s);
-    Z *ud = ws.get<Z>(n + 1);
-    uint32_t *ubits = ws.get<uint32_t>(n / 32 + 2);
-    uint32_t *mbits = ws.get<uint32_t>(m / 32 + 2);
-    Z *wd = ws.get<Z>(m + 1);
-    int32_t *wflag = ws.get<int32_t>(m + 1);
-    int64_t *pos = ws.get<int64_t>(m + 1);
-    if (ws.failed) return OUT_OF_MEMORY;
-    cudaMemsetAsync(ubits, 0, (size_t)(n / 32 + 2) * 4, s);
-    cudaMemsetAsync(mbits, 0, (size_t)(m / 32 + 2) * 4, s);
+    Carve cv(s);
+    uint32_t *ubits = nullptr, *mbits = nullptr;
+    unsigned long long *lbws = nullptr;
+    int64_t *tot = nullptr, *pos = nullptr;
+    Z *ud = nullptr, *wd = nullptr;
+    int32_t *wflag = nullptr;
+    auto layout = [&]() {
+        tot = cv.take<int64_t>(2);
+        ubits = cv.take<uint32_t>(n / 32 + 2);
+        mbits = cv.take<uint32_t>(m / 32 + 2);
+        lbws = cv.take<unsigned long long>(lb_ws_elems(m + 1));
+        ud = cv.take<Z>(n + 1);
+        wd = cv.take<Z>(m + 1);
+        wflag = cv.take<int32_t>(m + 1);
+        pos = cv.take<int64_t>(m + 1);
+    };
+    layout();
+    const bool shared = stream_scratch_enabled(s);
+    if (shared) {
+        cv.base = (char *)stream_scratch(s, cv.off + 256, nullptr);
+        cv.off = 0;
+        if (!cv.base) return OUT_OF_MEMORY;
+    } else if (!cv.alloc()) {
+        return OUT_OF_MEMORY;
+    }
+    layout();
+    struct Release { Carve &c; bool own; ~Release() { if (own) dfree(c.base, c.s); } }
+        release{cv, !shared};
+    cudaMemsetAsync(tot, 0, (size_t)((char *)(lbws + lb_ws_elems(m + 1)) - (char *)tot), s);
     if (u.nnz > 0)
         k_scatter_vec<Z><<<grid_v(u.nnz), 256, 0, s>>>(u.j, (const Z *)u.x, u.iso, u.nnz,
                                                        ud, ubits);
     if (mask && mask->nnz > 0)
         k_scatter_bits<<<grid_v(mask->nnz), 256, 0, s>>>(mask->j, mask->nnz, mbits);
     const int ps = prof_begin("mxv", s);
-    if (m > 0)
+    constexpr bool maxk = SR::add_op == OP_MAX &&
+                          (SR::mult_op == OP_SECONDI || SR::mult_op == OP_FIRSTJ);
+    if (m > 0 && maxk)
+        k_mxv_rows_maxk<SR><<<grid_v(m), 256, 0, s>>>(m, A.p, A.j, ubits, mbits,
+            mask != nullptr, comp, wd, wflag);
+    else if (m > 0)
         k_mxv_rows<SR><<<grid_v(m * 32), 256, 0, s>>>(m, A.p, A.j, A.x, A.iso, ud, ubits,
             mbits, mask != nullptr, comp, wd, wflag);
     prof_end(ps, s);
-    cudaMemsetAsync(wflag + m, 0, 4, s);
-    int info = scan_exclusive_i32_to_i64(wflag, pos, m + 1, s);
-    if (info != SUCCESS) return info;
-    int64_t nw = 0;
-    cudaError_t e = readback(&nw, pos + m, 8, s);
+    // tot[0]: the result's size; tot[1]: the scan's error word
+    lb_scan(MxvLoadFlag{wflag, m}, pos, m + 1, lbws, s, tot, nullptr, (int *)(tot + 1));
+    int64_t hv[2] = {0, 0};
+    cudaError_t e = readback(hv, tot, 16, s);
     if (e != cudaSuccess) return cuda_to_info(e);
+    if ((int)hv[1]) return PANIC;
+    const int64_t nw = hv[0];
     w = DevCSR();
-    w.nrows = 1; w.ncols = m; w.nnz = nw; w.iso = false;
+    w.nrows = 1; w.ncols = m; w.iso = false; w.nnz = nw;
     w.p = (int32_t *)dalloc(8, s);
     w.j = (int32_t *)dalloc((size_t)(nw ? nw : 1) * 4, s);
     w.x = dalloc((size_t)(nw ? nw : 1) * sizeof(Z), s);
     if (!w.p || !w.j || !w.x) { dev_free(w, s); return OUT_OF_MEMORY; }
-    int32_t hp[2] = {0, (int32_t)nw};
-    cudaMemcpyAsync(w.p, hp, 8, cudaMemcpyHostToDevice, s);
-    if (m > 0) k_compact_dense<Z><<<grid_v(m), 256, 0, s>>>(m, wflag, pos, wd, w.j, (Z *)w.x);
+    k_compact_dense<Z><<<grid_v(m > 0 ? m : 1), 256, 0, s>>>(m, wflag, pos, wd, w.p, w.j,
+                                                             (Z *)w.x);
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) { dev_free(w, s); return cuda_to_info(e); }
     return SUCCESS;
