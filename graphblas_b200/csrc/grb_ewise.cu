@@ -179,7 +179,7 @@ static inline int grid_n(int64_t n, int threads = 256)
 // shared memory by consecutive threads.
 // ---------------------------------------------------------------------------
 
-static constexpr int UN_THREADS = 256, UN_ITEMS = 8, UN_TILE = UN_THREADS * UN_ITEMS;
+static constexpr int UN_THREADS = 256, UN_ITEMS = 12, UN_TILE = UN_THREADS * UN_ITEMS;
 
 // T before C on equal keys: C[i-1] precedes T[d-i] iff C[i-1] < T[d-i].
 // The number of C entries among the first d merged positions: the largest

@@ -67,7 +67,7 @@ k_mxv_rows(int64_t m, const int32_t *__restrict__ Ap, const int32_t *__restrict_
            const void *__restrict__ Ax, bool a_iso,
            const typename SR::z_t *__restrict__ ud, const uint32_t *__restrict__ ubits,
            const uint32_t *__restrict__ mbits, bool has_mask, bool comp,
-           typename SR::z_t *__restrict__ wd, int32_t *__restrict__ wflag)
+           typename SR::z_t *__restrict__ wd, uint32_t *__restrict__ gbits)
 {
     using Z = typename SR::z_t;
     const int lane = threadIdx.x & 31;
@@ -80,7 +80,7 @@ k_mxv_rows(int64_t m, const int32_t *__restrict__ Ap, const int32_t *__restrict_
         } else if (comp) {
             ok = false;
         }
-        if (!ok) { if (lane == 0) wflag[i] = 0; continue; }
+        if (!ok) continue;
         Z acc = Z();
         bool has = false;
         const int32_t lo = Ap[i], hi = Ap[i + 1];
@@ -109,7 +109,10 @@ k_mxv_rows(int64_t m, const int32_t *__restrict__ Ap, const int32_t *__restrict_
             }
             if (SR::M::any && has) break;
         }
-        if (lane == 0) { wflag[i] = has ? 1 : 0; if (has) wd[i] = acc; }
+        if (lane == 0 && has) {
+            wd[i] = acc;
+            atomicOr(&gbits[i >> 5], 1u << (i & 31));
+        }
     }
 }
 
@@ -120,7 +123,7 @@ __global__ void __launch_bounds__(256)
 k_mxv_rows_maxk(int64_t m, const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
                 const uint32_t *__restrict__ ubits, const uint32_t *__restrict__ mbits,
                 bool has_mask, bool comp, typename SR::z_t *__restrict__ wd,
-                int32_t *__restrict__ wflag)
+                uint32_t *__restrict__ gbits)
 {
     using Z = typename SR::z_t;
     const int lane = threadIdx.x & 31;
@@ -185,31 +188,40 @@ k_mxv_rows_maxk(int64_t m, const int32_t *__restrict__ Ap, const int32_t *__rest
             }
             if (lane == b) { found = bf; kf = bk; }
         }
-        if (i < m) {
-            wflag[i] = found ? 1 : 0;
-            if (found) wd[i] = (Z)kf;
+        if (found) wd[i] = (Z)kf;
+        // the warp owns the 32 rows of its group: their bits in one word
+        const unsigned fb = __ballot_sync(0xffffffffu, found);
+        if (lane == 0) gbits[base >> 5] = fb;
+    }
+}
+
+// rows with a result are marked in gbits (bit i & 31 of word i >> 5); gpos[g]
+// is the number of marked rows before group g
+template <typename Z>
+__global__ void k_compact_dense(int64_t m, const uint32_t *__restrict__ gbits,
+                                const int64_t *__restrict__ gpos, const Z *__restrict__ wd,
+                                int32_t *__restrict__ wp, int32_t *__restrict__ wj,
+                                Z *__restrict__ wx)
+{
+    const int64_t ng = (m + 31) / 32;
+    if (blockIdx.x == 0 && threadIdx.x == 0) { wp[0] = 0; wp[1] = (int32_t)gpos[ng]; }
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = gbits[i >> 5];
+        const int r = (int)(i & 31);
+        if ((b >> r) & 1u) {
+            const int64_t q = gpos[i >> 5] + __popc(b & ((1u << r) - 1u));
+            wj[q] = (int32_t)i;
+            wx[q] = wd[i];
         }
     }
 }
 
-template <typename Z>
-__global__ void k_compact_dense(int64_t m, const int32_t *__restrict__ flag,
-                                const int64_t *__restrict__ pos, const Z *__restrict__ wd,
-                                int32_t *__restrict__ wp, int32_t *__restrict__ wj,
-                                Z *__restrict__ wx)
-{
-    if (blockIdx.x == 0 && threadIdx.x == 0) { wp[0] = 0; wp[1] = (int32_t)pos[m]; }
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        if (flag[i]) { wj[pos[i]] = (int32_t)i; wx[pos[i]] = wd[i]; }
-    }
-}
-
-// value i of the output-position scan: the row's flag (0 or 1)
-struct MxvLoadFlag {
-    const int32_t *flag;
-    int64_t m;
-    __device__ int64_t operator()(int64_t i) const { return i < m ? flag[i] : 0; }
+// value g of the output-position scan: the marked rows of group g
+struct MxvLoadGroup {
+    const uint32_t *gbits;
+    int64_t ng;
+    __device__ int64_t operator()(int64_t g) const { return g < ng ? __popc(gbits[g]) : 0; }
 };
 
 static inline int grid_v(int64_t n, int threads = 256)
@@ -233,18 +245,19 @@ static int mxv_t(DevCSR &w, const DevCSR *mask, bool comp, const DevCSR &A,
     Carve cv(s);
     uint32_t *ubits = nullptr, *mbits = nullptr;
     unsigned long long *lbws = nullptr;
+    const int64_t ng = (m + 31) / 32;
     int64_t *tot = nullptr, *pos = nullptr;
     Z *ud = nullptr, *wd = nullptr;
-    int32_t *wflag = nullptr;
+    uint32_t *gbits = nullptr;
     auto layout = [&]() {
         tot = cv.take<int64_t>(2);
         ubits = cv.take<uint32_t>(n / 32 + 2);
         mbits = cv.take<uint32_t>(m / 32 + 2);
-        lbws = cv.take<unsigned long long>(lb_ws_elems(m + 1));
+        gbits = cv.take<uint32_t>(ng + 1);
+        lbws = cv.take<unsigned long long>(lb_ws_elems(ng + 1));
         ud = cv.take<Z>(n + 1);
         wd = cv.take<Z>(m + 1);
-        wflag = cv.take<int32_t>(m + 1);
-        pos = cv.take<int64_t>(m + 1);
+        pos = cv.take<int64_t>(ng + 1);
     };
     layout();
     const bool shared = stream_scratch_enabled(s);
@@ -258,7 +271,7 @@ static int mxv_t(DevCSR &w, const DevCSR *mask, bool comp, const DevCSR &A,
     layout();
     struct Release { Carve &c; bool own; ~Release() { if (own) dfree(c.base, c.s); } }
         release{cv, !shared};
-    cudaMemsetAsync(tot, 0, (size_t)((char *)(lbws + lb_ws_elems(m + 1)) - (char *)tot), s);
+    cudaMemsetAsync(tot, 0, (size_t)((char *)(lbws + lb_ws_elems(ng + 1)) - (char *)tot), s);
     if (u.nnz > 0)
         k_scatter_vec<Z><<<grid_v(u.nnz), 256, 0, s>>>(u.j, (const Z *)u.x, u.iso, u.nnz,
                                                        ud, ubits);
@@ -269,13 +282,13 @@ static int mxv_t(DevCSR &w, const DevCSR *mask, bool comp, const DevCSR &A,
                           (SR::mult_op == OP_SECONDI || SR::mult_op == OP_FIRSTJ);
     if (m > 0 && maxk)
         k_mxv_rows_maxk<SR><<<grid_v(m), 256, 0, s>>>(m, A.p, A.j, ubits, mbits,
-            mask != nullptr, comp, wd, wflag);
+            mask != nullptr, comp, wd, gbits);
     else if (m > 0)
         k_mxv_rows<SR><<<grid_v(m * 32), 256, 0, s>>>(m, A.p, A.j, A.x, A.iso, ud, ubits,
-            mbits, mask != nullptr, comp, wd, wflag);
+            mbits, mask != nullptr, comp, wd, gbits);
     prof_end(ps, s);
     // tot[0]: the result's size; tot[1]: the scan's error word
-    lb_scan(MxvLoadFlag{wflag, m}, pos, m + 1, lbws, s, tot, nullptr, (int *)(tot + 1));
+    lb_scan(MxvLoadGroup{gbits, ng}, pos, ng + 1, lbws, s, tot, nullptr, (int *)(tot + 1));
     int64_t hv[2] = {0, 0};
     cudaError_t e = readback(hv, tot, 16, s);
     if (e != cudaSuccess) return cuda_to_info(e);
@@ -287,7 +300,7 @@ static int mxv_t(DevCSR &w, const DevCSR *mask, bool comp, const DevCSR &A,
     w.j = (int32_t *)dalloc((size_t)(nw ? nw : 1) * 4, s);
     w.x = dalloc((size_t)(nw ? nw : 1) * sizeof(Z), s);
     if (!w.p || !w.j || !w.x) { dev_free(w, s); return OUT_OF_MEMORY; }
-    k_compact_dense<Z><<<grid_v(m > 0 ? m : 1), 256, 0, s>>>(m, wflag, pos, wd, w.p, w.j,
+    k_compact_dense<Z><<<grid_v(m > 0 ? m : 1), 256, 0, s>>>(m, gbits, pos, wd, w.p, w.j,
                                                              (Z *)w.x);
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) { dev_free(w, s); return cuda_to_info(e); }

@@ -320,7 +320,7 @@ def test_assign_with_its_own_pattern_as_mask(api, oracle, accum, desc):
 @pytest.mark.parametrize("nw,nu", [(60000, 50000), (0, 3000), (3000, 0), (1, 1)])
 def test_assign_union_many_tiles(api, oracle, nw, nu):
     """w<u> = u (structural, no accumulator, no replace) on row vectors is
-    one merge-path union launch over tiles of 2048 merged positions: many
+    one merge-path union launch over tiles of 3072 merged positions: many
     tiles with ties across tile boundaries, and empty sides."""
     n = 200000
     rng = np.random.default_rng(nw + 7 * nu)
