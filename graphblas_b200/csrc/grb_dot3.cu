@@ -1160,9 +1160,11 @@ static int dot3_count_launch(DevCSR &C, const DevCSR &M, bool mask_struct, const
         mq = cv.take<D3Work>(spans_fit ? 1 : mnz);
     };
     layout();
-    const bool got = cv.alloc();
+    CallBlock blk(s);
+    const bool got = blk.get(cv.off);
+    cv.base = blk.base;
+    cv.off = 0;
     layout();
-    struct Release { Carve &c; ~Release() { dfree(c.base, c.s); } } release{cv};
     if (!C.p || !C.j || !C.x || !got) { dev_free(C, s); return OUT_OF_MEMORY; }
     cudaMemcpyAsync(C.p, M.p, (size_t)(M.nrows + 1) * 4, cudaMemcpyDeviceToDevice, s);
     cudaMemsetAsync(counter, 0, (size_t)((const char *)(gcnt + 2 * nkeys) - (const char *)counter),
@@ -1231,9 +1233,11 @@ static int dot3_launch(DevCSR &C, const DevCSR &M, bool mask_struct,
         queue = cv.take<D3Work>(mnz ? mnz : 1);
     };
     layout();
-    const bool got = cv.alloc();
+    CallBlock blk(s);
+    const bool got = blk.get(cv.off);
+    cv.base = blk.base;
+    cv.off = 0;
     layout();
-    struct Release { Carve &c; ~Release() { dfree(c.base, c.s); } } release{cv};
     if (!C.p || !C.j || !C.x || !got) {
         dev_free(C, s); return OUT_OF_MEMORY;
     }

@@ -260,17 +260,11 @@ static int mxv_t(DevCSR &w, const DevCSR *mask, bool comp, const DevCSR &A,
         pos = cv.take<int64_t>(ng + 1);
     };
     layout();
-    const bool shared = stream_scratch_enabled(s);
-    if (shared) {
-        cv.base = (char *)stream_scratch(s, cv.off + 256, nullptr);
-        cv.off = 0;
-        if (!cv.base) return OUT_OF_MEMORY;
-    } else if (!cv.alloc()) {
-        return OUT_OF_MEMORY;
-    }
+    CallBlock blk(s);
+    if (!blk.get(cv.off)) return OUT_OF_MEMORY;
+    cv.base = blk.base;
+    cv.off = 0;
     layout();
-    struct Release { Carve &c; bool own; ~Release() { if (own) dfree(c.base, c.s); } }
-        release{cv, !shared};
     cudaMemsetAsync(tot, 0, (size_t)((char *)(lbws + lb_ws_elems(ng + 1)) - (char *)tot), s);
     if (u.nnz > 0)
         k_scatter_vec<Z><<<grid_v(u.nnz), 256, 0, s>>>(u.j, (const Z *)u.x, u.iso, u.nnz,

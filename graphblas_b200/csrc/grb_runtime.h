@@ -102,6 +102,29 @@ struct Carve {
     }
 };
 
+// A call's scratch block: the stream's scratch buffer when the library owns
+// the stream (kept between calls, so a call of the same size allocates
+// nothing), else an allocation for this call, released with the block.
+struct CallBlock {
+    cudaStream_t s;
+    char *base = nullptr;
+    bool own = false;
+    explicit CallBlock(cudaStream_t st) : s(st) {}
+    bool get(size_t bytes)
+    {
+        if (bytes == 0) bytes = 16;
+        if (stream_scratch_enabled(s)) {
+            base = (char *)stream_scratch(s, bytes, nullptr);
+            own = false;
+        } else {
+            base = (char *)dalloc(bytes, s);
+            own = true;
+        }
+        return base != nullptr;
+    }
+    ~CallBlock() { if (own) dfree(base, s); }
+};
+
 // scratch buffers that live for one call on one stream
 struct Scratch {
     cudaStream_t s;
