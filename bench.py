@@ -489,9 +489,22 @@ class BfsPushPull(Bfs):
     as before.  Both directions pick the largest frontier neighbour, so the
     parents are those of the push-only traversal, bit for bit."""
 
+    # the roofline covers the whole traversal (pull and push levels): the
+    # traversal's algorithmic bytes over its device time
+    kernel = "bfs_traversal"
+
     def __init__(self, args):
         super().__init__(args)
         self.workload = "bfs_rmat%d_ef16_push_pull_max_secondi" % self.scale
+
+    def dev_setup(self, gb):
+        super().dev_setup(gb)
+        self.basis = ("S read once (offsets and indices), the parent vector written once, "
+                      "over the whole traversal's device time")
+        self.traffic_per_launch = None
+
+    def finish(self, ms_per_step):
+        self.kernel_ms_override = ms_per_step
 
     def bfs(self, Sg):
         api = self.api
