@@ -393,13 +393,14 @@ __global__ void k_narrow_check(const int64_t *__restrict__ in, int32_t *__restri
 }
 
 // bit p[r] of `starts` marks the first entry of every non-empty row r
-__global__ void k_row_starts(const int32_t *__restrict__ Ap, int64_t nrows,
+__global__ void k_row_starts(const int32_t *__restrict__ Ap, int64_t nrows, int64_t nnz,
                              unsigned *__restrict__ starts)
 {
     for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrows;
          r += (int64_t)gridDim.x * blockDim.x) {
         const int32_t q = Ap[r];
-        if (q < Ap[r + 1]) atomicOr(&starts[q >> 5], 1u << (q & 31));
+        // offsets not yet known to be valid stay inside the bitmap
+        if (q >= 0 && q < Ap[r + 1] && q < nnz) atomicOr(&starts[q >> 5], 1u << (q & 31));
     }
 }
 
@@ -422,7 +423,7 @@ static void check_rows(const DevCSR &A, unsigned *starts, unsigned *flag, unsign
                        cudaStream_t s)
 {
     cudaMemsetAsync(starts, 0, (size_t)((A.nnz + 31) / 32) * 4, s);
-    k_row_starts<<<grid_for(A.nrows, 256), 256, 0, s>>>(A.p, A.nrows, starts);
+    k_row_starts<<<grid_for(A.nrows, 256), 256, 0, s>>>(A.p, A.nrows, A.nnz, starts);
     k_check_rows<<<grid_for(A.nnz, 256), 256, 0, s>>>(A.j, A.nnz, starts, flag, bit);
 }
 
