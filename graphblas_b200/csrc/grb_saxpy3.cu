@@ -1195,10 +1195,12 @@ template <typename Z>
 __global__ void __launch_bounds__(256)
 k_pack(int64_t nrows, int span, const int64_t *__restrict__ slot_off,
        const int32_t *__restrict__ Tj, const Z *__restrict__ Tx,
-       const int64_t *__restrict__ Cp64, int32_t *__restrict__ Cj, Z *__restrict__ Cx)
+       const int64_t *__restrict__ Cp64, int32_t *__restrict__ Cj, Z *__restrict__ Cx,
+       int64_t cap)
 {
     const int lane = threadIdx.x & 31;
     const int64_t nnz = Cp64[nrows];
+    if (nnz > cap) return;                 // C's arrays are too small: packed later
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t s0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * span;
          s0 < nnz; s0 += nw * span) {
@@ -1689,11 +1691,16 @@ static void exec_counts(SaxpyPlan *P, int32_t *Cp, int64_t *Cnnz64, cudaStream_t
 
 // the slots, packed into C's exact arrays
 template <typename Z>
-static void exec_pack(const SaxpyPlan *P, int32_t *Cj, Z *Cx, cudaStream_t s)
+static void exec_pack(const SaxpyPlan *P, int32_t *Cj, Z *Cx, cudaStream_t s,
+                      int64_t cap = -1)
 {
-    if (P->m > 0 && P->total_cap > 0)
-        k_pack<Z><<<nblocks(P->total_cap, 256, 16), 256, 0, s>>>(P->m,
-            flat_span(P->total_cap), P->slot_off, P->Tj, (const Z *)P->Tx, P->Cp64, Cj, Cx);
+    // cap < 0: the host knows the sizes (total_cap bounds the entries);
+    // otherwise C holds cap entries and the kernel checks the count itself
+    const int64_t grid_n = cap < 0 ? P->total_cap : cap;
+    if (P->m > 0 && grid_n > 0)
+        k_pack<Z><<<nblocks(grid_n, 256, 16), 256, 0, s>>>(P->m, flat_span(grid_n),
+            P->slot_off, P->Tj, (const Z *)P->Tx, P->Cp64, Cj, Cx,
+            cap < 0 ? (int64_t)INT64_MAX : cap);
 }
 
 template <class SR>
@@ -1847,13 +1854,14 @@ static int saxpy3_row_dense(DevCSR &C, const DevCSR *M, bool mask_comp, const De
 }
 
 // One-shot C<M> = A*B with one host round trip in the common case.  The
-// symbolic phase, the shared-memory bins and the row offsets are queued
-// together: the bins write their slots into the stream's scratch buffer and
-// read their row counts and the slot total on the device.  One read brings
-// back the counts, the slot total and the output size; only if the slots
-// did not fit (the buffer then grows and the bins run again) or heavy rows
-// need their accumulators sized does a second read follow.  C's arrays are
-// then allocated at their exact size and the slots packed into them.
+// symbolic phase, the shared-memory bins, the row offsets and the pack are
+// queued together: the bins write their slots into the stream's scratch
+// buffer and read their row counts and the slot total on the device, and the
+// pack fills C's arrays, allocated beforehand from B's mean row length, if
+// the product fits them.  One read brings back the counts, the slot total
+// and the output size; only if the slots did not fit (the buffer then grows
+// and the bins run again), heavy rows need their accumulators sized, or C
+// needs larger arrays does more work follow the read.
 template <class SR>
 static int saxpy3_t(DevCSR &C, const DevCSR *M, bool mask_comp, const DevCSR &A,
                     const DevCSR &B, SemiringCode sr, cudaStream_t s)
@@ -1895,10 +1903,26 @@ static int saxpy3_t(DevCSR &C, const DevCSR *M, bool mask_comp, const DevCSR &A,
     void *slots = src.get(want);
     if (!slots) { dev_free(T, s); return OUT_OF_MEMORY; }
     plan_place_slots(P, slots, src.have);
+    // C's arrays before the read, sized from B's mean row length: when the
+    // product fits (as a product of evenly filled rows does), the pack runs
+    // before the read and nothing follows it
+    double cg = 1.15 * (double)A.nnz * (mean_b > 1.0 ? mean_b : 1.0) + 64.0;
+    const double cfull = (double)m * (double)B.ncols;
+    if (cg > cfull + 64.0) cg = cfull + 64.0;
+    if (cg > (double)(INT32_MAX - 1)) cg = (double)(INT32_MAX - 1);
+    int64_t cap = (int64_t)cg;
+    T.j = (int32_t *)dalloc((size_t)(cap + 1) * 4, s);
+    T.x = dalloc((size_t)(cap + 1) * sizeof(Z), s);
+    if (!T.j || !T.x) {
+        dfree(T.j, s); dfree(T.x, s);
+        T.j = nullptr; T.x = nullptr;
+        cap = -1;
+    }
     const int ps = prof_begin("saxpy3_numeric", s);
     exec_light<SR>(P, M, A, B, false, s);
     prof_end(ps, s);
     exec_counts(P, T.p, nullptr, s);
+    if (cap >= 0) exec_pack<Z>(P, T.j, (Z *)T.x, s, cap);
     info = plan_read(P, s);
     if (info != SUCCESS) { dev_free(T, s); return info; }
     bool again = false;
@@ -1924,10 +1948,28 @@ static int saxpy3_t(DevCSR &C, const DevCSR *M, bool mask_comp, const DevCSR &A,
     const int64_t nnz = P->nnz;
     if (nnz >= INT32_MAX) { dev_free(T, s); return OUT_OF_MEMORY; }
     T.nnz = nnz;
-    T.j = (int32_t *)dalloc((size_t)(nnz + 1) * 4, s);
-    T.x = dalloc((size_t)(nnz + 1) * sizeof(Z), s);
-    if (!T.j || !T.x) { dev_free(T, s); return OUT_OF_MEMORY; }
-    exec_pack<Z>(P, T.j, (Z *)T.x, s);
+    if (again || nnz > cap) {
+        // the early pack saw incomplete rows or did not fit: pack now
+        if (nnz > cap) {
+            dfree(T.j, s); dfree(T.x, s);
+            T.j = (int32_t *)dalloc((size_t)(nnz + 1) * 4, s);
+            T.x = dalloc((size_t)(nnz + 1) * sizeof(Z), s);
+            if (!T.j || !T.x) { dev_free(T, s); return OUT_OF_MEMORY; }
+        }
+        exec_pack<Z>(P, T.j, (Z *)T.x, s);
+    } else if (cap > 2 * nnz + (1 << 20)) {
+        // far more room than entries: exact arrays
+        int32_t *j2 = (int32_t *)dalloc((size_t)(nnz + 1) * 4, s);
+        void *x2 = dalloc((size_t)(nnz + 1) * sizeof(Z), s);
+        if (j2 && x2) {
+            cudaMemcpyAsync(j2, T.j, (size_t)nnz * 4, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(x2, T.x, (size_t)nnz * sizeof(Z), cudaMemcpyDeviceToDevice, s);
+            dfree(T.j, s); dfree(T.x, s);
+            T.j = j2; T.x = x2;
+        } else {
+            dfree(j2, s); dfree(x2, s);
+        }
+    }
     info = cuda_to_info(cudaGetLastError());
     if (info != SUCCESS) { dev_free(T, s); return info; }
     C = T;
