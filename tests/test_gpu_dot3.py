@@ -204,3 +204,28 @@ def test_dot3_count_groups_valued_mask_and_sum(gpu, oracle, tname, np_t, mask_st
     assert total == int(np.sum(want[2].astype(np.int64)).astype(np_t))
     for d in (dM, dA, dB, C):
         d.free()
+
+
+def test_dot3_on_a_caller_stream(gpu, oracle):
+    """On a caller's stream (grb_b200_set_stream) the counting path's scratch
+    is allocated for the call instead of taken from the library stream's
+    buffer; the results are the same."""
+    import ctypes
+    import torch
+    gb = gpu
+    L_ = gb.lib()
+    S = W.rmat(13, 16, seed=6)
+    Lc, Uc = W.tril_triu(S)
+    want = oracle.dot3(S.nrows, S.ncols, (Lc.p, Lc.i, None, 1), (Uc.p, Uc.i, None, 1),
+                       (Lc.p, Lc.i, None, 1), "PLUS", "PAIR", 8)
+    st = torch.cuda.Stream()
+    L_.grb_b200_set_stream(ctypes.c_void_p(st.cuda_stream))
+    try:
+        got, _ = _dot3_dev(gb, Lc, Lc, Uc, gb.semiring("PLUS", "PAIR", "int64"),
+                           type_name="bool")
+    finally:
+        L_.grb_b200_set_stream(None)
+    assert_exact(got, want, "C<L>=L*U' on a caller stream")
+    got2, _ = _dot3_dev(gb, Lc, Lc, Uc, gb.semiring("PLUS", "PAIR", "int64"),
+                        type_name="bool")
+    assert_exact(got2, want, "C<L>=L*U' on the library stream")

@@ -377,3 +377,50 @@ def test_bfs_push_pull_parents_exact(api, oracle):
     for v in (q, p):
         api.vfree(v)
     api.free(A)
+
+
+def test_pull_step_on_a_caller_stream(api, oracle):
+    """One pull BFS step through GrB_mxv on a caller's stream (its scratch
+    allocated for the call) and on the library's stream: the same parents."""
+    import ctypes
+    import torch
+    S = W.rmat(12, 16, seed=4)
+    n = S.nrows
+    rng = np.random.default_rng(3)
+    front = np.sort(rng.choice(n, 800, replace=False)).astype(np.int64)
+    visited = np.sort(np.unique(np.concatenate([front, rng.choice(n, 1500, replace=False)])))
+    A = api.matrix_from_csr(S, 1)
+    outs = []
+    for caller in (True, False):
+        q = api.vector_from(front, front, 8, n)
+        p = api.vector_from(visited, visited, 8, n)
+        L_ = api.L
+        st = torch.cuda.Stream()
+        if caller:
+            L_.grb_b200_set_stream(ctypes.c_void_p(st.cuda_stream))
+        try:
+            api.mxv(q, p, None, "GxB_MAX_SECONDI_INT64", A, q, "GrB_DESC_RSC")
+        finally:
+            if caller:
+                L_.grb_b200_set_stream(None)
+        outs.append(api.vector_to(q, 8))
+        api.vfree(q)
+        api.vfree(p)
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    # against the oracle: the largest frontier neighbour of every unvisited vertex
+    fr = np.zeros(n, bool)
+    fr[front] = True
+    seen = np.zeros(n, bool)
+    seen[visited] = True
+    wi, wx = [], []
+    for v in range(n):
+        if seen[v]:
+            continue
+        nb = S.i[S.p[v]:S.p[v + 1]]
+        nb = nb[fr[nb]]
+        if len(nb):
+            wi.append(v)
+            wx.append(int(nb.max()))
+    assert np.array_equal(outs[1][0], np.array(wi, np.int64))
+    assert np.array_equal(outs[1][1], np.array(wx, np.int64))
+    api.free(A)
