@@ -317,7 +317,7 @@ def test_assign_with_its_own_pattern_as_mask(api, oracle, accum, desc):
         api.vfree(v)
 
 
-@pytest.mark.parametrize("nw,nu", [(60000, 50000), (0, 3000), (3000, 0), (1, 1)])
+@pytest.mark.parametrize("nw,nu", [(60000, 50000), (0, 3000), (3000, 0), (1, 1), (0, 0)])
 def test_assign_union_many_tiles(api, oracle, nw, nu):
     """w<u> = u (structural, no accumulator, no replace) on row vectors is
     one merge-path union launch over tiles of 3072 merged positions: many
@@ -423,4 +423,46 @@ def test_pull_step_on_a_caller_stream(api, oracle):
             wx.append(int(nb.max()))
     assert np.array_equal(outs[1][0], np.array(wi, np.int64))
     assert np.array_equal(outs[1][1], np.array(wx, np.int64))
+    api.free(A)
+
+
+@pytest.mark.parametrize("case", ["empty_frontier", "all_visited", "no_mask", "plain_mask"])
+def test_pull_step_edge_cases(api, case):
+    """The pull step (GrB_mxv with MAX_SECONDI) with an empty frontier, a
+    visited set that covers every vertex, no mask, and a plain (not
+    complemented) mask, against a dense evaluation."""
+    S = W.rmat(10, 16, seed=8)
+    n = S.nrows
+    rng = np.random.default_rng(9)
+    front = (np.zeros(0, np.int64) if case == "empty_frontier"
+             else np.sort(rng.choice(n, 100, replace=False)).astype(np.int64))
+    mask_idx = (np.arange(n, dtype=np.int64) if case == "all_visited"
+                else np.sort(rng.choice(n, n // 2, replace=False)).astype(np.int64))
+    A = api.matrix_from_csr(S, 1)
+    q = api.vector_from(front, front, 8, n)
+    w = api.vector_new(8, n)
+    m = api.vector_from(mask_idx, mask_idx, 8, n)
+    desc = {"empty_frontier": "GrB_DESC_RSC", "all_visited": "GrB_DESC_RSC",
+            "no_mask": None, "plain_mask": "GrB_DESC_RS"}[case]
+    api.mxv(w, None if case == "no_mask" else m, None, "GxB_MAX_SECONDI_INT64", A, q, desc)
+    gi, gx = api.vector_to(w, 8)
+    fr = np.zeros(n, bool)
+    fr[front] = True
+    inm = np.zeros(n, bool)
+    inm[mask_idx] = True
+    wi, wx = [], []
+    for v in range(n):
+        if case in ("empty_frontier", "all_visited") and inm[v]:
+            continue
+        if case == "plain_mask" and not inm[v]:
+            continue
+        nb = S.i[S.p[v]:S.p[v + 1]]
+        nb = nb[fr[nb]]
+        if len(nb):
+            wi.append(v)
+            wx.append(int(nb.max()))
+    assert np.array_equal(gi, np.array(wi, np.int64)), case
+    assert np.array_equal(gx, np.array(wx, np.int64)), case
+    for v in (q, w, m):
+        api.vfree(v)
     api.free(A)
