@@ -219,13 +219,12 @@ k_union_row(const int32_t *__restrict__ Cj, const Z *__restrict__ Cx, bool c_iso
     __shared__ long long s_ex;
     __shared__ int64_t s_i0, s_i1;
     __shared__ int s_w[UN_THREADS / 32];
-    // the staged input ranges, then (after the merge) the staged output: its
-    // values over the inputs' space, its indices after them
-    __shared__ __align__(16) unsigned char s_buf[UN_TILE * (sizeof(Z) > 8 ? sizeof(Z) : 8) +
-                                                 UN_TILE * 4];
-    int32_t *s_c = (int32_t *)s_buf, *s_t = s_c + UN_TILE;
-    Z *s_ox = (Z *)s_buf;
-    int32_t *s_oj = (int32_t *)(s_buf + UN_TILE * (sizeof(Z) > 8 ? sizeof(Z) : 8));
+    // the staged input indices, then (after the merge) the staged output:
+    // its indices and the source of each (a position in C, or in T with the
+    // top bit set); the values are gathered while the output is written
+    __shared__ __align__(16) int32_t s_buf[2 * UN_TILE];
+    int32_t *s_c = s_buf, *s_t = s_buf + UN_TILE;
+    int32_t *s_oj = s_buf, *s_os = s_buf + UN_TILE;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     unsigned long long *status = ws + 2;
     if (tid == 0) s_tile = (int)atomicAdd(&ws[0], 1ull);
@@ -262,13 +261,12 @@ k_union_row(const int32_t *__restrict__ Cj, const Z *__restrict__ Cx, bool c_iso
         ci = lo;
         tj = dl - lo;
     }
-    int32_t oj[UN_ITEMS];
-    Z ox[UN_ITEMS];
+    int32_t oj[UN_ITEMS], os[UN_ITEMS];
     int kept = 0;
     for (int k = 0; k < UN_ITEMS && dl + k < nl; k++) {
         if (tj < nt && (ci >= nc || s_t[tj] <= s_c[ci])) {
             oj[kept] = s_t[tj];
-            ox[kept] = Tx[t_iso ? 0 : j0 + tj];
+            os[kept] = (int32_t)(0x80000000u | (uint32_t)tj);
             kept++;
             tj++;
         } else {
@@ -276,7 +274,7 @@ k_union_row(const int32_t *__restrict__ Cj, const Z *__restrict__ Cx, bool c_iso
             const int32_t before = tj > 0 ? s_t[tj - 1] : tprev;
             if (before != key) {
                 oj[kept] = key;
-                ox[kept] = Cx[c_iso ? 0 : i0 + ci];
+                os[kept] = ci;
                 kept++;
             }
             ci++;
@@ -317,12 +315,28 @@ k_union_row(const int32_t *__restrict__ Cj, const Z *__restrict__ Cx, bool c_iso
     // (the block barrier above also ends every read of the staged inputs)
     __syncthreads();
     int loc = s_w[w] + (x - kept);
-    for (int k = 0; k < kept; k++) { s_oj[loc + k] = oj[k]; s_ox[loc + k] = ox[k]; }
+    for (int k = 0; k < kept; k++) { s_oj[loc + k] = oj[k]; s_os[loc + k] = os[k]; }
     __syncthreads();
     const int64_t base = s_ex;
-    for (int k = tid; k < s_agg; k += UN_THREADS) {
-        Rj[base + k] = s_oj[k];
-        Rx[base + k] = s_ox[k];
+    const int agg = s_agg;
+    // all of a thread's value loads first (independent, so they overlap),
+    // then its stores
+    Z v[UN_ITEMS];
+    #pragma unroll
+    for (int r = 0; r < UN_ITEMS; r++) {
+        const int k = tid + r * UN_THREADS;
+        if (k < agg) {
+            const int32_t src = s_os[k];
+            v[r] = src < 0 ? Tx[t_iso ? 0 : j0 + (src & 0x7fffffff)] : Cx[c_iso ? 0 : i0 + src];
+        }
+    }
+    #pragma unroll
+    for (int r = 0; r < UN_ITEMS; r++) {
+        const int k = tid + r * UN_THREADS;
+        if (k < agg) {
+            Rj[base + k] = s_oj[k];
+            Rx[base + k] = v[r];
+        }
     }
     // the last tile to finish clears the workspace
     if (tid == 0) {
