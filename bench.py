@@ -531,14 +531,13 @@ class BfsPushPull(Bfs):
         return c
 
     def launches_per_step(self):
-        # a pull level: two bitmap scatters, the row kernel, the flag scan
-        # (multi-launch over n + 1 values) and the compaction; push levels
-        # as in the push-only traversal; one union per parent update
+        # a pull level: two bitmap scatters, the row kernel, the scan over
+        # the 32-row groups and the compaction (5); push levels as in the
+        # push-only traversal; one union per parent update
         lev = max(getattr(self, "levels", 1), 1)
         pulls = max(getattr(self, "pull_levels", 0), 0)
         push = lev - pulls
-        return (4 + scan_launches(self.n + 1)) * pulls + 14 * min(push, 2) + \
-            6 * max(push - 2, 0) + (lev - 1)
+        return 5 * pulls + 14 * min(push, 2) + 6 * max(push - 2, 0) + (lev - 1)
 
 
 CONFIGS = {"tc": TriCount, "saxpy": Saxpy, "bfs": Bfs, "bfs_pushpull": BfsPushPull}
