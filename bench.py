@@ -642,6 +642,9 @@ class Harness:
         self.L = gb.lib()
         self.stream = torch.cuda.Stream()
         self.L.grb_b200_set_stream(ctypes.c_void_p(self.stream.cuda_stream))
+        # the stream lives as long as the process: it keeps a scratch buffer,
+        # as the library's own streams do
+        self.L.grb_b200_stream_keep_scratch(ctypes.c_void_p(self.stream.cuda_stream), True)
         self.flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
         self.rank = int(os.environ.get("RANK", "0"))
         self.world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -113,6 +113,9 @@ def _optional_bindings(L):
     vp, i64, ci, cb = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_bool
     if hasattr(L, "grb_b200_set_stream"):
         L.grb_b200_set_stream.argtypes = [vp]
+    if hasattr(L, "grb_b200_stream_keep_scratch"):
+        L.grb_b200_stream_keep_scratch.argtypes = [vp, cb]
+        L.grb_b200_stream_keep_scratch.restype = ci
     if hasattr(L, "grb_b200_profile"):
         L.grb_b200_profile.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(i64)]

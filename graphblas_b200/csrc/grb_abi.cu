@@ -138,6 +138,14 @@ void grb_b200_debug_fail_alloc(int64_t n) { set_alloc_fail_countdown(n); }
 
 void grb_b200_set_stream(void *stream) { set_thread_stream((cudaStream_t)stream); }
 
+int grb_b200_stream_keep_scratch(void *stream, bool keep)
+{
+    if (!stream) return NULL_POINTER;
+    if (keep) stream_scratch_enable((cudaStream_t)stream);
+    else stream_scratch_release((cudaStream_t)stream);
+    return SUCCESS;
+}
+
 void grb_b200_profile_enable(bool on) { prof_enable(on); }
 
 void grb_b200_profile_reset(void) { prof_reset(); }

@@ -123,6 +123,14 @@ void grb_b200_debug_fail_alloc(int64_t n);
  * (CUDA/GB_cuda_AxB_dot3.cpp:54). */
 void grb_b200_set_stream(void *stream);
 
+/* Keep a scratch buffer with a caller's stream (keep = true), as the
+ * library's own streams have: the products, masked dot products, pull steps
+ * and uploads run on that stream then take their temporary arrays from it
+ * and stop allocating and freeing them call by call.  The buffer grows to
+ * the largest call's need.  keep = false releases it, in the stream's order;
+ * do that before destroying the stream.  No counterpart in the reference. */
+int grb_b200_stream_keep_scratch(void *stream, bool keep);
+
 /* Kernel timing with CUDA events recorded on the launching stream around
  * each launch of the hot kernels ("dot3", "saxpy3_numeric", ...).  Off by
  * default; the reference's equivalent is its GpuTimer

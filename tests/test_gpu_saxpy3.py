@@ -298,3 +298,44 @@ def test_saxpy_many_heavy_rows(gpu, oracle, add, mult, tname):
     got = _saxpy_dev(gb, A, B, gb.semiring(add, mult, tname))
     want = oracle.saxpy(m, n, (A.p, A.i, A.x, tc), (B.p, B.i, B.x, tc), add, mult, tc)
     assert_exact(got, want, "many heavy rows %s_%s" % (add, mult))
+
+
+def test_caller_stream_keeping_a_scratch_buffer(gpu, oracle):
+    """A caller's stream that keeps a scratch buffer (grb_b200_stream_keep_
+    scratch): products before and after the buffer grows, and a masked dot
+    product, give the results of the library's own streams; the buffer is
+    released before the stream goes."""
+    import ctypes
+    import torch
+    gb = gpu
+    L = gb.lib()
+    st = torch.cuda.Stream()
+    h = ctypes.c_void_p(st.cuda_stream)
+    assert L.grb_b200_stream_keep_scratch(h, True) == 0
+    L.grb_b200_set_stream(h)
+    try:
+        A = random_csr(300, 400, 0.02, 31)
+        B = random_csr(400, 500, 0.02, 32)
+        small = _saxpy_dev(gb, A, B, gb.semiring("PLUS", "TIMES", "fp64"))
+        A2 = random_csr(3000, 4000, 0.01, 33)
+        B2 = random_csr(4000, 5000, 0.01, 34)
+        big = _saxpy_dev(gb, A2, B2, gb.semiring("PLUS", "TIMES", "fp64"))
+        S = W.rmat(11, 16, seed=5)
+        Lc, Uc = W.tril_triu(S)
+        dL = gb.DMatrix.upload(Lc, "bool")
+        dU = gb.DMatrix.upload(Uc, "bool")
+        C = gb.dot3(dL, dL, dU, gb.semiring("PLUS", "PAIR", "int64"))
+        tri = C.download(prune=True)
+        for d in (dL, dU, C):
+            d.free()
+    finally:
+        L.grb_b200_set_stream(None)
+        assert L.grb_b200_stream_keep_scratch(h, False) == 0
+        st.synchronize()
+    assert_exact(small, oracle.saxpy(300, 500, (A.p, A.i, A.x, 11), (B.p, B.i, B.x, 11),
+                                     "PLUS", "TIMES", 11), "small product")
+    assert_exact(big, oracle.saxpy(3000, 5000, (A2.p, A2.i, A2.x, 11), (B2.p, B2.i, B2.x, 11),
+                                   "PLUS", "TIMES", 11), "larger product")
+    want = oracle.dot3(S.nrows, S.ncols, (Lc.p, Lc.i, None, 1), (Uc.p, Uc.i, None, 1),
+                       (Lc.p, Lc.i, None, 1), "PLUS", "PAIR", 8)
+    assert_exact(tri, want, "C<L>=L*U'")
