@@ -437,14 +437,26 @@ int dev_import(DevCSR &A, int64_t nrows, int64_t ncols, const int64_t *p,
     A = DevCSR();
     A.nrows = nrows; A.ncols = ncols; A.nnz = nnz; A.type = type; A.iso = false;
     const size_t ts = type_size(type);
-    Scratch ws(s);
-    int64_t *stage = ws.get<int64_t>((nrows + 1 > nnz) ? nrows + 1 : nnz);
-    unsigned *flag = ws.get<unsigned>(1);
-    unsigned *starts = ws.get<unsigned>((nnz + 31) / 32 + 1);
+    // the staging array, the error flag and the row-start bitmap in one
+    // block (the stream's scratch buffer when the stream keeps one)
+    Carve cv(s);
+    int64_t *stage = nullptr;
+    unsigned *flag = nullptr, *starts = nullptr;
+    auto layout = [&]() {
+        flag = cv.take<unsigned>(1);
+        starts = cv.take<unsigned>((nnz + 31) / 32 + 1);
+        stage = cv.take<int64_t>((nrows + 1 > nnz) ? nrows + 1 : nnz);
+    };
+    layout();
+    CallBlock blk(s);
+    const bool got = blk.get(cv.off);
+    cv.base = blk.base;
+    cv.off = 0;
+    layout();
     A.p = (int32_t *)dalloc((size_t)(nrows + 1) * 4, s);
     A.j = (int32_t *)dalloc((size_t)(nnz ? nnz : 1) * 4, s);
     A.x = dalloc((size_t)(nnz ? nnz : 1) * ts, s);
-    if (ws.failed || !A.p || !A.j || !A.x) { dev_free(A, s); return OUT_OF_MEMORY; }
+    if (!got || !A.p || !A.j || !A.x) { dev_free(A, s); return OUT_OF_MEMORY; }
     cudaMemsetAsync(flag, 0, 4, s);
     cudaMemcpyAsync(stage, p, (size_t)(nrows + 1) * 8, cudaMemcpyHostToDevice, s);
     k_narrow_check<<<grid_for(nrows + 1, 256), 256, 0, s>>>(stage, A.p, nrows + 1, 0, nnz,
@@ -500,12 +512,24 @@ __global__ void k_fill_value(T *__restrict__ out, const T *__restrict__ v, int64
 // values (iso values expanded); synchronises s
 int dev_copy_out(const DevCSR &A, int64_t *p, int64_t *i, void *x, cudaStream_t s)
 {
-    Scratch ws(s);
     const size_t ts = type_size(A.type);
     const int64_t nnz = A.nnz;
-    int64_t *stage = ws.get<int64_t>((A.nrows + 1 > nnz) ? A.nrows + 1 : nnz);
-    char *ex = (x && A.x && A.iso && nnz > 0) ? ws.get<char>((size_t)nnz * ts) : nullptr;
-    if (ws.failed) return OUT_OF_MEMORY;
+    // the widening stage (and the expanded iso values) in one block: the
+    // stream's scratch buffer when the stream keeps one
+    const bool expand = x && A.x && A.iso && nnz > 0;
+    Carve cv(s);
+    int64_t *stage = nullptr;
+    char *ex = nullptr;
+    auto layout = [&]() {
+        stage = cv.take<int64_t>((A.nrows + 1 > nnz) ? A.nrows + 1 : nnz);
+        if (expand) ex = cv.take<char>((size_t)nnz * ts);
+    };
+    layout();
+    CallBlock blk(s);
+    if (!blk.get(cv.off)) return OUT_OF_MEMORY;
+    cv.base = blk.base;
+    cv.off = 0;
+    layout();
     k_widen<<<grid_for(A.nrows + 1, 256), 256, 0, s>>>(A.p, stage, A.nrows + 1);
     cudaMemcpyAsync(p, stage, (size_t)(A.nrows + 1) * 8, cudaMemcpyDeviceToHost, s);
     if (nnz > 0) {
