@@ -500,7 +500,6 @@ k_ct_classify(const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
 // reached the error flag is set and the call fails.
 static constexpr unsigned long long CT_FLAG_AGG = 1ull << 62, CT_FLAG_INC = 2ull << 62;
 static constexpr unsigned long long CT_VAL = (1ull << 62) - 1;
-static constexpr int CT_SPIN_LIMIT = 1 << 22;
 
 // A group's entries c (long and short), its bucket share and its items:
 // about CT_WORK_* probes each, at most CT_ITEM_* entries each, at least 16
@@ -860,6 +859,19 @@ __device__ __forceinline__ void ct_batch(bool valid, int32_t q0, int32_t len, in
     __syncwarp();
 }
 
+// one long list by the whole warp: C(i,j) for the bucket entry r
+template <typename Z, class Hit>
+__device__ __forceinline__ void ct_long_rec(const CtRec &r, const int32_t *__restrict__ S,
+                                            bool vec, int32_t none, const Hit &hit,
+                                            int32_t *__restrict__ Cj, Z *__restrict__ Cx,
+                                            unsigned long long &sum, unsigned long long &zc)
+{
+    const int lane = threadIdx.x & 31;
+    int c = ct_count(S, r.q0, r.q0 + r.len, 32, lane, vec, none, hit);
+    c = (int)__reduce_add_sync(0xffffffffu, (unsigned)c);
+    if (lane == 0) ct_write<Z>(r.pm, r.j, c, Cj, Cx, sum, zc);
+}
+
 // one long list by the whole warp: C(i,j) for the entry in bucket slot e
 template <typename Z, class Hit>
 __device__ __forceinline__ void ct_long(const CtRec *__restrict__ bucket, int32_t e,
@@ -868,11 +880,7 @@ __device__ __forceinline__ void ct_long(const CtRec *__restrict__ bucket, int32_
                                         Z *__restrict__ Cx, unsigned long long &sum,
                                         unsigned long long &zc)
 {
-    const int lane = threadIdx.x & 31;
-    const CtRec r = bucket[e];
-    int c = ct_count(S, r.q0, r.q0 + r.len, 32, lane, vec, none, hit);
-    c = (int)__reduce_add_sync(0xffffffffu, (unsigned)c);
-    if (lane == 0) ct_write<Z>(r.pm, r.j, c, Cj, Cx, sum, zc);
+    ct_long_rec<Z>(bucket[e], S, vec, none, hit, Cj, Cx, sum, zc);
 }
 
 __device__ __forceinline__ void ct_load_entry(const CtItem &I, int32_t e,
@@ -1050,13 +1058,25 @@ k_ct_bitmap(const CtItem *__restrict__ items, const int32_t *__restrict__ totals
         };
         const int32_t none = klo + (int32_t)nbits;
         // long lists one at a time, each by the whole warp, so that no warp
-        // holds many of them; then the short ones 32 at a time
-        while (true) {
-            int e = 0;
-            if (lane == 0) e = atomicAdd(&s_long, 1);
-            e = __shfl_sync(0xffffffffu, e, 0) + I.e0;
-            if (e >= I.el) break;
-            ct_long<Z>(bucket, e, S, vec, none, hit, Cj, Cx, sum, zc);
+        // holds many of them (the next list's record is read while the
+        // current list is probed); then the short ones 32 at a time
+        {
+            auto grab = [&]() -> int {
+                int e = 0;
+                if (lane == 0) e = atomicAdd(&s_long, 1);
+                return __shfl_sync(0xffffffffu, e, 0) + I.e0;
+            };
+            int e = grab();
+            CtRec r{0, 0, 0, 0};
+            if (e < I.el) r = bucket[e];
+            while (e < I.el) {
+                const int en = grab();
+                CtRec rn{0, 0, 0, 0};
+                if (en < I.el) rn = bucket[en];
+                ct_long_rec<Z>(r, S, vec, none, hit, Cj, Cx, sum, zc);
+                e = en;
+                r = rn;
+            }
         }
         while (true) {
             int e = 0;
