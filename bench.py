@@ -245,9 +245,9 @@ class Saxpy:
         self.products = int(np.sum(deg[self.A.i]))
         self.flops = 2.0 * self.products
         self.workload = "saxpy3_er16384_d8_plus_times_fp64"
-        # DRAM bytes of the numeric kernel per launch (ncu capture of this
-        # workload at this size: the inputs come from L2, the written slots
-        # stay there)
+        # DRAM bytes of the one-launch product kernel per launch (ncu capture
+        # of this workload at this size: the inputs come from L2, the written
+        # slots stay there)
         self.traffic_per_launch = 3.54e6
 
     def config(self):
@@ -304,10 +304,10 @@ class Saxpy:
         return self.flops / 1e9
 
     def launches_per_step(self):
-        # flop counts, bins, slot-offset scan, bin fill, the three
-        # shared-memory bin kernels (expand-sort-compress, warp hash, block
-        # hash), the row-offset scan and the pack
-        return 9
+        # the one-launch product kernel (products per row, slots,
+        # expand-sort-compress, C's offsets and entries) and the read of
+        # nnz(C)
+        return 2
 
     def cpu_baseline(self, R, ncores):
         from oracle import csr_digest

@@ -246,23 +246,41 @@ void dfree(void *p, cudaStream_t s)
     if (p) cudaFreeAsync(p, s);
 }
 
-// the few bytes a call reads back (bin counts, totals, zombie counts) go
-// through a page-locked buffer of the calling host thread: the copy is a
-// direct DMA instead of a staged one
+// The few bytes a call reads back (bin counts, totals, zombie counts) go
+// through a page-locked, device-mapped buffer of the calling host thread,
+// written by a one-block kernel queued behind the call's last kernel: a
+// kernel that follows a kernel on the same stream starts within a
+// microsecond or two, where a copy-engine transfer first waits for the
+// compute engine's completion (several microseconds more per read).
 static constexpr size_t READBACK_MAX = 4096;
+
+__global__ void k_readback(const unsigned char *__restrict__ src, unsigned char *dst,
+                           uint32_t bytes)
+{
+    const bool words = ((((uintptr_t)src) | ((uintptr_t)dst) | bytes) & 3) == 0;
+    if (words) {
+        const uint32_t *s4 = reinterpret_cast<const uint32_t *>(src);
+        uint32_t *d4 = reinterpret_cast<uint32_t *>(dst);
+        for (uint32_t q = threadIdx.x; q < bytes / 4; q += blockDim.x) d4[q] = s4[q];
+    } else {
+        for (uint32_t q = threadIdx.x; q < bytes; q += blockDim.x) dst[q] = src[q];
+    }
+    __threadfence_system();
+}
 
 // A thread takes a buffer from a shared pool on first use and puts it back
 // when it exits, so the worker threads a server starts for each replay reuse
 // the same few buffers (page-locking memory, and unlocking it, is slow).
+struct ReadbackPage { void *host = nullptr, *dev = nullptr; };
 static std::mutex g_rb_mu;
-static std::vector<void *> g_rb_pool;
+static std::vector<ReadbackPage> g_rb_pool;
 
 struct ReadbackBuffer {
-    void *p = nullptr;
+    ReadbackPage pg;
     ~ReadbackBuffer() {
-        if (p) {
+        if (pg.host) {
             std::lock_guard<std::mutex> lk(g_rb_mu);
-            g_rb_pool.push_back(p);
+            g_rb_pool.push_back(pg);
         }
     }
 };
@@ -270,31 +288,43 @@ struct ReadbackBuffer {
 cudaError_t readback(void *dst, const void *src, size_t bytes, cudaStream_t s)
 {
     thread_local ReadbackBuffer rb;
-    void *&buf = rb.p;
-    if (!buf && bytes <= READBACK_MAX) {
+    ReadbackPage &pg = rb.pg;
+    if (!pg.host && bytes <= READBACK_MAX) {
         {
             std::lock_guard<std::mutex> lk(g_rb_mu);
             if (!g_rb_pool.empty()) {
-                buf = g_rb_pool.back();
+                pg = g_rb_pool.back();
                 g_rb_pool.pop_back();
             }
         }
-        if (!buf && cudaMallocHost(&buf, READBACK_MAX) != cudaSuccess) {
-            cudaGetLastError();
-            buf = nullptr;
+        if (!pg.host) {
+            void *h = nullptr, *d = nullptr;
+            if (cudaHostAlloc(&h, READBACK_MAX, cudaHostAllocMapped | cudaHostAllocPortable) !=
+                cudaSuccess) {
+                cudaGetLastError();
+            } else if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+                cudaGetLastError();
+                cudaFreeHost(h);
+            } else {
+                pg.host = h;
+                pg.dev = d;
+            }
         }
     }
     // a copy refused at submission leaves nothing for the synchronise to
     // report, so its own status is checked first (the bytes are not read)
-    if (!buf || bytes > READBACK_MAX) {
+    if (!pg.host || bytes > READBACK_MAX) {
         const cudaError_t c = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
         if (c != cudaSuccess) return c;
         return cudaStreamSynchronize(s);
     }
-    const cudaError_t c = cudaMemcpyAsync(buf, src, bytes, cudaMemcpyDeviceToHost, s);
+    if (bytes == 0) return cudaStreamSynchronize(s);
+    k_readback<<<1, 128, 0, s>>>((const unsigned char *)src, (unsigned char *)pg.dev,
+                                 (uint32_t)bytes);
+    const cudaError_t c = cudaGetLastError();
     if (c != cudaSuccess) return c;
     const cudaError_t e = cudaStreamSynchronize(s);
-    if (e == cudaSuccess) memcpy(dst, buf, bytes);
+    if (e == cudaSuccess) memcpy(dst, pg.host, bytes);
     return e;
 }
 

@@ -453,9 +453,163 @@ __device__ __forceinline__ void warp_sort_regs(KT *key, int n, int lane)
     }
 }
 
+// One row of the expand-sort-compress bin by one warp: the row's products
+// (at most cap) expand into key[] / val[] (the warp's shared-memory arrays),
+// the keys are sorted and each run of equal columns is folded into one entry
+// of Tj / Tx from position off() on (read only when the row is written).
+// Returns the row's entry count.
 // KT: 32-bit keys when (column << posb) fits, else 64-bit; posb = log2(cap)
 // bits hold the product's position, so only the keys move in the sort and
 // the values stay where the expansion wrote them.
+template <class SR, typename KT, class Off>
+__device__ __forceinline__ int esc_row(int32_t i, int posb, KT *key, typename SR::z_t *val,
+                                       const int32_t *__restrict__ Ap,
+                                       const int32_t *__restrict__ Aj,
+                                       const void *__restrict__ Ax, bool a_iso,
+                                       const int32_t *__restrict__ Bp,
+                                       const int32_t *__restrict__ Bj,
+                                       const void *__restrict__ Bx, bool b_iso,
+                                       const int32_t *__restrict__ Mp,
+                                       const int32_t *__restrict__ Mj,
+                                       bool has_mask, bool mask_comp, const Off &off_of,
+                                       int32_t *__restrict__ Tj, typename SR::z_t *__restrict__ Tx)
+{
+    using Z = typename SR::z_t;
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const KT posmask = ((KT)1 << posb) - 1;
+    const int32_t pa0 = Ap[i], pa1 = Ap[i + 1];
+    int32_t m0 = 0, m1 = 0;
+    if (has_mask) { m0 = Mp[i]; m1 = Mp[i + 1]; }
+    int n = 0;                                   // products kept so far
+    for (int32_t c0 = pa0; c0 < pa1; c0 += 32) {
+        // 32 entries of A(i,:) at a time: lane l holds k and nnz(B(k,:))
+        const int32_t pa = c0 + lane;
+        int32_t k = 0, b0 = 0, len = 0;
+        Z a = Z();
+        if (pa < pa1) {
+            k = Aj[pa];
+            b0 = Bp[k];
+            len = Bp[k + 1] - b0;
+            if (SR::needs_a) a = ld_val<Z>(Ax, pa, a_iso);
+        }
+        int incl = len;
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        for (int q0 = 0; q0 < total; q0 += 32) {
+            // product q of this chunk belongs to the first lane src whose
+            // inclusive count exceeds q
+            const int q = q0 + lane;
+            int src = 0;
+            #pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int v = __shfl_sync(0xffffffffu, incl, src + step - 1);
+                if (v <= q) src += step;
+            }
+            const int excl = __shfl_sync(0xffffffffu, incl - len, src);
+            const int32_t kk = __shfl_sync(0xffffffffu, k, src);
+            const int32_t bb = __shfl_sync(0xffffffffu, b0, src);
+            const Z aa = shfl<Z>(a, src);
+            bool keep = q < total;
+            int32_t j = 0, pb = 0;
+            if (keep) {
+                pb = bb + (q - excl);
+                j = Bj[pb];
+                if (has_mask) {
+                    const int32_t f = lower_bound(Mj, m0, m1, j);
+                    const bool present = f < m1 && Mj[f] == j;
+                    keep = mask_comp ? !present : present;
+                }
+            }
+            const unsigned km = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                const int pos = n + __popc(km & below);
+                Z b = Z();
+                if (SR::needs_b) b = ld_val<Z>(Bx, pb, b_iso);
+                key[pos] = ((KT)(uint32_t)j << posb) | (KT)pos;
+                val[pos] = SR::F::f(aa, b, i, kk, j);
+            }
+            n += __popc(km);
+        }
+    }
+    __syncwarp();
+    int n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    if (n <= 32) {
+        // one key per lane: bitonic network over the lanes in registers
+        KT kk = lane < n ? key[lane] : ~(KT)0;
+        #pragma unroll
+        for (int size = 2; size <= 32; size <<= 1) {
+            #pragma unroll
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                const KT other = __shfl_xor_sync(0xffffffffu, kk, stride);
+                const bool up = (lane & size) == 0;
+                const bool lower = (lane & stride) == 0;
+                kk = (lower == up) ? (kk < other ? kk : other) : (kk < other ? other : kk);
+            }
+        }
+        if (lane < n) key[lane] = kk;
+        n2 = 0;                                  // the shared-memory network is skipped
+    } else if (n <= 64) {
+        warp_sort_regs<2>(key, n, lane);
+        n2 = 0;
+    } else if (n <= 128) {
+        warp_sort_regs<4>(key, n, lane);
+        n2 = 0;
+    } else if (n <= 256) {
+        warp_sort_regs<8>(key, n, lane);
+        n2 = 0;
+    }
+    for (int q = n + lane; q < n2; q += 32) key[q] = ~(KT)0;
+    __syncwarp();
+    // bitonic sort of the keys; a lane owns every 32nd compare-exchange
+    for (int size = 2; size <= n2; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int q = lane; q < (n2 >> 1); q += 32) {
+                // q-th pair of this pass: lower index a, partner a + stride
+                const int a = ((q & ~(stride - 1)) << 1) | (q & (stride - 1));
+                const int b = a + stride;
+                const bool up = ((a & size) == 0);
+                const KT ka = key[a], kb = key[b];
+                if ((ka > kb) == up) { key[a] = kb; key[b] = ka; }
+            }
+            __syncwarp();
+        }
+    }
+    // the first entry of each run of equal columns folds the run in
+    // ascending k (its positions ascend) and writes one output entry
+    const int64_t off = off_of();
+    int out = 0;
+    for (int c0 = 0; c0 < n; c0 += 32) {
+        const int p = c0 + lane;
+        bool head = false;
+        KT kp = 0;
+        if (p < n) {
+            kp = key[p];
+            head = (p == 0) || ((key[p - 1] >> posb) != (kp >> posb));
+        }
+        const unsigned hm = __ballot_sync(0xffffffffu, head);
+        if (head) {
+            const KT jcol = kp >> posb;
+            Z z = val[kp & posmask];
+            for (int r = p + 1; r < n; r++) {
+                const KT kr = key[r];
+                if ((kr >> posb) != jcol) break;
+                z = SR::M::update(z, val[kr & posmask]);
+            }
+            const int64_t dst = off + out + __popc(hm & below);
+            Tj[dst] = (int32_t)jcol;
+            Tx[dst] = z;
+        }
+        out += __popc(hm);
+    }
+    return out;
+}
+
 template <class SR, typename KT>
 __global__ void __launch_bounds__(ESC_WARPS * 32, 6)
 k_saxpy_esc(BinRows br, int cap, int posb,
@@ -474,145 +628,246 @@ k_saxpy_esc(BinRows br, int cap, int posb,
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     KT *key = (KT *)(smem + (size_t)w * cap * (sizeof(KT) + sizeof(Z)));
     Z *val = (Z *)((unsigned char *)key + (size_t)cap * sizeof(KT));
-    const unsigned below = (1u << lane) - 1u;
-    const KT posmask = ((KT)1 << posb) - 1;
     const int32_t *rows;
     const int nrows_bin = br.get(rows);
 
     for (int64_t rb = (int64_t)blockIdx.x * ESC_WARPS + w; rb < nrows_bin;
          rb += (int64_t)gridDim.x * ESC_WARPS) {
         const int32_t i = rows[rb];
-        const int32_t pa0 = Ap[i], pa1 = Ap[i + 1];
-        int32_t m0 = 0, m1 = 0;
-        if (has_mask) { m0 = Mp[i]; m1 = Mp[i + 1]; }
-        int n = 0;                                   // products kept so far
-        for (int32_t c0 = pa0; c0 < pa1; c0 += 32) {
-            // 32 entries of A(i,:) at a time: lane l holds k and nnz(B(k,:))
-            const int32_t pa = c0 + lane;
-            int32_t k = 0, b0 = 0, len = 0;
-            Z a = Z();
-            if (pa < pa1) {
-                k = Aj[pa];
-                b0 = Bp[k];
-                len = Bp[k + 1] - b0;
-                if (SR::needs_a) a = ld_val<Z>(Ax, pa, a_iso);
-            }
-            int incl = len;
-            #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            for (int q0 = 0; q0 < total; q0 += 32) {
-                // product q of this chunk belongs to the first lane src whose
-                // inclusive count exceeds q
-                const int q = q0 + lane;
-                int src = 0;
-                #pragma unroll
-                for (int step = 16; step > 0; step >>= 1) {
-                    const int v = __shfl_sync(0xffffffffu, incl, src + step - 1);
-                    if (v <= q) src += step;
-                }
-                const int excl = __shfl_sync(0xffffffffu, incl - len, src);
-                const int32_t kk = __shfl_sync(0xffffffffu, k, src);
-                const int32_t bb = __shfl_sync(0xffffffffu, b0, src);
-                const Z aa = shfl<Z>(a, src);
-                bool keep = q < total;
-                int32_t j = 0, pb = 0;
-                if (keep) {
-                    pb = bb + (q - excl);
-                    j = Bj[pb];
-                    if (has_mask) {
-                        const int32_t f = lower_bound(Mj, m0, m1, j);
-                        const bool present = f < m1 && Mj[f] == j;
-                        keep = mask_comp ? !present : present;
-                    }
-                }
-                const unsigned km = __ballot_sync(0xffffffffu, keep);
-                if (keep) {
-                    const int pos = n + __popc(km & below);
-                    Z b = Z();
-                    if (SR::needs_b) b = ld_val<Z>(Bx, pb, b_iso);
-                    key[pos] = ((KT)(uint32_t)j << posb) | (KT)pos;
-                    val[pos] = SR::F::f(aa, b, i, kk, j);
-                }
-                n += __popc(km);
-            }
-        }
-        __syncwarp();
-        int n2 = 1;
-        while (n2 < n) n2 <<= 1;
-        if (n <= 32) {
-            // one key per lane: bitonic network over the lanes in registers
-            KT kk = lane < n ? key[lane] : ~(KT)0;
-            #pragma unroll
-            for (int size = 2; size <= 32; size <<= 1) {
-                #pragma unroll
-                for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                    const KT other = __shfl_xor_sync(0xffffffffu, kk, stride);
-                    const bool up = (lane & size) == 0;
-                    const bool lower = (lane & stride) == 0;
-                    kk = (lower == up) ? (kk < other ? kk : other) : (kk < other ? other : kk);
-                }
-            }
-            if (lane < n) key[lane] = kk;
-            n2 = 0;                                  // the shared-memory network is skipped
-        } else if (n <= 64) {
-            warp_sort_regs<2>(key, n, lane);
-            n2 = 0;
-        } else if (n <= 128) {
-            warp_sort_regs<4>(key, n, lane);
-            n2 = 0;
-        } else if (n <= 256) {
-            warp_sort_regs<8>(key, n, lane);
-            n2 = 0;
-        }
-        for (int q = n + lane; q < n2; q += 32) key[q] = ~(KT)0;
-        __syncwarp();
-        // bitonic sort of the keys; a lane owns every 32nd compare-exchange
-        for (int size = 2; size <= n2; size <<= 1) {
-            for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                for (int q = lane; q < (n2 >> 1); q += 32) {
-                    // q-th pair of this pass: lower index a, partner a + stride
-                    const int a = ((q & ~(stride - 1)) << 1) | (q & (stride - 1));
-                    const int b = a + stride;
-                    const bool up = ((a & size) == 0);
-                    const KT ka = key[a], kb = key[b];
-                    if ((ka > kb) == up) { key[a] = kb; key[b] = ka; }
-                }
-                __syncwarp();
-            }
-        }
-        // the first entry of each run of equal columns folds the run in
-        // ascending k (its positions ascend) and writes one output entry
-        const int64_t off = slot_off[i];
-        int out = 0;
-        for (int c0 = 0; c0 < n; c0 += 32) {
-            const int p = c0 + lane;
-            bool head = false;
-            KT kp = 0;
-            if (p < n) {
-                kp = key[p];
-                head = (p == 0) || ((key[p - 1] >> posb) != (kp >> posb));
-            }
-            const unsigned hm = __ballot_sync(0xffffffffu, head);
-            if (head) {
-                const KT jcol = kp >> posb;
-                Z z = val[kp & posmask];
-                for (int r = p + 1; r < n; r++) {
-                    const KT kr = key[r];
-                    if ((kr >> posb) != jcol) break;
-                    z = SR::M::update(z, val[kr & posmask]);
-                }
-                const int64_t dst = off + out + __popc(hm & below);
-                Tj[dst] = (int32_t)jcol;
-                Tx[dst] = z;
-            }
-            out += __popc(hm);
-        }
+        const int out = esc_row<SR, KT>(i, posb, key, val, Ap, Aj, Ax, a_iso, Bp, Bj, Bx, b_iso,
+                                        Mp, Mj, has_mask, mask_comp,
+                                        [&]() { return slot_off[i]; }, Tj, Tx);
         if (lane == 0) row_cnt[i] = out;
         __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// small products in one launch
+// ---------------------------------------------------------------------------
+
+// C = A*B (masked or not) in one launch, for products whose rows all fit the
+// expand-sort-compress bin.  Block b owns rows [b*chunk, (b+1)*chunk) and
+// the launch runs in four steps with two grid barriers (the grid is no
+// larger than the blocks the GPU holds at once):
+//
+//   1. every row's products (nnz(B(k,:)) summed over A(i,:)); the block's
+//      total goes to part[b], with SMALL_LONG set if a row has more than
+//      SMALL_CAP products
+//   2. every block sums part[]: a marked block, or a total past the slot
+//      buffer, ends the launch (the host then runs the general path);
+//      otherwise the block's slots start at the sum of part[0..b), and a
+//      row's at that plus the products of the block's earlier rows
+//   3. each row expands, sorts and compresses into its slots (esc_row); the
+//      block's entry count goes to part[G + b]
+//   4. C's row offsets: the sum of part[G..G+b) plus the block's earlier
+//      rows; when C's arrays hold every entry, the block's rows are copied
+//      from their slots into C
+//
+// tot[0] = nnz(C), tot[1] = 0 (done), SMALL_TOO_LONG, SMALL_NO_SLOTS or
+// SMALL_NO_ROOM (C's arrays too small: C.p is set, the entries are not);
+// tot[2] is set when a barrier gave up waiting (blocks of another kernel
+// held the GPU past the bound: the results are void), tot[3] counts the
+// blocks' arrivals.  The host zeroes tot[] before the launch.
+static constexpr int SMALL_CAP = 256;              // products per row, at most
+static constexpr long long SMALL_SPIN_LIMIT = 1 << 20;
+static constexpr int SMALL_POSB = 8;               // log2(SMALL_CAP)
+static constexpr int SMALL_CHUNK = 128;            // rows per block, at most
+static constexpr long long SMALL_LONG = 1ll << 62;
+enum { SMALL_DONE = 0, SMALL_TOO_LONG = 1, SMALL_NO_SLOTS = 2, SMALL_NO_ROOM = 3 };
+
+// exclusive scan of v[0..n) (n <= SMALL_CHUNK) in place by warp 0; returns
+// the total to every lane of warp 0
+template <typename T>
+__device__ __forceinline__ T small_warp_scan(T *v, int n, int lane)
+{
+    constexpr int PER = SMALL_CHUNK / 32;
+    T x[PER];
+    T sum = 0;
+    #pragma unroll
+    for (int q = 0; q < PER; q++) {
+        const int e = lane * PER + q;
+        x[q] = e < n ? v[e] : (T)0;
+        sum += x[q];
+    }
+    T incl = sum;
+    #pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const T y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const T total = __shfl_sync(0xffffffffu, incl, 31);
+    T run = incl - sum;
+    #pragma unroll
+    for (int q = 0; q < PER; q++) {
+        const int e = lane * PER + q;
+        if (e < n) v[e] = run;
+        run += x[q];
+    }
+    return total;
+}
+
+// the sum of part[0..b) and of part[0..G) over the block (every thread gets
+// both), and whether any of them has SMALL_LONG set
+__device__ __forceinline__ void small_part_sums(const long long *part, int b, int G,
+                                                long long &before, long long &all, bool &marked,
+                                                long long *s_red)
+{
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    long long pb = 0, pa = 0;
+    int mk = 0;
+    for (int q = tid; q < G; q += blockDim.x) {
+        const long long v = __ldcg(part + q);
+        const long long val = v & (SMALL_LONG - 1);
+        if (q < b) pb += val;
+        pa += val;
+        mk |= (v & SMALL_LONG) ? 1 : 0;
+    }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        pb += __shfl_xor_sync(0xffffffffu, pb, o);
+        pa += __shfl_xor_sync(0xffffffffu, pa, o);
+        mk |= __shfl_xor_sync(0xffffffffu, mk, o);
+    }
+    __syncthreads();
+    if (lane == 0) { s_red[3 * w] = pb; s_red[3 * w + 1] = pa; s_red[3 * w + 2] = mk; }
+    __syncthreads();
+    before = 0; all = 0;
+    long long m = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); q++) {
+        before += s_red[3 * q];
+        all += s_red[3 * q + 1];
+        m |= s_red[3 * q + 2];
+    }
+    marked = m != 0;
+}
+
+// grid barrier: every block adds one to *bar and waits until it reaches
+// target, with a bounded number of polls; a block that gives up sets *abort,
+// and a block that sees *abort stops waiting.  Returns false to the whole
+// block when the launch is void.
+__device__ __forceinline__ bool small_barrier(unsigned long long *bar, unsigned long long target,
+                                              unsigned long long *abort, int *s_ok)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1ull);
+        int ok = 1;
+        long long spins = 0;
+        while (*(volatile unsigned long long *)bar < target) {
+            if (*(volatile unsigned long long *)abort) { ok = 0; break; }
+            if (++spins > SMALL_SPIN_LIMIT) { atomicExch(abort, 1ull); ok = 0; break; }
+            __nanosleep(64);
+        }
+        __threadfence();
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+template <class SR>
+__global__ void __launch_bounds__(ESC_WARPS * 32, 6)
+k_saxpy_small(int32_t m, int32_t chunk,
+              const int32_t *__restrict__ Ap, const int32_t *__restrict__ Aj,
+              const void *__restrict__ Ax, bool a_iso,
+              const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
+              const void *__restrict__ Bx, bool b_iso,
+              const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
+              bool has_mask, bool mask_comp,
+              long long *__restrict__ part, int64_t slot_cap,
+              int32_t *__restrict__ Tj, typename SR::z_t *__restrict__ Tx,
+              int32_t *__restrict__ Cp, int32_t *__restrict__ Cj,
+              typename SR::z_t *__restrict__ Cx, int64_t ccap, long long *__restrict__ tot)
+{
+    using Z = typename SR::z_t;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ long long s_off[SMALL_CHUNK];     // the rows' slot offsets in the block
+    __shared__ int s_cnt[SMALL_CHUNK];           // the rows' entry counts
+    __shared__ int s_coff[SMALL_CHUNK];          // their offsets among the block's entries
+    __shared__ long long s_red[3 * ESC_WARPS];
+    __shared__ int s_ok;
+    unsigned long long *bar = (unsigned long long *)tot + 3, *abort = bar - 1;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int G = (int)gridDim.x, b = (int)blockIdx.x;
+    const int32_t r0 = b * chunk;
+    const int32_t r1 = r0 + chunk < m ? r0 + chunk : m;
+    const int nr = r1 > r0 ? r1 - r0 : 0;
+
+    // 1. products per row
+    for (int r = w; r < nr; r += ESC_WARPS) {
+        const int32_t i = r0 + r;
+        const int32_t pa0 = Ap[i], pa1 = Ap[i + 1];
+        long long f = 0;
+        for (int32_t pa = pa0 + lane; pa < pa1; pa += 32) {
+            const int32_t k = Aj[pa];
+            f += Bp[k + 1] - Bp[k];
+        }
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) f += __shfl_xor_sync(0xffffffffu, f, o);
+        if (lane == 0) s_off[r] = f;
+    }
+    __syncthreads();
+    if (w == 0) {
+        int lng = 0;
+        for (int r = lane; r < nr; r += 32) lng |= s_off[r] > SMALL_CAP ? 1 : 0;
+        lng = __any_sync(0xffffffffu, lng);
+        const long long total = small_warp_scan<long long>(s_off, nr, lane);
+        if (lane == 0) part[b] = total | (lng ? SMALL_LONG : 0);
+    }
+    if (!small_barrier(bar, (unsigned long long)G, abort, &s_ok)) return;
+
+    // 2. slots of the block's rows
+    long long before, all;
+    bool marked;
+    small_part_sums(part, b, G, before, all, marked, s_red);
+    if (marked || all > slot_cap) {
+        if (b == 0 && tid == 0) {
+            tot[0] = -1;
+            tot[1] = marked ? SMALL_TOO_LONG : SMALL_NO_SLOTS;
+        }
+        return;                          // every block takes this branch
+    }
+
+    // 3. expand-sort-compress into the slots
+    {
+        using KT = uint32_t;
+        KT *key = (KT *)(smem + (size_t)w * SMALL_CAP * (sizeof(KT) + sizeof(Z)));
+        Z *val = (Z *)((unsigned char *)key + (size_t)SMALL_CAP * sizeof(KT));
+        for (int r = w; r < nr; r += ESC_WARPS) {
+            const int out = esc_row<SR, KT>(r0 + r, SMALL_POSB, key, val, Ap, Aj, Ax, a_iso,
+                                            Bp, Bj, Bx, b_iso, Mp, Mj, has_mask, mask_comp,
+                                            [&]() { return before + s_off[r]; }, Tj, Tx);
+            if (lane == 0) s_cnt[r] = out;
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    if (w == 0) {
+        for (int r = lane; r < SMALL_CHUNK; r += 32) s_coff[r] = r < nr ? s_cnt[r] : 0;
+        __syncwarp();
+        const int total = small_warp_scan<int>(s_coff, nr, lane);
+        if (lane == 0) part[G + b] = total;
+    }
+    if (!small_barrier(bar, 2ull * G, abort, &s_ok)) return;
+
+    // 4. C's row offsets and entries
+    long long cbefore, nnz;
+    small_part_sums(part + G, b, G, cbefore, nnz, marked, s_red);
+    for (int r = tid; r < nr; r += blockDim.x) Cp[r0 + r] = (int32_t)(cbefore + s_coff[r]);
+    if (r1 == m && nr > 0 && tid == 0) Cp[m] = (int32_t)nnz;
+    if (b == 0 && tid == 0) {
+        tot[0] = nnz;
+        tot[1] = nnz > ccap ? SMALL_NO_ROOM : SMALL_DONE;
+    }
+    if (nnz > ccap) return;
+    for (int r = w; r < nr; r += ESC_WARPS) {
+        const long long src = before + s_off[r], dst = cbefore + s_coff[r];
+        for (int q = lane; q < s_cnt[r]; q += 32) {
+            Cj[dst + q] = Tj[src + q];
+            Cx[dst + q] = Tx[src + q];
+        }
     }
 }
 
@@ -1862,6 +2117,74 @@ static int saxpy3_row_dense(DevCSR &C, const DevCSR *M, bool mask_comp, const De
 // and the output size; only if the slots did not fit (the buffer then grows
 // and the bins run again), heavy rows need their accumulators sized, or C
 // needs larger arrays does more work follow the read.
+// The one-launch path (k_saxpy_small) for products of SMALL_MIN_ROWS to
+// SMALL_MAX_ROWS rows whose rows are expected to fit the expand-sort-compress
+// bin (A's entries times B's mean row length, per row, at most half the
+// bin), with fewer than 2^24 columns (32-bit sort keys).  C's arrays are
+// sized from B's mean row length as in the general path.  NO_VALUE when the
+// product is not taken, or when the launch found a row past the bin, too
+// few slots or too little room in C (the caller then runs the general path).
+static constexpr int64_t SMALL_MIN_ROWS = 256, SMALL_MAX_ROWS = 32768;
+
+template <class SR>
+static int saxpy3_small(DevCSR &C, const DevCSR *M, bool mask_comp, const DevCSR &A,
+                        const DevCSR &B, SemiringCode sr, cudaStream_t s)
+{
+    using Z = typename SR::z_t;
+    const int64_t m = A.nrows;
+    if (m < SMALL_MIN_ROWS || m > SMALL_MAX_ROWS || A.nnz <= 0 ||
+        B.ncols >= ((int64_t)1 << 24))
+        return NO_VALUE;
+    const double mean_b = B.nrows > 0 ? (double)B.nnz / (double)B.nrows : 0.0;
+    const double flops_est = (double)A.nnz * (mean_b > 1.0 ? mean_b : 1.0);
+    if (flops_est > 0.5 * SMALL_CAP * (double)m) return NO_VALUE;
+    const size_t smem = (size_t)ESC_WARPS * SMALL_CAP * (4 + sizeof(Z));
+    const int resident = resident_blocks((const void *)k_saxpy_small<SR>, ESC_WARPS * 32, smem);
+    const int64_t chunk = (m + resident - 1) / resident;
+    if (chunk > SMALL_CHUNK) return NO_VALUE;
+    const int G = (int)((m + chunk - 1) / chunk);
+
+    // one block: tot[4] and part[2G], then the slots' values and columns
+    const size_t hdr = ((size_t)(4 + 2 * (size_t)G) * 8 + 255) & ~(size_t)255;
+    double guess = 2.0 * flops_est + (double)m + 1024;
+    if (guess > (double)SMALL_CAP * (double)m) guess = (double)SMALL_CAP * (double)m;
+    SlotSource src(s);
+    size_t want = hdr + (size_t)(guess + 16) * (4 + sizeof(Z)) + 256;
+    if (src.have > want) want = src.have;
+    char *base = (char *)src.get(want);
+    if (!base) return NO_VALUE;
+    const int64_t slot_cap = (int64_t)((src.have - hdr - 256) / (4 + sizeof(Z)));
+    long long *tot = (long long *)base;
+    long long *part = tot + 4;
+    Z *Tx = (Z *)(base + hdr);
+    int32_t *Tj = (int32_t *)(base + hdr + (((size_t)slot_cap * sizeof(Z) + 15) & ~(size_t)15));
+
+    double cg = 1.15 * flops_est + 64.0;
+    const double cfull = (double)m * (double)B.ncols;
+    if (cg > cfull + 64.0) cg = cfull + 64.0;
+    const int64_t ccap = (int64_t)cg;
+    DevCSR T;
+    T.nrows = m; T.ncols = B.ncols; T.type = sr.type; T.iso = false;
+    T.p = (int32_t *)dalloc((size_t)(m + 1) * 4, s);
+    T.j = (int32_t *)dalloc((size_t)(ccap + 1) * 4, s);
+    T.x = dalloc((size_t)(ccap + 1) * sizeof(Z), s);
+    if (!T.p || !T.j || !T.x) { dev_free(T, s); return NO_VALUE; }
+    cudaMemsetAsync(tot, 0, 4 * sizeof(long long), s);
+    const int ps = prof_begin("saxpy3_numeric", s);
+    k_saxpy_small<SR><<<G, ESC_WARPS * 32, smem, s>>>((int32_t)m, (int32_t)chunk,
+        A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
+        M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, mask_comp,
+        part, slot_cap, Tj, Tx, T.p, T.j, (Z *)T.x, ccap, tot);
+    prof_end(ps, s);
+    long long h[3] = {0, 0, 0};
+    const cudaError_t e = readback(h, tot, sizeof(h), s);
+    if (e != cudaSuccess) { dev_free(T, s); return cuda_to_info(e); }
+    if (h[2] != 0 || h[1] != SMALL_DONE) { dev_free(T, s); return NO_VALUE; }
+    T.nnz = h[0];
+    C = T;
+    return SUCCESS;
+}
+
 template <class SR>
 static int saxpy3_t(DevCSR &C, const DevCSR *M, bool mask_comp, const DevCSR &A,
                     const DevCSR &B, SemiringCode sr, cudaStream_t s)
@@ -1877,6 +2200,10 @@ static int saxpy3_t(DevCSR &C, const DevCSR *M, bool mask_comp, const DevCSR &A,
         if (m == 1 && A.nnz > 0 && est >= 2.0 * (double)dc.bin[dc.nb - 1].limit &&
             (double)B.ncols * (1.0 + sizeof(Z)) <= (double)((int64_t)4 << 30))
             return saxpy3_row_dense<SR>(C, M, mask_comp, A, B, sr, s);
+    }
+    {
+        const int r = saxpy3_small<SR>(C, M, mask_comp, A, B, sr, s);
+        if (r != NO_VALUE) return r;
     }
     SaxpyPlan *P = new SaxpyPlan();
     P->sr = sr;

@@ -339,3 +339,101 @@ def test_caller_stream_keeping_a_scratch_buffer(gpu, oracle):
     want = oracle.dot3(S.nrows, S.ncols, (Lc.p, Lc.i, None, 1), (Uc.p, Uc.i, None, 1),
                        (Lc.p, Lc.i, None, 1), "PLUS", "PAIR", 8)
     assert_exact(tri, want, "C<L>=L*U'")
+
+
+# ---- the one-launch path for small products (k_saxpy_small) ----------------
+
+@pytest.mark.parametrize("add,mult,tname,np_t", SEMIRINGS)
+def test_one_launch_small_products(gpu, oracle, add, mult, tname, np_t):
+    """256+ rows whose products fit the expand-sort-compress bin: the product
+    runs in one launch (products per row, slots, expand-sort-compress, C's
+    offsets and entries, with two grid barriers between them)."""
+    gb = gpu
+    tc = gb.TYPES[tname]
+    m, k, n = 700, 500, 800
+    A = random_csr(m, k, 0.012, 51, np_t, empty_rows=0.1)
+    B = random_csr(k, n, 0.012, 52, np_t, empty_rows=0.1)
+    got = _saxpy_dev(gb, A, B, gb.semiring(add, mult, tname))
+    want = oracle.saxpy(m, n, (A.p, A.i, A.x, tc), (B.p, B.i, B.x, tc), add, mult, tc)
+    assert_exact(got, want, "one launch %s_%s_%s" % (add, mult, tname))
+
+
+@pytest.mark.parametrize("add,mult,tname,np_t", SEMIRINGS[:10])
+@pytest.mark.parametrize("comp", [False, True])
+def test_one_launch_small_products_masked(gpu, oracle, add, mult, tname, np_t, comp):
+    gb = gpu
+    tc = gb.TYPES[tname]
+    m, k, n = 520, 400, 450
+    A = random_csr(m, k, 0.015, 61, np_t)
+    B = random_csr(k, n, 0.015, 62, np_t)
+    M = random_csr(m, n, 0.05, 63, np.bool_)
+    M.x = None
+    got = _saxpy_dev(gb, A, B, gb.semiring(add, mult, tname), M=M, mask_comp=comp)
+    want = oracle.saxpy(m, n, (A.p, A.i, A.x, tc), (B.p, B.i, B.x, tc), add, mult,
+                        tc, M=(M.p, M.i, None, 1), mask_comp=comp)
+    assert_exact(got, want, "one launch masked comp=%s" % comp)
+
+
+def _csr_from_rows(nrows, ncols, rows, seed):
+    rng = np.random.default_rng(seed)
+    p = np.zeros(nrows + 1, np.int64)
+    for r, c in rows.items():
+        p[r + 1] = len(c)
+    p = np.cumsum(p)
+    i = np.concatenate([np.sort(np.asarray(rows[r], np.int64)) for r in sorted(rows)]) \
+        if rows else np.zeros(0, np.int64)
+    return W.Csr(nrows, ncols, p, i, rng.random(len(i)) - 0.5)
+
+
+@pytest.mark.parametrize("case", ["row_past_bin", "c_past_estimate", "slots_past_estimate"])
+def test_one_launch_fallbacks(gpu, oracle, case):
+    """Products the one-launch path starts but cannot finish go to the general
+    path with the same result: a row of more than 256 products, more entries
+    than C's arrays sized from B's mean row length, and more products than
+    the slots sized from it."""
+    gb = gpu
+    rng = np.random.default_rng(7)
+    m, k, n = 600, 400, 3000
+    if case == "row_past_bin":
+        B = random_csr(k, n, 0.004, 71)                      # about 12 per row
+        arows = {r: rng.choice(k, 4, replace=False) for r in range(m)}
+        arows[17] = rng.choice(k, 120, replace=False)        # about 1400 products
+    elif case == "c_past_estimate":
+        # half of B's rows hold 200 columns, the other half none; A reads only
+        # the long ones, so every row has about twice B's mean row length
+        brows = {r: (rng.choice(n, 200, replace=False) if r % 2 == 0 else [])
+                 for r in range(k)}
+        B = _csr_from_rows(k, n, brows, 72)
+        arows = {r: [2 * int(rng.integers(0, k // 2))] for r in range(m)}
+    else:
+        # one row of B holds 250 columns (mean row length under 1): every
+        # product is about 250 products past the slots' estimate
+        brows = {r: (rng.choice(n, 250, replace=False) if r == 5 else []) for r in range(k)}
+        B = _csr_from_rows(k, n, brows, 73)
+        arows = {r: [5] for r in range(m)}
+    A = _csr_from_rows(m, k, arows, 74)
+    got = _saxpy_dev(gb, A, B, gb.semiring("PLUS", "TIMES", "fp64"))
+    want = oracle.saxpy(m, n, (A.p, A.i, A.x, 11), (B.p, B.i, B.x, 11), "PLUS", "TIMES", 11)
+    assert_exact(got, want, case)
+
+
+def test_one_launch_route(gpu):
+    """The saxpy configuration's product (Erdos-Renyi, 8 per row) at 4096 rows
+    launches the one-launch kernel and none of the general path's."""
+    import torch
+    from torch.profiler import profile, ProfilerActivity
+    gb = gpu
+    A = W.er_fixed(4096, 4096, 8, seed=1)
+    B = W.er_fixed(4096, 4096, 8, seed=2)
+    dA, dB = gb.DMatrix.upload(A), gb.DMatrix.upload(B)
+    sr = gb.semiring("PLUS", "TIMES", "fp64")
+    gb.saxpy3(dA, dB, sr).free()
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        C = gb.saxpy3(dA, dB, sr)
+        torch.cuda.synchronize()
+    names = [e.name for e in prof.events() if e.device_type.name == "CUDA"]
+    C.free(); dA.free(); dB.free()
+    assert any("k_saxpy_small" in s for s in names), names
+    assert not any("k_saxpy_esc" in s or "k_flops_flat" in s or "k_pack" in s
+                   for s in names), names
