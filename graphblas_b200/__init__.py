@@ -124,6 +124,9 @@ def _optional_bindings(L):
         L.grb_b200_profile_reset.argtypes = []
     if hasattr(L, "grb_b200_profile_enable"):
         L.grb_b200_profile_enable.argtypes = [cb]
+    if hasattr(L, "grb_b200_profile_select"):
+        L.grb_b200_profile_select.argtypes = [ctypes.c_char_p, ci]
+        L.grb_b200_profile_select.restype = ci
 
 
 def check(info, what=""):

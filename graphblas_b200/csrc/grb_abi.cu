@@ -148,6 +148,13 @@ int grb_b200_stream_keep_scratch(void *stream, bool keep)
 
 void grb_b200_profile_enable(bool on) { prof_enable(on); }
 
+int grb_b200_profile_select(const char *kernel, int every)
+{
+    if (every < 1) return INVALID_VALUE;
+    prof_select(kernel, every);
+    return SUCCESS;
+}
+
 void grb_b200_profile_reset(void) { prof_reset(); }
 
 int grb_b200_profile(const char *kernel, double *total_ms, int64_t *launches)

@@ -2,6 +2,7 @@
 // upload/download, scans and zombie pruning for the B200 SpGEMM library.
 
 #include <mutex>
+#include <string>
 #include <vector>
 #include <atomic>
 #include <cstring>
@@ -164,24 +165,80 @@ cudaStream_t thread_stream() { return t_stream; }
 // kernel timing
 // ---------------------------------------------------------------------------
 
-struct ProfPending { const char *name; cudaEvent_t a, b; };
+struct ProfPending { const char *name; cudaEvent_t a, b; int dev; };
 struct ProfTotal { const char *name; double ms; int64_t count; };
+struct ProfEvent { cudaEvent_t e; int dev; };
 static std::atomic<bool> g_prof{false};
 static std::mutex g_prof_mu;
 static std::vector<ProfPending> g_pending;
 static std::vector<ProfTotal> g_totals;
+// events are kept for reuse (creating two per range would cost more host
+// time than the launches the range brackets)
+static std::vector<ProfEvent> g_free_events;
+// the kernel whose ranges are recorded (empty: all) and one range in every
+static std::string g_prof_name;
+static int g_prof_every = 1;
+static uint64_t g_prof_seen = 0;
 
-void prof_enable(bool on) { g_prof.store(on); }
+void prof_select(const char *name, int every)
+{
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_prof_name = name ? name : "";
+    g_prof_every = every < 1 ? 1 : every;
+    g_prof_seen = 0;
+}
+
 bool prof_on() { return g_prof.load(); }
+
+// an event of device dev from the pool, or a new one; g_prof_mu held
+static cudaEvent_t prof_event(int dev)
+{
+    for (size_t q = g_free_events.size(); q-- > 0;) {
+        if (g_free_events[q].dev == dev) {
+            const cudaEvent_t e = g_free_events[q].e;
+            g_free_events.erase(g_free_events.begin() + q);
+            return e;
+        }
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); e = nullptr; }
+    return e;
+}
+
+// Turning ranges on fills the current device's share of the pool to 256
+// events, so that ranges opened in a timed loop create none.
+void prof_enable(bool on)
+{
+    if (on) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        std::lock_guard<std::mutex> lk(g_prof_mu);
+        int have = 0;
+        for (const ProfEvent &e : g_free_events) have += e.dev == dev;
+        for (; have < 256; have++) {
+            cudaEvent_t e = nullptr;
+            if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); break; }
+            g_free_events.push_back({e, dev});
+        }
+    }
+    g_prof.store(on);
+}
 
 int prof_begin(const char *name, cudaStream_t s)
 {
     if (!g_prof.load()) return -1;
-    ProfPending p{name, nullptr, nullptr};
-    cudaEventCreate(&p.a);
-    cudaEventCreate(&p.b);
-    cudaEventRecord(p.a, s);
+    int dev = 0;
+    cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (!g_prof_name.empty() && g_prof_name != name) return -1;
+    if (g_prof_seen++ % (uint64_t)g_prof_every != 0) return -1;
+    ProfPending p{name, prof_event(dev), prof_event(dev), dev};
+    if (!p.a || !p.b) {
+        if (p.a) g_free_events.push_back({p.a, dev});
+        if (p.b) g_free_events.push_back({p.b, dev});
+        return -1;
+    }
+    cudaEventRecord(p.a, s);
     g_pending.push_back(p);
     return (int)g_pending.size() - 1;
 }
@@ -204,8 +261,8 @@ void prof_flush()
         for (auto &t : g_totals)
             if (strcmp(t.name, p.name) == 0) { t.ms += ms; t.count++; found = true; break; }
         if (!found) g_totals.push_back({p.name, (double)ms, 1});
-        cudaEventDestroy(p.a);
-        cudaEventDestroy(p.b);
+        g_free_events.push_back({p.a, p.dev});
+        g_free_events.push_back({p.b, p.dev});
     }
     g_pending.clear();
 }

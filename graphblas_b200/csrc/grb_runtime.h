@@ -43,6 +43,7 @@ cudaStream_t thread_stream();
 // prof_begin/prof_end bracket a launch; prof_flush, called after the stream
 // is synchronised, adds the elapsed time to the kernel's running total
 void prof_enable(bool on);
+void prof_select(const char *name, int every);   // name null: every kernel
 bool prof_on();
 int prof_begin(const char *name, cudaStream_t s);
 void prof_end(int slot, cudaStream_t s);

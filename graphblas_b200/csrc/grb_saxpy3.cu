@@ -39,6 +39,7 @@
 // checks each product's column against M(i,:) by binary search; heavy rows
 // mark the dense row's flags.
 
+#include <atomic>
 #include <functional>
 #include <mutex>
 #include <vector>
@@ -457,12 +458,14 @@ __device__ __forceinline__ void warp_sort_regs(KT *key, int n, int lane)
 // (at most cap) expand into key[] / val[] (the warp's shared-memory arrays),
 // the keys are sorted and each run of equal columns is folded into one entry
 // of Tj / Tx from position off() on (read only when the row is written).
-// Returns the row's entry count.
+// Returns the row's entry count; with LIMIT, -1 (and nothing written) when
+// the row keeps more than cap products.
 // KT: 32-bit keys when (column << posb) fits, else 64-bit; posb = log2(cap)
 // bits hold the product's position, so only the keys move in the sort and
 // the values stay where the expansion wrote them.
-template <class SR, typename KT, class Off>
-__device__ __forceinline__ int esc_row(int32_t i, int posb, KT *key, typename SR::z_t *val,
+template <class SR, typename KT, bool LIMIT = false, class Off>
+__device__ __forceinline__ int esc_row(int32_t i, int cap, int posb, KT *key,
+                                       typename SR::z_t *val,
                                        const int32_t *__restrict__ Ap,
                                        const int32_t *__restrict__ Aj,
                                        const void *__restrict__ Ax, bool a_iso,
@@ -526,6 +529,7 @@ __device__ __forceinline__ int esc_row(int32_t i, int posb, KT *key, typename SR
                 }
             }
             const unsigned km = __ballot_sync(0xffffffffu, keep);
+            if (LIMIT && n + __popc(km) > cap) return -1;
             if (keep) {
                 const int pos = n + __popc(km & below);
                 Z b = Z();
@@ -634,7 +638,8 @@ k_saxpy_esc(BinRows br, int cap, int posb,
     for (int64_t rb = (int64_t)blockIdx.x * ESC_WARPS + w; rb < nrows_bin;
          rb += (int64_t)gridDim.x * ESC_WARPS) {
         const int32_t i = rows[rb];
-        const int out = esc_row<SR, KT>(i, posb, key, val, Ap, Aj, Ax, a_iso, Bp, Bj, Bx, b_iso,
+        const int out = esc_row<SR, KT>(i, cap, posb, key, val, Ap, Aj, Ax, a_iso, Bp, Bj, Bx,
+                                        b_iso,
                                         Mp, Mj, has_mask, mask_comp,
                                         [&]() { return slot_off[i]; }, Tj, Tx);
         if (lane == 0) row_cnt[i] = out;
@@ -647,34 +652,29 @@ k_saxpy_esc(BinRows br, int cap, int posb,
 // ---------------------------------------------------------------------------
 
 // C = A*B (masked or not) in one launch, for products whose rows all fit the
-// expand-sort-compress bin.  Block b owns rows [b*chunk, (b+1)*chunk) and
-// the launch runs in four steps with two grid barriers (the grid is no
-// larger than the blocks the GPU holds at once):
+// expand-sort-compress bin.  Blocks take row ranges of `chunk` rows from a
+// ticket in the order they start, and row i's slots are [i*SMALL_CAP,
+// (i+1)*SMALL_CAP):
 //
-//   1. every row's products (nnz(B(k,:)) summed over A(i,:)); the block's
-//      total goes to part[b], with SMALL_LONG set if a row has more than
-//      SMALL_CAP products
-//   2. every block sums part[]: a marked block, or a total past the slot
-//      buffer, ends the launch (the host then runs the general path);
-//      otherwise the block's slots start at the sum of part[0..b), and a
-//      row's at that plus the products of the block's earlier rows
-//   3. each row expands, sorts and compresses into its slots (esc_row); the
-//      block's entry count goes to part[G + b]
-//   4. C's row offsets: the sum of part[G..G+b) plus the block's earlier
-//      rows; when C's arrays hold every entry, the block's rows are copied
-//      from their slots into C
+//   1. each row expands, sorts and compresses into its slots (esc_row); a
+//      row that keeps more than SMALL_CAP products sets tot[1] instead
+//   2. the block's entry count is posted, and a decoupled look-back over the
+//      blocks before it (they started earlier, so they are running or done)
+//      gives its offset among C's entries; the last block's inclusive sum is
+//      nnz(C)
+//   3. C's row offsets for the block's rows, and its entries copied from the
+//      slots, flat over the block's threads
 //
-// tot[0] = nnz(C), tot[1] = 0 (done), SMALL_TOO_LONG, SMALL_NO_SLOTS or
-// SMALL_NO_ROOM (C's arrays too small: C.p is set, the entries are not);
-// tot[2] is set when a barrier gave up waiting (blocks of another kernel
-// held the GPU past the bound: the results are void), tot[3] counts the
-// blocks' arrivals.  The host zeroes tot[] before the launch.
+// No block waits for one that has not started, so the launch needs no
+// co-residency and runs beside other kernels.  tot[0] = nnz(C), tot[1] = 0
+// (done), SMALL_TOO_LONG or SMALL_NO_ROOM (C's arrays too small; the blocks
+// past the capacity write nothing), tot[2] is set when a look-back gave up
+// waiting (the results are void), tot[3] is the ticket counter; part[G] are
+// the blocks' look-back words.  The host zeroes tot[] and part[] first.
 static constexpr int SMALL_CAP = 256;              // products per row, at most
-static constexpr long long SMALL_SPIN_LIMIT = 1 << 20;
 static constexpr int SMALL_POSB = 8;               // log2(SMALL_CAP)
 static constexpr int SMALL_CHUNK = 128;            // rows per block, at most
-static constexpr long long SMALL_LONG = 1ll << 62;
-enum { SMALL_DONE = 0, SMALL_TOO_LONG = 1, SMALL_NO_SLOTS = 2, SMALL_NO_ROOM = 3 };
+enum { SMALL_DONE = 0, SMALL_TOO_LONG = 1, SMALL_NO_ROOM = 3 };
 
 // exclusive scan of v[0..n) (n <= SMALL_CHUNK) in place by warp 0; returns
 // the total to every lane of warp 0
@@ -707,66 +707,6 @@ __device__ __forceinline__ T small_warp_scan(T *v, int n, int lane)
     return total;
 }
 
-// the sum of part[0..b) and of part[0..G) over the block (every thread gets
-// both), and whether any of them has SMALL_LONG set
-__device__ __forceinline__ void small_part_sums(const long long *part, int b, int G,
-                                                long long &before, long long &all, bool &marked,
-                                                long long *s_red)
-{
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    long long pb = 0, pa = 0;
-    int mk = 0;
-    for (int q = tid; q < G; q += blockDim.x) {
-        const long long v = __ldcg(part + q);
-        const long long val = v & (SMALL_LONG - 1);
-        if (q < b) pb += val;
-        pa += val;
-        mk |= (v & SMALL_LONG) ? 1 : 0;
-    }
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        pb += __shfl_xor_sync(0xffffffffu, pb, o);
-        pa += __shfl_xor_sync(0xffffffffu, pa, o);
-        mk |= __shfl_xor_sync(0xffffffffu, mk, o);
-    }
-    __syncthreads();
-    if (lane == 0) { s_red[3 * w] = pb; s_red[3 * w + 1] = pa; s_red[3 * w + 2] = mk; }
-    __syncthreads();
-    before = 0; all = 0;
-    long long m = 0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); q++) {
-        before += s_red[3 * q];
-        all += s_red[3 * q + 1];
-        m |= s_red[3 * q + 2];
-    }
-    marked = m != 0;
-}
-
-// grid barrier: every block adds one to *bar and waits until it reaches
-// target, with a bounded number of polls; a block that gives up sets *abort,
-// and a block that sees *abort stops waiting.  Returns false to the whole
-// block when the launch is void.
-__device__ __forceinline__ bool small_barrier(unsigned long long *bar, unsigned long long target,
-                                              unsigned long long *abort, int *s_ok)
-{
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(bar, 1ull);
-        int ok = 1;
-        long long spins = 0;
-        while (*(volatile unsigned long long *)bar < target) {
-            if (*(volatile unsigned long long *)abort) { ok = 0; break; }
-            if (++spins > SMALL_SPIN_LIMIT) { atomicExch(abort, 1ull); ok = 0; break; }
-            __nanosleep(64);
-        }
-        __threadfence();
-        *s_ok = ok;
-    }
-    __syncthreads();
-    return *s_ok != 0;
-}
-
 template <class SR>
 __global__ void __launch_bounds__(ESC_WARPS * 32, 6)
 k_saxpy_small(int32_t m, int32_t chunk,
@@ -775,71 +715,48 @@ k_saxpy_small(int32_t m, int32_t chunk,
               const int32_t *__restrict__ Bp, const int32_t *__restrict__ Bj,
               const void *__restrict__ Bx, bool b_iso,
               const int32_t *__restrict__ Mp, const int32_t *__restrict__ Mj,
-              bool has_mask, bool mask_comp,
-              long long *__restrict__ part, int64_t slot_cap,
+              bool has_mask, bool mask_comp, long long *__restrict__ part,
               int32_t *__restrict__ Tj, typename SR::z_t *__restrict__ Tx,
               int32_t *__restrict__ Cp, int32_t *__restrict__ Cj,
               typename SR::z_t *__restrict__ Cx, int64_t ccap, long long *__restrict__ tot)
 {
     using Z = typename SR::z_t;
+    using KT = uint32_t;
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ long long s_off[SMALL_CHUNK];     // the rows' slot offsets in the block
     __shared__ int s_cnt[SMALL_CHUNK];           // the rows' entry counts
     __shared__ int s_coff[SMALL_CHUNK];          // their offsets among the block's entries
-    __shared__ long long s_red[3 * ESC_WARPS];
-    __shared__ int s_ok;
-    unsigned long long *bar = (unsigned long long *)tot + 3, *abort = bar - 1;
+    __shared__ long long s_ex;
+    __shared__ int s_btot, s_long, s_tile;
+    unsigned long long *status = (unsigned long long *)part;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int G = (int)gridDim.x, b = (int)blockIdx.x;
+    const int G = (int)gridDim.x;
+    // blocks take their row ranges from a ticket, in the order they start,
+    // so a block's predecessors are running or done when it looks back
+    if (tid == 0) {
+        s_long = 0;
+        s_tile = (int)atomicAdd((unsigned long long *)tot + 3, 1ull);
+    }
+    __syncthreads();
+    const int b = s_tile;
     const int32_t r0 = b * chunk;
     const int32_t r1 = r0 + chunk < m ? r0 + chunk : m;
     const int nr = r1 > r0 ? r1 - r0 : 0;
 
-    // 1. products per row
-    for (int r = w; r < nr; r += ESC_WARPS) {
-        const int32_t i = r0 + r;
-        const int32_t pa0 = Ap[i], pa1 = Ap[i + 1];
-        long long f = 0;
-        for (int32_t pa = pa0 + lane; pa < pa1; pa += 32) {
-            const int32_t k = Aj[pa];
-            f += Bp[k + 1] - Bp[k];
-        }
-        #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) f += __shfl_xor_sync(0xffffffffu, f, o);
-        if (lane == 0) s_off[r] = f;
-    }
-    __syncthreads();
-    if (w == 0) {
-        int lng = 0;
-        for (int r = lane; r < nr; r += 32) lng |= s_off[r] > SMALL_CAP ? 1 : 0;
-        lng = __any_sync(0xffffffffu, lng);
-        const long long total = small_warp_scan<long long>(s_off, nr, lane);
-        if (lane == 0) part[b] = total | (lng ? SMALL_LONG : 0);
-    }
-    if (!small_barrier(bar, (unsigned long long)G, abort, &s_ok)) return;
-
-    // 2. slots of the block's rows
-    long long before, all;
-    bool marked;
-    small_part_sums(part, b, G, before, all, marked, s_red);
-    if (marked || all > slot_cap) {
-        if (b == 0 && tid == 0) {
-            tot[0] = -1;
-            tot[1] = marked ? SMALL_TOO_LONG : SMALL_NO_SLOTS;
-        }
-        return;                          // every block takes this branch
-    }
-
-    // 3. expand-sort-compress into the slots
+    // 1. expand-sort-compress each row into its slots
     {
-        using KT = uint32_t;
         KT *key = (KT *)(smem + (size_t)w * SMALL_CAP * (sizeof(KT) + sizeof(Z)));
         Z *val = (Z *)((unsigned char *)key + (size_t)SMALL_CAP * sizeof(KT));
         for (int r = w; r < nr; r += ESC_WARPS) {
-            const int out = esc_row<SR, KT>(r0 + r, SMALL_POSB, key, val, Ap, Aj, Ax, a_iso,
-                                            Bp, Bj, Bx, b_iso, Mp, Mj, has_mask, mask_comp,
-                                            [&]() { return before + s_off[r]; }, Tj, Tx);
-            if (lane == 0) s_cnt[r] = out;
+            const int32_t i = r0 + r;
+            const int out = esc_row<SR, KT, true>(i, SMALL_CAP, SMALL_POSB, key, val, Ap, Aj, Ax,
+                                                  a_iso, Bp, Bj, Bx, b_iso, Mp, Mj, has_mask,
+                                                  mask_comp,
+                                                  [&]() { return (int64_t)i * SMALL_CAP; },
+                                                  Tj, Tx);
+            if (lane == 0) {
+                s_cnt[r] = out < 0 ? 0 : out;
+                if (out < 0) s_long = 1;
+            }
             __syncwarp();
         }
     }
@@ -848,25 +765,64 @@ k_saxpy_small(int32_t m, int32_t chunk,
         for (int r = lane; r < SMALL_CHUNK; r += 32) s_coff[r] = r < nr ? s_cnt[r] : 0;
         __syncwarp();
         const int total = small_warp_scan<int>(s_coff, nr, lane);
-        if (lane == 0) part[G + b] = total;
+        // the block's offset among C's entries: decoupled look-back over the
+        // blocks before it (bounded waits; a wait past the bound sets tot[2])
+        long long ex = 0;
+        if (b == 0) {
+            if (lane == 0) atomicExch(&status[0], LB_INC | (unsigned long long)total);
+        } else {
+            if (lane == 0) atomicExch(&status[b], LB_AGG | (unsigned long long)total);
+            ex = lb_lookback(status, b, lane, (int *)(tot + 2));
+            if (lane == 0)
+                atomicExch(&status[b], LB_INC | ((unsigned long long)(ex + total) & LB_VAL));
+        }
+        if (lane == 0) {
+            s_ex = ex;
+            s_btot = total;
+            if (s_long) atomicExch((unsigned long long *)tot + 1, (unsigned long long)SMALL_TOO_LONG);
+            if (b == G - 1) {
+                tot[0] = ex + total;
+                if (ex + total > ccap)
+                    atomicCAS((unsigned long long *)tot + 1, 0ull,
+                              (unsigned long long)SMALL_NO_ROOM);
+            }
+        }
     }
-    if (!small_barrier(bar, 2ull * G, abort, &s_ok)) return;
+    __syncthreads();
 
-    // 4. C's row offsets and entries
-    long long cbefore, nnz;
-    small_part_sums(part + G, b, G, cbefore, nnz, marked, s_red);
+    // 2. C's row offsets and entries (a block whose entries would pass C's
+    //    capacity writes nothing: the call then runs the general path)
+    const long long cbefore = s_ex;
+    const long long nnz_end = cbefore + s_btot;
+    if (nnz_end > ccap) return;
     for (int r = tid; r < nr; r += blockDim.x) Cp[r0 + r] = (int32_t)(cbefore + s_coff[r]);
-    if (r1 == m && nr > 0 && tid == 0) Cp[m] = (int32_t)nnz;
-    if (b == 0 && tid == 0) {
-        tot[0] = nnz;
-        tot[1] = nnz > ccap ? SMALL_NO_ROOM : SMALL_DONE;
-    }
-    if (nnz > ccap) return;
-    for (int r = w; r < nr; r += ESC_WARPS) {
-        const long long src = before + s_off[r], dst = cbefore + s_coff[r];
-        for (int q = lane; q < s_cnt[r]; q += 32) {
-            Cj[dst + q] = Tj[src + q];
-            Cx[dst + q] = Tx[src + q];
+    if (r1 == m && nr > 0 && tid == 0) Cp[m] = (int32_t)nnz_end;
+    // the block's entries flat over its threads, four per thread in flight
+    const int btot = s_btot;
+    for (int e0 = tid; e0 < btot; e0 += 4 * (int)blockDim.x) {
+        int32_t jv[4];
+        Z xv[4];
+        #pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int e = e0 + u * (int)blockDim.x;
+            if (e < btot) {
+                int lo = 0, hi = nr - 1;        // the last row starting at or before e
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_coff[mid] <= e) lo = mid; else hi = mid - 1;
+                }
+                const long long src = (long long)(r0 + lo) * SMALL_CAP + (e - s_coff[lo]);
+                jv[u] = Tj[src];
+                xv[u] = Tx[src];
+            }
+        }
+        #pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int e = e0 + u * (int)blockDim.x;
+            if (e < btot) {
+                Cj[cbefore + e] = jv[u];
+                Cx[cbefore + e] = xv[u];
+            }
         }
     }
 }
@@ -2120,11 +2076,13 @@ static int saxpy3_row_dense(DevCSR &C, const DevCSR *M, bool mask_comp, const De
 // The one-launch path (k_saxpy_small) for products of SMALL_MIN_ROWS to
 // SMALL_MAX_ROWS rows whose rows are expected to fit the expand-sort-compress
 // bin (A's entries times B's mean row length, per row, at most half the
-// bin), with fewer than 2^24 columns (32-bit sort keys).  C's arrays are
-// sized from B's mean row length as in the general path.  NO_VALUE when the
-// product is not taken, or when the launch found a row past the bin, too
-// few slots or too little room in C (the caller then runs the general path).
+// bin), with fewer than 2^24 columns (32-bit sort keys).  The slots take
+// SMALL_CAP entries a row from the stream's buffer; C's arrays are sized
+// from B's mean row length as in the general path.  NO_VALUE when the
+// product is not taken, or when the launch found a row past the bin or too
+// little room in C (the caller then runs the general path).
 static constexpr int64_t SMALL_MIN_ROWS = 256, SMALL_MAX_ROWS = 32768;
+
 
 template <class SR>
 static int saxpy3_small(DevCSR &C, const DevCSR *M, bool mask_comp, const DevCSR &A,
@@ -2144,20 +2102,17 @@ static int saxpy3_small(DevCSR &C, const DevCSR *M, bool mask_comp, const DevCSR
     if (chunk > SMALL_CHUNK) return NO_VALUE;
     const int G = (int)((m + chunk - 1) / chunk);
 
-    // one block: tot[4] and part[2G], then the slots' values and columns
-    const size_t hdr = ((size_t)(4 + 2 * (size_t)G) * 8 + 255) & ~(size_t)255;
-    double guess = 2.0 * flops_est + (double)m + 1024;
-    if (guess > (double)SMALL_CAP * (double)m) guess = (double)SMALL_CAP * (double)m;
+    // one block: tot[8] and the blocks' look-back words part[G], then
+    // SMALL_CAP slots per row (values, then columns)
+    const size_t hdr = ((size_t)(8 + (size_t)G) * 8 + 255) & ~(size_t)255;
+    const size_t xbytes = ((size_t)m * SMALL_CAP * sizeof(Z) + 255) & ~(size_t)255;
     SlotSource src(s);
-    size_t want = hdr + (size_t)(guess + 16) * (4 + sizeof(Z)) + 256;
-    if (src.have > want) want = src.have;
-    char *base = (char *)src.get(want);
+    char *base = (char *)src.get(hdr + xbytes + (size_t)m * SMALL_CAP * 4);
     if (!base) return NO_VALUE;
-    const int64_t slot_cap = (int64_t)((src.have - hdr - 256) / (4 + sizeof(Z)));
     long long *tot = (long long *)base;
-    long long *part = tot + 4;
+    long long *part = tot + 8;
     Z *Tx = (Z *)(base + hdr);
-    int32_t *Tj = (int32_t *)(base + hdr + (((size_t)slot_cap * sizeof(Z) + 15) & ~(size_t)15));
+    int32_t *Tj = (int32_t *)(base + hdr + xbytes);
 
     double cg = 1.15 * flops_est + 64.0;
     const double cfull = (double)m * (double)B.ncols;
@@ -2169,12 +2124,12 @@ static int saxpy3_small(DevCSR &C, const DevCSR *M, bool mask_comp, const DevCSR
     T.j = (int32_t *)dalloc((size_t)(ccap + 1) * 4, s);
     T.x = dalloc((size_t)(ccap + 1) * sizeof(Z), s);
     if (!T.p || !T.j || !T.x) { dev_free(T, s); return NO_VALUE; }
-    cudaMemsetAsync(tot, 0, 4 * sizeof(long long), s);
+    cudaMemsetAsync(tot, 0, (8 + (size_t)G) * sizeof(long long), s);
     const int ps = prof_begin("saxpy3_numeric", s);
     k_saxpy_small<SR><<<G, ESC_WARPS * 32, smem, s>>>((int32_t)m, (int32_t)chunk,
         A.p, A.j, A.x, A.iso, B.p, B.j, B.x, B.iso,
         M ? M->p : nullptr, M ? M->j : nullptr, M != nullptr, mask_comp,
-        part, slot_cap, Tj, Tx, T.p, T.j, (Z *)T.x, ccap, tot);
+        part, Tj, Tx, T.p, T.j, (Z *)T.x, ccap, tot);
     prof_end(ps, s);
     long long h[3] = {0, 0, 0};
     const cudaError_t e = readback(h, tot, sizeof(h), s);

@@ -136,6 +136,11 @@ int grb_b200_stream_keep_scratch(void *stream, bool keep);
  * default; the reference's equivalent is its GpuTimer
  * (CUDA/include/GB_cuda_timer.hpp) around the dot3 launches. */
 void grb_b200_profile_enable(bool on);
+/* Which launches get events: only those of kernel `kernel` (NULL: every
+ * kernel), and of those one in `every` (a timed launch's two events cost
+ * the stream several microseconds, which sampling spreads).  Applies to
+ * launches after the call; the default is every launch of every kernel. */
+int grb_b200_profile_select(const char *kernel, int every);
 void grb_b200_profile_reset(void);
 int grb_b200_profile(const char *kernel, double *total_ms, int64_t *launches);
 

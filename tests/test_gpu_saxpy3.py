@@ -385,12 +385,12 @@ def _csr_from_rows(nrows, ncols, rows, seed):
     return W.Csr(nrows, ncols, p, i, rng.random(len(i)) - 0.5)
 
 
-@pytest.mark.parametrize("case", ["row_past_bin", "c_past_estimate", "slots_past_estimate"])
+@pytest.mark.parametrize("case", ["row_past_bin", "c_past_estimate", "b_mean_under_one"])
 def test_one_launch_fallbacks(gpu, oracle, case):
     """Products the one-launch path starts but cannot finish go to the general
-    path with the same result: a row of more than 256 products, more entries
-    than C's arrays sized from B's mean row length, and more products than
-    the slots sized from it."""
+    path with the same result: a row of more than 256 products, and more
+    entries than C's arrays sized from B's mean row length (rows reading
+    only B's long rows; B's mean row length under one)."""
     gb = gpu
     rng = np.random.default_rng(7)
     m, k, n = 600, 400, 3000
@@ -407,7 +407,7 @@ def test_one_launch_fallbacks(gpu, oracle, case):
         arows = {r: [2 * int(rng.integers(0, k // 2))] for r in range(m)}
     else:
         # one row of B holds 250 columns (mean row length under 1): every
-        # product is about 250 products past the slots' estimate
+        # row of C has 250 entries against an estimate of one
         brows = {r: (rng.choice(n, 250, replace=False) if r == 5 else []) for r in range(k)}
         B = _csr_from_rows(k, n, brows, 73)
         arows = {r: [5] for r in range(m)}
