@@ -250,7 +250,7 @@ class Saxpy:
         # DRAM bytes of the one-launch product kernel per launch (ncu capture
         # of this workload at this size: the inputs come from L2, the written
         # slots stay there)
-        self.traffic_per_launch = 3.54e6
+        self.traffic_per_launch = 3.46e6
 
     def config(self):
         return {"n": self.n, "nnz_A": int(self.A.nnz), "products": self.products,
